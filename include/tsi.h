@@ -1,0 +1,300 @@
+/*
+ * tsi.h — C ABI of the B200 (sm_100a) temporal set inversion library.
+ *
+ * The library replaces the device hot path of TemporalSetInversion
+ * (src/compute.wgsl entry points `main`, `rt_main`, `buf_main`) and the
+ * host contract around it (src/main.rs `State::compute` / `State::render`,
+ * src/ir.rs tape lowering, src/uniforms.rs, src/camera.rs).  The reference
+ * binds its path through a wgpu bind group (main.rs:305-427,
+ * compute.wgsl:3066-3087,3431-3435); this header is the FFI that replaces
+ * it.  Every entry point names the reference interface it stands in for.
+ *
+ * Conventions
+ *  - Every function returns tsi_status (0 = TSI_OK).  Device-side failures
+ *    (pool exhausted, work list full, bounded wait expired) are reported as
+ *    error words read back by the host, never as traps.
+ *  - The caller owns host memory; the library owns device memory.
+ *  - Handles are not thread safe.  One CUDA stream per tsi_ctx; a server
+ *    owns its own worker thread and stream.
+ *  - No CPU fallback: when no sm_100 device is present, tsi_create returns
+ *    TSI_ERR_NO_DEVICE.  Only tsi_ir_lower, tsi_status_string and
+ *    tsi_version work without a device.
+ */
+#ifndef TSI_H
+#define TSI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TSI_ABI_VERSION 1u
+
+#if defined(_WIN32)
+#define TSI_API __declspec(dllexport)
+#else
+#define TSI_API __attribute__((visibility("default")))
+#endif
+
+typedef enum tsi_status {
+  TSI_OK = 0,
+  TSI_ERR_INVALID_ARGUMENT = 1,
+  TSI_ERR_PARSE = 2,          /* LLVM IR text the lowering cannot read (ir.rs panics there) */
+  TSI_ERR_CUDA = 3,           /* a CUDA runtime call failed */
+  TSI_ERR_OOM = 4,            /* voxel pool or device arena exhausted */
+  TSI_ERR_QUEUE_FULL = 5,     /* a device work list overflowed (compute.wgsl:3159 drops silently) */
+  TSI_ERR_WATCHDOG = 6,       /* a bounded device wait gave up */
+  TSI_ERR_BAD_OPCODE = 7,     /* opcode outside ir.rs:8-43 in an uploaded tape */
+  TSI_ERR_TAPE_TOO_WIDE = 8,  /* tape needs more than 256 interval registers */
+  TSI_ERR_NO_DEVICE = 9,      /* no sm_100 CUDA device */
+  TSI_ERR_BUFFER_TOO_SMALL = 10,
+  TSI_ERR_BUSY = 11,
+  TSI_ERR_NOT_FOUND = 12,
+  TSI_ERR_SHUTDOWN = 13
+} tsi_status;
+
+/* ---------------------------------------------------------------------
+ * Tape instruction in the reference's own 32-byte layout.
+ * Mirrors ir.rs:88-97 (GPUInstruction) and compute.wgsl:2989-2996.
+ *   opcode_uses = ((op | op_top << 14) << 16) | uses      (ir.rs:171-175)
+ *   larg_rarg   = larg << 16 | rarg                        (ir.rs:176)
+ *   op_top: 0 reg,reg  1 reg,literal (and unary)  2 literal,reg  3 none
+ * ------------------------------------------------------------------- */
+typedef struct tsi_gpu_instruction {
+  uint32_t index_;
+  uint32_t opcode_uses;
+  uint32_t larg_rarg;
+  float literal;
+  float val[2];
+  float sens[2];
+} tsi_gpu_instruction;
+
+/* Opcode numbers, ir.rs:9-41. */
+enum {
+  TSI_OP_NOP = 0, TSI_OP_ARGX = 1, TSI_OP_ARGY = 2, TSI_OP_ARGZ = 3, TSI_OP_ARGW = 4,
+  TSI_OP_ADD = 5, TSI_OP_SUB = 6, TSI_OP_MUL = 7, TSI_OP_DIV = 8, TSI_OP_EXP = 9,
+  TSI_OP_LOG = 10, TSI_OP_SQR = 11, TSI_OP_SQRT = 12, TSI_OP_POW = 13, TSI_OP_SIN = 14,
+  TSI_OP_COS = 15, TSI_OP_NEG = 16, TSI_OP_MIN = 17, TSI_OP_MAX = 18, TSI_OP_ABS = 19,
+  TSI_OP_CUP = 20, TSI_OP_CAP = 21, TSI_OP_BR = 22, TSI_OP_PHI = 23, TSI_OP_TRUNC = 24,
+  TSI_OP_FLOOR = 25, TSI_OP_CEIL = 26, TSI_OP_SIGN = 27, TSI_OP_RET = 28, TSI_OP_MOD = 29,
+  TSI_OP_ATAN2 = 30
+};
+
+typedef enum tsi_rounding {
+  TSI_ROUND_NEAREST = 0,   /* plain f32 as compute.wgsl:2539-2975 (parity mode) */
+  TSI_ROUND_DIRECTED = 1   /* outward rounded, rigorous enclosures */
+} tsi_rounding;
+
+/* Runtime form of the compile-time PARAMETERS block, compute.wgsl:3494-3511. */
+typedef struct tsi_params {
+  int32_t localsubdiv;          /* epsilon = 10 * 2^-localsubdiv (compute.wgsl:3521) */
+  float delta;                  /* temporal error tolerance */
+  int32_t pointsample;          /* point_sample */
+  int32_t fastenabled;
+  int32_t lipschitz_corrected;
+  int32_t swept_volume;         /* sweptvolume */
+  int32_t fast_normals;         /* per-pixel finite-difference normals in the tracer */
+  int32_t normal_viz;
+  int32_t rounding_mode;        /* tsi_rounding */
+  float fast_multiplier;        /* 1.0 in the reference */
+  int32_t scene_id;             /* `scene`: camera offsets of rt_main (compute.wgsl:4670-4683) */
+  float octree_darken_factor;   /* 0.98 */
+  float root_lo[3];             /* root box, ir.rs:343-347: [-5,5]^3 */
+  float root_hi[3];
+  int32_t pruning;              /* per-cell tape pruning (1 = on); never changes results */
+  float swept_dt;               /* swept interval length when t0 is NaN (1/60, compute.wgsl:3605) */
+} tsi_params;
+
+/* Uniforms, uniforms.rs:8-17 / compute.wgsl:3419-3428 (96 bytes).
+ * view_matrix is camera-to-world, column major (camera.rs:78-80). */
+typedef struct tsi_uniforms {
+  float view_matrix[16];
+  uint32_t resolution[2];
+  float time;
+  float lasttime;
+  float rendermode;
+  float _padding[3];
+} tsi_uniforms;
+
+/* Per-call counters (there are none in the reference; Memory at
+ * compute.wgsl:3041-3048 only tracks allocated voxels and work_left). */
+typedef struct tsi_stats {
+  uint64_t parents_expanded;    /* work items dequeued (compute.wgsl:3528) */
+  uint64_t cells_evaluated;     /* child cells whose tape ran forward (3633) */
+  uint64_t cells_reverse;       /* of which ran reverse AD (3785) */
+  uint64_t cells_skipped;       /* swept interior cells not evaluated (3629) */
+  uint64_t cells_ambiguous;
+  uint64_t cells_empty;
+  uint64_t cells_full;
+  uint64_t cells_enqueued;      /* re-enqueued for subdivision (4024) */
+  uint64_t cells_reused;        /* ambiguous internal cells kept with their subtree */
+  uint64_t instr_forward;       /* interval instructions executed forward */
+  uint64_t instr_reverse;       /* interval instructions executed in reverse */
+  uint64_t instr_full_equiv;    /* cells_evaluated x full tape length */
+  uint64_t fp32_ops;            /* algorithmic FP32 ops of the executed instructions (opcost.h) */
+  uint64_t bricks_allocated;    /* 8-voxel bricks taken from the pool */
+  uint64_t bricks_freed;
+  uint64_t voxels_live;
+  uint64_t items_high_water;    /* largest per-level work list */
+  uint64_t tape_words;          /* pruned tape instructions written */
+  uint64_t prune_fallbacks;     /* warps that re-ran on the full tape */
+  uint32_t levels;
+  uint32_t error_flags;
+  float device_ms;              /* device time of the call (CUDA events) */
+  float reserved;
+} tsi_stats;
+
+/* A cell of the resident octree, keyed by (level, ix, iy, iz). */
+typedef struct tsi_cell {
+  uint32_t level, ix, iy, iz;
+  float f;          /* -1 full, 0 ambiguous, +1 empty (compute.wgsl:4012-4033) */
+  float t;          /* time of last evaluation */
+  float time_err;
+  float fast;
+  float dx, dy, dz; /* interval-gradient midpoints (compute.wgsl:3967-3969) */
+  uint32_t has_children;
+  float x[2], y[2], z[2];
+} tsi_cell;
+
+/* Rendered frame.  Pointers are HOST pointers owned by the caller; any may
+ * be NULL to skip that output.  rgba is compute.wgsl:4687 `pixels[]`. */
+typedef struct tsi_image {
+  uint32_t width, height;
+  float *rgba;      /* width*height*4 */
+  float *depth;     /* width*height, -1 on miss (compute.wgsl:4398-4401) */
+  float *normal;    /* width*height*3, normal at hit */
+} tsi_image;
+
+/* Device pointers to a scene's last rendered frame (library owned). */
+typedef struct tsi_image_device {
+  uint32_t width, height;
+  const float *rgba, *depth, *normal;
+} tsi_image_device;
+
+typedef struct tsi_device_opts {
+  int32_t device;               /* CUDA ordinal */
+  uint64_t work_item_capacity;  /* per-level work list capacity (0 = default) */
+  uint64_t tape_arena_words;    /* pruned tape arena, 8-byte words (0 = default) */
+  uint64_t log_arena_bytes;     /* reverse-AD operand log (0 = default) */
+  uint32_t watchdog_iters;      /* bound on every device wait (0 = default) */
+  uint32_t max_scenes_per_launch; /* batch width (0 = default 64) */
+} tsi_device_opts;
+
+typedef struct tsi_ctx tsi_ctx;
+typedef struct tsi_tape tsi_tape;
+typedef struct tsi_scene tsi_scene;
+
+typedef struct tsi_tape_info {
+  uint32_t instruction_count;   /* including the 4 ARG slots (main.rs:744) */
+  uint32_t registers;           /* interval registers after allocation */
+  uint32_t minmax_count;
+  uint32_t reserved;
+} tsi_tape_info;
+
+/* ---------------- library ---------------- */
+TSI_API uint32_t tsi_version(void);
+TSI_API const char *tsi_status_string(tsi_status s);
+TSI_API void tsi_default_params(tsi_params *p);
+
+/* Replaces State::new's adapter/device setup (main.rs:97-122) and the
+ * buffer allocations of main.rs:208-303 (now lazily sized, HBM resident). */
+TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out);
+TSI_API void tsi_destroy(tsi_ctx *ctx);
+TSI_API tsi_status tsi_synchronize(tsi_ctx *ctx);
+
+/* ---------------- tapes ---------------- */
+/* Host-only restatement of ir.rs:190-366 (parseLLVMIR + IR::new + to_gpu):
+ * lowers the `@_Z1fffff` function of `text` into the 32-byte layout, with
+ * the four ARG slots first (values = root box, time).  Writes at most `cap`
+ * instructions and stores the full count in *n (no 4096 cap). */
+TSI_API tsi_status tsi_ir_lower(const char *text, size_t len, float time,
+                                tsi_gpu_instruction *out, uint32_t cap, uint32_t *n);
+
+/* Uploads a tape in the ir.rs layout (main.rs:743-746 writes it into
+ * tapes[0]); the library repacks it into the packed device tape. */
+TSI_API tsi_status tsi_tape_upload(tsi_ctx *ctx, const tsi_gpu_instruction *instr, uint32_t n,
+                                   tsi_tape **out);
+/* tsi_ir_lower + tsi_tape_upload without the 16-bit limits of ir.rs:99-101. */
+TSI_API tsi_status tsi_tape_from_llvm_ir(tsi_ctx *ctx, const char *text, size_t len,
+                                         tsi_tape **out);
+TSI_API tsi_status tsi_tape_info_get(const tsi_tape *tape, tsi_tape_info *info);
+TSI_API void tsi_tape_destroy(tsi_tape *tape);
+
+/* Interval evaluation of a tape on n space-time boxes (the body of
+ * compute.wgsl:3632-3970 without the octree).  boxes: n x 8 floats
+ * (x.lo,x.hi,y.lo,y.hi,z.lo,z.hi,t.lo,t.hi), host memory.  out: n x 10
+ * floats: field (lo,hi) then sens of x,y,z,t (lo,hi each); sens are written
+ * when `reverse` is nonzero, else zero. */
+TSI_API tsi_status tsi_tape_eval_boxes(tsi_ctx *ctx, const tsi_tape *tape, uint32_t n,
+                                       const float *boxes, int32_t rounding_mode,
+                                       int32_t reverse, float *out);
+
+/* ---------------- scenes (plain path) ---------------- */
+TSI_API tsi_status tsi_scene_create(tsi_ctx *ctx, const tsi_tape *tape, const tsi_params *params,
+                                    uint64_t voxel_capacity, tsi_scene **out);
+TSI_API void tsi_scene_destroy(tsi_scene *scene);
+/* first_eval of main.rs:730-766: empty pool, root voxel 0 = root box. */
+TSI_API tsi_status tsi_scene_reset(tsi_scene *scene);
+/* One dispatch of `main` (main.rs:776-783) preceded by buf_main's
+ * re-seeding of the root (compute.wgsl:4706).  time = uniforms.time;
+ * t0_or_nan: start of the swept interval (NaN = time - swept_dt). */
+TSI_API tsi_status tsi_scene_invert(tsi_scene *scene, float time, float t0_or_nan,
+                                    tsi_stats *stats);
+/* One dispatch of `rt_main` (main.rs:649-656).  `out` may be NULL to keep
+ * the frame on the device only (see tsi_scene_image_device). */
+TSI_API tsi_status tsi_scene_trace(tsi_scene *scene, const tsi_uniforms *u, tsi_image *out,
+                                   tsi_stats *stats);
+TSI_API tsi_status tsi_scene_image_device(tsi_scene *scene, tsi_image_device *out);
+/* Octree as cells keyed by (level, ix, iy, iz), depth-first order.
+ * With out == NULL only the count is returned. */
+TSI_API tsi_status tsi_scene_readback_cells(tsi_scene *scene, tsi_cell *out, uint64_t cap,
+                                            uint64_t *n);
+TSI_API tsi_status tsi_scene_get_params(const tsi_scene *scene, tsi_params *out);
+TSI_API uint64_t tsi_scene_device_bytes(const tsi_scene *scene);
+
+/* ---------------- batched form ---------------- */
+typedef struct tsi_request {
+  tsi_scene *scene;
+  float time;
+  float t0_or_nan;
+  const tsi_uniforms *uniforms;  /* NULL: invert only */
+  tsi_image *out;                /* NULL: keep the frame on the device */
+  tsi_stats *stats;              /* may be NULL */
+} tsi_request;
+
+/* Inverts all requests' scenes in one fused launch sequence (every level
+ * of every scene shares each launch), then traces them.  Scenes must be
+ * distinct. */
+TSI_API tsi_status tsi_batch_run(tsi_ctx *ctx, tsi_request *reqs, uint32_t n);
+
+/* Captures tsi_batch_run for a fixed request set into a CUDA graph and
+ * replays it; times and cameras are re-read from the requests each replay. */
+typedef struct tsi_batch_graph tsi_batch_graph;
+TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *ctx, tsi_request *reqs, uint32_t n,
+                                          tsi_batch_graph **out);
+TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g);
+TSI_API void tsi_batch_graph_destroy(tsi_batch_graph *g);
+
+/* ---------------- diagnostics (tests and tools) ---------------- */
+/* Message of the last failing call on this thread. */
+TSI_API const char *tsi_last_error(void);
+/* Host-only: lower `text` and report the register allocation (no device).
+ * slot_reg, if not NULL, receives the register of each SSA slot. */
+TSI_API tsi_status tsi_ir_tape_info(const char *text, size_t len, tsi_tape_info *info, uint32_t *slot_reg,
+                                    uint32_t cap);
+/* Host-only: packed device words (2 per instruction after the ARG slots) of
+ * a tape given in the ir.rs layout. */
+TSI_API tsi_status tsi_compile_gpu_instructions(const tsi_gpu_instruction *instr, uint32_t n, uint32_t *words,
+                                                uint32_t cap_words, tsi_tape_info *info);
+/* Elementwise device f32 math, for the math tests: which = 0 sin(a),
+ * 1 exp(a), 2 log(a), 3 atan2(a, b), 4 powi(a, (int)b), 5 min(a, b),
+ * 6 max(a, b) (minimumNumber / maximumNumber), 7 fminf, 8 fmaxf. */
+TSI_API tsi_status tsi_debug_math(tsi_ctx *ctx, int32_t which, uint32_t n, const float *a, const float *b,
+                                  float *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TSI_H */

@@ -1,0 +1,289 @@
+"""Python host over the C ABI, mirroring the reference's host interface.
+
+The reference host (Rust) lowers the scene (`ir::IR::new`, src/ir.rs:334),
+seeds and dispatches `main` once per frame (`State::compute`,
+src/main.rs:724-820) and dispatches `rt_main` (`State::render`,
+main.rs:639-656) with the uniforms of src/uniforms.rs.  The same steps here
+go through libtsi.so:
+
+    ir = IR.new(text, time)                 # ir.rs IR::new
+    dev = Device()                          # State::new's device setup
+    state = State(dev, text, params)        # + tapes[0] upload, first_eval
+    ms = state.compute(time)                # State::compute -> device ms
+    img = state.render(uniforms)            # State::render (headless)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+
+__all__ = ["IR", "Device", "Tape", "Scene", "State", "default_params", "make_uniforms", "CELL_DTYPE"]
+
+CELL_DTYPE = np.dtype([
+    ("level", "<u4"), ("ix", "<u4"), ("iy", "<u4"), ("iz", "<u4"), ("f", "<f4"), ("t", "<f4"),
+    ("time_err", "<f4"), ("fast", "<f4"), ("dx", "<f4"), ("dy", "<f4"), ("dz", "<f4"), ("has_children", "<u4"),
+    ("x", "<f4", 2), ("y", "<f4", 2), ("z", "<f4", 2),
+])
+GPU_INSTR_DTYPE = np.dtype([("index_", "<u4"), ("opcode_uses", "<u4"), ("larg_rarg", "<u4"), ("literal", "<f4"),
+                            ("val", "<f4", 2), ("sens", "<f4", 2)])
+assert CELL_DTYPE.itemsize == C.sizeof(N.Cell)
+assert GPU_INSTR_DTYPE.itemsize == C.sizeof(N.GPUInstruction)
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def default_params(**kw) -> N.Params:
+    """PARAMETERS block defaults (compute.wgsl:3494-3511), overridable by name."""
+    lib = N.load()
+    p = N.Params()
+    lib.tsi_default_params(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        if k in ("root_lo", "root_hi"):
+            for i in range(3):
+                getattr(p, k)[i] = float(v[i])
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def make_uniforms(view, resolution, time: float = 0.0, lasttime: float = 0.0, rendermode: float = 0.0) -> N.Uniforms:
+    """uniforms.rs:8-45: camera-to-world view matrix (16 floats, column
+    major), resolution, time."""
+    u = N.Uniforms()
+    for i, v in enumerate(view):
+        u.view_matrix[i] = float(v)
+    u.resolution[0], u.resolution[1] = int(resolution[0]), int(resolution[1])
+    u.time = float(time)
+    u.lasttime = float(lasttime)
+    u.rendermode = float(rendermode)
+    return u
+
+
+class IR:
+    """ir.rs `IR`: `instructions` in the 32-byte GPUInstruction layout."""
+
+    def __init__(self, gpu_instructions: np.ndarray):
+        self.gpu_instructions = gpu_instructions
+
+    @classmethod
+    def new(cls, text: str, time: float = 0.0) -> "IR":
+        lib = N.load()
+        raw = text.encode()
+        n = C.c_uint32(0)
+        N.check(lib.tsi_ir_lower(raw, len(raw), float(time), None, 0, C.byref(n)), "tsi_ir_lower")
+        arr = np.zeros(n.value, dtype=GPU_INSTR_DTYPE)
+        N.check(lib.tsi_ir_lower(raw, len(raw), float(time), arr.ctypes.data_as(C.POINTER(N.GPUInstruction)),
+                                 n.value, C.byref(n)), "tsi_ir_lower")
+        return cls(arr)
+
+    def __len__(self) -> int:
+        return len(self.gpu_instructions)
+
+
+class Device:
+    """A tsi_ctx on one CUDA device (fails with TSI_ERR_NO_DEVICE without one)."""
+
+    def __init__(self, device: int = 0, work_item_capacity: int = 0, tape_arena_words: int = 0,
+                 log_arena_bytes: int = 0, max_scenes_per_launch: int = 0):
+        self.lib = N.load()
+        opts = N.DeviceOpts(device, work_item_capacity, tape_arena_words, log_arena_bytes, 0, max_scenes_per_launch)
+        h = C.c_void_p()
+        N.check(self.lib.tsi_create(C.byref(opts), C.byref(h)), "tsi_create")
+        self.handle = h
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.tsi_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self) -> None:
+        N.check(self.lib.tsi_synchronize(self.handle), "tsi_synchronize")
+
+    def math(self, which: int, a: np.ndarray, b: np.ndarray | None = None) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        b = np.zeros_like(a) if b is None else np.ascontiguousarray(b, dtype=np.float32)
+        out = np.empty_like(a)
+        N.check(self.lib.tsi_debug_math(self.handle, which, a.size, _fptr(a), _fptr(b), _fptr(out)), "tsi_debug_math")
+        return out
+
+
+class Tape:
+    def __init__(self, device: Device, handle: C.c_void_p):
+        self.device = device
+        self.handle = handle
+        info = N.TapeInfo()
+        N.check(device.lib.tsi_tape_info_get(handle, C.byref(info)), "tsi_tape_info_get")
+        self.instruction_count = info.instruction_count
+        self.registers = info.registers
+        self.minmax_count = info.minmax_count
+
+    @classmethod
+    def from_llvm_ir(cls, device: Device, text: str) -> "Tape":
+        raw = text.encode()
+        h = C.c_void_p()
+        N.check(device.lib.tsi_tape_from_llvm_ir(device.handle, raw, len(raw), C.byref(h)), "tsi_tape_from_llvm_ir")
+        return cls(device, h)
+
+    @classmethod
+    def upload(cls, device: Device, gpu_instructions: np.ndarray) -> "Tape":
+        arr = np.ascontiguousarray(gpu_instructions, dtype=GPU_INSTR_DTYPE)
+        h = C.c_void_p()
+        N.check(device.lib.tsi_tape_upload(device.handle, arr.ctypes.data_as(C.POINTER(N.GPUInstruction)), len(arr),
+                                           C.byref(h)), "tsi_tape_upload")
+        return cls(device, h)
+
+    def eval_boxes(self, boxes: np.ndarray, rounding_mode: int = 0, reverse: bool = True) -> np.ndarray:
+        boxes = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 8)
+        out = np.zeros((len(boxes), 10), dtype=np.float32)
+        N.check(self.device.lib.tsi_tape_eval_boxes(self.device.handle, self.handle, len(boxes), _fptr(boxes),
+                                                    rounding_mode, int(reverse), _fptr(out)), "tsi_tape_eval_boxes")
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.device.lib.tsi_tape_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scene:
+    """Resident octree of one scene (tsi_scene)."""
+
+    def __init__(self, device: Device, tape: Tape, params: N.Params, voxel_capacity: int = 0):
+        self.device, self.tape, self.params = device, tape, params
+        h = C.c_void_p()
+        N.check(device.lib.tsi_scene_create(device.handle, tape.handle, C.byref(params), voxel_capacity, C.byref(h)),
+                "tsi_scene_create")
+        self.handle = h
+
+    def reset(self) -> None:
+        N.check(self.device.lib.tsi_scene_reset(self.handle), "tsi_scene_reset")
+
+    def invert(self, time: float, t0: float = math.nan) -> N.Stats:
+        st = N.Stats()
+        N.check(self.device.lib.tsi_scene_invert(self.handle, float(time), float(t0), C.byref(st)), "tsi_scene_invert")
+        return st
+
+    def trace(self, uniforms: N.Uniforms, rgba: bool = True, depth: bool = True, normal: bool = True) -> dict:
+        w, h = uniforms.resolution[0], uniforms.resolution[1]
+        out = {}
+        img = N.Image(w, h, None, None, None)
+        if rgba:
+            out["rgba"] = np.empty((h, w, 4), dtype=np.float32)
+            img.rgba = _fptr(out["rgba"])
+        if depth:
+            out["depth"] = np.empty((h, w), dtype=np.float32)
+            img.depth = _fptr(out["depth"])
+        if normal:
+            out["normal"] = np.empty((h, w, 3), dtype=np.float32)
+            img.normal = _fptr(out["normal"])
+        st = N.Stats()
+        N.check(self.device.lib.tsi_scene_trace(self.handle, C.byref(uniforms), C.byref(img), C.byref(st)),
+                "tsi_scene_trace")
+        out["device_ms"] = st.device_ms
+        out["visits"] = st.reserved
+        return out
+
+    def cells(self) -> np.ndarray:
+        lib = self.device.lib
+        n = C.c_uint64(0)
+        N.check(lib.tsi_scene_readback_cells(self.handle, None, 0, C.byref(n)), "tsi_scene_readback_cells")
+        arr = np.zeros(n.value, dtype=CELL_DTYPE)
+        N.check(lib.tsi_scene_readback_cells(self.handle, arr.ctypes.data_as(C.POINTER(N.Cell)), n.value,
+                                             C.byref(n)), "tsi_scene_readback_cells")
+        return arr
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.device.lib.tsi_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class FrameResult:
+    stats: N.Stats
+    rootfind_ms: float
+
+
+class State:
+    """The per-scene state of src/main.rs `State`, headless: compute() is one
+    `main` dispatch (with the root re-seeded), render() one `rt_main`."""
+
+    def __init__(self, device: Device, text: str, params: N.Params | None = None, voxel_capacity: int = 0):
+        self.device = device
+        self.tape = Tape.from_llvm_ir(device, text)
+        self.params = params or default_params()
+        self.scene = Scene(device, self.tape, self.params, voxel_capacity)
+        self.first_eval = False  # the scene is created fresh (main.rs:730)
+
+    def compute(self, time: float, t0: float = math.nan) -> FrameResult:
+        if self.first_eval:
+            self.scene.reset()
+            self.first_eval = False
+        st = self.scene.invert(time, t0)
+        return FrameResult(st, st.device_ms)
+
+    def render(self, uniforms: N.Uniforms) -> dict:
+        return self.scene.trace(uniforms)
+
+
+def run_batch(device: Device, requests: list, graph: bool = False) -> list:
+    """Invert (and trace) several distinct scenes in one fused launch sequence
+    (tsi_batch_run).  requests: list of (scene, time, t0, uniforms or None).
+    Returns per-request dicts with the frame arrays when uniforms are given."""
+    n = len(requests)
+    reqs = (N.Request * n)()
+    keep = []
+    outs = []
+    for i, (scene, time, t0, uni) in enumerate(requests):
+        reqs[i].scene = scene.handle
+        reqs[i].time = float(time)
+        reqs[i].t0_or_nan = float(t0)
+        st = N.Stats()
+        keep.append(st)
+        reqs[i].stats = C.pointer(st)
+        out = {"stats": st}
+        if uni is not None:
+            w, h = uni.resolution[0], uni.resolution[1]
+            out["rgba"] = np.empty((h, w, 4), np.float32)
+            out["depth"] = np.empty((h, w), np.float32)
+            out["normal"] = np.empty((h, w, 3), np.float32)
+            img = N.Image(w, h, _fptr(out["rgba"]), _fptr(out["depth"]), _fptr(out["normal"]))
+            keep += [uni, img]
+            reqs[i].uniforms = C.pointer(uni)
+            reqs[i].out = C.pointer(img)
+        outs.append(out)
+    N.check(device.lib.tsi_batch_run(device.handle, reqs, n), "tsi_batch_run")
+    return outs

@@ -1,0 +1,1105 @@
+// api.cu — host runtime behind include/tsi.h.
+//
+// Replaces the reference's host side of the hot path: State::new buffer
+// setup (src/main.rs:97-303), State::compute (main.rs:724-820: first_eval
+// reseed, one `main` dispatch, blocking timestamp readback) and
+// State::render's rt_main dispatch (main.rs:639-656).  All device state of a
+// scene (voxel pool, counters, frame buffers) stays resident in HBM between
+// calls; only the per-frame launch descriptor goes up and the counters come
+// back.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "device_types.h"
+#include "ir_lower.h"
+#include "tape_compile.h"
+#include "tsi.h"
+
+namespace tsi {
+cudaError_t launch_refine(const LaunchParams &P, uint32_t level, uint32_t rcap, int grid, int block, size_t smem,
+                          cudaStream_t st);
+cudaError_t launch_frame_begin(const LaunchParams &P, cudaStream_t st);
+cudaError_t launch_frame_end(const LaunchParams &P, cudaStream_t st);
+cudaError_t refine_set_smem(size_t bytes);
+cudaError_t refine_occupancy(int block, size_t smem, int *blocks_per_sm);
+cudaError_t launch_evalbox(bool directed, const uint2 *code, uint32_t len, uint32_t nregs, uint32_t out_reg,
+                           uint32_t n, const float *boxes, int reverse, float *out, float2 *regs, float4 *log,
+                           cudaStream_t st);
+cudaError_t launch_math(int which, uint32_t n, const float *a, const float *b, float *out, cudaStream_t st);
+
+struct TraceParams {
+  float eye[3];
+  float m[16];
+  float zdist;
+  float yshift;
+  uint32_t W, H;
+  float time;
+  float rendermode;
+  uint32_t normal_viz;
+  float darken;
+  VoxelPoolDev pool;
+  float4 *rgba;
+  float *depth;
+  float *normal;
+  unsigned long long *visits;
+};
+cudaError_t launch_trace(const TraceParams &T, cudaStream_t st);
+}  // namespace tsi
+
+using namespace tsi;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+#define CK(call)                                                                     \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);             \
+      return TSI_ERR_CUDA;                                                           \
+    }                                                                                \
+  } while (0)
+
+constexpr int kBlock = 256;
+constexpr int kWarpsPerBlock = kBlock / 32;
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return cudaSuccess;
+  return cudaMalloc((void **)p, count * sizeof(T));
+}
+
+struct Readback {
+  uint32_t error;
+  uint32_t pad;
+  unsigned long long stats[ST_COUNT];
+  unsigned long long visits;
+  uint32_t item_count[TSI_MAX_LEVELS + 1];
+};
+
+}  // namespace
+
+struct tsi_tape {
+  tsi_ctx *ctx = nullptr;
+  uint2 *d_code = nullptr;
+  uint32_t len = 0;  // instructions after the 4 ARG slots
+  uint32_t count = 0, nregs = 0, out_reg = 0, n_minmax = 0;
+  uint64_t fwd_cost = 0;
+};
+
+struct tsi_scene {
+  tsi_ctx *ctx = nullptr;
+  const tsi_tape *tape = nullptr;
+  tsi_params p{};
+  uint32_t cap_bricks = 0;
+  VoxelPoolDev pool{};
+  SceneCounters *d_ctr = nullptr;
+  uint32_t img_w = 0, img_h = 0;
+  float4 *d_rgba = nullptr;
+  float *d_depth = nullptr;
+  float *d_normal = nullptr;
+  uint64_t bytes = 0;
+};
+
+struct tsi_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t max_scenes = 64;
+  SceneLaunch *d_scenes = nullptr, *h_scenes = nullptr;
+  TapeRec *d_recs = nullptr, *h_recs = nullptr;
+  uint32_t rec_cap = 0;
+  uint32_t *d_rec_count = nullptr;
+  uint2 *d_code = nullptr;
+  unsigned long long *d_code_count = nullptr;
+  uint64_t code_cap = 0;
+  WorkItem *d_items[2] = {nullptr, nullptr};
+  uint32_t item_cap = 0;
+  uint32_t *d_item_count = nullptr, *d_item_cursor = nullptr;
+  uint2 *d_dealloc[2] = {nullptr, nullptr};
+  uint32_t dealloc_cap = 0;
+  uint32_t *d_dealloc_count = nullptr, *d_dealloc_cursor = nullptr;
+  float4 *d_log = nullptr;
+  uint2 *d_dec = nullptr;
+  uint32_t slice_len = 0;
+  uint32_t max_warps = 0;
+  float4 *d_log_overflow = nullptr;
+  unsigned long long *d_log_used = nullptr;
+  uint64_t log_overflow_cap = 0;
+  uint32_t *d_error = nullptr;
+  unsigned long long *d_stats = nullptr;
+  unsigned long long *d_visits = nullptr;
+  Readback *h_rb = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  size_t smem_set = 0;
+  // scratch for tsi_tape_eval_boxes
+  void *d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  uint32_t watchdog = 0;
+};
+
+struct tsi_batch_graph {
+  tsi_ctx *ctx = nullptr;
+  std::vector<tsi_request> reqs;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+tsi_status set_err(tsi_status s, const std::string &msg) {
+  g_last_error = msg;
+  return s;
+}
+
+LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes) {
+  LaunchParams P{};
+  P.scenes = c->d_scenes;
+  P.n_scenes = n_scenes;
+  P.rec_cap = c->rec_cap;
+  P.recs = c->d_recs;
+  P.rec_count = c->d_rec_count;
+  P.code_arena = c->d_code;
+  P.code_count = c->d_code_count;
+  P.code_cap = c->code_cap;
+  P.items[0] = c->d_items[0];
+  P.items[1] = c->d_items[1];
+  P.item_count = c->d_item_count;
+  P.item_cursor = c->d_item_cursor;
+  P.item_cap = c->item_cap;
+  P.dealloc_cap = c->dealloc_cap;
+  P.dealloc[0] = c->d_dealloc[0];
+  P.dealloc[1] = c->d_dealloc[1];
+  P.dealloc_count = c->d_dealloc_count;
+  P.dealloc_cursor = c->d_dealloc_cursor;
+  P.log_slices = c->d_log;
+  P.dec_slices = c->d_dec;
+  P.slice_len = c->slice_len;
+  P.log_overflow = c->d_log_overflow;
+  P.log_overflow_used = c->d_log_used;
+  P.log_overflow_cap = c->log_overflow_cap;
+  P.error = c->d_error;
+  P.stats = c->d_stats;
+  return P;
+}
+
+tsi_status status_from_error_bits(uint32_t e) {
+  if (e & EB_OOM) return set_err(TSI_ERR_OOM, "voxel pool exhausted");
+  if (e & EB_LOG_OOM) return set_err(TSI_ERR_OOM, "reverse-AD log arena exhausted");
+  if (e & EB_QUEUE_FULL) return set_err(TSI_ERR_QUEUE_FULL, "work list capacity exceeded");
+  if (e & EB_WATCHDOG) return set_err(TSI_ERR_WATCHDOG, "bounded device wait expired");
+  return TSI_OK;
+}
+
+void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, SceneLaunch &L, TapeRec &R) {
+  const tsi_params &p = s->p;
+  L.pool = s->pool;
+  L.ctr = s->d_ctr;
+  L.eps = 10.0f * ldexpf(1.0f, -p.localsubdiv);  // compute.wgsl:3521 (exact power of two)
+  L.delta = p.delta;
+  L.fast_thresh = p.delta * p.fast_multiplier;
+  L.time = time;
+  L.t0 = (t0_or_nan != t0_or_nan) ? time - p.swept_dt : t0_or_nan;
+  uint32_t f = 0;
+  if (p.pointsample) f |= SF_POINTSAMPLE;
+  if (p.fastenabled) f |= SF_FASTENABLED;
+  if (p.lipschitz_corrected) f |= SF_LIPSCHITZ;
+  if (p.swept_volume) f |= SF_SWEPT;
+  if (!p.fast_normals && p.normal_viz) f |= SF_ALWAYS_DERIV;
+  if (p.pruning) f |= SF_PRUNING;
+  if (p.rounding_mode == TSI_ROUND_DIRECTED) f |= SF_DIRECTED;
+  L.flags = f;
+  L.root_rec = slot;
+  L.levels = (uint32_t)p.localsubdiv;
+  L.full_len = s->tape->len;
+  R.code = s->tape->d_code;
+  R.len = s->tape->len;
+  R.nregs = s->tape->nregs;
+  R.out_reg = s->tape->out_reg;
+  R.n_minmax = s->tape->n_minmax;
+  R.t_lo = -INFINITY;
+  R.t_hi = INFINITY;
+  R.parent = TSI_NONE;
+  R.pad = 0;
+}
+
+// One frame of set inversion for n scenes, all levels in one launch sequence.
+tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *times, const float *t0s, uint32_t n) {
+  if (n == 0) return TSI_OK;
+  if (n > c->max_scenes) return set_err(TSI_ERR_INVALID_ARGUMENT, "too many scenes in one launch");
+  uint32_t lmax = 0, rmax = 4;
+  for (uint32_t i = 0; i < n; ++i) {
+    fill_launch(scenes[i], i, times[i], t0s[i], c->h_scenes[i], c->h_recs[i]);
+    lmax = std::max(lmax, (uint32_t)scenes[i]->p.localsubdiv);
+    rmax = std::max(rmax, scenes[i]->tape->nregs);
+  }
+  const uint32_t rcap = (rmax + 3u) & ~3u;
+  const size_t smem = (size_t)kWarpsPerBlock * rcap * 32u * sizeof(float2);
+  if (smem > c->smem_set) {
+    CK(refine_set_smem(smem));
+    c->smem_set = smem;
+  }
+  int bps = 0;
+  CK(refine_occupancy(kBlock, smem, &bps));
+  if (bps < 1) return set_err(TSI_ERR_TAPE_TOO_WIDE, "register file does not fit in shared memory");
+  int grid = bps * c->sm_count;
+  grid = std::min<int>(grid, (int)(c->max_warps / kWarpsPerBlock));
+  CK(cudaMemcpyAsync(c->d_scenes, c->h_scenes, n * sizeof(SceneLaunch), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_recs, c->h_recs, n * sizeof(TapeRec), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_error, 0, sizeof(uint32_t), c->stream));
+  CK(cudaMemsetAsync(c->d_stats, 0, ST_COUNT * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(c->d_log_used, 0, sizeof(unsigned long long), c->stream));
+  const LaunchParams P = make_params(c, n);
+  CK(launch_frame_begin(P, c->stream));
+  for (uint32_t level = 0; level < lmax; ++level) CK(launch_refine(P, level, rcap, grid, kBlock, smem, c->stream));
+  CK(launch_frame_end(P, c->stream));
+  return TSI_OK;
+}
+
+tsi_status enqueue_readback(tsi_ctx *c) {
+  CK(cudaMemcpyAsync(&c->h_rb->error, c->d_error, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_rb->stats, c->d_stats, ST_COUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaMemcpyAsync(c->h_rb->item_count, c->d_item_count, sizeof(c->h_rb->item_count), cudaMemcpyDeviceToHost,
+                     c->stream));
+  return TSI_OK;
+}
+
+void fill_stats(const Readback &rb, tsi_stats *st, uint64_t voxels_live) {
+  if (!st) return;
+  memset(st, 0, sizeof(*st));
+  st->parents_expanded = rb.stats[ST_PARENTS];
+  st->cells_evaluated = rb.stats[ST_EVAL];
+  st->cells_reverse = rb.stats[ST_REVERSE];
+  st->cells_skipped = rb.stats[ST_SKIPPED];
+  st->cells_ambiguous = rb.stats[ST_AMBIG];
+  st->cells_empty = rb.stats[ST_EMPTY];
+  st->cells_full = rb.stats[ST_FULL];
+  st->cells_enqueued = rb.stats[ST_ENQUEUED];
+  st->cells_reused = rb.stats[ST_REUSED];
+  st->instr_forward = rb.stats[ST_INSTR_FWD];
+  st->instr_reverse = rb.stats[ST_INSTR_REV];
+  st->instr_full_equiv = rb.stats[ST_INSTR_FULL];
+  st->fp32_ops = rb.stats[ST_FP32];
+  st->bricks_allocated = rb.stats[ST_BRICK_ALLOC];
+  st->bricks_freed = rb.stats[ST_BRICK_FREE];
+  st->tape_words = rb.stats[ST_TAPE_WORDS];
+  st->prune_fallbacks = rb.stats[ST_PRUNE_FALLBACK];
+  st->voxels_live = voxels_live;
+  uint64_t hw = 0;
+  uint32_t levels = 0;
+  for (int l = 0; l <= TSI_MAX_LEVELS; ++l) {
+    hw = std::max<uint64_t>(hw, rb.item_count[l]);
+    if (rb.item_count[l]) levels = (uint32_t)l + 1;
+  }
+  st->items_high_water = hw;
+  st->levels = levels;
+  st->error_flags = rb.error;
+}
+
+// camera of rt_main (compute.wgsl:4651-4685), computed once per frame
+void rotation_matrix(const float axis_in[3], float angle, float out[16]) {
+  float l = sqrtf((axis_in[0] * axis_in[0] + axis_in[1] * axis_in[1]) + axis_in[2] * axis_in[2]);
+  const float ax = axis_in[0] / l, ay = axis_in[1] / l, az = axis_in[2] / l;
+  const float s = sinf(angle), cc = cosf(angle), oc = 1.0f - cc;
+  const float m[16] = {oc * ax * ax + cc, oc * ax * ay - az * s, oc * az * ax + ay * s, 0.0f,
+                       oc * ax * ay + az * s, oc * ay * ay + cc, oc * ay * az - ax * s, 0.0f,
+                       oc * az * ax - ay * s, oc * ay * az + ax * s, oc * az * az + cc, 0.0f,
+                       0.0f, 0.0f, 0.0f, 1.0f};
+  memcpy(out, m, sizeof(m));
+}
+
+void matmul4(const float a[16], const float b[16], float out[16]) {
+  float r[16];
+  for (int col = 0; col < 4; ++col)
+    for (int row = 0; row < 4; ++row) {
+      float s = a[0 * 4 + row] * b[col * 4 + 0];
+      s = s + a[1 * 4 + row] * b[col * 4 + 1];
+      s = s + a[2 * 4 + row] * b[col * 4 + 2];
+      s = s + a[3 * 4 + row] * b[col * 4 + 3];
+      r[col * 4 + row] = s;
+    }
+  memcpy(out, r, sizeof(r));
+}
+
+void make_camera(const tsi_params &p, const tsi_uniforms &u, TraceParams &T) {
+  float view[16];
+  memcpy(view, u.view_matrix, sizeof(view));
+  float eye[3] = {view[12], view[13], view[14]};
+  const float PI = 3.1415927410125732f;
+  if (p.scene_id == 3) {
+    eye[0] = eye[0] + 7.7f;
+    eye[1] = eye[1] + -2.21f;
+    eye[2] = eye[2] + 7.7f;
+    const float ax[3] = {0.0f, 1.0f, 0.0f};
+    float r[16];
+    rotation_matrix(ax, (PI / 4.0f) * 3.0f, r);
+    matmul4(r, view, view);
+  } else if (p.scene_id == 4) {
+    eye[0] = eye[0] + 0.0f;
+    eye[1] = eye[1] + -0.78f;
+    eye[2] = eye[2] + -7.0f;
+  } else if (p.scene_id == 5) {
+    eye[0] = eye[0] + 7.13f;
+    eye[1] = eye[1] + 2.14f;
+    eye[2] = eye[2] + -5.6f;
+    float r[16];
+    const float ax1[3] = {0.0f, 1.0f, 0.0f};
+    rotation_matrix(ax1, PI / 4.0f, r);
+    matmul4(r, view, view);
+    const float ax2[3] = {-1.0f, 0.0f, -1.0f};
+    rotation_matrix(ax2, (PI / 4.0f) * 0.45f, r);
+    matmul4(r, view, view);
+  }
+  memcpy(T.eye, eye, sizeof(eye));
+  memcpy(T.m, view, sizeof(view));
+  const float fov = 90.0f;
+  const float rad = fov * 0.017453292519943295474f;
+  T.zdist = (float)u.resolution[1] / tanf(rad / 2.0f);
+  T.yshift = (p.scene_id == 0) ? (float)u.resolution[1] * 0.32f : 0.0f;
+  T.W = u.resolution[0];
+  T.H = u.resolution[1];
+  T.time = u.time;
+  T.rendermode = u.rendermode;
+  T.normal_viz = p.normal_viz ? 1u : 0u;
+  T.darken = p.octree_darken_factor;
+}
+
+tsi_status ensure_image(tsi_scene *s, uint32_t w, uint32_t h) {
+  if (s->img_w == w && s->img_h == h && s->d_rgba) return TSI_OK;
+  cudaFree(s->d_rgba);
+  cudaFree(s->d_depth);
+  cudaFree(s->d_normal);
+  s->d_rgba = nullptr;
+  s->d_depth = nullptr;
+  s->d_normal = nullptr;
+  const size_t np = (size_t)w * h;
+  CK(dalloc(&s->d_rgba, np));
+  CK(dalloc(&s->d_depth, np));
+  CK(dalloc(&s->d_normal, np * 3));
+  s->img_w = w;
+  s->img_h = h;
+  return TSI_OK;
+}
+
+tsi_status enqueue_trace(tsi_scene *s, const tsi_uniforms *u) {
+  tsi_ctx *c = s->ctx;
+  const tsi_status st = ensure_image(s, u->resolution[0], u->resolution[1]);
+  if (st != TSI_OK) return st;
+  TraceParams T{};
+  make_camera(s->p, *u, T);
+  T.pool = s->pool;
+  T.rgba = s->d_rgba;
+  T.depth = s->d_depth;
+  T.normal = s->d_normal;
+  T.visits = c->d_visits;
+  if (T.W == 0 || T.H == 0) return TSI_OK;
+  CK(launch_trace(T, c->stream));
+  return TSI_OK;
+}
+
+tsi_status copy_image_out(tsi_scene *s, tsi_image *out) {
+  tsi_ctx *c = s->ctx;
+  if (!out) return TSI_OK;
+  if (out->width != s->img_w || out->height != s->img_h)
+    return set_err(TSI_ERR_BUFFER_TOO_SMALL, "tsi_image size does not match the uniforms' resolution");
+  const size_t np = (size_t)s->img_w * s->img_h;
+  if (out->rgba) CK(cudaMemcpyAsync(out->rgba, s->d_rgba, np * 16, cudaMemcpyDeviceToHost, c->stream));
+  if (out->depth) CK(cudaMemcpyAsync(out->depth, s->d_depth, np * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (out->normal) CK(cudaMemcpyAsync(out->normal, s->d_normal, np * 12, cudaMemcpyDeviceToHost, c->stream));
+  return TSI_OK;
+}
+
+tsi_status reset_scene(tsi_scene *s) {
+  tsi_ctx *c = s->ctx;
+  // main.rs:749-766: root voxel 0 = root box, t 0, no children, f 0
+  const float4 xy = make_float4(s->p.root_lo[0], s->p.root_hi[0], s->p.root_lo[1], s->p.root_hi[1]);
+  const float2 z = make_float2(s->p.root_lo[2], s->p.root_hi[2]);
+  const float zero = 0.0f;
+  const uint32_t none = TSI_NONE;
+  const float4 n0 = make_float4(0, 0, 0, 0);
+  CK(cudaMemcpyAsync(s->pool.box_xy, &xy, sizeof(xy), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s->pool.box_z, &z, sizeof(z), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s->pool.t, &zero, 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s->pool.time_err, &zero, 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s->pool.f, &zero, 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s->pool.fast, &zero, 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s->pool.child, &none, 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s->pool.normal, &n0, sizeof(n0), cudaMemcpyHostToDevice, c->stream));
+  SceneCounters ctr{0, 1u, 0u, 1u};
+  CK(cudaMemcpyAsync(s->d_ctr, &ctr, sizeof(ctr), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return TSI_OK;
+}
+
+tsi_status read_counters(tsi_scene *s, SceneCounters &ctr) {
+  CK(cudaMemcpy(&ctr, s->d_ctr, sizeof(ctr), cudaMemcpyDeviceToHost));
+  return TSI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+TSI_API uint32_t tsi_version(void) { return TSI_ABI_VERSION; }
+
+TSI_API const char *tsi_status_string(tsi_status s) {
+  switch (s) {
+    case TSI_OK: return "ok";
+    case TSI_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case TSI_ERR_PARSE: return "cannot parse LLVM IR";
+    case TSI_ERR_CUDA: return "CUDA error";
+    case TSI_ERR_OOM: return "out of device memory or pool capacity";
+    case TSI_ERR_QUEUE_FULL: return "device work list full";
+    case TSI_ERR_WATCHDOG: return "bounded device wait expired";
+    case TSI_ERR_BAD_OPCODE: return "bad opcode";
+    case TSI_ERR_TAPE_TOO_WIDE: return "tape needs more than 256 registers";
+    case TSI_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    case TSI_ERR_BUFFER_TOO_SMALL: return "buffer too small";
+    case TSI_ERR_BUSY: return "busy";
+    case TSI_ERR_NOT_FOUND: return "not found";
+    case TSI_ERR_SHUTDOWN: return "shut down";
+  }
+  return "unknown status";
+}
+
+TSI_API const char *tsi_last_error(void) { return g_last_error.c_str(); }
+
+TSI_API void tsi_default_params(tsi_params *p) {  // compute.wgsl:3494-3511, ir.rs:343-347
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->localsubdiv = 8;
+  p->delta = 0.01f;
+  p->pointsample = 1;
+  p->fastenabled = 1;
+  p->lipschitz_corrected = 0;
+  p->swept_volume = 0;
+  p->fast_normals = 0;
+  p->normal_viz = 0;
+  p->rounding_mode = TSI_ROUND_NEAREST;
+  p->fast_multiplier = 1.0f;
+  p->scene_id = 1;
+  p->octree_darken_factor = 0.98f;
+  for (int i = 0; i < 3; ++i) {
+    p->root_lo[i] = -5.0f;
+    p->root_hi[i] = 5.0f;
+  }
+  p->pruning = 1;
+  p->swept_dt = 1.0f / 60.0f;
+}
+
+TSI_API tsi_status tsi_ir_lower(const char *text, size_t len, float time, tsi_gpu_instruction *out, uint32_t cap,
+                                uint32_t *n) {
+  if (!text || !n) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  std::vector<IrInstr> ins;
+  IrError err;
+  const float lo[3] = {-5.0f, -5.0f, -5.0f}, hi[3] = {5.0f, 5.0f, 5.0f};
+  if (!ir_new(std::string(text, len), time, lo, hi, ins, err))
+    return set_err(TSI_ERR_PARSE, "line " + std::to_string(err.line) + ": " + err.message);
+  *n = (uint32_t)ins.size();
+  if (out)
+    for (uint32_t i = 0; i < std::min<uint32_t>(cap, *n); ++i) out[i] = ir_to_gpu(ins[i]);
+  return (out && cap < *n) ? TSI_ERR_BUFFER_TOO_SMALL : TSI_OK;
+}
+
+// host-only: register allocation summary of an LLVM IR scene (no device)
+TSI_API tsi_status tsi_ir_tape_info(const char *text, size_t len, tsi_tape_info *info, uint32_t *slot_reg,
+                                    uint32_t cap) {
+  if (!text || !info) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  std::vector<IrInstr> ins;
+  IrError err;
+  const float lo[3] = {-5.0f, -5.0f, -5.0f}, hi[3] = {5.0f, 5.0f, 5.0f};
+  if (!ir_new(std::string(text, len), 0.0f, lo, hi, ins, err))
+    return set_err(TSI_ERR_PARSE, "line " + std::to_string(err.line) + ": " + err.message);
+  PackedTape pt;
+  tsi_status st = TSI_OK;
+  std::string why;
+  if (!compile_tape(ins, pt, st, why)) return set_err(st, why);
+  info->instruction_count = pt.count;
+  info->registers = pt.nregs;
+  info->minmax_count = pt.n_minmax;
+  info->reserved = pt.out_reg;
+  if (slot_reg)
+    for (uint32_t i = 0; i < std::min<uint32_t>(cap, pt.count); ++i) slot_reg[i] = pt.slot_reg[i];
+  return TSI_OK;
+}
+
+// host-only: the packed device tape words of an uploaded-format tape (tests)
+TSI_API tsi_status tsi_compile_gpu_instructions(const tsi_gpu_instruction *instr, uint32_t n, uint32_t *words,
+                                                uint32_t cap_words, tsi_tape_info *info) {
+  if (!instr || !info) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  std::vector<IrInstr> ins;
+  tsi_status st = TSI_OK;
+  std::string why;
+  if (!ir_from_gpu(instr, n, ins, st, why)) return set_err(st, why);
+  PackedTape pt;
+  if (!compile_tape(ins, pt, st, why)) return set_err(st, why);
+  info->instruction_count = pt.count;
+  info->registers = pt.nregs;
+  info->minmax_count = pt.n_minmax;
+  info->reserved = pt.out_reg;
+  if (words)
+    for (uint32_t i = 0; i < std::min<uint32_t>(cap_words, (uint32_t)pt.code.size()); ++i) words[i] = pt.code[i];
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
+  if (!out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_err(TSI_ERR_NO_DEVICE, "no CUDA device");
+  }
+  const int dev = opts ? opts->device : 0;
+  if (dev < 0 || dev >= ndev) return set_err(TSI_ERR_NO_DEVICE, "device ordinal out of range");
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major != 10) return set_err(TSI_ERR_NO_DEVICE, std::string("not an sm_100 device: ") + prop.name);
+  CK(cudaSetDevice(dev));
+  tsi_ctx *c = new tsi_ctx();
+  c->device = dev;
+  c->sm_count = prop.multiProcessorCount;
+  auto fail = [&](tsi_status s) {
+    tsi_destroy(c);
+    return s;
+  };
+#define CKC(call)                                                          \
+  do {                                                                     \
+    cudaError_t e_ = (call);                                               \
+    if (e_ != cudaSuccess) {                                               \
+      g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);   \
+      return fail(TSI_ERR_CUDA);                                           \
+    }                                                                      \
+  } while (0)
+  CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  c->max_scenes = (opts && opts->max_scenes_per_launch) ? opts->max_scenes_per_launch : 64u;
+  c->item_cap = (opts && opts->work_item_capacity) ? (uint32_t)opts->work_item_capacity : (4u << 20);
+  c->dealloc_cap = c->item_cap * 2u;
+  c->rec_cap = c->item_cap * 2u;
+  c->code_cap = (opts && opts->tape_arena_words) ? opts->tape_arena_words : (96ull << 20);
+  c->log_overflow_cap = (opts && opts->log_arena_bytes) ? opts->log_arena_bytes / 16 : ((2ull << 30) / 16);
+  c->watchdog = (opts && opts->watchdog_iters) ? opts->watchdog_iters : (1u << 22);
+  c->slice_len = 1024;
+  // resident warps at the smallest register file
+  {
+    const size_t smem_min = (size_t)kWarpsPerBlock * 4u * 32u * sizeof(float2);
+    CKC(refine_set_smem(smem_min));
+    c->smem_set = smem_min;
+    int bps = 0;
+    CKC(refine_occupancy(kBlock, smem_min, &bps));
+    c->max_warps = (uint32_t)std::max(1, bps) * (uint32_t)c->sm_count * kWarpsPerBlock;
+  }
+  CKC(dalloc(&c->d_scenes, c->max_scenes));
+  CKC(cudaMallocHost((void **)&c->h_scenes, c->max_scenes * sizeof(SceneLaunch)));
+  CKC(dalloc(&c->d_recs, c->rec_cap));
+  CKC(cudaMallocHost((void **)&c->h_recs, c->max_scenes * sizeof(TapeRec)));
+  CKC(dalloc(&c->d_rec_count, 1));
+  CKC(dalloc(&c->d_code, c->code_cap));
+  CKC(dalloc(&c->d_code_count, 1));
+  CKC(dalloc(&c->d_items[0], c->item_cap));
+  CKC(dalloc(&c->d_items[1], c->item_cap));
+  CKC(dalloc(&c->d_item_count, TSI_MAX_LEVELS + 1));
+  CKC(dalloc(&c->d_item_cursor, TSI_MAX_LEVELS + 1));
+  CKC(dalloc(&c->d_dealloc[0], c->dealloc_cap));
+  CKC(dalloc(&c->d_dealloc[1], c->dealloc_cap));
+  CKC(dalloc(&c->d_dealloc_count, TSI_MAX_LEVELS + 1));
+  CKC(dalloc(&c->d_dealloc_cursor, TSI_MAX_LEVELS + 1));
+  CKC(dalloc(&c->d_log, (size_t)c->max_warps * c->slice_len * 32u));
+  CKC(dalloc(&c->d_dec, (size_t)c->max_warps * c->slice_len));
+  CKC(dalloc(&c->d_log_overflow, c->log_overflow_cap));
+  CKC(dalloc(&c->d_log_used, 1));
+  CKC(dalloc(&c->d_error, 1));
+  CKC(dalloc(&c->d_stats, ST_COUNT));
+  CKC(dalloc(&c->d_visits, 1));
+  CKC(cudaMallocHost((void **)&c->h_rb, sizeof(Readback)));
+  CKC(cudaEventCreate(&c->ev0));
+  CKC(cudaEventCreate(&c->ev1));
+  CKC(cudaEventCreate(&c->ev2));
+  CKC(cudaMemsetAsync(c->d_item_count, 0, (TSI_MAX_LEVELS + 1) * sizeof(uint32_t), c->stream));
+  CKC(cudaStreamSynchronize(c->stream));
+#undef CKC
+  *out = c;
+  return TSI_OK;
+}
+
+TSI_API void tsi_destroy(tsi_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->d_scenes);
+  cudaFreeHost(c->h_scenes);
+  cudaFree(c->d_recs);
+  cudaFreeHost(c->h_recs);
+  cudaFree(c->d_rec_count);
+  cudaFree(c->d_code);
+  cudaFree(c->d_code_count);
+  cudaFree(c->d_items[0]);
+  cudaFree(c->d_items[1]);
+  cudaFree(c->d_item_count);
+  cudaFree(c->d_item_cursor);
+  cudaFree(c->d_dealloc[0]);
+  cudaFree(c->d_dealloc[1]);
+  cudaFree(c->d_dealloc_count);
+  cudaFree(c->d_dealloc_cursor);
+  cudaFree(c->d_log);
+  cudaFree(c->d_dec);
+  cudaFree(c->d_log_overflow);
+  cudaFree(c->d_log_used);
+  cudaFree(c->d_error);
+  cudaFree(c->d_stats);
+  cudaFree(c->d_visits);
+  cudaFree(c->d_scratch);
+  cudaFreeHost(c->h_rb);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev2) cudaEventDestroy(c->ev2);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+TSI_API tsi_status tsi_synchronize(tsi_ctx *c) {
+  if (!c) return set_err(TSI_ERR_INVALID_ARGUMENT, "null ctx");
+  CK(cudaStreamSynchronize(c->stream));
+  return TSI_OK;
+}
+
+static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tape **out) {
+  PackedTape pt;
+  tsi_status st = TSI_OK;
+  std::string why;
+  if (!compile_tape(ins, pt, st, why)) return set_err(st, why);
+  tsi_tape *t = new tsi_tape();
+  t->ctx = c;
+  t->len = pt.count - 4u;
+  t->count = pt.count;
+  t->nregs = pt.nregs;
+  t->out_reg = pt.out_reg;
+  t->n_minmax = pt.n_minmax;
+  t->fwd_cost = pt.fwd_cost;
+  if (t->len) {
+    cudaError_t e = dalloc(&t->d_code, t->len);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(t->d_code, pt.code.data(), (size_t)t->len * sizeof(uint2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      g_last_error = cudaGetErrorString(e);
+      cudaFree(t->d_code);
+      delete t;
+      return TSI_ERR_CUDA;
+    }
+  }
+  *out = t;
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_tape_upload(tsi_ctx *c, const tsi_gpu_instruction *instr, uint32_t n, tsi_tape **out) {
+  if (!c || !instr || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  std::vector<IrInstr> ins;
+  tsi_status st = TSI_OK;
+  std::string why;
+  if (!ir_from_gpu(instr, n, ins, st, why)) return set_err(st, why);
+  CK(cudaSetDevice(c->device));
+  return upload_ir(c, ins, out);
+}
+
+TSI_API tsi_status tsi_tape_from_llvm_ir(tsi_ctx *c, const char *text, size_t len, tsi_tape **out) {
+  if (!c || !text || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  std::vector<IrInstr> ins;
+  IrError err;
+  const float lo[3] = {-5.0f, -5.0f, -5.0f}, hi[3] = {5.0f, 5.0f, 5.0f};
+  if (!ir_new(std::string(text, len), 0.0f, lo, hi, ins, err))
+    return set_err(TSI_ERR_PARSE, "line " + std::to_string(err.line) + ": " + err.message);
+  CK(cudaSetDevice(c->device));
+  return upload_ir(c, ins, out);
+}
+
+TSI_API tsi_status tsi_tape_info_get(const tsi_tape *t, tsi_tape_info *info) {
+  if (!t || !info) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  info->instruction_count = t->count;
+  info->registers = t->nregs;
+  info->minmax_count = t->n_minmax;
+  info->reserved = t->out_reg;
+  return TSI_OK;
+}
+
+TSI_API void tsi_tape_destroy(tsi_tape *t) {
+  if (!t) return;
+  cudaFree(t->d_code);
+  delete t;
+}
+
+TSI_API tsi_status tsi_tape_eval_boxes(tsi_ctx *c, const tsi_tape *t, uint32_t n, const float *boxes,
+                                       int32_t rounding_mode, int32_t reverse, float *out) {
+  if (!c || !t || (!boxes && n) || (!out && n)) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  if (n == 0) return TSI_OK;
+  CK(cudaSetDevice(c->device));
+  const size_t nb = (size_t)n * 8 * 4, no = (size_t)n * 10 * 4;
+  const size_t nr = (size_t)n * t->nregs * 8, nl = (size_t)n * std::max<uint32_t>(t->len, 1u) * 16;
+  const size_t need = nb + no + nr + nl + 1024;
+  if (need > c->scratch_bytes) {
+    cudaFree(c->d_scratch);
+    c->d_scratch = nullptr;
+    c->scratch_bytes = 0;
+    CK(cudaMalloc(&c->d_scratch, need));
+    c->scratch_bytes = need;
+  }
+  char *base = (char *)c->d_scratch;
+  float *d_boxes = (float *)base;
+  float *d_out = (float *)(base + ((nb + 255) & ~(size_t)255));
+  float2 *d_regs = (float2 *)(base + ((nb + 255) & ~(size_t)255) + ((no + 255) & ~(size_t)255));
+  float4 *d_log = (float4 *)((char *)d_regs + ((nr + 255) & ~(size_t)255));
+  CK(cudaMemcpyAsync(d_boxes, boxes, nb, cudaMemcpyHostToDevice, c->stream));
+  CK(launch_evalbox(rounding_mode == TSI_ROUND_DIRECTED, t->d_code, t->len, t->nregs, t->out_reg, n, d_boxes, reverse,
+                    d_out, d_regs, d_log, c->stream));
+  CK(cudaMemcpyAsync(out, d_out, no, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return TSI_OK;
+}
+
+// device f32 math on host arrays (GPU math tests)
+TSI_API tsi_status tsi_debug_math(tsi_ctx *c, int32_t which, uint32_t n, const float *a, const float *b, float *out) {
+  if (!c || !a || !b || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  if (n == 0) return TSI_OK;
+  CK(cudaSetDevice(c->device));
+  const size_t need = (size_t)n * 12 + 1024;
+  if (need > c->scratch_bytes) {
+    cudaFree(c->d_scratch);
+    c->d_scratch = nullptr;
+    c->scratch_bytes = 0;
+    CK(cudaMalloc(&c->d_scratch, need));
+    c->scratch_bytes = need;
+  }
+  float *da = (float *)c->d_scratch, *db = da + n, *dout = db + n;
+  CK(cudaMemcpyAsync(da, a, (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(db, b, (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(launch_math(which, n, da, db, dout, c->stream));
+  CK(cudaMemcpyAsync(out, dout, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_scene_create(tsi_ctx *c, const tsi_tape *tape, const tsi_params *params,
+                                    uint64_t voxel_capacity, tsi_scene **out) {
+  if (!c || !tape || !params || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (params->localsubdiv < 1 || params->localsubdiv > TSI_MAX_LEVELS - 1)
+    return set_err(TSI_ERR_INVALID_ARGUMENT, "localsubdiv out of range");
+  if (tape->ctx != c) return set_err(TSI_ERR_INVALID_ARGUMENT, "tape belongs to another context");
+  CK(cudaSetDevice(c->device));
+  if (voxel_capacity == 0) voxel_capacity = 4ull << 20;
+  uint64_t bricks = (voxel_capacity + 7) / 8;
+  if (bricks < 2) bricks = 2;
+  if (bricks > 0x1fffffffull) return set_err(TSI_ERR_INVALID_ARGUMENT, "voxel capacity too large");
+  tsi_scene *s = new tsi_scene();
+  s->ctx = c;
+  s->tape = tape;
+  s->p = *params;
+  s->cap_bricks = (uint32_t)bricks;
+  const size_t nv = (size_t)bricks * 8;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](cudaError_t r) {
+    if (e == cudaSuccess) e = r;
+  };
+  A(dalloc(&s->pool.box_xy, nv));
+  A(dalloc(&s->pool.box_z, nv));
+  A(dalloc(&s->pool.t, nv));
+  A(dalloc(&s->pool.time_err, nv));
+  A(dalloc(&s->pool.f, nv));
+  A(dalloc(&s->pool.fast, nv));
+  A(dalloc(&s->pool.child, nv));
+  A(dalloc(&s->pool.normal, nv));
+  A(dalloc(&s->pool.free_list, bricks));
+  A(dalloc(&s->pool.pending, bricks));
+  A(dalloc(&s->d_ctr, 1));
+  s->pool.cap_bricks = s->cap_bricks;
+  s->bytes = nv * (16 + 8 + 4 * 5 + 16) + bricks * 8 + sizeof(SceneCounters);
+  if (e != cudaSuccess) {
+    g_last_error = cudaGetErrorString(e);
+    tsi_scene_destroy(s);
+    return e == cudaErrorMemoryAllocation ? TSI_ERR_OOM : TSI_ERR_CUDA;
+  }
+  tsi_status st = reset_scene(s);
+  if (st != TSI_OK) {
+    tsi_scene_destroy(s);
+    return st;
+  }
+  *out = s;
+  return TSI_OK;
+}
+
+TSI_API void tsi_scene_destroy(tsi_scene *s) {
+  if (!s) return;
+  if (s->ctx) {
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+  }
+  cudaFree(s->pool.box_xy);
+  cudaFree(s->pool.box_z);
+  cudaFree(s->pool.t);
+  cudaFree(s->pool.time_err);
+  cudaFree(s->pool.f);
+  cudaFree(s->pool.fast);
+  cudaFree(s->pool.child);
+  cudaFree(s->pool.normal);
+  cudaFree(s->pool.free_list);
+  cudaFree(s->pool.pending);
+  cudaFree(s->d_ctr);
+  cudaFree(s->d_rgba);
+  cudaFree(s->d_depth);
+  cudaFree(s->d_normal);
+  delete s;
+}
+
+TSI_API tsi_status tsi_scene_reset(tsi_scene *s) {
+  if (!s) return set_err(TSI_ERR_INVALID_ARGUMENT, "null scene");
+  CK(cudaSetDevice(s->ctx->device));
+  return reset_scene(s);
+}
+
+TSI_API tsi_status tsi_scene_invert(tsi_scene *s, float time, float t0_or_nan, tsi_stats *stats) {
+  if (!s) return set_err(TSI_ERR_INVALID_ARGUMENT, "null scene");
+  tsi_ctx *c = s->ctx;
+  CK(cudaSetDevice(c->device));
+  CK(cudaEventRecord(c->ev0, c->stream));
+  tsi_status st = enqueue_invert(c, &s, &time, &t0_or_nan, 1);
+  if (st != TSI_OK) return st;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  st = enqueue_readback(c);
+  if (st != TSI_OK) return st;
+  CK(cudaStreamSynchronize(c->stream));
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  if (stats) {
+    SceneCounters ctr;
+    st = read_counters(s, ctr);
+    if (st != TSI_OK) return st;
+    fill_stats(*c->h_rb, stats, (uint64_t)ctr.live_bricks * 8u);
+    stats->device_ms = ms;
+  }
+  return status_from_error_bits(c->h_rb->error);
+}
+
+TSI_API tsi_status tsi_scene_trace(tsi_scene *s, const tsi_uniforms *u, tsi_image *out, tsi_stats *stats) {
+  if (!s || !u) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  tsi_ctx *c = s->ctx;
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemsetAsync(c->d_visits, 0, sizeof(unsigned long long), c->stream));
+  CK(cudaEventRecord(c->ev0, c->stream));
+  tsi_status st = enqueue_trace(s, u);
+  if (st != TSI_OK) return st;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  st = copy_image_out(s, out);
+  if (st != TSI_OK) return st;
+  CK(cudaMemcpyAsync(&c->h_rb->visits, c->d_visits, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (stats) {
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    memset(stats, 0, sizeof(*stats));
+    stats->device_ms = ms;
+    stats->reserved = (float)c->h_rb->visits;
+  }
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_scene_image_device(tsi_scene *s, tsi_image_device *out) {
+  if (!s || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  out->width = s->img_w;
+  out->height = s->img_h;
+  out->rgba = (const float *)s->d_rgba;
+  out->depth = s->d_depth;
+  out->normal = s->d_normal;
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_scene_readback_cells(tsi_scene *s, tsi_cell *out, uint64_t cap, uint64_t *n) {
+  if (!s || !n) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  tsi_ctx *c = s->ctx;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  SceneCounters ctr;
+  tsi_status st = read_counters(s, ctr);
+  if (st != TSI_OK) return st;
+  const size_t nv = (size_t)std::min(ctr.bump, s->cap_bricks) * 8;
+  std::vector<float4> xy(nv), nrm(nv);
+  std::vector<float2> z(nv);
+  std::vector<float> t(nv), te(nv), f(nv), fast(nv);
+  std::vector<uint32_t> child(nv);
+  CK(cudaMemcpy(xy.data(), s->pool.box_xy, nv * sizeof(float4), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(z.data(), s->pool.box_z, nv * sizeof(float2), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(t.data(), s->pool.t, nv * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(te.data(), s->pool.time_err, nv * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(f.data(), s->pool.f, nv * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(fast.data(), s->pool.fast, nv * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(child.data(), s->pool.child, nv * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(nrm.data(), s->pool.normal, nv * sizeof(float4), cudaMemcpyDeviceToHost));
+  struct E {
+    uint32_t v, level, ix, iy, iz;
+  };
+  std::vector<E> stack{{0, 0, 0, 0, 0}};
+  uint64_t cnt = 0;
+  while (!stack.empty()) {
+    const E e = stack.back();
+    stack.pop_back();
+    if (e.v >= nv) return set_err(TSI_ERR_INVALID_ARGUMENT, "corrupt octree (child index out of range)");
+    if (out && cnt < cap) {
+      tsi_cell &o = out[cnt];
+      o.level = e.level;
+      o.ix = e.ix;
+      o.iy = e.iy;
+      o.iz = e.iz;
+      o.f = f[e.v];
+      o.t = t[e.v];
+      o.time_err = te[e.v];
+      o.fast = fast[e.v];
+      o.dx = nrm[e.v].x;
+      o.dy = nrm[e.v].y;
+      o.dz = nrm[e.v].z;
+      o.has_children = child[e.v] != TSI_NONE;
+      o.x[0] = xy[e.v].x;
+      o.x[1] = xy[e.v].y;
+      o.y[0] = xy[e.v].z;
+      o.y[1] = xy[e.v].w;
+      o.z[0] = z[e.v].x;
+      o.z[1] = z[e.v].y;
+    }
+    ++cnt;
+    if (child[e.v] != TSI_NONE) {
+      if (e.level >= 32) return set_err(TSI_ERR_INVALID_ARGUMENT, "corrupt octree (too deep)");
+      for (int k = 7; k >= 0; --k)
+        stack.push_back(E{child[e.v] + (uint32_t)k, e.level + 1, 2 * e.ix + (k & 1), 2 * e.iy + ((k >> 1) & 1),
+                          2 * e.iz + (k >> 2)});
+    }
+  }
+  *n = cnt;
+  return (out && cap < cnt) ? TSI_ERR_BUFFER_TOO_SMALL : TSI_OK;
+}
+
+TSI_API tsi_status tsi_scene_get_params(const tsi_scene *s, tsi_params *out) {
+  if (!s || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  *out = s->p;
+  return TSI_OK;
+}
+
+TSI_API uint64_t tsi_scene_device_bytes(const tsi_scene *s) { return s ? s->bytes : 0; }
+
+static tsi_status batch_enqueue(tsi_ctx *c, tsi_request *reqs, uint32_t n) {
+  std::vector<tsi_scene *> sc(n);
+  std::vector<float> times(n), t0s(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!reqs[i].scene || reqs[i].scene->ctx != c) return set_err(TSI_ERR_INVALID_ARGUMENT, "bad request scene");
+    for (uint32_t j = 0; j < i; ++j)
+      if (reqs[j].scene == reqs[i].scene) return set_err(TSI_ERR_INVALID_ARGUMENT, "scenes in a batch must differ");
+    sc[i] = reqs[i].scene;
+    times[i] = reqs[i].time;
+    t0s[i] = reqs[i].t0_or_nan;
+  }
+  for (uint32_t i0 = 0; i0 < n; i0 += c->max_scenes) {
+    const uint32_t m = std::min(c->max_scenes, n - i0);
+    tsi_status st = enqueue_invert(c, sc.data() + i0, times.data() + i0, t0s.data() + i0, m);
+    if (st != TSI_OK) return st;
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!reqs[i].uniforms) continue;
+    tsi_status st = enqueue_trace(reqs[i].scene, reqs[i].uniforms);
+    if (st != TSI_OK) return st;
+  }
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_batch_run(tsi_ctx *c, tsi_request *reqs, uint32_t n) {
+  if (!c || (!reqs && n)) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  CK(cudaSetDevice(c->device));
+  CK(cudaEventRecord(c->ev0, c->stream));
+  tsi_status st = batch_enqueue(c, reqs, n);
+  if (st != TSI_OK) return st;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  for (uint32_t i = 0; i < n; ++i) {
+    if (reqs[i].uniforms && reqs[i].out) {
+      st = copy_image_out(reqs[i].scene, reqs[i].out);
+      if (st != TSI_OK) return st;
+    }
+  }
+  st = enqueue_readback(c);
+  if (st != TSI_OK) return st;
+  CK(cudaStreamSynchronize(c->stream));
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  for (uint32_t i = 0; i < n; ++i) {
+    if (reqs[i].stats) {
+      fill_stats(*c->h_rb, reqs[i].stats, 0);
+      reqs[i].stats->device_ms = ms;
+    }
+  }
+  return status_from_error_bits(c->h_rb->error);
+}
+
+TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *c, tsi_request *reqs, uint32_t n, tsi_batch_graph **out) {
+  if (!c || !reqs || !out || n == 0) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  if (n > c->max_scenes) return set_err(TSI_ERR_INVALID_ARGUMENT, "graph batch wider than one launch");
+  CK(cudaSetDevice(c->device));
+  tsi_batch_graph *g = new tsi_batch_graph();
+  g->ctx = c;
+  g->reqs.assign(reqs, reqs + n);
+  CK(cudaStreamSynchronize(c->stream));
+  // grow the shared-memory attribute and the frame buffers before capture
+  for (uint32_t i = 0; i < n; ++i)
+    if (reqs[i].uniforms) {
+      tsi_status st = ensure_image(reqs[i].scene, reqs[i].uniforms->resolution[0], reqs[i].uniforms->resolution[1]);
+      if (st != TSI_OK) {
+        delete g;
+        return st;
+      }
+    }
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  tsi_status st = batch_enqueue(c, g->reqs.data(), n);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+  if (st != TSI_OK || e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    delete g;
+    if (st != TSI_OK) return st;
+    return set_err(TSI_ERR_CUDA, cudaGetErrorString(e));
+  }
+  g->graph = graph;
+  e = cudaGraphInstantiate(&g->exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    delete g;
+    return set_err(TSI_ERR_CUDA, cudaGetErrorString(e));
+  }
+  *out = g;
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g) {
+  if (!g) return set_err(TSI_ERR_INVALID_ARGUMENT, "null graph");
+  tsi_ctx *c = g->ctx;
+  CK(cudaSetDevice(c->device));
+  // the captured uploads read the pinned launch descriptors: refresh times
+  const uint32_t n = (uint32_t)g->reqs.size();
+  for (uint32_t i = 0; i < n; ++i) {
+    const tsi_request &r = g->reqs[i];
+    fill_launch(r.scene, i, r.time, r.t0_or_nan, c->h_scenes[i], c->h_recs[i]);
+  }
+  CK(cudaGraphLaunch(g->exec, c->stream));
+  return TSI_OK;
+}
+
+TSI_API void tsi_batch_graph_destroy(tsi_batch_graph *g) {
+  if (!g) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+}
+
+}  // extern "C"

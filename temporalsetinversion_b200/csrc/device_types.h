@@ -1,0 +1,127 @@
+// device_types.h — HBM data layout shared by the host runtime and kernels.
+//
+// The reference stores each voxel as one 88-byte struct (compute.wgsl:
+// 3003-3016) allocated one at a time from a free-list queue (3437-3460), and
+// gives every thread a private 128 KB copy of the tape (3562).  Here:
+//  - voxels live in structure-of-arrays form, allocated in bricks of 8
+//    siblings, so a parent stores one child index (the first voxel of its
+//    brick) instead of children[8];
+//  - tapes are shared, read-only, 8 bytes per instruction (tape_format.h);
+//    per-sibling-group pruned tapes are appended to a per-frame arena and
+//    chained to the tape they were derived from.
+#pragma once
+#include <stdint.h>
+#include <vector_types.h>
+
+#include "tape_format.h"
+
+#define TSI_MAX_LEVELS 24
+#define TSI_PRUNE_MAX_REGS 64u  // pruning tracks liveness in one 64-bit mask
+#define TSI_PRUNE_MIN_LEN 8u    // shorter tapes are not worth pruning
+
+enum tsi_scene_flags {
+  SF_POINTSAMPLE = 1u << 0,
+  SF_FASTENABLED = 1u << 1,
+  SF_LIPSCHITZ = 1u << 2,
+  SF_SWEPT = 1u << 3,
+  SF_ALWAYS_DERIV = 1u << 4,  // !fast_normals && normal_viz (compute.wgsl:3780)
+  SF_PRUNING = 1u << 5,
+  SF_DIRECTED = 1u << 6,  // outward rounding (tsi_rounding TSI_ROUND_DIRECTED)
+};
+
+enum tsi_error_bits {
+  EB_OOM = 1u << 0,
+  EB_QUEUE_FULL = 1u << 1,
+  EB_WATCHDOG = 1u << 2,
+  EB_LOG_OOM = 1u << 3,
+};
+
+struct VoxelPoolDev {
+  float4 *box_xy;    // x.lo, x.hi, y.lo, y.hi
+  float2 *box_z;     // z.lo, z.hi
+  float *t;          // time of last evaluation
+  float *time_err;
+  float *f;          // -1 full, 0 ambiguous, +1 empty
+  float *fast;
+  uint32_t *child;   // first voxel of the child brick, TSI_NONE = no children
+  float4 *normal;    // dx, dy, dz, 0
+  uint32_t *free_list;  // brick ids free since earlier frames
+  uint32_t *pending;    // brick ids freed during the current frame
+  uint32_t cap_bricks;
+  uint32_t pad;
+};
+
+struct SceneCounters {
+  int32_t free_count;      // may dip below 0 while popping; fixed at frame end
+  uint32_t bump;           // next never-used brick (brick 0 holds the root)
+  uint32_t pending_count;
+  uint32_t live_bricks;
+};
+
+struct SceneLaunch {
+  VoxelPoolDev pool;
+  SceneCounters *ctr;
+  float eps;          // 10 * 2^-localsubdiv
+  float delta;
+  float fast_thresh;  // delta * fast_multiplier
+  float time;
+  float t0;           // start of the swept interval
+  uint32_t flags;
+  uint32_t root_rec;
+  uint32_t levels;    // localsubdiv
+  uint32_t full_len;  // full tape length (instr_full_equiv counter)
+};
+
+struct TapeRec {
+  const uint2 *code;
+  uint32_t len;
+  uint32_t nregs;
+  uint32_t out_reg;
+  uint32_t n_minmax;
+  float t_lo, t_hi;   // valid for cells inside the group's boxes with time in [t_lo, t_hi]
+  uint32_t parent;    // record it was pruned from (TSI_NONE for a full tape)
+  uint32_t pad;
+};
+
+struct WorkItem {
+  uint32_t scene;
+  uint32_t rec;
+  uint32_t n;         // valid parents (1..4)
+  uint32_t level;     // level of the parents
+  uint32_t parent[4];
+};
+
+enum tsi_stat_index {
+  ST_PARENTS = 0, ST_EVAL, ST_REVERSE, ST_SKIPPED, ST_AMBIG, ST_EMPTY, ST_FULL, ST_ENQUEUED,
+  ST_REUSED, ST_INSTR_FWD, ST_INSTR_REV, ST_INSTR_FULL, ST_FP32, ST_BRICK_ALLOC, ST_BRICK_FREE,
+  ST_TAPE_WORDS, ST_PRUNE_FALLBACK, ST_COUNT
+};
+
+struct LaunchParams {
+  SceneLaunch *scenes;
+  uint32_t n_scenes;
+  uint32_t rec_cap;
+  TapeRec *recs;
+  uint32_t *rec_count;
+  uint2 *code_arena;
+  unsigned long long *code_count;
+  unsigned long long code_cap;
+  WorkItem *items[2];
+  uint32_t *item_count;    // [TSI_MAX_LEVELS + 1]
+  uint32_t *item_cursor;   // [TSI_MAX_LEVELS + 1]
+  uint32_t item_cap;
+  uint32_t dealloc_cap;
+  uint2 *dealloc[2];       // (scene, brick)
+  uint32_t *dealloc_count; // [TSI_MAX_LEVELS + 1]
+  uint32_t *dealloc_cursor;
+  // per-warp scratch: operand log [slice_len][32] float4, then decisions [slice_len] uint2
+  float4 *log_slices;
+  uint2 *dec_slices;
+  uint32_t slice_len;
+  uint32_t pad0;
+  float4 *log_overflow;
+  unsigned long long *log_overflow_used;  // in float4 units
+  unsigned long long log_overflow_cap;
+  uint32_t *error;
+  unsigned long long *stats;  // [ST_COUNT]
+};

@@ -1,0 +1,662 @@
+// refine.cu — octree refinement step kernel (compute.wgsl `main`, 3513-4056).
+//
+// One launch per octree level, over every scene of the launch.  A warp takes
+// one work item: up to four sibling parents (children of one grandparent,
+// sharing one tape record) x 8 octants, one child cell per lane.  The tape is
+// warp-uniform, so instruction fetch is a broadcast and the handler switch
+// never diverges.  Interval registers live in shared memory as
+// regs[register][lane] (one column per lane, conflict free).
+//
+// Per child cell the lane runs, as in the reference:
+//   cell setup and temporal interval         compute.wgsl:3582-3626
+//   forward interval tape                    3632-3774
+//   reverse interval AD (operand log replay) 3776-3970
+//   temporal error bound, fast flag          3971-4009
+//   classify, re-enqueue or deallocate       4011-4045
+// then, per sibling group that re-enqueues cells, prunes the tape: min/max
+// instructions whose branch is decided for every enqueued sibling become
+// copies (or constants), instructions that no longer reach the output are
+// dropped.  Pruning never changes a result: a decided MIN/MAX returns its
+// chosen operand bit for bit, and the reverse pass falls back to the full
+// tape when a sensitivity overflows (the only case where the dead branch of
+// the full tape would contribute, through 0 * inf).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_types.h"
+#include "interval.cuh"
+#include "opcost.h"
+
+namespace tsi {
+
+#define FULL_MASK 0xffffffffu
+
+__constant__ uint32_t c_cost_fwd[H_COUNT] = TSI_OPCOST_FWD_INIT;
+__constant__ uint32_t c_cost_rr[H_COUNT] = TSI_OPCOST_RR_INIT;
+
+struct WarpStats {
+  unsigned long long v[ST_COUNT];
+};
+
+__device__ __forceinline__ bool finite2(Iv a) { return isfinite(a.lo) && isfinite(a.hi); }
+
+__device__ __forceinline__ Iv ld_reg(const float2 *rf, uint32_t r, uint32_t lane) {
+  float2 v = rf[r * 32u + lane];
+  return Iv{v.x, v.y};
+}
+__device__ __forceinline__ void st_reg(float2 *rf, uint32_t r, uint32_t lane, Iv v) {
+  rf[r * 32u + lane] = make_float2(v.lo, v.hi);
+}
+
+// mallocV (compute.wgsl:3437-3450) for a whole brick of 8 siblings.
+__device__ uint32_t alloc_brick(const SceneLaunch &S, uint32_t *error, unsigned long long &nalloc) {
+  SceneCounters *c = S.ctr;
+  int32_t fc = atomicSub(&c->free_count, 1);
+  uint32_t b;
+  if (fc > 0) {
+    b = S.pool.free_list[fc - 1];
+  } else {
+    b = atomicAdd(&c->bump, 1u);
+    if (b >= S.pool.cap_bricks) {
+      atomicOr(error, EB_OOM);
+      return TSI_NONE;
+    }
+  }
+  nalloc++;
+  return b * 8u;
+}
+
+template <bool D>
+__device__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t level, float2 *rf,
+                             float4 *slice_log, uint2 *slice_dec, WarpStats &ws) {
+  using A = IA<D>;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t g = lane >> 3, k = lane & 7u;
+  const SceneLaunch &S = P.scenes[it.scene];
+  const VoxelPoolDev &pool = S.pool;
+  const uint32_t flags = S.flags;
+  const bool swept = (flags & SF_SWEPT) != 0;
+
+  bool active = g < it.n;
+  const uint32_t Pv = it.parent[active ? g : 0];
+  const float4 pxy = pool.box_xy[Pv];
+  const float2 pz = pool.box_z[Pv];
+  const uint32_t pchild = pool.child[Pv];
+  const float pfast = pool.fast[Pv];
+  const bool new_voxel = (pchild == TSI_NONE);
+
+  // ---- allocate or reuse the 8 children (3564-3580)
+  uint32_t base = pchild;
+  if (active && new_voxel && k == 0) base = alloc_brick(S, P.error, ws.v[ST_BRICK_ALLOC]);
+  base = __shfl_sync(FULL_MASK, base, lane & ~7u);
+  if (base == TSI_NONE) active = false;
+  const uint32_t C = active ? base + k : 0u;
+  float c_t = 0.0f, c_f = 1.0f, c_te = 0.0f, c_fast = 0.0f;
+  uint32_t c_child = TSI_NONE;
+  if (active) {
+    if (new_voxel) {
+      pool.child[C] = TSI_NONE;
+      pool.normal[C] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (k == 0) pool.child[Pv] = base;
+    } else {
+      c_t = pool.t[C];
+      c_f = pool.f[C];
+      c_te = pool.time_err[C];
+      c_fast = pool.fast[C];
+      c_child = pool.child[C];
+    }
+  }
+
+  // ---- cell setup (3582-3626)
+  const float dx = __fdiv_rn(__fsub_rn(pxy.y, pxy.x), 2.0f);
+  const float dy = __fdiv_rn(__fsub_rn(pxy.w, pxy.z), 2.0f);
+  const float dz = __fdiv_rn(__fsub_rn(pz.y, pz.x), 2.0f);
+  float width = fm_max(dx, fm_max(dy, dz));
+  const float kx = (float)(k & 1u), ky = (float)((k >> 1) & 1u), kz = (float)(k >> 2);
+  Iv cx = Iv{__fadd_rn(pxy.x, __fmul_rn(dx, kx)), __fadd_rn(pxy.x, __fmul_rn(dx, 1.0f + kx))};
+  Iv cy = Iv{__fadd_rn(pxy.z, __fmul_rn(dy, ky)), __fadd_rn(pxy.z, __fmul_rn(dy, 1.0f + ky))};
+  Iv cz = Iv{__fadd_rn(pz.x, __fmul_rn(dz, kz)), __fadd_rn(pz.x, __fmul_rn(dz, 1.0f + kz))};
+  const bool point_branch = new_voxel || pfast == 1.0f || width <= S.eps;
+  Iv cur_t;
+  if (point_branch) {
+    cur_t = swept ? Iv{S.t0, S.time} : iv(S.time);
+    c_fast = 0.0f;
+  } else {
+    cur_t = Iv{c_t, S.time};
+  }
+  if (active) {
+    pool.box_xy[C] = make_float4(cx.lo, cx.hi, cy.lo, cy.hi);
+    pool.box_z[C] = make_float2(cz.lo, cz.hi);
+    pool.t[C] = S.time;
+  }
+  if ((flags & SF_POINTSAMPLE) && width <= S.eps) {
+    cx = iv(__fdiv_rn(__fadd_rn(cx.lo, cx.hi), 2.0f));
+    cy = iv(__fdiv_rn(__fadd_rn(cy.lo, cy.hi), 2.0f));
+    cz = iv(__fdiv_rn(__fadd_rn(cz.lo, cz.hi), 2.0f));
+    width = 0.0f;
+  }
+  const Iv targ = Iv{fm_min(cur_t.lo, cur_t.hi), fm_max(cur_t.lo, cur_t.hi)};
+  const bool evaluate = active && (new_voxel || c_f >= 0.0f || c_child == TSI_NONE);
+  const bool take_deriv = evaluate && ((cur_t.lo != cur_t.hi) || (flags & SF_ALWAYS_DERIV));
+
+  Iv field = iv(0.0f);
+  Iv sens[4] = {iv(0.0f), iv(0.0f), iv(0.0f), iv(0.0f)};
+  uint32_t rec = it.rec;
+  TapeRec TR;
+  const bool any_eval = __any_sync(FULL_MASK, evaluate);
+  const bool any_deriv = __any_sync(FULL_MASK, take_deriv);
+  bool want_prune = false;
+  float4 *lg = nullptr;
+  uint2 *dg = nullptr;
+
+  if (any_eval) {
+    // ---- choose the most pruned tape valid for every evaluated cell
+    float tl = evaluate ? targ.lo : fm_inf();
+    float th = evaluate ? targ.hi : -fm_inf();
+    for (int o = 16; o > 0; o >>= 1) {
+      tl = fminf(tl, __shfl_xor_sync(FULL_MASK, tl, o));
+      th = fmaxf(th, __shfl_xor_sync(FULL_MASK, th, o));
+    }
+    TR = P.recs[rec];
+    while (TR.parent != TSI_NONE && !(TR.t_lo <= tl && th <= TR.t_hi)) {
+      rec = TR.parent;
+      TR = P.recs[rec];
+    }
+    const uint32_t root_rec = S.root_rec;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      const uint32_t len = TR.len;
+      want_prune = (flags & SF_PRUNING) && len >= TSI_PRUNE_MIN_LEN && TR.nregs <= TSI_PRUNE_MAX_REGS;
+      lg = nullptr;
+      dg = nullptr;
+      if (any_deriv || want_prune) {
+        if (len <= P.slice_len) {
+          lg = slice_log;
+          dg = slice_dec;
+        } else {
+          unsigned long long need = (unsigned long long)len * 32ull + ((unsigned long long)len + 1ull) / 2ull;
+          unsigned long long off = 0;
+          if (lane == 0) off = atomicAdd(P.log_overflow_used, need);
+          off = __shfl_sync(FULL_MASK, off, 0);
+          if (off + need > P.log_overflow_cap) {
+            if (lane == 0) atomicOr(P.error, EB_LOG_OOM);
+            return;
+          }
+          lg = P.log_overflow + off;
+          dg = reinterpret_cast<uint2 *>(P.log_overflow + off + (unsigned long long)len * 32ull);
+        }
+      }
+      // ---- forward pass (3633-3772)
+      st_reg(rf, 0, lane, cx);
+      st_reg(rf, 1, lane, cy);
+      st_reg(rf, 2, lane, cz);
+      st_reg(rf, 3, lane, targ);
+      const uint2 *code = TR.code;
+      uint32_t mm = 0;
+      uint32_t cost = 0;
+      for (uint32_t i = 0; i < len; ++i) {
+        const uint2 w = code[i];
+        const uint32_t h = TSI_W0_H(w.x);
+        const float lit = __uint_as_float(w.y);
+        const Iv Av = ld_reg(rf, TSI_W0_A(w.x), lane);
+        const Iv Bv = TSI_H_IS_II(h) ? ld_reg(rf, w.y & 255u, lane) : iv(lit);
+        const Iv r = A::forward(h, Av, Bv, lit);
+        if (any_deriv) lg[(size_t)i * 32u + lane] = make_float4(Av.lo, Av.hi, Bv.lo, Bv.hi);
+        if (want_prune && TSI_H_IS_MINMAX(h)) {
+          const bool amax = (h == H_MAX_II || h == H_MAX_IF);
+          const bool a_below = Av.hi < Bv.lo, b_below = Bv.hi < Av.lo;
+          const uint32_t ua = __ballot_sync(FULL_MASK, amax ? b_below : a_below);
+          const uint32_t ub = __ballot_sync(FULL_MASK, amax ? a_below : b_below);
+          if (lane == 0) dg[mm] = make_uint2(ua, ub);
+          ++mm;
+        }
+        st_reg(rf, TSI_W0_DST(w.x), lane, r);
+        cost += c_cost_fwd[h];
+      }
+      field = ld_reg(rf, TR.out_reg, lane);
+      {
+        const uint32_t ne = __popc(__ballot_sync(FULL_MASK, evaluate));
+        if (lane == 0) ws.v[ST_FP32] += (unsigned long long)(cost + TSI_FIX_COST * len) * ne;
+      }
+      // ---- reverse pass (3785-3964), sensitivities reuse the register file
+      bool bad = false;
+      if (any_deriv) {
+        for (uint32_t r = 0; r < TR.nregs; ++r) st_reg(rf, r, lane, iv(0.0f));
+        st_reg(rf, TR.out_reg, lane, iv(1.0f));
+        uint32_t rcost = 0;
+        for (int i = (int)len - 1; i >= 0; --i) {
+          const uint2 w = code[i];
+          const uint32_t h = TSI_W0_H(w.x);
+          const uint32_t d = TSI_W0_DST(w.x), a = TSI_W0_A(w.x), b = w.y & 255u;
+          const float lit = __uint_as_float(w.y);
+          const float4 L = lg[(size_t)i * 32u + lane];
+          const Iv Av = Iv{L.x, L.y}, Bv = Iv{L.z, L.w};
+          const Iv s = ld_reg(rf, d, lane);
+          st_reg(rf, d, lane, iv(0.0f));
+          rcost += c_cost_rr[h] + TSI_REV_OPERAND_COST * TSI_H_NREG(h);
+          if (!take_deriv || h == H_CONST) {
+            bad |= take_deriv && !finite2(s);
+            continue;
+          }
+          bad |= !finite2(s);
+          const bool s0 = (s.lo == 0.0f && s.hi == 0.0f);
+          if (TSI_H_IS_II(h)) {
+            if (s0 && TSI_W0_FA(w.x) && TSI_W0_FB(w.x)) {
+              st_reg(rf, a, lane, iv(0.0f));
+              st_reg(rf, b, lane, iv(0.0f));
+            } else {
+              Iv r0, r1;
+              A::reverse_rule(h, Av, Bv, lit, r0, r1);
+              r0 = A::fix(r0);
+              r1 = A::fix(r1);
+              r0 = A::mul(r0, s);
+              r1 = A::mul(r1, s);
+              const Iv n0 = A::add(r0, ld_reg(rf, a, lane));
+              const Iv n1 = A::add(r1, ld_reg(rf, b, lane));
+              st_reg(rf, a, lane, n0);
+              st_reg(rf, b, lane, n1);
+              bad |= !finite2(n0) || !finite2(n1);
+            }
+          } else {
+            if (s0 && TSI_W0_FA(w.x)) {
+              st_reg(rf, a, lane, iv(0.0f));
+            } else {
+              Iv r0, r1;
+              A::reverse_rule(h, Av, Bv, lit, r0, r1);
+              r0 = A::fix(r0);
+              r0 = A::mul(r0, s);
+              const Iv n0 = A::add(r0, ld_reg(rf, a, lane));
+              st_reg(rf, a, lane, n0);
+              bad |= !finite2(n0);
+            }
+          }
+        }
+        for (int q = 0; q < 4; ++q) sens[q] = ld_reg(rf, q, lane);
+        const uint32_t nrev = __popc(__ballot_sync(FULL_MASK, take_deriv));
+        if (lane == 0) ws.v[ST_FP32] += (unsigned long long)rcost * nrev;
+      }
+      // a pruned tape whose sensitivities overflowed: redo on the full tape
+      const bool redo = __any_sync(FULL_MASK, bad) && TR.parent != TSI_NONE;
+      if (!redo) break;
+      rec = root_rec;
+      TR = P.recs[rec];
+      if (lane == 0) ws.v[ST_PRUNE_FALLBACK]++;
+    }
+    {
+      const uint32_t ne = __popc(__ballot_sync(FULL_MASK, evaluate));
+      const uint32_t nr = __popc(__ballot_sync(FULL_MASK, take_deriv));
+      if (lane == 0) {
+        ws.v[ST_INSTR_FWD] += (unsigned long long)TR.len * ne;
+        ws.v[ST_INSTR_REV] += (unsigned long long)TR.len * nr;
+        ws.v[ST_INSTR_FULL] += (unsigned long long)S.full_len * ne;
+      }
+    }
+  }
+
+  // ---- temporal error bound (3966-3997)
+  Iv df = iv(0.0f), df_dt = iv(0.0f);
+  const float delta = S.delta;
+  if (take_deriv) {
+    const float nx = __fdiv_rn(__fadd_rn(sens[0].lo, sens[0].hi), 2.0f);
+    const float ny = __fdiv_rn(__fadd_rn(sens[1].lo, sens[1].hi), 2.0f);
+    const float nz = __fdiv_rn(__fadd_rn(sens[2].lo, sens[2].hi), 2.0f);
+    pool.normal[C] = make_float4(nx, ny, nz, 0.0f);
+    df_dt = sens[3];
+    const float dt = __fsub_rn(targ.hi, targ.lo);
+    df = A::mul_f(df_dt, dt);
+    const Iv W = A::mul_f(Iv{-1.0f, 1.0f}, __fsub_rn(field.hi, field.lo));
+    df = A::cap(df, W);
+    if ((flags & SF_LIPSCHITZ) && A::abs_(df).hi != 0.0f) {
+      const float lb =
+          A::abs_(A::sqrt_(A::add(A::sqr(sens[0]), A::add(A::sqr(sens[1]), A::sqr(sens[2]))))).lo;
+      if (!is_nan_f(lb)) df = A::div(df, iv(lb));
+    }
+    if (df.lo == -fm_inf() || df.hi == fm_inf() || is_nan_f(df.lo) || is_nan_f(df.hi)) df = iv(delta);
+    c_te = __fadd_rn(c_te, fm_min(fm_max(A::abs_(df).hi, 0.0f), delta));
+  }
+  // ---- fast flag (4003-4009)
+  if (evaluate && !swept && (flags & SF_FASTENABLED)) c_fast = (A::abs_(df).hi >= S.fast_thresh) ? 1.0f : 0.0f;
+
+  // ---- classification (4011-4045)
+  bool enq = false, dealloc = false, reused = false;
+  int cls = 3;
+  uint32_t dealloc_brick = 0;
+  if (evaluate) {
+    if (field.lo <= 0.0f && 0.0f <= field.hi) {
+      c_f = 0.0f;
+      cls = 0;
+      if (width > S.eps) {
+        if (new_voxel || is_nan_f(df_dt.lo) || is_nan_f(df_dt.hi) || fabsf(df_dt.lo) == fm_inf() ||
+            fabsf(df_dt.hi) == fm_inf() || pfast == 1.0f || cur_t.lo == cur_t.hi || c_te >= delta ||
+            c_child == TSI_NONE) {
+          c_te = 0.0f;
+          enq = true;
+        } else {
+          reused = true;
+        }
+      }
+    } else {
+      if (field.hi <= 0.0f) {
+        c_f = -1.0f;
+        cls = 2;
+      } else {
+        cls = 1;
+        if (!swept) c_f = 1.0f;
+      }
+      if (!swept && c_child != TSI_NONE) {
+        dealloc = true;
+        dealloc_brick = c_child >> 3;
+        c_child = TSI_NONE;
+      }
+    }
+  }
+  if (active) {
+    pool.f[C] = c_f;
+    pool.time_err[C] = c_te;
+    pool.fast[C] = c_fast;
+    if (dealloc || new_voxel) pool.child[C] = c_child;
+  }
+
+  // ---- deallocation of dropped subtrees (4036-4044)
+  {
+    const uint32_t m = __ballot_sync(FULL_MASK, dealloc);
+    if (m) {
+      uint32_t basei = 0;
+      if (lane == 0) basei = atomicAdd(&P.dealloc_count[level + 1], (uint32_t)__popc(m));
+      basei = __shfl_sync(FULL_MASK, basei, 0);
+      if (dealloc) {
+        const uint32_t pos = basei + __popc(m & ((1u << lane) - 1u));
+        if (pos < P.dealloc_cap) P.dealloc[(level + 1) & 1][pos] = make_uint2(it.scene, dealloc_brick);
+        else atomicOr(P.error, EB_QUEUE_FULL);
+      }
+    }
+  }
+
+  // ---- re-enqueue: one sibling group per parent, pruned tape per group
+  const uint32_t em = __ballot_sync(FULL_MASK, enq);
+  const uint32_t E = (em >> (g * 8u)) & 0xffu;
+  uint32_t new_rec = rec;
+  if (em) {
+    // validity of the group's pruned tape: intersection of the enqueued
+    // siblings' time intervals
+    float gl = enq ? targ.lo : -fm_inf();
+    float gh = enq ? targ.hi : fm_inf();
+    for (int o = 1; o < 8; o <<= 1) {
+      gl = fmaxf(gl, __shfl_xor_sync(FULL_MASK, gl, o));
+      gh = fminf(gh, __shfl_xor_sync(FULL_MASK, gh, o));
+    }
+    uint32_t cnt = 0, mmk = 0;
+    bool pruned = false;
+    uint2 *tmp = nullptr;
+    if (want_prune && lg != nullptr) tmp = reinterpret_cast<uint2 *>(lg) + (size_t)g * TR.len;
+    if (k == 0 && E != 0 && want_prune && tmp != nullptr) {
+      const uint2 *code = TR.code;
+      unsigned long long live = 1ull << TR.out_reg;
+      uint32_t m = TR.n_minmax;
+      for (int i = (int)TR.len - 1; i >= 0; --i) {
+        const uint2 w = code[i];
+        const uint32_t h = TSI_W0_H(w.x);
+        const uint32_t d = TSI_W0_DST(w.x), a = TSI_W0_A(w.x), b = w.y & 255u;
+        const bool mmx = TSI_H_IS_MINMAX(h);
+        uint2 dd = make_uint2(0u, 0u);
+        if (mmx) dd = dg[--m];
+        if (!((live >> d) & 1ull)) continue;
+        live &= ~(1ull << d);
+        uint2 out = w;
+        if (mmx) {
+          const uint32_t ga = (dd.x >> (g * 8u)) & 0xffu, gb = (dd.y >> (g * 8u)) & 0xffu;
+          if ((ga & E) == E) {
+            out = make_uint2(TSI_W0(H_COPY, TSI_W0_FA(w.x), 0u, d, a), 0u);
+            live |= 1ull << a;
+          } else if ((gb & E) == E) {
+            if (TSI_H_IS_II(h)) {
+              out = make_uint2(TSI_W0(H_COPY, TSI_W0_FB(w.x), 0u, d, b), 0u);
+              live |= 1ull << b;
+            } else {
+              out = make_uint2(TSI_W0(H_CONST, 0u, 0u, d, 0u), w.y);
+            }
+          } else {
+            live |= 1ull << a;
+            if (TSI_H_IS_II(h)) live |= 1ull << b;
+            ++mmk;
+          }
+        } else {
+          if (h != H_CONST) live |= 1ull << a;
+          if (TSI_H_IS_II(h)) live |= 1ull << b;
+        }
+        tmp[cnt++] = out;
+      }
+      pruned = cnt < TR.len;
+    }
+    // reserve arena space and a record (lane 8g), then copy with the group
+    unsigned long long off = 0;
+    uint32_t ri = TSI_NONE;
+    if (k == 0 && pruned) {
+      off = atomicAdd(P.code_count, (unsigned long long)cnt);
+      if (off + cnt <= P.code_cap) {
+        ri = atomicAdd(P.rec_count, 1u);
+        if (ri >= P.rec_cap) ri = TSI_NONE;
+      }
+    }
+    const uint32_t gl0 = lane & ~7u;
+    cnt = __shfl_sync(FULL_MASK, cnt, gl0);
+    off = __shfl_sync(FULL_MASK, off, gl0);
+    ri = __shfl_sync(FULL_MASK, ri, gl0);
+    if (ri != TSI_NONE) {
+      for (uint32_t j = k; j < cnt; j += 8u) P.code_arena[off + j] = tmp[cnt - 1u - j];
+      if (k == 0) {
+        TapeRec nr;
+        nr.code = P.code_arena + off;
+        nr.len = cnt;
+        nr.nregs = TR.nregs;
+        nr.out_reg = TR.out_reg;
+        nr.n_minmax = mmk;
+        nr.t_lo = gl;
+        nr.t_hi = gh;
+        nr.parent = rec;
+        nr.pad = 0;
+        P.recs[ri] = nr;
+        ws.v[ST_TAPE_WORDS] += cnt;
+      }
+      new_rec = ri;
+    }
+    // next-level work items: ceil(n/4) per group
+    uint32_t cb[8];
+#pragma unroll
+    for (int b2 = 0; b2 < 8; ++b2) cb[b2] = __shfl_sync(FULL_MASK, C, gl0 + b2);
+    if (k == 0 && E != 0) {
+      const uint32_t n = __popc(E);
+      const uint32_t nitems = (n + 3u) >> 2;
+      const uint32_t pos = atomicAdd(&P.item_count[level + 1], nitems);
+      if (pos + nitems > P.item_cap) {
+        atomicOr(P.error, EB_QUEUE_FULL);
+      } else {
+        WorkItem *dst = P.items[(level + 1) & 1];
+        uint32_t e = E;
+        for (uint32_t j = 0; j < nitems; ++j) {
+          WorkItem wi;
+          wi.scene = it.scene;
+          wi.rec = new_rec;
+          wi.level = level + 1;
+          uint32_t c = 0;
+          while (e && c < 4u) {
+            const uint32_t bit = __ffs(e) - 1u;
+            e &= e - 1u;
+            wi.parent[c++] = cb[bit];
+          }
+          wi.n = c;
+          for (uint32_t q = c; q < 4u; ++q) wi.parent[q] = wi.parent[0];
+          dst[pos + j] = wi;
+        }
+      }
+    }
+  }
+
+  // ---- counters
+  const uint32_t b_eval = __ballot_sync(FULL_MASK, evaluate);
+  const uint32_t b_rev = __ballot_sync(FULL_MASK, take_deriv);
+  const uint32_t b_skip = __ballot_sync(FULL_MASK, active && !evaluate);
+  const uint32_t b_amb = __ballot_sync(FULL_MASK, cls == 0);
+  const uint32_t b_emp = __ballot_sync(FULL_MASK, cls == 1);
+  const uint32_t b_full = __ballot_sync(FULL_MASK, cls == 2);
+  const uint32_t b_reu = __ballot_sync(FULL_MASK, reused);
+  if (lane == 0) {
+    ws.v[ST_PARENTS] += it.n;
+    ws.v[ST_EVAL] += __popc(b_eval);
+    ws.v[ST_REVERSE] += __popc(b_rev);
+    ws.v[ST_SKIPPED] += __popc(b_skip);
+    ws.v[ST_AMBIG] += __popc(b_amb);
+    ws.v[ST_EMPTY] += __popc(b_emp);
+    ws.v[ST_FULL] += __popc(b_full);
+    ws.v[ST_ENQUEUED] += __popc(em);
+    ws.v[ST_REUSED] += __popc(b_reu);
+  }
+}
+
+// Recursive free of a dropped subtree (compute.wgsl:3533-3543, freeV
+// 3452-3460): 8 lanes per brick; children bricks go to the next level's list.
+__device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level, bool valid, WarpStats &ws) {
+  const uint32_t lane = threadIdx.x & 31u, k = lane & 7u;
+  const SceneLaunch &S = P.scenes[valid ? item.x : 0];
+  const VoxelPoolDev &pool = S.pool;
+  const uint32_t v = item.y * 8u + k;
+  uint32_t ch = TSI_NONE;
+  if (valid) {
+    ch = pool.child[v];
+    pool.child[v] = TSI_NONE;
+    pool.f[v] = 0.0f;
+    pool.t[v] = 0.0f;
+    pool.time_err[v] = 0.0f;
+    pool.fast[v] = 0.0f;
+  }
+  const bool push = valid && ch != TSI_NONE;
+  const uint32_t m = __ballot_sync(FULL_MASK, push);
+  if (m) {
+    uint32_t basei = 0;
+    if (lane == 0) basei = atomicAdd(&P.dealloc_count[level + 1], (uint32_t)__popc(m));
+    basei = __shfl_sync(FULL_MASK, basei, 0);
+    if (push) {
+      const uint32_t pos = basei + __popc(m & ((1u << lane) - 1u));
+      if (pos < P.dealloc_cap) P.dealloc[(level + 1) & 1][pos] = make_uint2(item.x, ch >> 3);
+      else atomicOr(P.error, EB_QUEUE_FULL);
+    }
+  }
+  if (valid && k == 0) {
+    const uint32_t pos = atomicAdd(&S.ctr->pending_count, 1u);
+    if (pos < pool.cap_bricks) pool.pending[pos] = item.y;
+    ws.v[ST_BRICK_FREE]++;
+  }
+}
+
+__global__ void __launch_bounds__(256) refine_kernel(LaunchParams P, uint32_t level, uint32_t rcap) {
+  extern __shared__ float2 smem_regs[];
+  const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
+  float2 *rf = smem_regs + (size_t)wib * rcap * 32u;
+  float4 *slice_log = P.log_slices + (size_t)gw * P.slice_len * 32u;
+  uint2 *slice_dec = P.dec_slices + (size_t)gw * P.slice_len;
+  WarpStats ws;
+#pragma unroll
+  for (int i = 0; i < ST_COUNT; ++i) ws.v[i] = 0;
+
+  const uint32_t n_items = min(P.item_count[level], P.item_cap);
+  const WorkItem *items = P.items[level & 1];
+  while (true) {
+    uint32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(&P.item_cursor[level], 1u);
+    idx = __shfl_sync(FULL_MASK, idx, 0);
+    if (idx >= n_items) break;
+    const WorkItem it = items[idx];
+    if (P.scenes[it.scene].flags & SF_DIRECTED) process_item<true>(P, it, level, rf, slice_log, slice_dec, ws);
+    else process_item<false>(P, it, level, rf, slice_log, slice_dec, ws);
+  }
+  // deallocation items: 4 bricks per warp
+  const uint32_t n_dealloc = min(P.dealloc_count[level], P.dealloc_cap);
+  const uint2 *dl = P.dealloc[level & 1];
+  while (true) {
+    uint32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(&P.dealloc_cursor[level], 4u);
+    idx = __shfl_sync(FULL_MASK, idx, 0);
+    if (idx >= n_dealloc) break;
+    const uint32_t j = idx + (lane >> 3);
+    const bool valid = j < n_dealloc;
+    const uint2 item = valid ? dl[j] : make_uint2(0u, 0u);
+    dealloc_brick(P, item, level, valid, ws);
+  }
+  if (lane == 0) {
+    for (int i = 0; i < ST_COUNT; ++i)
+      if (ws.v[i]) atomicAdd(&P.stats[i], ws.v[i]);
+  }
+}
+
+// Per frame: reset level lists and the tape arena, seed the root of every
+// scene (buf_main's enqueue(0), compute.wgsl:4706).
+__global__ void frame_begin_kernel(LaunchParams P) {
+  const uint32_t t = threadIdx.x;
+  for (uint32_t l = t; l <= TSI_MAX_LEVELS; l += blockDim.x) {
+    P.item_count[l] = 0;
+    P.item_cursor[l] = 0;
+    P.dealloc_count[l] = 0;
+    P.dealloc_cursor[l] = 0;
+  }
+  if (t == 0) {
+    *P.rec_count = P.n_scenes;
+    *P.code_count = 0;
+  }
+  for (uint32_t s = t; s < P.n_scenes; s += blockDim.x) {
+    WorkItem w;
+    w.scene = s;
+    w.rec = P.scenes[s].root_rec;
+    w.n = 1;
+    w.level = 0;
+    w.parent[0] = w.parent[1] = w.parent[2] = w.parent[3] = 0u;
+    P.items[0][s] = w;
+  }
+  __syncthreads();
+  if (t == 0) P.item_count[0] = P.n_scenes;
+}
+
+// Per frame end: bricks freed this frame become allocatable.
+__global__ void frame_end_kernel(LaunchParams P) {
+  const uint32_t s = blockIdx.x;
+  if (s >= P.n_scenes) return;
+  const SceneLaunch &S = P.scenes[s];
+  SceneCounters *c = S.ctr;
+  __shared__ int32_t fc0;
+  __shared__ uint32_t np;
+  if (threadIdx.x == 0) {
+    fc0 = max(c->free_count, 0);
+    np = min(c->pending_count, S.pool.cap_bricks);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < np; i += blockDim.x) S.pool.free_list[fc0 + i] = S.pool.pending[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    c->free_count = fc0 + (int32_t)np;
+    c->pending_count = 0;
+    uint32_t used = min(c->bump, S.pool.cap_bricks);
+    c->live_bricks = used - (uint32_t)(fc0 + (int32_t)np);
+  }
+}
+
+// host-side launch helpers
+cudaError_t launch_refine(const LaunchParams &P, uint32_t level, uint32_t rcap, int grid, int block, size_t smem,
+                          cudaStream_t st) {
+  refine_kernel<<<grid, block, smem, st>>>(P, level, rcap);
+  return cudaGetLastError();
+}
+cudaError_t launch_frame_begin(const LaunchParams &P, cudaStream_t st) {
+  frame_begin_kernel<<<1, 64, 0, st>>>(P);
+  return cudaGetLastError();
+}
+cudaError_t launch_frame_end(const LaunchParams &P, cudaStream_t st) {
+  frame_end_kernel<<<P.n_scenes, 256, 0, st>>>(P);
+  return cudaGetLastError();
+}
+cudaError_t refine_set_smem(size_t bytes) {
+  return cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+cudaError_t refine_occupancy(int block, size_t smem, int *blocks_per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, refine_kernel, block, smem);
+}
+
+}  // namespace tsi

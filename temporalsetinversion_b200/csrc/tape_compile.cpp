@@ -1,0 +1,151 @@
+// tape_compile.cpp — handler selection and register allocation.
+#include "tape_compile.h"
+
+#include <cstring>
+
+#include "opcost.h"
+
+namespace tsi {
+namespace {
+
+uint32_t op_top_of(const IrInstr &in) {  // ir.rs:146-171
+  uint32_t side = 3;
+  if (in.larg.is_reg) side -= 2;
+  if (in.rarg.is_reg) side -= 1;
+  return side;
+}
+
+uint32_t handler_of(uint32_t op, uint32_t top) {
+  switch (top) {
+    case 0:  // compute.wgsl:3710-3749
+      switch (op) {
+        case TSI_OP_ADD: return H_ADD_II;
+        case TSI_OP_SUB: return H_SUB_II;
+        case TSI_OP_DIV: return H_DIV_II;
+        case TSI_OP_MUL: return H_MUL_II;
+        case TSI_OP_MIN: return H_MIN_II;
+        case TSI_OP_MAX: return H_MAX_II;
+        case TSI_OP_POW: return H_POW_II;
+        case TSI_OP_MOD: return H_MOD_II;
+        case TSI_OP_ATAN2: return H_ATAN2_II;
+        default: return H_BAD_II;
+      }
+    case 1:  // compute.wgsl:3643-3709
+      switch (op) {
+        case TSI_OP_SQR: return H_SQR;
+        case TSI_OP_SQRT: return H_SQRT;
+        case TSI_OP_EXP: return H_EXP;
+        case TSI_OP_LOG: return H_LOG;
+        case TSI_OP_NEG: return H_NEG;
+        case TSI_OP_ABS: return H_ABS;
+        case TSI_OP_FLOOR: return H_FLOOR;
+        case TSI_OP_SIN: return H_SIN;
+        case TSI_OP_COS: return H_COS;
+        case TSI_OP_ADD: return H_ADD_IF;
+        case TSI_OP_SUB: return H_SUB_IF;
+        case TSI_OP_DIV: return H_DIV_IF;
+        case TSI_OP_MUL: return H_MUL_IF;
+        case TSI_OP_MIN: return H_MIN_IF;
+        case TSI_OP_MAX: return H_MAX_IF;
+        case TSI_OP_POW: return H_POW_IF;
+        case TSI_OP_RET: return H_COPY;
+        case TSI_OP_MOD: return H_MOD_IF;
+        case TSI_OP_ATAN2: return H_ATAN2_IF;
+        default: return H_BAD_I;
+      }
+    case 2:  // compute.wgsl:3750-3764
+      switch (op) {
+        case TSI_OP_SUB: return H_SUB_FI;
+        case TSI_OP_DIV: return H_DIV_FI;
+        default: return H_BAD_FI;
+      }
+    default:  // compute.wgsl:3765, the value stays I_FROM(0.0)
+      return H_CONST;
+  }
+}
+
+}  // namespace
+
+bool compile_tape(const std::vector<IrInstr> &ins, PackedTape &out, tsi_status &status,
+                  std::string &why) {
+  const uint32_t n = uint32_t(ins.size());
+  if (n < 4) {
+    status = TSI_ERR_INVALID_ARGUMENT;
+    why = "a tape needs the four ARG slots";
+    return false;
+  }
+  out = PackedTape{};
+  out.count = n;
+  // last use of every slot; the field (slot n-1) stays live to the end
+  std::vector<int64_t> last_use(n, -1);
+  for (uint32_t j = 4; j < n; ++j) {
+    const IrInstr &in = ins[j];
+    uint32_t top = op_top_of(in);
+    if (top == 0 || top == 1) last_use[in.larg.reg] = j;
+    if (top == 0 || top == 2) last_use[in.rarg.reg] = j;
+  }
+  last_use[n - 1] = int64_t(n);
+
+  uint8_t used[TSI_MAX_REGS];
+  std::memset(used, 0, sizeof(used));
+  std::vector<uint32_t> reg(n, 0);
+  for (uint32_t a = 0; a < 4; ++a) {
+    reg[a] = a;
+    used[a] = (last_use[a] >= 0) ? 1 : 0;
+  }
+  uint32_t maxreg = 3;
+  static const uint32_t fwd_cost[H_COUNT] = TSI_OPCOST_FWD_INIT;
+  out.code.reserve(size_t(n - 4) * 2);
+  for (uint32_t j = 4; j < n; ++j) {
+    const IrInstr &in = ins[j];
+    const uint32_t top = op_top_of(in);
+    const uint32_t h = handler_of(in.op, top);
+    uint32_t a_slot = 0, b_slot = 0;
+    bool has_a = false, has_b = false;
+    uint32_t w1 = 0;
+    float lit = 0.0f;
+    if (top == 1) lit = in.rarg.lit;
+    else if (top == 2 || top == 3) lit = in.larg.is_reg ? 0.0f : in.larg.lit;
+    if (top == 3) lit = in.rarg.lit;  // ir.rs:160-168 keeps the rarg literal last
+    if (top == 0) {
+      a_slot = in.larg.reg; b_slot = in.rarg.reg; has_a = has_b = true;
+    } else if (top == 1) {
+      a_slot = in.larg.reg; has_a = true;
+    } else if (top == 2) {
+      a_slot = in.rarg.reg; has_a = true;
+    }
+    const uint32_t ra = has_a ? reg[a_slot] : 0;
+    const uint32_t rb = has_b ? reg[b_slot] : 0;
+    const uint32_t fa = has_a ? (((ins[a_slot].uses & 0xFFFFu) == 1u) ? 1u : 0u) : 0u;
+    const uint32_t fb = has_b ? (((ins[b_slot].uses & 0xFFFFu) == 1u) ? 1u : 0u) : 0u;
+    if (top == 0) {
+      w1 = rb;
+    } else {
+      float v = (h == H_CONST) ? 0.0f : lit;  // op_top 3 evaluates to [0,0]
+      std::memcpy(&w1, &v, 4);
+    }
+    // free operands at their last use (before allocating the destination)
+    if (has_a && last_use[a_slot] == int64_t(j)) used[ra] = 0;
+    if (has_b && last_use[b_slot] == int64_t(j)) used[rb] = 0;
+    uint32_t d = 0;
+    while (d < TSI_MAX_REGS && used[d]) ++d;
+    if (d >= TSI_MAX_REGS) {
+      status = TSI_ERR_TAPE_TOO_WIDE;
+      why = "more than 256 interval values live at slot " + std::to_string(j);
+      return false;
+    }
+    reg[j] = d;
+    used[d] = (last_use[j] >= 0) ? 1 : 0;  // a never-read value frees at once
+    if (d > maxreg) maxreg = d;
+    out.code.push_back(TSI_W0(h, fa, fb, d, ra));
+    out.code.push_back(w1);
+    if (TSI_H_IS_MINMAX(h)) out.n_minmax++;
+    out.fwd_cost += fwd_cost[h] + TSI_FIX_COST;
+  }
+  out.nregs = maxreg + 1;
+  out.out_reg = reg[n - 1];
+  out.slot_reg = reg;
+  return true;
+}
+
+}  // namespace tsi

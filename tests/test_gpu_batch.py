@@ -1,0 +1,44 @@
+"""Batched form: many scenes (different tapes, depths, times) in one fused
+launch sequence give exactly what each gives alone."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import assert_cells_equal
+from temporalsetinversion_b200 import Scene, Tape, api, scenes
+
+
+def _make(device, specs):
+    out = []
+    for text, L in specs:
+        tape = Tape.from_llvm_ir(device, text)
+        out.append(Scene(device, tape, api.default_params(localsubdiv=L)))
+    return out
+
+
+SPECS = [(scenes.csg(16, 1), 6), (scenes.spheres16(2), 7), (scenes.csg(40, 3), 5), (scenes.swept(6, 5), 6)]
+
+
+@pytest.mark.gpu
+def test_batch_equals_alone(device):
+    alone = _make(device, SPECS)
+    mixed = _make(device, SPECS)
+    times = [[0.0, 0.1, 0.3], [0.2, 0.25, 0.3], [0.9, 0.5, 0.1], [0.0, 1 / 60, 2 / 60]]
+    cam = scenes.camera_look_at((0.4, 0.8, 2.4))
+    for f in range(3):
+        reqs = []
+        for i, s in enumerate(mixed):
+            u = api.make_uniforms(cam, (96, 64), times[i][f])
+            reqs.append((s, times[i][f], math.nan, u))
+        res = api.run_batch(device, reqs)
+        for i, s in enumerate(alone):
+            st = s.invert(times[i][f])
+            u = api.make_uniforms(cam, (96, 64), times[i][f])
+            img = s.trace(u)
+            assert res[i]["stats"].error_flags == 0
+            assert_cells_equal(mixed[i].cells(), s.cells())
+            assert np.array_equal(res[i]["depth"], img["depth"])
+            assert np.array_equal(res[i]["rgba"], img["rgba"])

@@ -1,0 +1,71 @@
+"""Failure detection without a GPU fault: exhausted pools and work lists come
+back as error statuses from the host API and the device stays usable.  The
+reference silently drops work in both cases (compute.wgsl:3159-3161 `enqueue`
+returns false and its callers ignore it, 3537/4024/4041)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from temporalsetinversion_b200 import Device, Scene, Tape, _native as N, api, scenes
+
+
+@pytest.mark.gpu
+def test_voxel_pool_exhaustion_is_reported(device):
+    tape = Tape.from_llvm_ir(device, scenes.spheres16(0))
+    tiny = Scene(device, tape, api.default_params(localsubdiv=7), voxel_capacity=64)
+    with pytest.raises(N.TsiError) as e:
+        tiny.invert(0.0)
+    assert e.value.status == 4  # TSI_ERR_OOM
+    ok = Scene(device, tape, api.default_params(localsubdiv=5))
+    st = ok.invert(0.0)
+    assert st.cells_evaluated > 0 and st.error_flags == 0
+
+
+@pytest.mark.gpu
+def test_work_list_overflow_is_reported():
+    with Device(work_item_capacity=16) as dev:
+        tape = Tape.from_llvm_ir(dev, scenes.spheres16(0))
+        s = Scene(dev, tape, api.default_params(localsubdiv=6))
+        with pytest.raises(N.TsiError) as e:
+            s.invert(0.0)
+        assert e.value.status == 5  # TSI_ERR_QUEUE_FULL
+        s2 = Scene(dev, tape, api.default_params(localsubdiv=2))
+        assert s2.invert(0.0).cells_evaluated > 0
+
+
+@pytest.mark.gpu
+def test_bad_opcode_and_bad_tapes_rejected(device):
+    tape = api.IR.new(scenes.spheres16(0)).gpu_instructions.copy()
+    bad = tape.copy()
+    bad[10]["opcode_uses"] = (31 | (1 << 14)) << 16 | 1  # opcode 31 does not exist
+    with pytest.raises(N.TsiError) as e:
+        Tape.upload(device, bad)
+    assert e.value.status == 7  # TSI_ERR_BAD_OPCODE
+    fwd = tape.copy()
+    fwd[10]["larg_rarg"] = (12 << 16) | 11  # reads slots not yet computed
+    fwd[10]["opcode_uses"] = (5 << 16) | 1
+    with pytest.raises(N.TsiError) as e:
+        Tape.upload(device, fwd)
+    assert e.value.status == 1
+    with pytest.raises(N.TsiError) as e:
+        Tape.from_llvm_ir(device, "define float @_Z1fffff(float %0) {\n  %5 = fcmp olt float %0, %1\n}\n")
+    assert e.value.status == 2  # TSI_ERR_PARSE
+    # the device is still usable
+    s = Scene(device, Tape.upload(device, tape), api.default_params(localsubdiv=4))
+    assert s.invert(0.0).cells_evaluated > 0
+
+
+@pytest.mark.gpu
+def test_log_arena_exhaustion_is_reported():
+    with Device(log_arena_bytes=1 << 16) as dev:
+        text = scenes.csg(256, 1)  # 4.7k slots: longer than a per-warp log slice
+        s = Scene(dev, Tape.from_llvm_ir(dev, text), api.default_params(localsubdiv=4))
+        with pytest.raises(N.TsiError) as e:
+            for t in (0.0, 0.02):  # the second frame runs reverse AD on the long root tape
+                s.invert(t)
+        assert e.value.status == 4
+        s2 = Scene(dev, Tape.from_llvm_ir(dev, scenes.spheres16(0)), api.default_params(localsubdiv=4))
+        assert s2.invert(0.0).cells_evaluated > 0
