@@ -1,0 +1,372 @@
+"""Benchmark: frames/s of temporal set inversion + ray tracing at localsubdiv 10, 1080p.
+
+Workload (the headline configuration): 256 primitives (spheres, max-of-abs
+boxes, axis capsules) moving sinusoidally in t, combined by a random
+min/max tree (70% min); tape of 4697 slots; localsubdiv 10 (1024^3 leaves),
+delta 0.01, lipschitz_corrected on, pointsample on, fast_normals off;
+1920x1080 frames; 120 frames with t in [0, 1] (t_i = i / 119), the octree
+re-seeded from scratch at frame 0 (first_eval) and carried over between
+frames by the temporal error bound.
+
+A step is one frame: one set inversion (the `main` dispatch) plus one ray
+trace (`rt_main`).  Step i renders frame i mod 120, so the default 120 timed
+steps after 3 warm-up frames contain exactly one first_eval frame and 119
+temporally reused frames, like one run of the animation.
+
+  value : frames/s with the scene resident in HBM, device time (CUDA events)
+          of each step summed over the timed steps; the L2 cache is flushed
+          (a 256 MB write) between steps, outside the per-step events
+  e2e   : the same frames through the public C API from the host: per step
+          the uniforms go up, the frame's RGBA f32 pixels come back to pinned
+          host memory (compute.wgsl:4687 `pixels[]`), wall clock
+  roofline: the refinement kernel's algorithmic FP32 operations (opcost.h
+          table, per executed interval instruction) against the nominal
+          FP32 rate, plus the tracer's node traffic against measured HBM
+  cpu_baseline: the CPU oracle (C++ restatement of compute.wgsl, OpenMP)
+          on a bounded sample of the same animation
+
+--impl reference times the CPU restatement (the reference itself is WGSL
+under wgpu/Vulkan: no Vulkan driver or Rust toolchain exists on these
+machines) on the same workload and prints the same line with
+"impl": "reference".
+
+Multi-GPU (--gpus N, launched under torchrun): replicas.  The frames of one
+animation depend on each other through the resident octree, so each rank
+renders its own animation (scene seed = rank); per-GPU work is fixed
+("scaling": "weak") and value is the total frames/s of all ranks with the
+time taken as the maximum over ranks.  No collective is on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = dict(name="csg256_L10_1080p_120f", n_prims=256, seed=1, localsubdiv=10, delta=0.01,
+                lipschitz_corrected=1, pointsample=1, fast_normals=0, width=1920, height=1080, frames=120,
+                eye=(1.6, 1.0, 1.9))
+METRIC = "frames/s @ subdiv 10, 1080p"
+PEAK_FP32_NOMINAL_TOPS = 148 * 128 * 1.965  # G ops/s: 148 SMs x 128 FP32 lanes x 1.965 GHz (non-FMA)
+
+
+def frame_time(i: int, frames: int) -> float:
+    return (i % frames) / (frames - 1)
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            pass
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+def init_dist(world: int):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def reduce_max(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def build_workload(seed: int):
+    from temporalsetinversion_b200 import api, scenes
+    text = scenes.csg(WORKLOAD["n_prims"], seed)
+    params = api.default_params(localsubdiv=WORKLOAD["localsubdiv"], delta=WORKLOAD["delta"],
+                                lipschitz_corrected=WORKLOAD["lipschitz_corrected"],
+                                pointsample=WORKLOAD["pointsample"], fast_normals=WORKLOAD["fast_normals"])
+    view = scenes.camera_look_at(WORKLOAD["eye"])
+    return text, params, view
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_sample(text: str, params, view, frames: int = 3, threads: int = 0) -> dict:
+    """Oracle on the first `frames` frames of the animation (invert + trace)."""
+    import oracle
+    from temporalsetinversion_b200 import api
+    if threads:
+        oracle.set_threads(threads)
+    tape = api.IR.new(text).gpu_instructions
+    S = oracle.Scene(tape, params)
+    t0 = time.perf_counter()
+    for i in range(frames):
+        t = frame_time(i, WORKLOAD["frames"])
+        S.invert(t)
+        u = api.make_uniforms(view, (WORKLOAD["width"], WORKLOAD["height"]), t)
+        S.trace(u)
+    dt = time.perf_counter() - t0
+    return {"value": frames / dt, "unit": "frames/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": "CPU oracle (C++ restatement of compute.wgsl main + rt_main, OpenMP) on frames 0..%d of the "
+                      "workload (first_eval frame included), full 1920x1080 trace, %.1f s" % (frames - 1, dt)}
+
+
+def run_reference(args, rank, world, dist) -> None:
+    if rank != 0:
+        return
+    text, params, view = build_workload(WORKLOAD["seed"])
+    frames = max(1, min(args.steps, 3))
+    res = cpu_sample(text, params, view, frames=frames)
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": "frames/s", "n_gpus": world, "steps": frames,
+        "warmup": 0, "ms_per_step": 1000.0 / res["value"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded CSG scene, LLVM IR tape)",
+        "config": {"workload": WORKLOAD["name"], "localsubdiv": 10, "resolution": "1920x1080", "frames": 120,
+                   "tape_slots": 4697, "l2": "n/a (CPU)"},
+        "impl": "reference",
+        "cpu_baseline": {"value": res["value"], "unit": "frames/s", "cores": res["cores"], "kind": "port",
+                         "sample": res["sample"] + "; the reference's WGSL path (wgpu/Vulkan) cannot run here"},
+        "e2e": {"value": res["value"], "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU leg
+def run_gpu(args, rank, world, local, dist) -> None:
+    import ctypes as C
+
+    from temporalsetinversion_b200 import Device, Scene, Tape, _native as N, api
+
+    text, params, view = build_workload(WORKLOAD["seed"] + rank)
+    W, H, F = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["frames"]
+    dev = Device(local)
+    lib = dev.lib
+    tape = Tape.from_llvm_ir(dev, text)
+    scene = Scene(dev, tape, params, voxel_capacity=args.voxels)
+
+    # L2 flush buffer (256 MB) and events through torch on this device
+    import torch
+    torch.cuda.set_device(local)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+
+    totals = {k: 0 for k in ("cells_evaluated", "instr_forward", "instr_reverse", "instr_full_equiv", "fp32_ops",
+                             "cells_reused", "cells_reverse")}
+    inv_ms, trace_ms = [], []
+    visits = 0.0
+
+    def step(i: int, record: bool):
+        nonlocal visits
+        t = frame_time(i, F)
+        if i % F == 0:
+            scene.reset()
+        st = scene.invert(t)
+        u = api.make_uniforms(view, (W, H), t)
+        tst = N.Stats()
+        N.check(lib.tsi_scene_trace(scene.handle, C.byref(u), None, C.byref(tst)), "tsi_scene_trace")
+        if record:
+            inv_ms.append(st.device_ms)
+            trace_ms.append(tst.device_ms)
+            visits += tst.reserved
+            for k in totals:
+                totals[k] += getattr(st, k)
+        return st
+
+    for i in range(args.warmup):
+        step(i, False)
+    barrier(dist)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    t_wall0 = time.perf_counter()
+    for i in range(args.warmup, args.warmup + args.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        step(i, True)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall0
+    clocks = sampler.stop()
+    barrier(dist)
+    dev_ms = float(sum(inv_ms) + sum(trace_ms))
+    dev_ms_max = reduce_max(dist, dev_ms)
+    frames_total = reduce_sum(dist, float(args.steps))
+    value = frames_total / (dev_ms_max / 1000.0)
+
+    # ---- e2e through the C API with host buffers
+    pinned = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True)
+    img = N.Image(W, H, C.cast(pinned.data_ptr(), C.POINTER(C.c_float)), None, None)
+    e2e_steps = min(args.steps, F)
+    scene.reset()
+    barrier(dist)
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        t = frame_time(i, F)
+        st = N.Stats()
+        N.check(lib.tsi_scene_invert(scene.handle, t, math.nan, C.byref(st)), "tsi_scene_invert")
+        u = api.make_uniforms(view, (W, H), t)
+        N.check(lib.tsi_scene_trace(scene.handle, C.byref(u), C.byref(img), None), "tsi_scene_trace")
+    e2e_wall = reduce_max(dist, time.perf_counter() - t0)
+    e2e_value = reduce_sum(dist, float(e2e_steps)) / e2e_wall
+
+    if rank != 0:
+        dev.close()
+        return
+    peaks = measured_peaks()
+    inv_total_s = sum(inv_ms) / 1000.0
+    ops = totals["fp32_ops"]
+    achieved_gops = ops / inv_total_s / 1e9 if inv_total_s > 0 else 0.0
+    trace_s = sum(trace_ms) / 1000.0
+    trace_bytes = visits * 40.0 + W * H * 16.0 * len(trace_ms)
+    trace_gbs = trace_bytes / trace_s / 1e9 if trace_s > 0 else 0.0
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    gpu_launches = args.steps * (params.localsubdiv + 3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded CSG scene emitted as LLVM IR, lowered like scenes/*.ll)",
+        "config": {"workload": WORKLOAD["name"], "localsubdiv": 10, "resolution": "1920x1080", "frames": F,
+                   "tape_slots": tape.instruction_count, "registers": tape.registers,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed between steps (256 MB write outside the per-step events)"},
+        "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": C.sizeof(N.Uniforms) + 160,
+                "d2h_bytes_per_step": W * H * 16 + C.sizeof(N.Stats)},
+        "roofline": {"kernel": "refine_kernel (interval tape interpreter)", "bound": "fp32",
+                     "achieved": achieved_gops / 1000.0, "peak": PEAK_FP32_NOMINAL_TOPS / 1000.0, "unit": "TOP/s",
+                     "frac": achieved_gops / PEAK_FP32_NOMINAL_TOPS, "traffic": None,
+                     "peak_source": "nominal FP32 (MEASURED_PEAKS.json has no FP32 figure)",
+                     "ops_per_step": ops / args.steps},
+        "roofline_trace": {"kernel": "trace_kernel", "bound": "hbm", "achieved": trace_gbs, "peak": hbm_peak,
+                           "unit": "GB/s", "frac": trace_gbs / hbm_peak, "traffic": None,
+                           "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "breakdown_ms_per_step": {"invert": sum(inv_ms) / args.steps, "trace": sum(trace_ms) / args.steps},
+        "work_per_step": {k: v / args.steps for k, v in totals.items()},
+        "clocks": clocks,
+        "gpu_launches": gpu_launches,
+        "wall_s": wall,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            cb = cpu_sample(text, params, view, frames=2)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as e:  # the oracle needs g++ on the host
+            line["cpu_baseline"] = {"value": None, "unit": "frames/s", "cores": 0, "kind": "port",
+                                    "sample": "unavailable: %s" % e}
+    print(json.dumps(line), flush=True)
+    dev.close()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="tsi", choices=["tsi", "reference"])
+    ap.add_argument("--voxels", type=int, default=64 << 20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_env()
+    dist = init_dist(world)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world, dist)
+        else:
+            run_gpu(args, rank, world, local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -201,6 +201,8 @@ TSI_API void tsi_default_params(tsi_params *p);
 /* Replaces State::new's adapter/device setup (main.rs:97-122) and the
  * buffer allocations of main.rs:208-303 (now lazily sized, HBM resident). */
 TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out);
+/* Releases the context and every tape and scene still alive on it; their
+ * handles become invalid. */
 TSI_API void tsi_destroy(tsi_ctx *ctx);
 TSI_API tsi_status tsi_synchronize(tsi_ctx *ctx);
 

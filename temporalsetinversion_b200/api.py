@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -99,9 +100,15 @@ class Device:
         h = C.c_void_p()
         N.check(self.lib.tsi_create(C.byref(opts), C.byref(h)), "tsi_create")
         self.handle = h
+        self._children = weakref.WeakSet()
 
     def close(self) -> None:
         if getattr(self, "handle", None):
+            for child in list(self._children):  # scenes first, then tapes
+                if isinstance(child, Scene):
+                    child.close()
+            for child in list(self._children):
+                child.close()
             self.lib.tsi_destroy(self.handle)
             self.handle = None
 
@@ -132,6 +139,7 @@ class Tape:
     def __init__(self, device: Device, handle: C.c_void_p):
         self.device = device
         self.handle = handle
+        device._children.add(self)
         info = N.TapeInfo()
         N.check(device.lib.tsi_tape_info_get(handle, C.byref(info)), "tsi_tape_info_get")
         self.instruction_count = info.instruction_count
@@ -161,9 +169,9 @@ class Tape:
         return out
 
     def close(self) -> None:
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and getattr(self.device, "handle", None):
             self.device.lib.tsi_tape_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:
@@ -181,6 +189,7 @@ class Scene:
         N.check(device.lib.tsi_scene_create(device.handle, tape.handle, C.byref(params), voxel_capacity, C.byref(h)),
                 "tsi_scene_create")
         self.handle = h
+        device._children.add(self)
 
     def reset(self) -> None:
         N.check(self.device.lib.tsi_scene_reset(self.handle), "tsi_scene_reset")
@@ -220,9 +229,9 @@ class Scene:
         return arr
 
     def close(self) -> None:
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and getattr(self.device, "handle", None):
             self.device.lib.tsi_scene_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:

@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -145,6 +146,9 @@ struct tsi_ctx {
   void *d_scratch = nullptr;
   size_t scratch_bytes = 0;
   uint32_t watchdog = 0;
+  // objects created on this context, released by tsi_destroy if still alive
+  std::set<tsi_tape *> tapes;
+  std::set<tsi_scene *> scenes;
 };
 
 struct tsi_batch_graph {
@@ -636,6 +640,8 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  while (!c->scenes.empty()) tsi_scene_destroy(*c->scenes.begin());
+  while (!c->tapes.empty()) tsi_tape_destroy(*c->tapes.begin());
   cudaFree(c->d_scenes);
   cudaFreeHost(c->h_scenes);
   cudaFree(c->d_recs);
@@ -686,14 +692,14 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
   t->out_reg = pt.out_reg;
   t->n_minmax = pt.n_minmax;
   t->fwd_cost = pt.fwd_cost;
+  c->tapes.insert(t);
   if (t->len) {
     cudaError_t e = dalloc(&t->d_code, t->len);
     if (e == cudaSuccess)
       e = cudaMemcpy(t->d_code, pt.code.data(), (size_t)t->len * sizeof(uint2), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
       g_last_error = cudaGetErrorString(e);
-      cudaFree(t->d_code);
-      delete t;
+      tsi_tape_destroy(t);
       return TSI_ERR_CUDA;
     }
   }
@@ -733,6 +739,7 @@ TSI_API tsi_status tsi_tape_info_get(const tsi_tape *t, tsi_tape_info *info) {
 
 TSI_API void tsi_tape_destroy(tsi_tape *t) {
   if (!t) return;
+  if (t->ctx) t->ctx->tapes.erase(t);
   cudaFree(t->d_code);
   delete t;
 }
@@ -801,6 +808,7 @@ TSI_API tsi_status tsi_scene_create(tsi_ctx *c, const tsi_tape *tape, const tsi_
   if (bricks > 0x1fffffffull) return set_err(TSI_ERR_INVALID_ARGUMENT, "voxel capacity too large");
   tsi_scene *s = new tsi_scene();
   s->ctx = c;
+  c->scenes.insert(s);
   s->tape = tape;
   s->p = *params;
   s->cap_bricks = (uint32_t)bricks;
@@ -841,6 +849,7 @@ TSI_API void tsi_scene_destroy(tsi_scene *s) {
   if (s->ctx) {
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
+    s->ctx->scenes.erase(s);
   }
   cudaFree(s->pool.box_xy);
   cudaFree(s->pool.box_z);

@@ -19,7 +19,7 @@ def _make(device, specs):
     return out
 
 
-SPECS = [(scenes.csg(16, 1), 6), (scenes.spheres16(2), 7), (scenes.csg(40, 3), 5), (scenes.swept(6, 5), 6)]
+SPECS = [(scenes.csg(16, 1, 0.9), 6), (scenes.spheres16(2), 7), (scenes.csg(40, 3, 0.9), 5), (scenes.swept(6, 5), 6)]
 
 
 @pytest.mark.gpu

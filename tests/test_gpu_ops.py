@@ -8,6 +8,7 @@ operands).  Directed mode must enclose dense FP64 point samples."""
 from __future__ import annotations
 
 import math
+import zlib
 
 import numpy as np
 import pytest
@@ -69,9 +70,11 @@ def random_boxes(n, rng, scale=2.0):
     hi = (lo + w).astype(np.float32)
     b = np.empty((n, 8), np.float32)
     b[:, 0::2], b[:, 1::2] = lo, hi
-    # exact zeros and zero-straddling cases
+    # intervals starting at an exact zero, and [-0, +0]
     b[: n // 16, 0] = 0.0
+    b[: n // 16, 1] = np.abs(b[: n // 16, 1])
     b[n // 16: n // 8, 2:4] = [-0.0, 0.0]
+    assert np.all(b[:, 0::2] <= b[:, 1::2])
     return b
 
 
@@ -79,7 +82,7 @@ def random_boxes(n, rng, scale=2.0):
 @pytest.mark.parametrize("name", sorted(OPS))
 def test_op_rn_bit_exact(device, name):
     tape = api.IR.new(OPS[name]).gpu_instructions
-    boxes = random_boxes(4096, np.random.default_rng(abs(hash(name)) % 2**32))
+    boxes = random_boxes(4096, np.random.default_rng(zlib.crc32(name.encode())))
     g = Tape.upload(device, tape).eval_boxes(boxes, rounding_mode=0, reverse=True)
     o = oracle.eval_boxes(tape, boxes, reverse=True)
     same = (g == o) | (np.isnan(g) & np.isnan(o))
@@ -159,7 +162,7 @@ def test_math_bit_exact_and_accurate(device):
         if which in np_fn:
             with np.errstate(all="ignore"):
                 ref = np_fn[which](a32.astype(np.float64))
-            sel = np.isfinite(ref) & (np.abs(ref) > 1e-30) & (np.abs(a32) < 6000)
+            sel = np.isfinite(ref) & (np.abs(ref) > 1e-30) & (np.abs(ref) < 3.0e38) & (np.abs(a32) < 6000)
             if which == 0:
                 sel &= np.abs(ref) > 1e-3
             ulp = np.spacing(np.abs(ref[sel]).astype(np.float32)).astype(np.float64)

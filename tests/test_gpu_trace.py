@@ -39,7 +39,7 @@ def test_trace_matches_oracle(device, name, src, params, eye):
     if src == "spheres16":
         tape = api.IR.new(scenes.spheres16(0)).gpu_instructions
     elif src == "csg48":
-        tape = api.IR.new(scenes.csg(48, 2)).gpu_instructions
+        tape = api.IR.new(scenes.csg(48, 4)).gpu_instructions
     else:
         tape = load_tape(src)
     p = api.default_params(**params)
