@@ -295,6 +295,13 @@ TSI_API tsi_status tsi_compile_gpu_instructions(const tsi_gpu_instruction *instr
  * 6 max(a, b) (minimumNumber / maximumNumber), 7 fminf, 8 fmaxf. */
 TSI_API tsi_status tsi_debug_math(tsi_ctx *ctx, int32_t which, uint32_t n, const float *a, const float *b,
                                   float *out);
+/* Per-level profile of the context's last inversion: device ms of each
+ * level's refinement launch (-1 unless TSI_PROFILE_LEVELS is set in the
+ * environment when the context is created) and the 17 counters per level
+ * (order of the tsi_stats fields from parents_expanded to prune_fallbacks,
+ * without voxels_live and items_high_water). */
+TSI_API tsi_status tsi_debug_level_profile(tsi_ctx *ctx, uint32_t max_levels, float *ms, uint64_t *counters,
+                                           uint32_t *n_levels);
 
 #ifdef __cplusplus
 }

@@ -43,6 +43,11 @@ class Uniforms(C.Structure):  # uniforms.rs:8-17
                 ("rendermode", f32), ("_padding", f32 * 3)]
 
 
+LEVEL_COUNTERS = ["parents", "evaluated", "reverse", "skipped", "ambiguous", "empty", "full", "enqueued", "reused",
+                  "instr_fwd", "instr_rev", "instr_full", "fp32", "brick_alloc", "brick_free", "tape_words",
+                  "prune_fallback"]
+
+
 class Stats(C.Structure):
     _fields_ = [(n, u64) for n in (
         "parents_expanded", "cells_evaluated", "cells_reverse", "cells_skipped", "cells_ambiguous", "cells_empty",
@@ -114,6 +119,7 @@ SIGNATURES = {
     "tsi_ir_tape_info": (i32, [C.c_char_p, C.c_size_t, P(TapeInfo), P(u32), u32]),
     "tsi_compile_gpu_instructions": (i32, [P(GPUInstruction), u32, P(u32), u32, P(TapeInfo)]),
     "tsi_debug_math": (i32, [C.c_void_p, i32, u32, P(f32), P(f32), P(f32)]),
+    "tsi_debug_level_profile": (i32, [C.c_void_p, u32, P(f32), P(u64), P(u32)]),
 }
 
 _lib = None

@@ -127,6 +127,17 @@ class Device:
     def synchronize(self) -> None:
         N.check(self.lib.tsi_synchronize(self.handle), "tsi_synchronize")
 
+    def level_profile(self, max_levels: int = 24) -> list:
+        """Per-level ms and counters of the last inversion on this device."""
+        ms = np.zeros(max_levels, np.float32)
+        cnt = np.zeros((max_levels, len(N.LEVEL_COUNTERS)), np.uint64)
+        n = C.c_uint32(0)
+        N.check(self.lib.tsi_debug_level_profile(self.handle, max_levels, _fptr(ms),
+                                                 cnt.ctypes.data_as(C.POINTER(C.c_uint64)), C.byref(n)),
+                "tsi_debug_level_profile")
+        return [dict(level=l, ms=float(ms[l]), **{k: int(cnt[l, i]) for i, k in enumerate(N.LEVEL_COUNTERS)})
+                for l in range(min(n.value, max_levels))]
+
     def math(self, which: int, a: np.ndarray, b: np.ndarray | None = None) -> np.ndarray:
         a = np.ascontiguousarray(a, dtype=np.float32)
         b = np.zeros_like(a) if b is None else np.ascontiguousarray(b, dtype=np.float32)

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -94,7 +95,7 @@ struct tsi_tape {
   uint2 *d_code = nullptr;
   uint32_t len = 0;  // instructions after the 4 ARG slots
   uint32_t count = 0, nregs = 0, out_reg = 0, n_minmax = 0;
-  uint64_t fwd_cost = 0;
+  uint64_t fwd_cost = 0, rev_cost = 0;
 };
 
 struct tsi_scene {
@@ -138,8 +139,13 @@ struct tsi_ctx {
   uint64_t log_overflow_cap = 0;
   uint32_t *d_error = nullptr;
   unsigned long long *d_stats = nullptr;
+  unsigned long long *d_level_stats = nullptr;
   unsigned long long *d_visits = nullptr;
   Readback *h_rb = nullptr;
+  // per-level profile of the last inversion (events when profiling is on)
+  bool profile_levels = false;
+  std::vector<cudaEvent_t> level_events;
+  uint32_t last_levels = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   size_t smem_set = 0;
   // scratch for tsi_tape_eval_boxes
@@ -193,6 +199,7 @@ LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes) {
   P.log_overflow_cap = c->log_overflow_cap;
   P.error = c->d_error;
   P.stats = c->d_stats;
+  P.level_stats = c->d_level_stats;
   return P;
 }
 
@@ -233,6 +240,8 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, Scene
   R.t_lo = -INFINITY;
   R.t_hi = INFINITY;
   R.parent = TSI_NONE;
+  R.fwd_cost = (uint32_t)std::min<uint64_t>(s->tape->fwd_cost, 0xffffffffull);
+  R.rev_cost = (uint32_t)std::min<uint64_t>(s->tape->rev_cost, 0xffffffffull);
   R.pad = 0;
 }
 
@@ -261,10 +270,17 @@ tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *tim
   CK(cudaMemcpyAsync(c->d_recs, c->h_recs, n * sizeof(TapeRec), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->d_error, 0, sizeof(uint32_t), c->stream));
   CK(cudaMemsetAsync(c->d_stats, 0, ST_COUNT * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(c->d_level_stats, 0, (TSI_MAX_LEVELS + 1) * ST_COUNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(c->d_log_used, 0, sizeof(unsigned long long), c->stream));
   const LaunchParams P = make_params(c, n);
   CK(launch_frame_begin(P, c->stream));
-  for (uint32_t level = 0; level < lmax; ++level) CK(launch_refine(P, level, rcap, grid, kBlock, smem, c->stream));
+  const bool prof = c->profile_levels && c->level_events.size() >= lmax + 1;
+  for (uint32_t level = 0; level < lmax; ++level) {
+    if (prof) CK(cudaEventRecord(c->level_events[level], c->stream));
+    CK(launch_refine(P, level, rcap, grid, kBlock, smem, c->stream));
+  }
+  if (prof) CK(cudaEventRecord(c->level_events[lmax], c->stream));
+  c->last_levels = lmax;
   CK(launch_frame_end(P, c->stream));
   return TSI_OK;
 }
@@ -624,6 +640,12 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   CKC(dalloc(&c->d_log_used, 1));
   CKC(dalloc(&c->d_error, 1));
   CKC(dalloc(&c->d_stats, ST_COUNT));
+  CKC(dalloc(&c->d_level_stats, (TSI_MAX_LEVELS + 1) * ST_COUNT));
+  if (getenv("TSI_PROFILE_LEVELS")) {
+    c->profile_levels = true;
+    c->level_events.resize(TSI_MAX_LEVELS + 1);
+    for (auto &ev : c->level_events) CKC(cudaEventCreate(&ev));
+  }
   CKC(dalloc(&c->d_visits, 1));
   CKC(cudaMallocHost((void **)&c->h_rb, sizeof(Readback)));
   CKC(cudaEventCreate(&c->ev0));
@@ -663,6 +685,8 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   cudaFree(c->d_log_used);
   cudaFree(c->d_error);
   cudaFree(c->d_stats);
+  cudaFree(c->d_level_stats);
+  for (auto &ev : c->level_events) cudaEventDestroy(ev);
   cudaFree(c->d_visits);
   cudaFree(c->d_scratch);
   cudaFreeHost(c->h_rb);
@@ -692,6 +716,7 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
   t->out_reg = pt.out_reg;
   t->n_minmax = pt.n_minmax;
   t->fwd_cost = pt.fwd_cost;
+  t->rev_cost = pt.rev_cost;
   c->tapes.insert(t);
   if (t->len) {
     cudaError_t e = dalloc(&t->d_code, t->len);
@@ -791,6 +816,29 @@ TSI_API tsi_status tsi_debug_math(tsi_ctx *c, int32_t which, uint32_t n, const f
   CK(launch_math(which, n, da, db, dout, c->stream));
   CK(cudaMemcpyAsync(out, dout, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_debug_level_profile(tsi_ctx *c, uint32_t max_levels, float *ms, uint64_t *counters,
+                                           uint32_t *n_levels) {
+  if (!c || !n_levels) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  const uint32_t L = std::min(c->last_levels, max_levels);
+  *n_levels = c->last_levels;
+  if (counters) {
+    std::vector<unsigned long long> h((size_t)(TSI_MAX_LEVELS + 1) * ST_COUNT);
+    CK(cudaMemcpy(h.data(), c->d_level_stats, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    for (uint32_t l = 0; l < L; ++l)
+      for (int i = 0; i < ST_COUNT; ++i) counters[(size_t)l * ST_COUNT + i] = h[(size_t)l * ST_COUNT + i];
+  }
+  if (ms) {
+    for (uint32_t l = 0; l < L; ++l) {
+      ms[l] = -1.0f;
+      if (c->profile_levels && c->level_events.size() > l + 1)
+        CK(cudaEventElapsedTime(&ms[l], c->level_events[l], c->level_events[l + 1]));
+    }
+  }
   return TSI_OK;
 }
 

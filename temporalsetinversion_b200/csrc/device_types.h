@@ -80,6 +80,8 @@ struct TapeRec {
   uint32_t n_minmax;
   float t_lo, t_hi;   // valid for cells inside the group's boxes with time in [t_lo, t_hi]
   uint32_t parent;    // record it was pruned from (TSI_NONE for a full tape)
+  uint32_t fwd_cost;  // opcost.h forward ops of one cell (fix included)
+  uint32_t rev_cost;  // opcost.h reverse ops of one cell
   uint32_t pad;
 };
 
@@ -123,5 +125,6 @@ struct LaunchParams {
   unsigned long long *log_overflow_used;  // in float4 units
   unsigned long long log_overflow_cap;
   uint32_t *error;
-  unsigned long long *stats;  // [ST_COUNT]
+  unsigned long long *stats;        // [ST_COUNT]
+  unsigned long long *level_stats;  // [TSI_MAX_LEVELS + 1][ST_COUNT], per refine launch
 };

@@ -391,12 +391,9 @@ struct IA {
   }
   // fix, compute.wgsl:3462-3472; directed mode keeps the enclosure
   static TSI_DEV Iv fix(Iv x) {
-    if (!D) {
-      float lo = x.lo, hi = x.hi;
-      if (is_nan_f(x.hi)) hi = kBIG;
-      if (is_nan_f(x.lo)) lo = -kBIG;
-      return Iv{fm_max(lo, -kBIG), fm_min(hi, kBIG)};
-    }
+    // a NaN bound loses against +-BIG in minimumNumber/maximumNumber, which
+    // is exactly the reference's NaN -> +-BIG replacement followed by the clamp
+    if (!D) return Iv{fm_max(x.lo, -kBIG), fm_min(x.hi, kBIG)};
     return Iv{is_nan_f(x.lo) ? -fm_inf() : x.lo, is_nan_f(x.hi) ? fm_inf() : x.hi};
   }
 

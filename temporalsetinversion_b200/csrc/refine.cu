@@ -20,6 +20,14 @@
 // chosen operand bit for bit, and the reverse pass falls back to the full
 // tape when a sensitivity overflows (the only case where the dead branch of
 // the full tape would contribute, through 0 * inf).
+//
+// A pruned tape is valid for cells inside its group's boxes whose time
+// interval lies inside the interval the decisions were taken on.  The
+// children of a re-enqueued cell are evaluated over [child.t, time]; when
+// that reaches further back than the cell's own evaluation interval (the
+// cell was evaluated at a point in time), the branch decisions are taken
+// again by a second forward pass over the widened interval, so the children
+// can use the pruned tape instead of an ancestor's.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -34,22 +42,234 @@ namespace tsi {
 __constant__ uint32_t c_cost_fwd[H_COUNT] = TSI_OPCOST_FWD_INIT;
 __constant__ uint32_t c_cost_rr[H_COUNT] = TSI_OPCOST_RR_INIT;
 
-struct WarpStats {
-  unsigned long long v[ST_COUNT];
-};
+constexpr int kWarps = 8;  // warps per block (block of 256)
 
 __device__ __forceinline__ bool finite2(Iv a) { return isfinite(a.lo) && isfinite(a.hi); }
 
 __device__ __forceinline__ Iv ld_reg(const float2 *rf, uint32_t r, uint32_t lane) {
-  float2 v = rf[r * 32u + lane];
+  const float2 v = rf[r * 32u + lane];
   return Iv{v.x, v.y};
 }
 __device__ __forceinline__ void st_reg(float2 *rf, uint32_t r, uint32_t lane, Iv v) {
   rf[r * 32u + lane] = make_float2(v.lo, v.hi);
 }
 
+// ---------------------------------------------------------------- handlers
+// Rare handlers live out of line so the interpreter loop stays small.
+template <bool D>
+__device__ __noinline__ Iv cold_forward(uint32_t h, Iv A, Iv B, float lit) {
+  return IA<D>::forward(h, A, B, lit);
+}
+
+template <bool D>
+__device__ __forceinline__ Iv op_forward(uint32_t h, Iv A, Iv B, float lit) {
+  using I = IA<D>;
+  Iv v;
+  switch (h) {
+    case H_CONST: v = iv(lit); break;
+    case H_COPY: v = A; break;
+    case H_ADD_II: v = I::add(A, B); break;
+    case H_SUB_II: v = I::sub(A, B); break;
+    case H_MUL_II: v = I::mul(A, B); break;
+    case H_MIN_II: v = I::min_(A, B); break;
+    case H_MAX_II: v = I::max_(A, B); break;
+    case H_ADD_IF: v = I::add_f(A, lit); break;
+    case H_SUB_IF: v = I::sub_f(A, lit); break;
+    case H_MUL_IF: v = I::mul_f(A, lit); break;
+    case H_MIN_IF: v = Iv{fm_min(A.lo, lit), fm_min(A.hi, lit)}; break;
+    case H_MAX_IF: v = Iv{fm_max(A.lo, lit), fm_max(A.hi, lit)}; break;
+    case H_SQR: v = I::sqr(A); break;
+    case H_SQRT: v = I::sqrt_(A); break;
+    case H_NEG: v = I::neg(A); break;
+    case H_ABS: v = I::abs_(A); break;
+    case H_SUB_FI: v = I::sub(iv(lit), A); break;
+    default: return cold_forward<D>(h, A, B, lit);  // fixed inside
+  }
+  return I::fix(v);
+}
+
+template <bool D>
+__device__ __noinline__ int cold_reverse_rule(uint32_t h, Iv A, Iv B, float lit, Iv &r0, Iv &r1) {
+  return IA<D>::reverse_rule(h, A, B, lit, r0, r1);
+}
+
+template <bool D>
+__device__ __forceinline__ void op_reverse_rule(uint32_t h, Iv A, Iv B, float lit, Iv &r0, Iv &r1) {
+  using I = IA<D>;
+  switch (h) {
+    case H_COPY: r0 = iv(1.0f); break;
+    case H_ADD_II: r0 = iv(1.0f); r1 = iv(1.0f); break;
+    case H_SUB_II: r0 = iv(1.0f); r1 = iv(-1.0f); break;
+    case H_MUL_II: r0 = B; r1 = A; break;
+    case H_MIN_II: I::min_rr(A, B, r0, r1); break;
+    case H_MAX_II: I::max_rr(A, B, r0, r1); break;
+    case H_ADD_IF: r0 = iv(1.0f); break;
+    case H_SUB_IF: r0 = iv(1.0f); break;
+    case H_MUL_IF: r0 = iv(lit); break;
+    case H_SQR: r0 = I::mul_f(A, 2.0f); break;
+    case H_NEG: r0 = iv(-1.0f); break;
+    case H_ABS: r0 = I::abs_rr(A); break;
+    case H_SUB_FI: r0 = iv(-1.0f); break;
+    case H_MIN_IF: { Iv t; I::min_rr(A, iv(lit), r0, t); break; }
+    case H_MAX_IF: { Iv t; I::max_rr(A, iv(lit), r0, t); break; }
+    default: cold_reverse_rule<D>(h, A, B, lit, r0, r1); break;
+  }
+}
+
+// ---------------------------------------------------------------- passes
+// Forward pass over `len` instructions (compute.wgsl:3633-3772).  Writes the
+// operand log when `lg` is set and the min/max branch ballots when `dg` is
+// set.  Returns the output register's value.
+template <bool D>
+__device__ __forceinline__ Iv forward_pass(const uint2 *__restrict__ code, uint32_t len, uint32_t out_reg, float2 *rf,
+                                           uint32_t lane, Iv x, Iv y, Iv z, Iv t, float4 *lg, uint2 *dg) {
+  st_reg(rf, 0, lane, x);
+  st_reg(rf, 1, lane, y);
+  st_reg(rf, 2, lane, z);
+  st_reg(rf, 3, lane, t);
+  uint32_t mm = 0;
+  uint2 w = len ? code[0] : make_uint2(0u, 0u);
+  for (uint32_t i = 0; i < len; ++i) {
+    const uint2 wn = (i + 1 < len) ? code[i + 1] : w;  // fetched while this one executes
+    const uint32_t h = TSI_W0_H(w.x);
+    const float lit = __uint_as_float(w.y);
+    const Iv Av = ld_reg(rf, TSI_W0_A(w.x), lane);
+    const Iv Bv = TSI_H_IS_II(h) ? ld_reg(rf, w.y & 255u, lane) : iv(lit);
+    const Iv r = op_forward<D>(h, Av, Bv, lit);
+    if (lg) lg[(size_t)i * 32u + lane] = make_float4(Av.lo, Av.hi, Bv.lo, Bv.hi);
+    if (dg && TSI_H_IS_MINMAX(h)) {
+      const bool amax = (h == H_MAX_II || h == H_MAX_IF);
+      const bool a_below = Av.hi < Bv.lo, b_below = Bv.hi < Av.lo;
+      const uint32_t ua = __ballot_sync(FULL_MASK, amax ? b_below : a_below);
+      const uint32_t ub = __ballot_sync(FULL_MASK, amax ? a_below : b_below);
+      if (lane == 0) dg[mm] = make_uint2(ua, ub);
+      ++mm;
+    }
+    st_reg(rf, TSI_W0_DST(w.x), lane, r);
+    w = wn;
+  }
+  return ld_reg(rf, out_reg, lane);
+}
+
+// Reverse pass (compute.wgsl:3785-3964): sensitivities reuse the register
+// file; a register's accumulator is consumed and cleared at the definition
+// it holds.  `bad` collects non-finite sensitivities.
+template <bool D>
+__device__ __forceinline__ void reverse_pass(const uint2 *__restrict__ code, uint32_t len, uint32_t nregs,
+                                             uint32_t out_reg, float2 *rf, uint32_t lane, const float4 *lg,
+                                             bool take, Iv sens[4], bool &bad) {
+  using I = IA<D>;
+  for (uint32_t r = 0; r < nregs; ++r) st_reg(rf, r, lane, iv(0.0f));
+  st_reg(rf, out_reg, lane, iv(1.0f));
+  if (len) {
+    uint2 w = code[len - 1];
+    float4 L = lg[(size_t)(len - 1) * 32u + lane];
+    for (int i = (int)len - 1; i >= 0; --i) {
+      uint2 wn = w;
+      float4 Ln = L;
+      if (i > 0) {
+        wn = code[i - 1];
+        Ln = lg[(size_t)(i - 1) * 32u + lane];
+      }
+      const uint32_t h = TSI_W0_H(w.x);
+      const uint32_t d = TSI_W0_DST(w.x), a = TSI_W0_A(w.x), b = w.y & 255u;
+      const float lit = __uint_as_float(w.y);
+      const Iv Av = Iv{L.x, L.y}, Bv = Iv{L.z, L.w};
+      const Iv s = ld_reg(rf, d, lane);
+      st_reg(rf, d, lane, iv(0.0f));
+      if (take && h != H_CONST) {
+        bad |= !finite2(s);
+        const bool s0 = (s.lo == 0.0f && s.hi == 0.0f);
+        if (TSI_H_IS_II(h)) {
+          if (s0 && TSI_W0_FA(w.x) && TSI_W0_FB(w.x)) {
+            st_reg(rf, a, lane, iv(0.0f));
+            st_reg(rf, b, lane, iv(0.0f));
+          } else {
+            Iv r0, r1;
+            op_reverse_rule<D>(h, Av, Bv, lit, r0, r1);
+            r0 = I::mul(I::fix(r0), s);
+            r1 = I::mul(I::fix(r1), s);
+            const Iv n0 = I::add(r0, ld_reg(rf, a, lane));
+            const Iv n1 = I::add(r1, ld_reg(rf, b, lane));
+            st_reg(rf, a, lane, n0);
+            st_reg(rf, b, lane, n1);
+            bad |= !finite2(n0) || !finite2(n1);
+          }
+        } else if (s0 && TSI_W0_FA(w.x)) {
+          st_reg(rf, a, lane, iv(0.0f));
+        } else {
+          Iv r0, r1;
+          op_reverse_rule<D>(h, Av, Bv, lit, r0, r1);
+          r0 = I::mul(I::fix(r0), s);
+          const Iv n0 = I::add(r0, ld_reg(rf, a, lane));
+          st_reg(rf, a, lane, n0);
+          bad |= !finite2(n0);
+        }
+      } else if (take) {
+        bad |= !finite2(s);
+      }
+      w = wn;
+      L = Ln;
+    }
+  }
+  for (int q = 0; q < 4; ++q) sens[q] = ld_reg(rf, q, lane);
+}
+
+// Backward liveness scan of one sibling group (lane 8g): decided min/max
+// become copies/constants, dead instructions vanish.  The kept instructions
+// are written in reverse order to `tmp`; returns their count.
+__device__ uint32_t prune_scan(const uint2 *__restrict__ code, uint32_t len, uint32_t n_minmax, uint32_t out_reg,
+                               const uint2 *dg, uint32_t g, uint32_t E, uint2 *tmp, uint32_t &mm_kept,
+                               uint32_t &fwd_cost, uint32_t &rev_cost) {
+  unsigned long long live = 1ull << out_reg;
+  uint32_t m = n_minmax, cnt = 0;
+  mm_kept = 0;
+  fwd_cost = 0;
+  rev_cost = 0;
+  for (int i = (int)len - 1; i >= 0; --i) {
+    const uint2 w = code[i];
+    const uint32_t h = TSI_W0_H(w.x);
+    const uint32_t d = TSI_W0_DST(w.x), a = TSI_W0_A(w.x), b = w.y & 255u;
+    const bool mmx = TSI_H_IS_MINMAX(h);
+    uint2 dd = make_uint2(0u, 0u);
+    if (mmx) dd = dg[--m];
+    if (!((live >> d) & 1ull)) continue;
+    live &= ~(1ull << d);
+    uint2 out = w;
+    uint32_t hk = h;
+    if (mmx) {
+      const uint32_t ga = (dd.x >> (g * 8u)) & 0xffu, gb = (dd.y >> (g * 8u)) & 0xffu;
+      if ((ga & E) == E) {
+        out = make_uint2(TSI_W0(H_COPY, TSI_W0_FA(w.x), 0u, d, a), 0u);
+        hk = H_COPY;
+        live |= 1ull << a;
+      } else if ((gb & E) == E) {
+        if (TSI_H_IS_II(h)) {
+          out = make_uint2(TSI_W0(H_COPY, TSI_W0_FB(w.x), 0u, d, b), 0u);
+          hk = H_COPY;
+          live |= 1ull << b;
+        } else {
+          out = make_uint2(TSI_W0(H_CONST, 0u, 0u, d, 0u), w.y);
+          hk = H_CONST;
+        }
+      } else {
+        live |= 1ull << a;
+        if (TSI_H_IS_II(h)) live |= 1ull << b;
+        ++mm_kept;
+      }
+    } else {
+      if (h != H_CONST) live |= 1ull << a;
+      if (TSI_H_IS_II(h)) live |= 1ull << b;
+    }
+    fwd_cost += c_cost_fwd[hk] + TSI_FIX_COST;
+    rev_cost += c_cost_rr[hk] + TSI_REV_OPERAND_COST * TSI_H_NREG(hk);
+    tmp[cnt++] = out;
+  }
+  return cnt;
+}
+
 // mallocV (compute.wgsl:3437-3450) for a whole brick of 8 siblings.
-__device__ uint32_t alloc_brick(const SceneLaunch &S, uint32_t *error, unsigned long long &nalloc) {
+__device__ uint32_t alloc_brick(const SceneLaunch &S, uint32_t *error) {
   SceneCounters *c = S.ctr;
   int32_t fc = atomicSub(&c->free_count, 1);
   uint32_t b;
@@ -62,13 +282,51 @@ __device__ uint32_t alloc_brick(const SceneLaunch &S, uint32_t *error, unsigned 
       return TSI_NONE;
     }
   }
-  nalloc++;
   return b * 8u;
 }
 
+__device__ __forceinline__ void find_valid(const LaunchParams &P, uint32_t &rec, TapeRec &TR, float tl, float th) {
+  TR = P.recs[rec];
+  while (TR.parent != TSI_NONE && !(TR.t_lo <= tl && th <= TR.t_hi)) {
+    rec = TR.parent;
+    TR = P.recs[rec];
+  }
+}
+
+__device__ __forceinline__ float warp_min(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(FULL_MASK, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(FULL_MASK, v, o));
+  return v;
+}
+
+// scratch for one item: operand log + decisions, in the warp's slice or the
+// shared overflow arena (long tapes)
+__device__ __forceinline__ bool item_scratch(const LaunchParams &P, uint32_t len, uint32_t lane, float4 *slice_log,
+                                             uint2 *slice_dec, float4 *&lg, uint2 *&dg) {
+  if (len <= P.slice_len) {
+    lg = slice_log;
+    dg = slice_dec;
+    return true;
+  }
+  const unsigned long long need = (unsigned long long)len * 32ull + ((unsigned long long)len + 1ull) / 2ull;
+  unsigned long long off = 0;
+  if (lane == 0) off = atomicAdd(P.log_overflow_used, need);
+  off = __shfl_sync(FULL_MASK, off, 0);
+  if (off + need > P.log_overflow_cap) {
+    if (lane == 0) atomicOr(P.error, EB_LOG_OOM);
+    return false;
+  }
+  lg = P.log_overflow + off;
+  dg = reinterpret_cast<uint2 *>(P.log_overflow + off + (unsigned long long)len * 32ull);
+  return true;
+}
+
 template <bool D>
-__device__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t level, float2 *rf,
-                             float4 *slice_log, uint2 *slice_dec, WarpStats &ws) {
+__device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t level, float2 *rf,
+                                          float4 *slice_log, uint2 *slice_dec, unsigned long long *ws) {
   using A = IA<D>;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t g = lane >> 3, k = lane & 7u;
@@ -87,7 +345,10 @@ __device__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t
 
   // ---- allocate or reuse the 8 children (3564-3580)
   uint32_t base = pchild;
-  if (active && new_voxel && k == 0) base = alloc_brick(S, P.error, ws.v[ST_BRICK_ALLOC]);
+  if (active && new_voxel && k == 0) {
+    base = alloc_brick(S, P.error);
+    if (base != TSI_NONE) atomicAdd(&ws[ST_BRICK_ALLOC], 1ull);
+  }
   base = __shfl_sync(FULL_MASK, base, lane & ~7u);
   if (base == TSI_NONE) active = false;
   const uint32_t C = active ? base + k : 0u;
@@ -143,152 +404,45 @@ __device__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t
   Iv sens[4] = {iv(0.0f), iv(0.0f), iv(0.0f), iv(0.0f)};
   uint32_t rec = it.rec;
   TapeRec TR;
-  const bool any_eval = __any_sync(FULL_MASK, evaluate);
-  const bool any_deriv = __any_sync(FULL_MASK, take_deriv);
+  const uint32_t b_eval = __ballot_sync(FULL_MASK, evaluate);
+  const uint32_t b_rev = __ballot_sync(FULL_MASK, take_deriv);
+  const bool any_deriv = b_rev != 0;
   bool want_prune = false;
   float4 *lg = nullptr;
   uint2 *dg = nullptr;
 
-  if (any_eval) {
-    // ---- choose the most pruned tape valid for every evaluated cell
-    float tl = evaluate ? targ.lo : fm_inf();
-    float th = evaluate ? targ.hi : -fm_inf();
-    for (int o = 16; o > 0; o >>= 1) {
-      tl = fminf(tl, __shfl_xor_sync(FULL_MASK, tl, o));
-      th = fmaxf(th, __shfl_xor_sync(FULL_MASK, th, o));
-    }
-    TR = P.recs[rec];
-    while (TR.parent != TSI_NONE && !(TR.t_lo <= tl && th <= TR.t_hi)) {
-      rec = TR.parent;
-      TR = P.recs[rec];
-    }
-    const uint32_t root_rec = S.root_rec;
+  if (b_eval) {
+    // ---- the most pruned tape valid for every evaluated cell
+    const float tl = warp_min(evaluate ? targ.lo : fm_inf());
+    const float th = warp_max(evaluate ? targ.hi : -fm_inf());
+    find_valid(P, rec, TR, tl, th);
     for (int attempt = 0; attempt < 2; ++attempt) {
-      const uint32_t len = TR.len;
-      want_prune = (flags & SF_PRUNING) && len >= TSI_PRUNE_MIN_LEN && TR.nregs <= TSI_PRUNE_MAX_REGS;
+      want_prune = (flags & SF_PRUNING) && TR.len >= TSI_PRUNE_MIN_LEN && TR.nregs <= TSI_PRUNE_MAX_REGS;
       lg = nullptr;
       dg = nullptr;
       if (any_deriv || want_prune) {
-        if (len <= P.slice_len) {
-          lg = slice_log;
-          dg = slice_dec;
-        } else {
-          unsigned long long need = (unsigned long long)len * 32ull + ((unsigned long long)len + 1ull) / 2ull;
-          unsigned long long off = 0;
-          if (lane == 0) off = atomicAdd(P.log_overflow_used, need);
-          off = __shfl_sync(FULL_MASK, off, 0);
-          if (off + need > P.log_overflow_cap) {
-            if (lane == 0) atomicOr(P.error, EB_LOG_OOM);
-            return;
-          }
-          lg = P.log_overflow + off;
-          dg = reinterpret_cast<uint2 *>(P.log_overflow + off + (unsigned long long)len * 32ull);
-        }
+        float4 *lgs = nullptr;
+        uint2 *dgs = nullptr;
+        if (!item_scratch(P, TR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
+        lg = lgs;
+        dg = want_prune ? dgs : nullptr;
       }
-      // ---- forward pass (3633-3772)
-      st_reg(rf, 0, lane, cx);
-      st_reg(rf, 1, lane, cy);
-      st_reg(rf, 2, lane, cz);
-      st_reg(rf, 3, lane, targ);
-      const uint2 *code = TR.code;
-      uint32_t mm = 0;
-      uint32_t cost = 0;
-      for (uint32_t i = 0; i < len; ++i) {
-        const uint2 w = code[i];
-        const uint32_t h = TSI_W0_H(w.x);
-        const float lit = __uint_as_float(w.y);
-        const Iv Av = ld_reg(rf, TSI_W0_A(w.x), lane);
-        const Iv Bv = TSI_H_IS_II(h) ? ld_reg(rf, w.y & 255u, lane) : iv(lit);
-        const Iv r = A::forward(h, Av, Bv, lit);
-        if (any_deriv) lg[(size_t)i * 32u + lane] = make_float4(Av.lo, Av.hi, Bv.lo, Bv.hi);
-        if (want_prune && TSI_H_IS_MINMAX(h)) {
-          const bool amax = (h == H_MAX_II || h == H_MAX_IF);
-          const bool a_below = Av.hi < Bv.lo, b_below = Bv.hi < Av.lo;
-          const uint32_t ua = __ballot_sync(FULL_MASK, amax ? b_below : a_below);
-          const uint32_t ub = __ballot_sync(FULL_MASK, amax ? a_below : b_below);
-          if (lane == 0) dg[mm] = make_uint2(ua, ub);
-          ++mm;
-        }
-        st_reg(rf, TSI_W0_DST(w.x), lane, r);
-        cost += c_cost_fwd[h];
-      }
-      field = ld_reg(rf, TR.out_reg, lane);
-      {
-        const uint32_t ne = __popc(__ballot_sync(FULL_MASK, evaluate));
-        if (lane == 0) ws.v[ST_FP32] += (unsigned long long)(cost + TSI_FIX_COST * len) * ne;
-      }
-      // ---- reverse pass (3785-3964), sensitivities reuse the register file
+      field = forward_pass<D>(TR.code, TR.len, TR.out_reg, rf, lane, cx, cy, cz, targ, any_deriv ? lg : nullptr, dg);
       bool bad = false;
-      if (any_deriv) {
-        for (uint32_t r = 0; r < TR.nregs; ++r) st_reg(rf, r, lane, iv(0.0f));
-        st_reg(rf, TR.out_reg, lane, iv(1.0f));
-        uint32_t rcost = 0;
-        for (int i = (int)len - 1; i >= 0; --i) {
-          const uint2 w = code[i];
-          const uint32_t h = TSI_W0_H(w.x);
-          const uint32_t d = TSI_W0_DST(w.x), a = TSI_W0_A(w.x), b = w.y & 255u;
-          const float lit = __uint_as_float(w.y);
-          const float4 L = lg[(size_t)i * 32u + lane];
-          const Iv Av = Iv{L.x, L.y}, Bv = Iv{L.z, L.w};
-          const Iv s = ld_reg(rf, d, lane);
-          st_reg(rf, d, lane, iv(0.0f));
-          rcost += c_cost_rr[h] + TSI_REV_OPERAND_COST * TSI_H_NREG(h);
-          if (!take_deriv || h == H_CONST) {
-            bad |= take_deriv && !finite2(s);
-            continue;
-          }
-          bad |= !finite2(s);
-          const bool s0 = (s.lo == 0.0f && s.hi == 0.0f);
-          if (TSI_H_IS_II(h)) {
-            if (s0 && TSI_W0_FA(w.x) && TSI_W0_FB(w.x)) {
-              st_reg(rf, a, lane, iv(0.0f));
-              st_reg(rf, b, lane, iv(0.0f));
-            } else {
-              Iv r0, r1;
-              A::reverse_rule(h, Av, Bv, lit, r0, r1);
-              r0 = A::fix(r0);
-              r1 = A::fix(r1);
-              r0 = A::mul(r0, s);
-              r1 = A::mul(r1, s);
-              const Iv n0 = A::add(r0, ld_reg(rf, a, lane));
-              const Iv n1 = A::add(r1, ld_reg(rf, b, lane));
-              st_reg(rf, a, lane, n0);
-              st_reg(rf, b, lane, n1);
-              bad |= !finite2(n0) || !finite2(n1);
-            }
-          } else {
-            if (s0 && TSI_W0_FA(w.x)) {
-              st_reg(rf, a, lane, iv(0.0f));
-            } else {
-              Iv r0, r1;
-              A::reverse_rule(h, Av, Bv, lit, r0, r1);
-              r0 = A::fix(r0);
-              r0 = A::mul(r0, s);
-              const Iv n0 = A::add(r0, ld_reg(rf, a, lane));
-              st_reg(rf, a, lane, n0);
-              bad |= !finite2(n0);
-            }
-          }
-        }
-        for (int q = 0; q < 4; ++q) sens[q] = ld_reg(rf, q, lane);
-        const uint32_t nrev = __popc(__ballot_sync(FULL_MASK, take_deriv));
-        if (lane == 0) ws.v[ST_FP32] += (unsigned long long)rcost * nrev;
-      }
+      if (any_deriv) reverse_pass<D>(TR.code, TR.len, TR.nregs, TR.out_reg, rf, lane, lg, take_deriv, sens, bad);
       // a pruned tape whose sensitivities overflowed: redo on the full tape
       const bool redo = __any_sync(FULL_MASK, bad) && TR.parent != TSI_NONE;
       if (!redo) break;
-      rec = root_rec;
+      rec = S.root_rec;
       TR = P.recs[rec];
-      if (lane == 0) ws.v[ST_PRUNE_FALLBACK]++;
+      if (lane == 0) ws[ST_PRUNE_FALLBACK]++;
     }
-    {
-      const uint32_t ne = __popc(__ballot_sync(FULL_MASK, evaluate));
-      const uint32_t nr = __popc(__ballot_sync(FULL_MASK, take_deriv));
-      if (lane == 0) {
-        ws.v[ST_INSTR_FWD] += (unsigned long long)TR.len * ne;
-        ws.v[ST_INSTR_REV] += (unsigned long long)TR.len * nr;
-        ws.v[ST_INSTR_FULL] += (unsigned long long)S.full_len * ne;
-      }
+    if (lane == 0) {
+      const uint32_t ne = __popc(b_eval), nr = __popc(b_rev);
+      ws[ST_INSTR_FWD] += (unsigned long long)TR.len * ne;
+      ws[ST_INSTR_REV] += (unsigned long long)TR.len * nr;
+      ws[ST_INSTR_FULL] += (unsigned long long)S.full_len * ne;
+      ws[ST_FP32] += (unsigned long long)TR.fwd_cost * ne + (unsigned long long)TR.rev_cost * nr;
     }
   }
 
@@ -345,10 +499,11 @@ __device__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t
       if (!swept && c_child != TSI_NONE) {
         dealloc = true;
         dealloc_brick = c_child >> 3;
-        c_child = TSI_NONE;
       }
     }
   }
+  const uint32_t old_child = c_child;
+  if (dealloc) c_child = TSI_NONE;
   if (active) {
     pool.f[C] = c_f;
     pool.time_err[C] = c_te;
@@ -376,56 +531,57 @@ __device__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t
   const uint32_t E = (em >> (g * 8u)) & 0xffu;
   uint32_t new_rec = rec;
   if (em) {
+    // time range the children will be evaluated over: [child.t, time]
+    float nl = targ.lo, nh = targ.hi;
+    if (enq && old_child != TSI_NONE) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float ct = pool.t[old_child + q];
+        nl = fm_min(nl, fm_min(ct, S.time));
+        nh = fm_max(nh, fm_max(ct, S.time));
+      }
+    }
+    if (enq && swept) {  // swept children start their point-branch interval at t0
+      nl = fm_min(nl, fm_min(S.t0, S.time));
+      nh = fm_max(nh, fm_max(S.t0, S.time));
+    }
+    if (!enq) {
+      nl = fm_inf();
+      nh = -fm_inf();
+    }
+    const bool widen = enq && (nl < targ.lo || nh > targ.hi);
+    uint32_t prec = rec;  // record the group tapes are pruned from
+    TapeRec PR = TR;
+    if (want_prune && __any_sync(FULL_MASK, widen)) {
+      // decisions over the widened interval, from a tape valid there
+      const float wl = warp_min(nl), wh = warp_max(nh);
+      find_valid(P, prec, PR, wl, wh);
+      want_prune = (flags & SF_PRUNING) && PR.len >= TSI_PRUNE_MIN_LEN && PR.nregs <= TSI_PRUNE_MAX_REGS;
+      if (want_prune) {
+        float4 *lgs;
+        uint2 *dgs;
+        if (!item_scratch(P, PR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
+        lg = lgs;
+        dg = dgs;
+        const Iv tw = enq ? Iv{nl, nh} : targ;
+        (void)forward_pass<D>(PR.code, PR.len, PR.out_reg, rf, lane, cx, cy, cz, tw, nullptr, dg);
+        if (lane == 0) ws[ST_FP32] += (unsigned long long)PR.fwd_cost * __popc(em);
+      }
+    }
     // validity of the group's pruned tape: intersection of the enqueued
-    // siblings' time intervals
-    float gl = enq ? targ.lo : -fm_inf();
-    float gh = enq ? targ.hi : fm_inf();
+    // siblings' decision intervals
+    float gl = enq ? nl : -fm_inf();
+    float gh = enq ? nh : fm_inf();
     for (int o = 1; o < 8; o <<= 1) {
       gl = fmaxf(gl, __shfl_xor_sync(FULL_MASK, gl, o));
       gh = fminf(gh, __shfl_xor_sync(FULL_MASK, gh, o));
     }
-    uint32_t cnt = 0, mmk = 0;
+    uint32_t cnt = 0, mmk = 0, fcost = 0, rcost = 0;
     bool pruned = false;
-    uint2 *tmp = nullptr;
-    if (want_prune && lg != nullptr) tmp = reinterpret_cast<uint2 *>(lg) + (size_t)g * TR.len;
-    if (k == 0 && E != 0 && want_prune && tmp != nullptr) {
-      const uint2 *code = TR.code;
-      unsigned long long live = 1ull << TR.out_reg;
-      uint32_t m = TR.n_minmax;
-      for (int i = (int)TR.len - 1; i >= 0; --i) {
-        const uint2 w = code[i];
-        const uint32_t h = TSI_W0_H(w.x);
-        const uint32_t d = TSI_W0_DST(w.x), a = TSI_W0_A(w.x), b = w.y & 255u;
-        const bool mmx = TSI_H_IS_MINMAX(h);
-        uint2 dd = make_uint2(0u, 0u);
-        if (mmx) dd = dg[--m];
-        if (!((live >> d) & 1ull)) continue;
-        live &= ~(1ull << d);
-        uint2 out = w;
-        if (mmx) {
-          const uint32_t ga = (dd.x >> (g * 8u)) & 0xffu, gb = (dd.y >> (g * 8u)) & 0xffu;
-          if ((ga & E) == E) {
-            out = make_uint2(TSI_W0(H_COPY, TSI_W0_FA(w.x), 0u, d, a), 0u);
-            live |= 1ull << a;
-          } else if ((gb & E) == E) {
-            if (TSI_H_IS_II(h)) {
-              out = make_uint2(TSI_W0(H_COPY, TSI_W0_FB(w.x), 0u, d, b), 0u);
-              live |= 1ull << b;
-            } else {
-              out = make_uint2(TSI_W0(H_CONST, 0u, 0u, d, 0u), w.y);
-            }
-          } else {
-            live |= 1ull << a;
-            if (TSI_H_IS_II(h)) live |= 1ull << b;
-            ++mmk;
-          }
-        } else {
-          if (h != H_CONST) live |= 1ull << a;
-          if (TSI_H_IS_II(h)) live |= 1ull << b;
-        }
-        tmp[cnt++] = out;
-      }
-      pruned = cnt < TR.len;
+    uint2 *tmp = (want_prune && lg != nullptr) ? reinterpret_cast<uint2 *>(lg) + (size_t)g * PR.len : nullptr;
+    if (k == 0 && E != 0 && tmp != nullptr) {
+      cnt = prune_scan(PR.code, PR.len, PR.n_minmax, PR.out_reg, dg, g, E, tmp, mmk, fcost, rcost);
+      pruned = cnt < PR.len;
     }
     // reserve arena space and a record (lane 8g), then copy with the group
     unsigned long long off = 0;
@@ -447,17 +603,21 @@ __device__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t
         TapeRec nr;
         nr.code = P.code_arena + off;
         nr.len = cnt;
-        nr.nregs = TR.nregs;
-        nr.out_reg = TR.out_reg;
+        nr.nregs = PR.nregs;
+        nr.out_reg = PR.out_reg;
         nr.n_minmax = mmk;
         nr.t_lo = gl;
         nr.t_hi = gh;
-        nr.parent = rec;
+        nr.parent = prec;
+        nr.fwd_cost = fcost;
+        nr.rev_cost = rcost;
         nr.pad = 0;
         P.recs[ri] = nr;
-        ws.v[ST_TAPE_WORDS] += cnt;
+        atomicAdd(&ws[ST_TAPE_WORDS], (unsigned long long)cnt);
       }
       new_rec = ri;
+    } else if (E != 0 && want_prune) {
+      new_rec = prec;  // not pruned (or no arena room): the widened-valid tape
     }
     // next-level work items: ceil(n/4) per group
     uint32_t cb[8];
@@ -492,29 +652,28 @@ __device__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t
   }
 
   // ---- counters
-  const uint32_t b_eval = __ballot_sync(FULL_MASK, evaluate);
-  const uint32_t b_rev = __ballot_sync(FULL_MASK, take_deriv);
   const uint32_t b_skip = __ballot_sync(FULL_MASK, active && !evaluate);
   const uint32_t b_amb = __ballot_sync(FULL_MASK, cls == 0);
   const uint32_t b_emp = __ballot_sync(FULL_MASK, cls == 1);
   const uint32_t b_full = __ballot_sync(FULL_MASK, cls == 2);
   const uint32_t b_reu = __ballot_sync(FULL_MASK, reused);
   if (lane == 0) {
-    ws.v[ST_PARENTS] += it.n;
-    ws.v[ST_EVAL] += __popc(b_eval);
-    ws.v[ST_REVERSE] += __popc(b_rev);
-    ws.v[ST_SKIPPED] += __popc(b_skip);
-    ws.v[ST_AMBIG] += __popc(b_amb);
-    ws.v[ST_EMPTY] += __popc(b_emp);
-    ws.v[ST_FULL] += __popc(b_full);
-    ws.v[ST_ENQUEUED] += __popc(em);
-    ws.v[ST_REUSED] += __popc(b_reu);
+    ws[ST_PARENTS] += it.n;
+    ws[ST_EVAL] += __popc(b_eval);
+    ws[ST_REVERSE] += __popc(b_rev);
+    ws[ST_SKIPPED] += __popc(b_skip);
+    ws[ST_AMBIG] += __popc(b_amb);
+    ws[ST_EMPTY] += __popc(b_emp);
+    ws[ST_FULL] += __popc(b_full);
+    ws[ST_ENQUEUED] += __popc(em);
+    ws[ST_REUSED] += __popc(b_reu);
   }
 }
 
 // Recursive free of a dropped subtree (compute.wgsl:3533-3543, freeV
 // 3452-3460): 8 lanes per brick; children bricks go to the next level's list.
-__device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level, bool valid, WarpStats &ws) {
+__device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level, bool valid,
+                              unsigned long long *ws) {
   const uint32_t lane = threadIdx.x & 31u, k = lane & 7u;
   const SceneLaunch &S = P.scenes[valid ? item.x : 0];
   const VoxelPoolDev &pool = S.pool;
@@ -540,23 +699,25 @@ __device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level,
       else atomicOr(P.error, EB_QUEUE_FULL);
     }
   }
+  const uint32_t fm = __ballot_sync(FULL_MASK, valid && k == 0);
   if (valid && k == 0) {
     const uint32_t pos = atomicAdd(&S.ctr->pending_count, 1u);
     if (pos < pool.cap_bricks) pool.pending[pos] = item.y;
-    ws.v[ST_BRICK_FREE]++;
   }
+  if (lane == 0) ws[ST_BRICK_FREE] += __popc(fm);
 }
 
 __global__ void __launch_bounds__(256) refine_kernel(LaunchParams P, uint32_t level, uint32_t rcap) {
   extern __shared__ float2 smem_regs[];
+  __shared__ unsigned long long s_stats[kWarps][ST_COUNT];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
   float2 *rf = smem_regs + (size_t)wib * rcap * 32u;
   float4 *slice_log = P.log_slices + (size_t)gw * P.slice_len * 32u;
   uint2 *slice_dec = P.dec_slices + (size_t)gw * P.slice_len;
-  WarpStats ws;
-#pragma unroll
-  for (int i = 0; i < ST_COUNT; ++i) ws.v[i] = 0;
+  unsigned long long *ws = s_stats[wib];
+  if (lane < ST_COUNT) ws[lane] = 0;
+  __syncwarp();
 
   const uint32_t n_items = min(P.item_count[level], P.item_cap);
   const WorkItem *items = P.items[level & 1];
@@ -568,6 +729,7 @@ __global__ void __launch_bounds__(256) refine_kernel(LaunchParams P, uint32_t le
     const WorkItem it = items[idx];
     if (P.scenes[it.scene].flags & SF_DIRECTED) process_item<true>(P, it, level, rf, slice_log, slice_dec, ws);
     else process_item<false>(P, it, level, rf, slice_log, slice_dec, ws);
+    __syncwarp();
   }
   // deallocation items: 4 bricks per warp
   const uint32_t n_dealloc = min(P.dealloc_count[level], P.dealloc_cap);
@@ -582,9 +744,10 @@ __global__ void __launch_bounds__(256) refine_kernel(LaunchParams P, uint32_t le
     const uint2 item = valid ? dl[j] : make_uint2(0u, 0u);
     dealloc_brick(P, item, level, valid, ws);
   }
-  if (lane == 0) {
-    for (int i = 0; i < ST_COUNT; ++i)
-      if (ws.v[i]) atomicAdd(&P.stats[i], ws.v[i]);
+  __syncwarp();
+  if (lane < ST_COUNT && ws[lane]) {
+    atomicAdd(&P.stats[lane], ws[lane]);
+    atomicAdd(&P.level_stats[level * ST_COUNT + lane], ws[lane]);
   }
 }
 

@@ -95,6 +95,7 @@ bool compile_tape(const std::vector<IrInstr> &ins, PackedTape &out, tsi_status &
   }
   uint32_t maxreg = 3;
   static const uint32_t fwd_cost[H_COUNT] = TSI_OPCOST_FWD_INIT;
+  static const uint32_t rr_cost[H_COUNT] = TSI_OPCOST_RR_INIT;
   out.code.reserve(size_t(n - 4) * 2);
   for (uint32_t j = 4; j < n; ++j) {
     const IrInstr &in = ins[j];
@@ -141,6 +142,7 @@ bool compile_tape(const std::vector<IrInstr> &ins, PackedTape &out, tsi_status &
     out.code.push_back(w1);
     if (TSI_H_IS_MINMAX(h)) out.n_minmax++;
     out.fwd_cost += fwd_cost[h] + TSI_FIX_COST;
+    out.rev_cost += rr_cost[h] + TSI_REV_OPERAND_COST * TSI_H_NREG(h);
   }
   out.nregs = maxreg + 1;
   out.out_reg = reg[n - 1];

@@ -16,6 +16,7 @@ struct PackedTape {
   uint32_t out_reg = 0;        // register holding the field (slot count-1)
   uint32_t n_minmax = 0;
   uint64_t fwd_cost = 0;       // opcost.h, forward, one cell
+  uint64_t rev_cost = 0;       // opcost.h, reverse, one cell
   std::vector<uint32_t> slot_reg;  // register of every SSA slot (debug, tests)
 };
 

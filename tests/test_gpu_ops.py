@@ -183,9 +183,10 @@ def test_min_max_semantics(device):
     assert [np.signbit(v) for v in mn[:2]] == [True, True]
     assert [np.signbit(v) for v in mx[:2]] == [False, False]
     assert mn[2] == 1.0 and mn[3] == 1.0 and mx[2] == 1.0 and mx[3] == 1.0 and np.isnan(mn[6])
+    hw_mn, hw_mx = device.math(7, a, b), device.math(8, a, b)  # raw fminf / fmaxf
     lib = oracle.load()
     for i in range(len(a)):
-        for which, fn in ((5, lib.oracle_fmin), (6, lib.oracle_fmax)):
+        for which, fn in ((5, lib.oracle_fmin), (6, lib.oracle_fmax), (7, lib.oracle_fmin), (8, lib.oracle_fmax)):
             o = np.float32(fn(float(a[i]), float(b[i])))
-            g = (mn if which == 5 else mx)[i]
+            g = {5: mn, 6: mx, 7: hw_mn, 8: hw_mx}[which][i]
             assert (np.isnan(o) and np.isnan(g)) or (o == g and np.signbit(o) == np.signbit(g))
