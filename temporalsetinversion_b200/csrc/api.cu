@@ -96,6 +96,11 @@ struct tsi_tape {
   uint32_t len = 0;  // instructions after the 4 ARG slots
   uint32_t count = 0, nregs = 0, out_reg = 0, n_minmax = 0;
   uint64_t fwd_cost = 0, rev_cost = 0;
+  // bundled form for the wide path (absent when the tape is short)
+  uint4 *d_wslots = nullptr;
+  uint2 *d_wbundles = nullptr;
+  uint32_t *d_wmm = nullptr;
+  uint32_t wbundles = 0, wregs = 0, wout = 0, wmin_len = 0xffffffffu;
 };
 
 struct tsi_scene {
@@ -127,6 +132,11 @@ struct tsi_ctx {
   WorkItem *d_items[2] = {nullptr, nullptr};
   uint32_t item_cap = 0;
   uint32_t *d_item_count = nullptr, *d_item_cursor = nullptr;
+  WorkItem *d_witems[2] = {nullptr, nullptr};
+  uint32_t *d_witem_count = nullptr, *d_witem_cursor = nullptr;
+  uint2 *d_wide_dec = nullptr;
+  uint8_t *d_wide_flags = nullptr;
+  uint32_t wide_dec_stride = 0, wide_flag_stride = 0;
   uint2 *d_dealloc[2] = {nullptr, nullptr};
   uint32_t dealloc_cap = 0;
   uint32_t *d_dealloc_count = nullptr, *d_dealloc_cursor = nullptr;
@@ -186,6 +196,14 @@ LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes) {
   P.item_count = c->d_item_count;
   P.item_cursor = c->d_item_cursor;
   P.item_cap = c->item_cap;
+  P.witems[0] = c->d_witems[0];
+  P.witems[1] = c->d_witems[1];
+  P.witem_count = c->d_witem_count;
+  P.witem_cursor = c->d_witem_cursor;
+  P.wide_dec = c->d_wide_dec;
+  P.wide_flags = c->d_wide_flags;
+  P.wide_dec_stride = c->wide_dec_stride;
+  P.wide_flag_stride = c->wide_flag_stride;
   P.dealloc_cap = c->dealloc_cap;
   P.dealloc[0] = c->d_dealloc[0];
   P.dealloc[1] = c->d_dealloc[1];
@@ -232,6 +250,13 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, Scene
   L.root_rec = slot;
   L.levels = (uint32_t)p.localsubdiv;
   L.full_len = s->tape->len;
+  L.wide.slots = s->tape->d_wslots;
+  L.wide.bundles = s->tape->d_wbundles;
+  L.wide.narrow_mm = s->tape->d_wmm;
+  L.wide.nbundles = s->tape->wbundles;
+  L.wide.nregs = s->tape->wregs;
+  L.wide.out_reg = s->tape->wout;
+  L.wide.min_len = s->tape->wmin_len;
   R.code = s->tape->d_code;
   R.len = s->tape->len;
   R.nregs = s->tape->nregs;
@@ -249,11 +274,34 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, Scene
 tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *times, const float *t0s, uint32_t n) {
   if (n == 0) return TSI_OK;
   if (n > c->max_scenes) return set_err(TSI_ERR_INVALID_ARGUMENT, "too many scenes in one launch");
-  uint32_t lmax = 0, rmax = 4;
+  uint32_t lmax = 0, rmax = 4, mm_max = 1, slots_max = 8;
   for (uint32_t i = 0; i < n; ++i) {
     fill_launch(scenes[i], i, times[i], t0s[i], c->h_scenes[i], c->h_recs[i]);
     lmax = std::max(lmax, (uint32_t)scenes[i]->p.localsubdiv);
     rmax = std::max(rmax, scenes[i]->tape->nregs);
+    if (scenes[i]->tape->d_wslots) {
+      rmax = std::max(rmax, (scenes[i]->tape->wregs + 31u) / 32u);
+      mm_max = std::max(mm_max, scenes[i]->tape->n_minmax);
+      slots_max = std::max(slots_max, scenes[i]->tape->count);
+    }
+  }
+  {  // per-block scratch of the wide path
+    const uint32_t blocks = c->max_warps / kWarpsPerBlock;
+    const uint32_t dstride = (mm_max + 31u) & ~31u, fstride = (slots_max + 255u) & ~255u;
+    if (dstride > c->wide_dec_stride) {
+      cudaFree(c->d_wide_dec);
+      c->d_wide_dec = nullptr;
+      c->wide_dec_stride = 0;
+      CK(dalloc(&c->d_wide_dec, (size_t)blocks * dstride));
+      c->wide_dec_stride = dstride;
+    }
+    if (fstride > c->wide_flag_stride) {
+      cudaFree(c->d_wide_flags);
+      c->d_wide_flags = nullptr;
+      c->wide_flag_stride = 0;
+      CK(dalloc(&c->d_wide_flags, (size_t)blocks * fstride));
+      c->wide_flag_stride = fstride;
+    }
   }
   const uint32_t rcap = (rmax + 3u) & ~3u;
   const size_t smem = (size_t)kWarpsPerBlock * rcap * 32u * sizeof(float2);
@@ -630,6 +678,10 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   CKC(dalloc(&c->d_items[1], c->item_cap));
   CKC(dalloc(&c->d_item_count, TSI_MAX_LEVELS + 1));
   CKC(dalloc(&c->d_item_cursor, TSI_MAX_LEVELS + 1));
+  CKC(dalloc(&c->d_witems[0], c->item_cap));
+  CKC(dalloc(&c->d_witems[1], c->item_cap));
+  CKC(dalloc(&c->d_witem_count, TSI_MAX_LEVELS + 1));
+  CKC(dalloc(&c->d_witem_cursor, TSI_MAX_LEVELS + 1));
   CKC(dalloc(&c->d_dealloc[0], c->dealloc_cap));
   CKC(dalloc(&c->d_dealloc[1], c->dealloc_cap));
   CKC(dalloc(&c->d_dealloc_count, TSI_MAX_LEVELS + 1));
@@ -675,6 +727,12 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   cudaFree(c->d_items[1]);
   cudaFree(c->d_item_count);
   cudaFree(c->d_item_cursor);
+  cudaFree(c->d_witems[0]);
+  cudaFree(c->d_witems[1]);
+  cudaFree(c->d_witem_count);
+  cudaFree(c->d_witem_cursor);
+  cudaFree(c->d_wide_dec);
+  cudaFree(c->d_wide_flags);
   cudaFree(c->d_dealloc[0]);
   cudaFree(c->d_dealloc[1]);
   cudaFree(c->d_dealloc_count);
@@ -728,6 +786,31 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
       return TSI_ERR_CUDA;
     }
   }
+  // bundled form for long tapes (the wide path pays off once a tape has
+  // several times more instructions than bundles)
+  if (t->len >= 256) {
+    WideTape wt;
+    if (compile_wide(ins, pt, wt, st, why) && wt.nbundles > 0 && wt.nregs <= 32u * 255u) {
+      cudaError_t e = dalloc(&t->d_wslots, wt.slots.size() / 4);
+      if (e == cudaSuccess) e = dalloc(&t->d_wbundles, wt.bundles.size() / 2);
+      if (e == cudaSuccess) e = dalloc(&t->d_wmm, wt.narrow_mm.size());
+      if (e == cudaSuccess)
+        e = cudaMemcpy(t->d_wslots, wt.slots.data(), wt.slots.size() * 4, cudaMemcpyHostToDevice);
+      if (e == cudaSuccess)
+        e = cudaMemcpy(t->d_wbundles, wt.bundles.data(), wt.bundles.size() * 4, cudaMemcpyHostToDevice);
+      if (e == cudaSuccess)
+        e = cudaMemcpy(t->d_wmm, wt.narrow_mm.data(), wt.narrow_mm.size() * 4, cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        g_last_error = cudaGetErrorString(e);
+        tsi_tape_destroy(t);
+        return TSI_ERR_CUDA;
+      }
+      t->wbundles = wt.nbundles;
+      t->wregs = wt.nregs;
+      t->wout = wt.out_reg;
+      t->wmin_len = std::max<uint32_t>(256u, 3u * wt.nbundles);
+    }
+  }
   *out = t;
   return TSI_OK;
 }
@@ -766,6 +849,9 @@ TSI_API void tsi_tape_destroy(tsi_tape *t) {
   if (!t) return;
   if (t->ctx) t->ctx->tapes.erase(t);
   cudaFree(t->d_code);
+  cudaFree(t->d_wslots);
+  cudaFree(t->d_wbundles);
+  cudaFree(t->d_wmm);
   delete t;
 }
 

@@ -58,7 +58,20 @@ struct SceneCounters {
   uint32_t live_bricks;
 };
 
+// Bundled form of a scene's full tape (tape_compile.h WideTape), evaluated
+// with one warp per cell for items whose tape is long.
+struct WideDev {
+  const uint4 *slots;         // 2 x uint4 per slot
+  const uint2 *bundles;       // slot offset, count | max_round << 16
+  const uint32_t *narrow_mm;  // min/max ordinal per narrow instruction
+  uint32_t nbundles;
+  uint32_t nregs;
+  uint32_t out_reg;           // wide register of the field
+  uint32_t min_len;           // tapes at least this long go to the wide path
+};
+
 struct SceneLaunch {
+  WideDev wide;
   VoxelPoolDev pool;
   SceneCounters *ctr;
   float eps;          // 10 * 2^-localsubdiv
@@ -111,6 +124,13 @@ struct LaunchParams {
   WorkItem *items[2];
   uint32_t *item_count;    // [TSI_MAX_LEVELS + 1]
   uint32_t *item_cursor;   // [TSI_MAX_LEVELS + 1]
+  WorkItem *witems[2];     // wide items: one parent each, one block per item
+  uint32_t *witem_count;   // [TSI_MAX_LEVELS + 1]
+  uint32_t *witem_cursor;  // [TSI_MAX_LEVELS + 1]
+  uint2 *wide_dec;         // per block: branch ballots of the 8 cells, [wide_dec_stride]
+  uint32_t wide_dec_stride;
+  uint32_t wide_flag_stride;
+  uint8_t *wide_flags;     // per block: liveness flags, [wide_flag_stride]
   uint32_t item_cap;
   uint32_t dealloc_cap;
   uint2 *dealloc[2];       // (scene, brick)

@@ -623,7 +623,27 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     uint32_t cb[8];
 #pragma unroll
     for (int b2 = 0; b2 < 8; ++b2) cb[b2] = __shfl_sync(FULL_MASK, C, gl0 + b2);
-    if (k == 0 && E != 0) {
+    const uint32_t next_len = (new_rec == prec) ? PR.len : ((new_rec == rec) ? TR.len : cnt);
+    if (k == 0 && E != 0 && next_len >= S.wide.min_len) {  // long tape: wide path, one item per child
+      const uint32_t n = __popc(E);
+      const uint32_t pos = atomicAdd(&P.witem_count[level + 1], n);
+      if (pos + n > P.item_cap) {
+        atomicOr(P.error, EB_QUEUE_FULL);
+      } else {
+        uint32_t e = E, j = 0;
+        while (e) {
+          const uint32_t bit = __ffs(e) - 1u;
+          e &= e - 1u;
+          WorkItem wi;
+          wi.scene = it.scene;
+          wi.rec = new_rec;
+          wi.n = 1;
+          wi.level = level + 1;
+          wi.parent[0] = wi.parent[1] = wi.parent[2] = wi.parent[3] = cb[bit];
+          P.witems[(level + 1) & 1][pos + j++] = wi;
+        }
+      }
+    } else if (k == 0 && E != 0) {
       const uint32_t n = __popc(E);
       const uint32_t nitems = (n + 3u) >> 2;
       const uint32_t pos = atomicAdd(&P.item_count[level + 1], nitems);
@@ -707,6 +727,552 @@ __device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level,
   if (lane == 0) ws[ST_BRICK_FREE] += __popc(fm);
 }
 
+// ======================================================================
+// Wide path: one block per parent, one warp per child cell, one lane per
+// instruction of a bundle (tape_compile.h WideTape).  Long tapes at the top
+// of the octree leave the narrow path latency bound (few items, thousands of
+// dependent instructions each); here a cell takes one step per bundle.
+// The reverse pass applies, bundle by bundle, the accumulations into each
+// sensitivity register in the sequential order (rounds), so the results
+// are those of the narrow path bit for bit.
+
+__device__ __forceinline__ void wide_slot(const WideDev &W, uint32_t si, uint32_t &h, uint32_t &fa, uint32_t &fb,
+                                          uint32_t &dst, uint32_t &a, uint32_t &b, uint32_t &round, float &lit) {
+  const uint4 s0 = W.slots[2u * si];
+  h = s0.x & 63u;
+  fa = (s0.x >> 6) & 1u;
+  fb = (s0.x >> 7) & 1u;
+  dst = s0.y & 0xffffu;
+  a = s0.y >> 16;
+  b = s0.z & 0xffffu;
+  round = s0.z >> 16;
+  lit = __uint_as_float(s0.w);
+}
+
+template <bool D>
+__device__ Iv wide_forward(const WideDev &W, float2 *rfw, uint32_t lane, Iv x, Iv y, Iv z, Iv t, float4 *lg,
+                           uint2 *dec, uint32_t cellbit) {
+  if (lane == 0) {
+    rfw[0] = make_float2(x.lo, x.hi);
+    rfw[1] = make_float2(y.lo, y.hi);
+    rfw[2] = make_float2(z.lo, z.hi);
+    rfw[3] = make_float2(t.lo, t.hi);
+  }
+  __syncwarp();
+  for (uint32_t k = 0; k < W.nbundles; ++k) {
+    const uint2 bt = W.bundles[k];
+    const bool act = lane < (bt.y & 0xffffu);
+    Iv r = iv(0.0f);
+    uint32_t dst = 0;
+    if (act) {
+      uint32_t h, fa, fb, a, b, round;
+      float lit;
+      wide_slot(W, bt.x + lane, h, fa, fb, dst, a, b, round, lit);
+      const float2 av = rfw[a];
+      const Iv A = Iv{av.x, av.y};
+      Iv B = iv(lit);
+      if (TSI_H_IS_II(h)) {
+        const float2 bv = rfw[b];
+        B = Iv{bv.x, bv.y};
+      }
+      r = op_forward<D>(h, A, B, lit);
+      if (lg) lg[(size_t)k * 32u + lane] = make_float4(A.lo, A.hi, B.lo, B.hi);
+      if (dec && TSI_H_IS_MINMAX(h)) {
+        const uint32_t mm = W.slots[2u * (bt.x + lane) + 1u].w;
+        const bool amax = (h == H_MAX_II || h == H_MAX_IF);
+        const bool a_below = A.hi < B.lo, b_below = B.hi < A.lo;
+        if (amax ? b_below : a_below) atomicOr(&dec[mm].x, cellbit);
+        if (amax ? a_below : b_below) atomicOr(&dec[mm].y, cellbit);
+      }
+    }
+    __syncwarp();
+    if (act) rfw[dst] = make_float2(r.lo, r.hi);
+    __syncwarp();
+  }
+  const float2 f = rfw[W.out_reg];
+  __syncwarp();
+  return Iv{f.x, f.y};
+}
+
+template <bool D>
+__device__ void wide_reverse(const WideDev &W, float2 *rfw, uint32_t lane, const float4 *lg, Iv sens[4]) {
+  using I = IA<D>;
+  for (uint32_t r = lane; r < W.nregs; r += 32u) rfw[r] = make_float2(0.0f, 0.0f);
+  __syncwarp();
+  if (lane == 0) rfw[W.out_reg] = make_float2(1.0f, 1.0f);
+  __syncwarp();
+  for (int k = (int)W.nbundles - 1; k >= 0; --k) {
+    const uint2 bt = W.bundles[k];
+    const bool act = lane < (bt.y & 0xffffu);
+    const uint32_t maxr = bt.y >> 16;
+    uint32_t h = H_CONST, fa = 0, fb = 0, dst = 0, a = 0, b = 0, round = 0;
+    float lit = 0.0f;
+    Iv A = iv(0.0f), B = iv(0.0f), s = iv(0.0f);
+    if (act) {
+      wide_slot(W, bt.x + lane, h, fa, fb, dst, a, b, round, lit);
+      const float4 L = lg[(size_t)k * 32u + lane];
+      A = Iv{L.x, L.y};
+      B = Iv{L.z, L.w};
+      const float2 sv = rfw[dst];
+      s = Iv{sv.x, sv.y};
+    }
+    __syncwarp();
+    if (act) rfw[dst] = make_float2(0.0f, 0.0f);
+    __syncwarp();
+    const bool II = TSI_H_IS_II(h);
+    bool skip = false;
+    Iv c0 = iv(0.0f), c1 = iv(0.0f);
+    if (act && h != H_CONST) {
+      const bool s0 = (s.lo == 0.0f && s.hi == 0.0f);
+      skip = II ? (s0 && fa && fb) : (s0 && fa);
+      if (!skip) {
+        Iv r0, r1;
+        op_reverse_rule<D>(h, A, B, lit, r0, r1);
+        c0 = I::mul(I::fix(r0), s);
+        if (II) c1 = I::mul(I::fix(r1), s);
+      }
+    }
+    for (uint32_t rd = 0; rd <= maxr; ++rd) {
+      if (act && h != H_CONST && round == rd) {
+        if (II) {
+          if (skip) {
+            rfw[a] = make_float2(0.0f, 0.0f);
+            rfw[b] = make_float2(0.0f, 0.0f);
+          } else {
+            const float2 pa = rfw[a], pb = rfw[b];
+            const Iv n0 = I::add(c0, Iv{pa.x, pa.y});
+            const Iv n1 = I::add(c1, Iv{pb.x, pb.y});
+            rfw[a] = make_float2(n0.lo, n0.hi);
+            rfw[b] = make_float2(n1.lo, n1.hi);
+          }
+        } else if (skip) {
+          rfw[a] = make_float2(0.0f, 0.0f);
+        } else {
+          const float2 pa = rfw[a];
+          const Iv n0 = I::add(c0, Iv{pa.x, pa.y});
+          rfw[a] = make_float2(n0.lo, n0.hi);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  for (int q = 0; q < 4; ++q) {
+    const float2 v = rfw[q];
+    sens[q] = Iv{v.x, v.y};
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *scratch, uint32_t &total) {
+  const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULL_MASK, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) scratch[wib] = x;
+  __syncthreads();
+  uint32_t base = 0, tot = 0;
+  for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) {
+    if (w < wib) base += scratch[w];
+    tot += scratch[w];
+  }
+  __syncthreads();
+  total = tot;
+  return base + x - v;
+}
+
+struct WideShared {
+  uint32_t base, is_new, E, widen, cnt, mmk, fcost, rcost, ri;
+  unsigned long long off;
+  float nl[kWarps], nh[kWarps];
+  uint32_t scan[kWarps];
+};
+
+template <bool D>
+__device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem &it, uint32_t level, float2 *rfw,
+                                          float4 *slice_log, uint2 *dec, uint8_t *flags, WideShared &sh,
+                                          unsigned long long *ws) {
+  using A = IA<D>;
+  const uint32_t lane = threadIdx.x & 31u, k = threadIdx.x >> 5;  // warp = octant
+  const SceneLaunch &S = P.scenes[it.scene];
+  const VoxelPoolDev &pool = S.pool;
+  const WideDev &W = S.wide;
+  const uint32_t flg = S.flags;
+  const bool swept = (flg & SF_SWEPT) != 0;
+  const uint32_t Pv = it.parent[0];
+  const TapeRec root = P.recs[S.root_rec];
+  const uint32_t n_narrow = root.len;
+
+  if (threadIdx.x == 0) {
+    const uint32_t pc = pool.child[Pv];
+    sh.is_new = pc == TSI_NONE;
+    sh.base = pc;
+    if (sh.is_new) {
+      sh.base = alloc_brick(S, P.error);
+      if (sh.base != TSI_NONE) {
+        pool.child[Pv] = sh.base;
+        ws[ST_BRICK_ALLOC]++;
+      }
+    }
+    sh.E = 0;
+    sh.widen = 0;
+  }
+  for (uint32_t i = threadIdx.x; i < root.n_minmax; i += blockDim.x) dec[i] = make_uint2(0u, 0u);
+  __syncthreads();
+  const uint32_t base = sh.base;
+  const bool new_voxel = sh.is_new != 0;
+  if (base == TSI_NONE) return;  // pool exhausted (error bit set)
+  const uint32_t C = base + k;
+
+  // ---- cell setup (compute.wgsl:3582-3626), uniform across the warp
+  const float4 pxy = pool.box_xy[Pv];
+  const float2 pz = pool.box_z[Pv];
+  const float pfast = pool.fast[Pv];
+  float c_t = 0.0f, c_f = 1.0f, c_te = 0.0f, c_fast = 0.0f;
+  uint32_t c_child = TSI_NONE;
+  if (!new_voxel) {
+    c_t = pool.t[C];
+    c_f = pool.f[C];
+    c_te = pool.time_err[C];
+    c_fast = pool.fast[C];
+    c_child = pool.child[C];
+  }
+  __syncwarp();
+  if (new_voxel && lane == 0) {
+    pool.child[C] = TSI_NONE;
+    pool.normal[C] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+  const float dx = __fdiv_rn(__fsub_rn(pxy.y, pxy.x), 2.0f);
+  const float dy = __fdiv_rn(__fsub_rn(pxy.w, pxy.z), 2.0f);
+  const float dz = __fdiv_rn(__fsub_rn(pz.y, pz.x), 2.0f);
+  float width = fm_max(dx, fm_max(dy, dz));
+  const float kx = (float)(k & 1u), ky = (float)((k >> 1) & 1u), kz = (float)(k >> 2);
+  Iv cx = Iv{__fadd_rn(pxy.x, __fmul_rn(dx, kx)), __fadd_rn(pxy.x, __fmul_rn(dx, 1.0f + kx))};
+  Iv cy = Iv{__fadd_rn(pxy.z, __fmul_rn(dy, ky)), __fadd_rn(pxy.z, __fmul_rn(dy, 1.0f + ky))};
+  Iv cz = Iv{__fadd_rn(pz.x, __fmul_rn(dz, kz)), __fadd_rn(pz.x, __fmul_rn(dz, 1.0f + kz))};
+  const bool point_branch = new_voxel || pfast == 1.0f || width <= S.eps;
+  Iv cur_t;
+  if (point_branch) {
+    cur_t = swept ? Iv{S.t0, S.time} : iv(S.time);
+    c_fast = 0.0f;
+  } else {
+    cur_t = Iv{c_t, S.time};
+  }
+  if (lane == 0) {
+    pool.box_xy[C] = make_float4(cx.lo, cx.hi, cy.lo, cy.hi);
+    pool.box_z[C] = make_float2(cz.lo, cz.hi);
+    pool.t[C] = S.time;
+  }
+  if ((flg & SF_POINTSAMPLE) && width <= S.eps) {
+    cx = iv(__fdiv_rn(__fadd_rn(cx.lo, cx.hi), 2.0f));
+    cy = iv(__fdiv_rn(__fadd_rn(cy.lo, cy.hi), 2.0f));
+    cz = iv(__fdiv_rn(__fadd_rn(cz.lo, cz.hi), 2.0f));
+    width = 0.0f;
+  }
+  const Iv targ = Iv{fm_min(cur_t.lo, cur_t.hi), fm_max(cur_t.lo, cur_t.hi)};
+  const bool evaluate = new_voxel || c_f >= 0.0f || c_child == TSI_NONE;
+  const bool take_deriv = evaluate && ((cur_t.lo != cur_t.hi) || (flg & SF_ALWAYS_DERIV));
+  const bool want_prune = (flg & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS;
+
+  // ---- forward and reverse over the full tape, bundle by bundle
+  Iv field = iv(0.0f);
+  Iv sens[4] = {iv(0.0f), iv(0.0f), iv(0.0f), iv(0.0f)};
+  float4 *lg = nullptr;
+  bool ok = true;
+  if (take_deriv) {
+    if (W.nbundles <= P.slice_len) {
+      lg = slice_log;
+    } else {
+      const unsigned long long need = (unsigned long long)W.nbundles * 32ull;
+      unsigned long long off = 0;
+      if (lane == 0) off = atomicAdd(P.log_overflow_used, need);
+      off = __shfl_sync(FULL_MASK, off, 0);
+      if (off + need > P.log_overflow_cap) {
+        if (lane == 0) atomicOr(P.error, EB_LOG_OOM);
+        ok = false;
+      } else {
+        lg = P.log_overflow + off;
+      }
+    }
+  }
+  if (evaluate && ok) {
+    field = wide_forward<D>(W, rfw, lane, cx, cy, cz, targ, lg, want_prune ? dec : nullptr, 1u << k);
+    if (take_deriv) wide_reverse<D>(W, rfw, lane, lg, sens);
+  }
+
+  // ---- temporal error bound, fast flag, classification (3966-4045)
+  Iv df = iv(0.0f), df_dt = iv(0.0f);
+  const float delta = S.delta;
+  if (take_deriv && ok) {
+    const float nx = __fdiv_rn(__fadd_rn(sens[0].lo, sens[0].hi), 2.0f);
+    const float ny = __fdiv_rn(__fadd_rn(sens[1].lo, sens[1].hi), 2.0f);
+    const float nz = __fdiv_rn(__fadd_rn(sens[2].lo, sens[2].hi), 2.0f);
+    if (lane == 0) pool.normal[C] = make_float4(nx, ny, nz, 0.0f);
+    df_dt = sens[3];
+    const float dt = __fsub_rn(targ.hi, targ.lo);
+    df = A::mul_f(df_dt, dt);
+    const Iv Wd = A::mul_f(Iv{-1.0f, 1.0f}, __fsub_rn(field.hi, field.lo));
+    df = A::cap(df, Wd);
+    if ((flg & SF_LIPSCHITZ) && A::abs_(df).hi != 0.0f) {
+      const float lb =
+          A::abs_(A::sqrt_(A::add(A::sqr(sens[0]), A::add(A::sqr(sens[1]), A::sqr(sens[2]))))).lo;
+      if (!is_nan_f(lb)) df = A::div(df, iv(lb));
+    }
+    if (df.lo == -fm_inf() || df.hi == fm_inf() || is_nan_f(df.lo) || is_nan_f(df.hi)) df = iv(delta);
+    c_te = __fadd_rn(c_te, fm_min(fm_max(A::abs_(df).hi, 0.0f), delta));
+  }
+  if (evaluate && !swept && (flg & SF_FASTENABLED)) c_fast = (A::abs_(df).hi >= S.fast_thresh) ? 1.0f : 0.0f;
+  bool enq = false, dealloc = false, reused = false;
+  int cls = 3;
+  if (evaluate && ok) {
+    if (field.lo <= 0.0f && 0.0f <= field.hi) {
+      c_f = 0.0f;
+      cls = 0;
+      if (width > S.eps) {
+        if (new_voxel || is_nan_f(df_dt.lo) || is_nan_f(df_dt.hi) || fabsf(df_dt.lo) == fm_inf() ||
+            fabsf(df_dt.hi) == fm_inf() || pfast == 1.0f || cur_t.lo == cur_t.hi || c_te >= delta ||
+            c_child == TSI_NONE) {
+          c_te = 0.0f;
+          enq = true;
+        } else {
+          reused = true;
+        }
+      }
+    } else {
+      if (field.hi <= 0.0f) {
+        c_f = -1.0f;
+        cls = 2;
+      } else {
+        cls = 1;
+        if (!swept) c_f = 1.0f;
+      }
+      if (!swept && c_child != TSI_NONE) dealloc = true;
+    }
+  }
+  const uint32_t old_child = c_child;
+  if (dealloc) c_child = TSI_NONE;
+  if (lane == 0) {
+    pool.f[C] = c_f;
+    pool.time_err[C] = c_te;
+    pool.fast[C] = c_fast;
+    if (dealloc || new_voxel) pool.child[C] = c_child;
+    if (dealloc) {
+      const uint32_t pos = atomicAdd(&P.dealloc_count[level + 1], 1u);
+      if (pos < P.dealloc_cap) P.dealloc[(level + 1) & 1][pos] = make_uint2(it.scene, old_child >> 3);
+      else atomicOr(P.error, EB_QUEUE_FULL);
+    }
+    if (enq) atomicOr(&sh.E, 1u << k);
+    atomicAdd(&ws[ST_EVAL], evaluate ? 1ull : 0ull);
+    atomicAdd(&ws[ST_REVERSE], take_deriv ? 1ull : 0ull);
+    atomicAdd(&ws[ST_SKIPPED], evaluate ? 0ull : 1ull);
+    if (cls == 0) atomicAdd(&ws[ST_AMBIG], 1ull);
+    if (cls == 1) atomicAdd(&ws[ST_EMPTY], 1ull);
+    if (cls == 2) atomicAdd(&ws[ST_FULL], 1ull);
+    if (enq) atomicAdd(&ws[ST_ENQUEUED], 1ull);
+    if (reused) atomicAdd(&ws[ST_REUSED], 1ull);
+    if (evaluate) {
+      atomicAdd(&ws[ST_INSTR_FWD], (unsigned long long)n_narrow);
+      atomicAdd(&ws[ST_INSTR_FULL], (unsigned long long)S.full_len);
+      atomicAdd(&ws[ST_FP32], (unsigned long long)root.fwd_cost + (take_deriv ? root.rev_cost : 0u));
+    }
+    if (take_deriv) atomicAdd(&ws[ST_INSTR_REV], (unsigned long long)n_narrow);
+  }
+  // time range the children will be evaluated over
+  float nl = targ.lo, nh = targ.hi;
+  if (enq && old_child != TSI_NONE) {
+    for (int q = 0; q < 8; ++q) {
+      const float ct = pool.t[old_child + q];
+      nl = fm_min(nl, fm_min(ct, S.time));
+      nh = fm_max(nh, fm_max(ct, S.time));
+    }
+  }
+  if (enq && swept) {
+    nl = fm_min(nl, fm_min(S.t0, S.time));
+    nh = fm_max(nh, fm_max(S.t0, S.time));
+  }
+  if (lane == 0) {
+    sh.nl[k] = enq ? nl : -fm_inf();
+    sh.nh[k] = enq ? nh : fm_inf();
+    if (enq && (nl < targ.lo || nh > targ.hi)) atomicOr(&sh.widen, 1u);
+  }
+  __syncthreads();
+  const uint32_t E = sh.E;
+  if (E == 0) return;
+  if (lane == 0 && k == 0) ws[ST_PARENTS] += 1;
+
+  uint32_t new_rec = S.root_rec;
+  if (want_prune) {
+    if (sh.widen) {  // decisions over the children's (wider) time range
+      for (uint32_t i = threadIdx.x; i < root.n_minmax; i += blockDim.x) dec[i] = make_uint2(0u, 0u);
+      __syncthreads();
+      if (enq) (void)wide_forward<D>(W, rfw, lane, cx, cy, cz, Iv{nl, nh}, nullptr, dec, 1u << k);
+      if (lane == 0 && enq) atomicAdd(&ws[ST_FP32], (unsigned long long)root.fwd_cost);
+      __syncthreads();
+    }
+    // liveness from the field backwards, by bundles (warp 0)
+    for (uint32_t i = threadIdx.x; i < root.len + 4u; i += blockDim.x) flags[i] = 0;
+    __syncthreads();
+    if (k == 0) {
+      if (lane == 0) flags[root.len + 3u] = 1;
+      __syncwarp();
+      for (int kb = (int)W.nbundles - 1; kb >= 0; --kb) {
+        const uint2 bt = W.bundles[kb];
+        if (lane < (bt.y & 0xffffu)) {
+          const uint32_t si = bt.x + lane;
+          const uint4 s1 = W.slots[2u * si + 1u];
+          if (flags[s1.x]) {
+            const uint32_t h = W.slots[2u * si].x & 63u;
+            bool la = s1.y != TSI_NONE, lb = s1.z != TSI_NONE;
+            if (TSI_H_IS_MINMAX(h)) {
+              const uint2 d = dec[s1.w];
+              if ((d.x & E) == E) lb = false;
+              else if ((d.y & E) == E) { la = false; }
+            }
+            if (la) flags[s1.y] = 1;
+            if (lb) flags[s1.z] = 1;
+          }
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    // compaction of the narrow full tape in program order
+    const uint32_t per = (n_narrow + blockDim.x - 1) / blockDim.x;
+    const uint32_t i0 = min(n_narrow, threadIdx.x * per), i1 = min(n_narrow, i0 + per);
+    uint32_t mine = 0;
+    for (uint32_t i = i0; i < i1; ++i) mine += flags[i + 4u];
+    uint32_t total = 0;
+    const uint32_t pos0 = block_exclusive_scan(mine, sh.scan, total);
+    if (threadIdx.x == 0) {
+      sh.ri = TSI_NONE;
+      sh.off = 0;
+      sh.cnt = total;
+      sh.mmk = 0;
+      sh.fcost = 0;
+      sh.rcost = 0;
+      if (total < n_narrow) {
+        const unsigned long long off = atomicAdd(P.code_count, (unsigned long long)total);
+        if (off + total <= P.code_cap) {
+          const uint32_t ri = atomicAdd(P.rec_count, 1u);
+          if (ri < P.rec_cap) {
+            sh.ri = ri;
+            sh.off = off;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (sh.ri != TSI_NONE) {
+      uint32_t p = pos0, mmk = 0, fc = 0, rc = 0;
+      for (uint32_t i = i0; i < i1; ++i) {
+        if (!flags[i + 4u]) continue;
+        const uint2 w = root.code[i];
+        const uint32_t h = TSI_W0_H(w.x);
+        uint2 out = w;
+        uint32_t hk = h;
+        if (TSI_H_IS_MINMAX(h)) {
+          const uint2 d = dec[W.narrow_mm[i]];
+          const uint32_t dd = TSI_W0_DST(w.x);
+          if ((d.x & E) == E) {
+            out = make_uint2(TSI_W0(H_COPY, TSI_W0_FA(w.x), 0u, dd, TSI_W0_A(w.x)), 0u);
+            hk = H_COPY;
+          } else if ((d.y & E) == E) {
+            if (TSI_H_IS_II(h)) {
+              out = make_uint2(TSI_W0(H_COPY, TSI_W0_FB(w.x), 0u, dd, w.y & 255u), 0u);
+              hk = H_COPY;
+            } else {
+              out = make_uint2(TSI_W0(H_CONST, 0u, 0u, dd, 0u), w.y);
+              hk = H_CONST;
+            }
+          } else {
+            ++mmk;
+          }
+        }
+        fc += c_cost_fwd[hk] + TSI_FIX_COST;
+        rc += c_cost_rr[hk] + TSI_REV_OPERAND_COST * TSI_H_NREG(hk);
+        P.code_arena[sh.off + p] = out;
+        ++p;
+      }
+      atomicAdd(&sh.mmk, mmk);
+      atomicAdd(&sh.fcost, fc);
+      atomicAdd(&sh.rcost, rc);
+    }
+    __syncthreads();
+    if (sh.ri != TSI_NONE) {
+      if (threadIdx.x == 0) {
+        float gl = -fm_inf(), gh = fm_inf();
+        for (int q = 0; q < kWarps; ++q) {
+          gl = fmaxf(gl, sh.nl[q]);
+          gh = fminf(gh, sh.nh[q]);
+        }
+        TapeRec nr;
+        nr.code = P.code_arena + sh.off;
+        nr.len = sh.cnt;
+        nr.nregs = root.nregs;
+        nr.out_reg = root.out_reg;
+        nr.n_minmax = sh.mmk;
+        nr.t_lo = gl;
+        nr.t_hi = gh;
+        nr.parent = S.root_rec;
+        nr.fwd_cost = sh.fcost;
+        nr.rev_cost = sh.rcost;
+        nr.pad = 0;
+        P.recs[sh.ri] = nr;
+        ws[ST_TAPE_WORDS] += sh.cnt;
+      }
+      new_rec = sh.ri;
+    }
+  }
+  // ---- next-level items for the enqueued children
+  if (threadIdx.x == 0) {
+    const uint32_t len = (new_rec == S.root_rec) ? root.len : sh.cnt;
+    const uint32_t n = __popc(E);
+    if (len >= W.min_len) {  // stay on the wide path: one item per child
+      const uint32_t pos = atomicAdd(&P.witem_count[level + 1], n);
+      if (pos + n > P.item_cap) {
+        atomicOr(P.error, EB_QUEUE_FULL);
+      } else {
+        uint32_t e = E, j = 0;
+        while (e) {
+          const uint32_t bit = __ffs(e) - 1u;
+          e &= e - 1u;
+          WorkItem wi;
+          wi.scene = it.scene;
+          wi.rec = new_rec;
+          wi.n = 1;
+          wi.level = level + 1;
+          wi.parent[0] = wi.parent[1] = wi.parent[2] = wi.parent[3] = base + bit;
+          P.witems[(level + 1) & 1][pos + j++] = wi;
+        }
+      }
+    } else {
+      const uint32_t nitems = (n + 3u) >> 2;
+      const uint32_t pos = atomicAdd(&P.item_count[level + 1], nitems);
+      if (pos + nitems > P.item_cap) {
+        atomicOr(P.error, EB_QUEUE_FULL);
+      } else {
+        uint32_t e = E;
+        for (uint32_t j = 0; j < nitems; ++j) {
+          WorkItem wi;
+          wi.scene = it.scene;
+          wi.rec = new_rec;
+          wi.level = level + 1;
+          uint32_t c = 0;
+          while (e && c < 4u) {
+            const uint32_t bit = __ffs(e) - 1u;
+            e &= e - 1u;
+            wi.parent[c++] = base + bit;
+          }
+          wi.n = c;
+          for (uint32_t q = c; q < 4u; ++q) wi.parent[q] = wi.parent[0];
+          P.items[(level + 1) & 1][pos + j] = wi;
+        }
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256) refine_kernel(LaunchParams P, uint32_t level, uint32_t rcap) {
   extern __shared__ float2 smem_regs[];
   __shared__ unsigned long long s_stats[kWarps][ST_COUNT];
@@ -718,6 +1284,28 @@ __global__ void __launch_bounds__(256) refine_kernel(LaunchParams P, uint32_t le
   unsigned long long *ws = s_stats[wib];
   if (lane < ST_COUNT) ws[lane] = 0;
   __syncwarp();
+
+  // wide items: the whole block per parent
+  {
+    __shared__ WideShared sh;
+    __shared__ uint32_t s_idx;
+    const uint32_t n_w = min(P.witem_count[level], P.item_cap);
+    uint2 *dec = P.wide_dec + (size_t)blockIdx.x * P.wide_dec_stride;
+    uint8_t *flg = P.wide_flags + (size_t)blockIdx.x * P.wide_flag_stride;
+    while (true) {
+      if (threadIdx.x == 0) s_idx = atomicAdd(&P.witem_cursor[level], 1u);
+      __syncthreads();
+      const uint32_t idx = s_idx;
+      __syncthreads();
+      if (idx >= n_w) break;
+      const WorkItem it = P.witems[level & 1][idx];
+      if (P.scenes[it.scene].flags & SF_DIRECTED)
+        process_wide<true>(P, it, level, rf, slice_log, dec, flg, sh, s_stats[0]);
+      else
+        process_wide<false>(P, it, level, rf, slice_log, dec, flg, sh, s_stats[0]);
+      __syncthreads();
+    }
+  }
 
   const uint32_t n_items = min(P.item_count[level], P.item_cap);
   const WorkItem *items = P.items[level & 1];
@@ -758,6 +1346,8 @@ __global__ void frame_begin_kernel(LaunchParams P) {
   for (uint32_t l = t; l <= TSI_MAX_LEVELS; l += blockDim.x) {
     P.item_count[l] = 0;
     P.item_cursor[l] = 0;
+    P.witem_count[l] = 0;
+    P.witem_cursor[l] = 0;
     P.dealloc_count[l] = 0;
     P.dealloc_cursor[l] = 0;
   }
@@ -765,6 +1355,7 @@ __global__ void frame_begin_kernel(LaunchParams P) {
     *P.rec_count = P.n_scenes;
     *P.code_count = 0;
   }
+  __syncthreads();
   for (uint32_t s = t; s < P.n_scenes; s += blockDim.x) {
     WorkItem w;
     w.scene = s;
@@ -772,10 +1363,11 @@ __global__ void frame_begin_kernel(LaunchParams P) {
     w.n = 1;
     w.level = 0;
     w.parent[0] = w.parent[1] = w.parent[2] = w.parent[3] = 0u;
-    P.items[0][s] = w;
+    const SceneLaunch &S = P.scenes[s];
+    const uint32_t len = P.recs[S.root_rec].len;
+    if (len >= S.wide.min_len) P.witems[0][atomicAdd(&P.witem_count[0], 1u)] = w;
+    else P.items[0][atomicAdd(&P.item_count[0], 1u)] = w;
   }
-  __syncthreads();
-  if (t == 0) P.item_count[0] = P.n_scenes;
 }
 
 // Per frame end: bricks freed this frame become allocatable.

@@ -1,6 +1,7 @@
 // tape_compile.cpp — handler selection and register allocation.
 #include "tape_compile.h"
 
+#include <algorithm>
 #include <cstring>
 
 #include "opcost.h"
@@ -147,6 +148,167 @@ bool compile_tape(const std::vector<IrInstr> &ins, PackedTape &out, tsi_status &
   out.nregs = maxreg + 1;
   out.out_reg = reg[n - 1];
   out.slot_reg = reg;
+  return true;
+}
+
+bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, WideTape &out, tsi_status &status,
+                  std::string &why) {
+  const uint32_t n = uint32_t(ins.size());
+  out = WideTape{};
+  if (n <= 4) return true;
+  // operands of every slot
+  std::vector<uint32_t> opa(n, TSI_NONE), opb(n, TSI_NONE);
+  for (uint32_t j = 4; j < n; ++j) {
+    const uint32_t top = op_top_of(ins[j]);
+    if (top == 0) {
+      opa[j] = ins[j].larg.reg;
+      opb[j] = ins[j].rarg.reg;
+    } else if (top == 1) {
+      opa[j] = ins[j].larg.reg;
+    } else if (top == 2) {
+      opa[j] = ins[j].rarg.reg;
+    }
+  }
+  // List scheduling in program order, width 32.  Users of one value keep
+  // their program order across bundles (a later user is never placed in an
+  // earlier bundle): the reverse pass accumulates into that value's
+  // sensitivity user by user, and the order fixes the rounding.
+  std::vector<std::vector<uint32_t>> users(n);
+  for (uint32_t j = 4; j < n; ++j) {
+    if (opa[j] != TSI_NONE) users[opa[j]].push_back(j);
+    if (opb[j] != TSI_NONE && opb[j] != opa[j]) users[opb[j]].push_back(j);
+  }
+  std::vector<uint32_t> next_user(n, 0);  // index into users[v] of its first unscheduled user
+  std::vector<int32_t> bundle_of(n, -1);
+  for (uint32_t a = 0; a < 4; ++a) bundle_of[a] = -2;  // arguments: before everything
+  std::vector<std::vector<uint32_t>> bundles;
+  std::vector<uint32_t> pending;
+  pending.reserve(n - 4);
+  for (uint32_t j = 4; j < n; ++j) pending.push_back(j);
+  auto in_turn = [&](uint32_t v, uint32_t j) { return v == TSI_NONE || users[v][next_user[v]] == j; };
+  while (!pending.empty()) {
+    std::vector<uint32_t> b;
+    const int32_t k = int32_t(bundles.size());
+    std::vector<uint32_t> rest;
+    rest.reserve(pending.size());
+    for (uint32_t j : pending) {
+      const bool deps = (opa[j] == TSI_NONE || (bundle_of[opa[j]] != -1 && bundle_of[opa[j]] < k)) &&
+                        (opb[j] == TSI_NONE || (bundle_of[opb[j]] != -1 && bundle_of[opb[j]] < k));
+      if (b.size() < 32 && deps && in_turn(opa[j], j) && in_turn(opb[j], j)) {
+        b.push_back(j);
+        bundle_of[j] = k;
+        if (opa[j] != TSI_NONE) next_user[opa[j]]++;
+        if (opb[j] != TSI_NONE && opb[j] != opa[j]) next_user[opb[j]]++;
+      } else {
+        rest.push_back(j);
+      }
+    }
+    if (b.empty()) {
+      status = TSI_ERR_INVALID_ARGUMENT;
+      why = "bundle scheduling made no progress";
+      return false;
+    }
+    bundles.push_back(b);
+    pending.swap(rest);
+  }
+  const uint32_t nb = uint32_t(bundles.size());
+  // last bundle reading each value; the field lives to the end
+  std::vector<int64_t> last(n, -1);
+  for (uint32_t j = 4; j < n; ++j) {
+    if (opa[j] != TSI_NONE) last[opa[j]] = std::max<int64_t>(last[opa[j]], bundle_of[j]);
+    if (opb[j] != TSI_NONE) last[opb[j]] = std::max<int64_t>(last[opb[j]], bundle_of[j]);
+  }
+  last[n - 1] = int64_t(nb) + 1;
+  // register allocation: a bundle reads before it writes
+  std::vector<uint32_t> reg(n, 0);
+  std::vector<uint8_t> used(64, 0);
+  for (uint32_t a = 0; a < 4; ++a) {
+    reg[a] = a;
+    used[a] = last[a] >= 0 ? 1 : 0;
+  }
+  uint32_t maxreg = 3;
+  for (uint32_t k = 0; k < nb; ++k) {
+    for (uint32_t j : bundles[k]) {  // operands whose last read is this bundle
+      if (opa[j] != TSI_NONE && last[opa[j]] == int64_t(k)) used[reg[opa[j]]] = 0;
+      if (opb[j] != TSI_NONE && last[opb[j]] == int64_t(k)) used[reg[opb[j]]] = 0;
+    }
+    std::vector<uint32_t> dead;
+    for (uint32_t j : bundles[k]) {
+      uint32_t d = 0;
+      while (d < used.size() && used[d]) ++d;
+      if (d == used.size()) used.push_back(0);
+      if (d >= 65535u) {
+        status = TSI_ERR_TAPE_TOO_WIDE;
+        why = "bundled tape needs more than 65535 registers";
+        return false;
+      }
+      reg[j] = d;
+      used[d] = 1;
+      if (last[j] < 0) dead.push_back(d);
+      maxreg = std::max(maxreg, d);
+    }
+    for (uint32_t d : dead) used[d] = 0;
+  }
+  // slots
+  const uint32_t nslots = n - 4;
+  out.slots.assign(size_t(nslots) * 8, 0);
+  out.bundles.assign(size_t(nb) * 2, 0);
+  out.narrow_mm.assign(nslots, TSI_NONE);
+  {
+    uint32_t mm = 0;
+    for (uint32_t j = 4; j < n; ++j) {
+      const uint32_t h = TSI_W0_H(narrow.code[2 * (j - 4)]);
+      if (TSI_H_IS_MINMAX(h)) out.narrow_mm[j - 4] = mm++;
+    }
+  }
+  uint32_t off = 0;
+  for (uint32_t k = 0; k < nb; ++k) {
+    const std::vector<uint32_t> &b = bundles[k];
+    // reverse rounds: descending slot order, a slot waits for every higher
+    // slot that accumulates into one of its target registers
+    std::vector<uint32_t> round(b.size(), 0);
+    uint32_t maxr = 0;
+    for (int s = int(b.size()) - 1; s >= 0; --s) {
+      const uint32_t j = b[size_t(s)];
+      uint32_t r = 0;
+      for (int t = int(b.size()) - 1; t > s; --t) {
+        const uint32_t q = b[size_t(t)];
+        bool share = false;
+        for (uint32_t x : {opa[j], opb[j]})
+          for (uint32_t y : {opa[q], opb[q]})
+            if (x != TSI_NONE && y != TSI_NONE && reg[x] == reg[y]) share = true;
+        if (share) r = std::max(r, round[size_t(t)] + 1);
+      }
+      round[size_t(s)] = r;
+      maxr = std::max(maxr, r);
+    }
+    if (maxr > 0xffffu) {
+      status = TSI_ERR_TAPE_TOO_WIDE;
+      why = "too many accumulation rounds in one bundle";
+      return false;
+    }
+    for (size_t s = 0; s < b.size(); ++s) {
+      const uint32_t j = b[s];
+      const uint32_t w0 = narrow.code[2 * (j - 4)], w1 = narrow.code[2 * (j - 4) + 1];
+      const uint32_t h = TSI_W0_H(w0);
+      uint32_t *S = &out.slots[size_t(off + s) * 8];
+      S[0] = h | (TSI_W0_FA(w0) << 6) | (TSI_W0_FB(w0) << 7);
+      const uint32_t ra = opa[j] != TSI_NONE ? reg[opa[j]] : 0, rb = opb[j] != TSI_NONE ? reg[opb[j]] : 0;
+      S[1] = reg[j] | (ra << 16);
+      S[2] = rb | (round[s] << 16);
+      S[3] = TSI_H_IS_II(h) ? 0u : w1;  // literal bits
+      S[4] = j;
+      S[5] = opa[j];
+      S[6] = opb[j];
+      S[7] = out.narrow_mm[j - 4];
+    }
+    out.bundles[2 * k] = off;
+    out.bundles[2 * k + 1] = uint32_t(b.size()) | (maxr << 16);
+    off += uint32_t(b.size());
+  }
+  out.nregs = maxreg + 1;
+  out.nbundles = nb;
+  out.out_reg = reg[n - 1];
   return true;
 }
 

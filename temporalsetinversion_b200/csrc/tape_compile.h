@@ -20,6 +20,31 @@ struct PackedTape {
   std::vector<uint32_t> slot_reg;  // register of every SSA slot (debug, tests)
 };
 
+// Bundled ("wide") form of a full tape, for evaluating one cell with a whole
+// warp: instructions are list-scheduled, in program order, into bundles of
+// at most 32 mutually independent instructions (one per lane), and given
+// their own register allocation in which a bundle reads all its operands
+// before it writes any result.  Per slot (2 x uint4):
+//   s0.x  handler | single-use A << 6 | single-use B << 7
+//   s0.y  dst register | A register << 16
+//   s0.z  B register | reverse round << 16
+//   s0.w  f32 literal
+//   s1    SSA slot of dst, A, B (TSI_NONE if absent), min/max ordinal
+// The reverse round orders, within a bundle, the slots that accumulate into
+// the same sensitivity register: highest slot first, as the sequential
+// reverse pass (compute.wgsl:3786) does.
+struct WideTape {
+  std::vector<uint32_t> slots;    // 8 words per slot
+  std::vector<uint32_t> bundles;  // 2 words per bundle: slot offset, count | max_round << 16
+  std::vector<uint32_t> narrow_mm;  // per narrow instruction: min/max ordinal or TSI_NONE
+  uint32_t nregs = 0;
+  uint32_t nbundles = 0;
+  uint32_t out_reg = 0;
+};
+
+bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, WideTape &out, tsi_status &status,
+                  std::string &why);
+
 // Maps (op, op_top) to a handler and allocates registers by linear scan
 // over SSA last uses.  Fails with TSI_ERR_TAPE_TOO_WIDE beyond 256 live
 // values and TSI_ERR_INVALID_ARGUMENT for tapes shorter than the 4 ARGs.
