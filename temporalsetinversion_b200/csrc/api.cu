@@ -267,7 +267,9 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, Scene
   R.parent = TSI_NONE;
   R.fwd_cost = (uint32_t)std::min<uint64_t>(s->tape->fwd_cost, 0xffffffffull);
   R.rev_cost = (uint32_t)std::min<uint64_t>(s->tape->rev_cost, 0xffffffffull);
-  R.pad = 0;
+  R.c_lo = -INFINITY;
+  R.c_hi = INFINITY;
+  R.c_level = TSI_NONE;
 }
 
 // One frame of set inversion for n scenes, all levels in one launch sequence.

@@ -91,11 +91,18 @@ struct TapeRec {
   uint32_t nregs;
   uint32_t out_reg;
   uint32_t n_minmax;
-  float t_lo, t_hi;   // valid for cells inside the group's boxes with time in [t_lo, t_hi]
+  float t_lo, t_hi;   // valid for any cell inside the group's boxes with time in [t_lo, t_hi]
   uint32_t parent;    // record it was pruned from (TSI_NONE for a full tape)
   uint32_t fwd_cost;  // opcost.h forward ops of one cell (fix included)
   uint32_t rev_cost;  // opcost.h reverse ops of one cell
-  uint32_t pad;
+  // A work item of level c_level built from this group holds children of the
+  // group's enqueued cells, and each child's time range lies inside its own
+  // parent's decision interval, for which that parent's decisions hold.
+  // [c_lo, c_hi] is the hull of those intervals: such an item may use the
+  // record for any time inside it.  Deeper items (which inherit the record
+  // when their group prunes nothing) check [t_lo, t_hi] instead.
+  float c_lo, c_hi;
+  uint32_t c_level;
 };
 
 struct WorkItem {

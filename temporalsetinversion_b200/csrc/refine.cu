@@ -415,7 +415,8 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     // ---- the most pruned tape valid for every evaluated cell
     const float tl = warp_min(evaluate ? targ.lo : fm_inf());
     const float th = warp_max(evaluate ? targ.hi : -fm_inf());
-    find_valid(P, rec, TR, tl, th);
+    TR = P.recs[rec];
+    if (!(TR.c_level == level && TR.c_lo <= tl && th <= TR.c_hi)) find_valid(P, rec, TR, tl, th);
     for (int attempt = 0; attempt < 2; ++attempt) {
       want_prune = (flags & SF_PRUNING) && TR.len >= TSI_PRUNE_MIN_LEN && TR.nregs <= TSI_PRUNE_MAX_REGS;
       lg = nullptr;
@@ -569,12 +570,17 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
       }
     }
     // validity of the group's pruned tape: intersection of the enqueued
-    // siblings' decision intervals
+    // siblings' decision intervals (any cell), and their hull (the group's
+    // own children, each covered by its parent's decisions)
     float gl = enq ? nl : -fm_inf();
     float gh = enq ? nh : fm_inf();
+    float hl = enq ? nl : fm_inf();
+    float hh = enq ? nh : -fm_inf();
     for (int o = 1; o < 8; o <<= 1) {
       gl = fmaxf(gl, __shfl_xor_sync(FULL_MASK, gl, o));
       gh = fminf(gh, __shfl_xor_sync(FULL_MASK, gh, o));
+      hl = fminf(hl, __shfl_xor_sync(FULL_MASK, hl, o));
+      hh = fmaxf(hh, __shfl_xor_sync(FULL_MASK, hh, o));
     }
     uint32_t cnt = 0, mmk = 0, fcost = 0, rcost = 0;
     bool pruned = false;
@@ -611,7 +617,9 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
         nr.parent = prec;
         nr.fwd_cost = fcost;
         nr.rev_cost = rcost;
-        nr.pad = 0;
+        nr.c_lo = hl;
+        nr.c_hi = hh;
+        nr.c_level = level + 1u;
         P.recs[ri] = nr;
         atomicAdd(&ws[ST_TAPE_WORDS], (unsigned long long)cnt);
       }
@@ -759,15 +767,28 @@ __device__ Iv wide_forward(const WideDev &W, float2 *rfw, uint32_t lane, Iv x, I
     rfw[3] = make_float2(t.lo, t.hi);
   }
   __syncwarp();
+  // descriptors and slots are fetched two bundles ahead of their use
+  uint2 bt0 = W.bundles[0];
+  uint2 bt1 = W.nbundles > 1 ? W.bundles[1] : bt0;
+  uint4 sl0 = lane < (bt0.y & 0xffffu) ? W.slots[2u * (bt0.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
+  uint4 sl1 = (W.nbundles > 1 && lane < (bt1.y & 0xffffu)) ? W.slots[2u * (bt1.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
   for (uint32_t k = 0; k < W.nbundles; ++k) {
-    const uint2 bt = W.bundles[k];
+    const uint2 bt = bt0;
+    const uint4 sl = sl0;
+    bt0 = bt1;
+    sl0 = sl1;
+    if (k + 2 < W.nbundles) {
+      bt1 = W.bundles[k + 2];
+      sl1 = lane < (bt1.y & 0xffffu) ? W.slots[2u * (bt1.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
+    }
     const bool act = lane < (bt.y & 0xffffu);
     Iv r = iv(0.0f);
     uint32_t dst = 0;
     if (act) {
-      uint32_t h, fa, fb, a, b, round;
-      float lit;
-      wide_slot(W, bt.x + lane, h, fa, fb, dst, a, b, round, lit);
+      const uint32_t h = sl.x & 63u;
+      dst = sl.y & 0xffffu;
+      const uint32_t a = sl.y >> 16, b = sl.z & 0xffffu;
+      const float lit = __uint_as_float(sl.w);
       const float2 av = rfw[a];
       const Iv A = Iv{av.x, av.y};
       Iv B = iv(lit);
@@ -801,16 +822,34 @@ __device__ void wide_reverse(const WideDev &W, float2 *rfw, uint32_t lane, const
   __syncwarp();
   if (lane == 0) rfw[W.out_reg] = make_float2(1.0f, 1.0f);
   __syncwarp();
-  for (int k = (int)W.nbundles - 1; k >= 0; --k) {
-    const uint2 bt = W.bundles[k];
+  const int nb = (int)W.nbundles;
+  uint2 btn = W.bundles[nb - 1];
+  uint4 sln = lane < (btn.y & 0xffffu) ? W.slots[2u * (btn.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
+  float4 Ln = lane < (btn.y & 0xffffu) ? lg[(size_t)(nb - 1) * 32u + lane] : make_float4(0, 0, 0, 0);
+  for (int k = nb - 1; k >= 0; --k) {
+    const uint2 bt = btn;
+    const uint4 sl = sln;
+    const float4 L = Ln;
+    if (k > 0) {  // next (lower) bundle, fetched while this one runs
+      btn = W.bundles[k - 1];
+      const bool an = lane < (btn.y & 0xffffu);
+      sln = an ? W.slots[2u * (btn.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
+      Ln = an ? lg[(size_t)(k - 1) * 32u + lane] : make_float4(0, 0, 0, 0);
+    }
     const bool act = lane < (bt.y & 0xffffu);
     const uint32_t maxr = bt.y >> 16;
     uint32_t h = H_CONST, fa = 0, fb = 0, dst = 0, a = 0, b = 0, round = 0;
     float lit = 0.0f;
     Iv A = iv(0.0f), B = iv(0.0f), s = iv(0.0f);
     if (act) {
-      wide_slot(W, bt.x + lane, h, fa, fb, dst, a, b, round, lit);
-      const float4 L = lg[(size_t)k * 32u + lane];
+      h = sl.x & 63u;
+      fa = (sl.x >> 6) & 1u;
+      fb = (sl.x >> 7) & 1u;
+      dst = sl.y & 0xffffu;
+      a = sl.y >> 16;
+      b = sl.z & 0xffffu;
+      round = sl.z >> 16;
+      lit = __uint_as_float(sl.w);
       A = Iv{L.x, L.y};
       B = Iv{L.z, L.w};
       const float2 sv = rfw[dst];
@@ -905,6 +944,7 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
   const uint32_t n_narrow = root.len;
 
   if (threadIdx.x == 0) {
+    ws[ST_PARENTS] += 1;  // every processed parent, as the narrow path counts it.n
     const uint32_t pc = pool.child[Pv];
     sh.is_new = pc == TSI_NONE;
     sh.base = pc;
@@ -1099,7 +1139,6 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
   __syncthreads();
   const uint32_t E = sh.E;
   if (E == 0) return;
-  if (lane == 0 && k == 0) ws[ST_PARENTS] += 1;
 
   uint32_t new_rec = S.root_rec;
   if (want_prune) {
@@ -1201,10 +1240,14 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
     __syncthreads();
     if (sh.ri != TSI_NONE) {
       if (threadIdx.x == 0) {
-        float gl = -fm_inf(), gh = fm_inf();
+        float gl = -fm_inf(), gh = fm_inf(), hl = fm_inf(), hh = -fm_inf();
         for (int q = 0; q < kWarps; ++q) {
           gl = fmaxf(gl, sh.nl[q]);
           gh = fminf(gh, sh.nh[q]);
+          if ((E >> q) & 1u) {
+            hl = fminf(hl, sh.nl[q]);
+            hh = fmaxf(hh, sh.nh[q]);
+          }
         }
         TapeRec nr;
         nr.code = P.code_arena + sh.off;
@@ -1217,7 +1260,9 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
         nr.parent = S.root_rec;
         nr.fwd_cost = sh.fcost;
         nr.rev_cost = sh.rcost;
-        nr.pad = 0;
+        nr.c_lo = hl;
+        nr.c_hi = hh;
+        nr.c_level = level + 1u;
         P.recs[sh.ri] = nr;
         ws[ST_TAPE_WORDS] += sh.cnt;
       }

@@ -61,8 +61,9 @@ def test_bad_opcode_and_bad_tapes_rejected(device):
 @pytest.mark.gpu
 def test_log_arena_exhaustion_is_reported():
     with Device(log_arena_bytes=1 << 16) as dev:
-        text = scenes.csg(256, 1)  # 4.7k slots: longer than a per-warp log slice
-        s = Scene(dev, Tape.from_llvm_ir(dev, text), api.default_params(localsubdiv=4))
+        # 37.5k slots in ~1.2k bundles: the reverse-AD log outgrows a warp's slice
+        text = scenes.csg(2048, 7)
+        s = Scene(dev, Tape.from_llvm_ir(dev, text), api.default_params(localsubdiv=3))
         with pytest.raises(N.TsiError) as e:
             for t in (0.0, 0.02):  # the second frame runs reverse AD on the long root tape
                 s.invert(t)
