@@ -279,6 +279,31 @@ TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *ctx, tsi_request *reqs, uint3
 TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g);
 TSI_API void tsi_batch_graph_destroy(tsi_batch_graph *g);
 
+/* ---------------- allocation-free evaluation ---------------- */
+/* No counterpart in the reference.  tsi_tape_eval_boxes allocates device
+ * scratch with cudaMalloc; callers that cannot allocate at call time (a
+ * loop recorded into a CUDA graph, a host with a memory budget fixed at
+ * start-up, a runtime that forbids allocation on its request path) use this
+ * variant instead.  It evaluates `tape` on n boxes already in device memory
+ * (n x 8 floats as in tsi_tape_eval_boxes) and writes n x 10 floats to
+ * out_dev, on cuda_stream (NULL: the tape context's stream), and returns
+ * after enqueueing.  It calls no cudaMalloc, cudaFree or other allocating
+ * routine: its scratch is a static device array of TSI_STATIC_SCRATCH_BYTES
+ * per device (held by every GPU that loads the library until the process
+ * exits), and n x (8 x registers + 16 x tape length) bytes must fit in it,
+ * else TSI_ERR_BUFFER_TOO_SMALL (split the call).  Nothing in the array needs
+ * to start at zero: each launch writes every register and log entry before
+ * reading it.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make it before any stream capture.  All
+ * calls share the one array per device: calls that can overlap on the GPU
+ * (different streams, or different contexts on the same device) race on it
+ * and must be ordered by the caller. */
+#define TSI_STATIC_SCRATCH_BYTES (16u << 20)
+TSI_API tsi_status tsi_tape_eval_boxes_static(const tsi_tape *tape, uint32_t n, const float *boxes_dev,
+                                              int32_t rounding_mode, int32_t reverse, float *out_dev,
+                                              void *cuda_stream);
+TSI_API uint64_t tsi_static_scratch_bytes(void);
+
 /* ---------------- diagnostics (tests and tools) ---------------- */
 /* Message of the last failing call on this thread. */
 TSI_API const char *tsi_last_error(void);

@@ -120,6 +120,8 @@ SIGNATURES = {
     "tsi_compile_gpu_instructions": (i32, [P(GPUInstruction), u32, P(u32), u32, P(TapeInfo)]),
     "tsi_debug_math": (i32, [C.c_void_p, i32, u32, P(f32), P(f32), P(f32)]),
     "tsi_debug_level_profile": (i32, [C.c_void_p, u32, P(f32), P(u64), P(u32)]),
+    "tsi_tape_eval_boxes_static": (i32, [C.c_void_p, u32, C.c_void_p, i32, i32, C.c_void_p, C.c_void_p]),
+    "tsi_static_scratch_bytes": (u64, []),
 }
 
 _lib = None

@@ -19,6 +19,7 @@
 #include <string>
 #include <vector>
 
+#include "api_internal.h"
 #include "device_types.h"
 #include "ir_lower.h"
 #include "tape_compile.h"
@@ -884,6 +885,23 @@ TSI_API tsi_status tsi_tape_eval_boxes(tsi_ctx *c, const tsi_tape *t, uint32_t n
   CK(cudaStreamSynchronize(c->stream));
   return TSI_OK;
 }
+
+}  // extern "C"
+
+// Internal view of a tape for the library's other translation units.
+tsi_status tsi_internal_tape_view(const tsi_tape *t, TsiTapeView *v) {
+  if (!t || !v || !t->ctx) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  v->code = t->d_code;
+  v->len = t->len;
+  v->nregs = t->nregs;
+  v->out_reg = t->out_reg;
+  v->device = t->ctx->device;
+  v->stream = t->ctx->stream;
+  return TSI_OK;
+}
+void tsi_internal_set_error(const char *msg) { g_last_error = msg; }
+
+extern "C" {
 
 // device f32 math on host arrays (GPU math tests)
 TSI_API tsi_status tsi_debug_math(tsi_ctx *c, int32_t which, uint32_t n, const float *a, const float *b, float *out) {
