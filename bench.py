@@ -230,7 +230,10 @@ def run_gpu(args, rank, world, local, dist) -> None:
 
     text, params, view = build_workload(WORKLOAD["seed"] + rank)
     W, H, F = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["frames"]
-    dev = Device(local)
+    if args.small_arenas:  # a few GB on the device in all, for profiler captures
+        dev = Device(local, work_item_capacity=1 << 20, tape_arena_words=16 << 20, log_arena_bytes=1 << 30)
+    else:
+        dev = Device(local)
     lib = dev.lib
     tape = Tape.from_llvm_ir(dev, text)
     scene = Scene(dev, tape, params, voxel_capacity=args.voxels)
@@ -354,6 +357,8 @@ def main() -> None:
     ap.add_argument("--impl", default="tsi", choices=["tsi", "reference"])
     ap.add_argument("--voxels", type=int, default=64 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--small-arenas", action="store_true",
+                    help="small work-item, tape and log arenas (use with --voxels 4194304 under a profiler)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()

@@ -315,6 +315,17 @@ TSI_API tsi_status tsi_ir_tape_info(const char *text, size_t len, tsi_tape_info 
  * a tape given in the ir.rs layout. */
 TSI_API tsi_status tsi_compile_gpu_instructions(const tsi_gpu_instruction *instr, uint32_t n, uint32_t *words,
                                                 uint32_t cap_words, tsi_tape_info *info);
+/* Host-only: the bundled (wide) form of a tape given in the ir.rs layout:
+ * 12 words per slot after the ARG slots ({handler | fa << 6 | fb << 7,
+ * dst | a << 16, b, literal bits, ssa dst, ssa a, ssa b, min/max index,
+ * contribution record of a, of b, first record of dst, record count of
+ * dst}, TSI_NONE for absent operands and records), 2 words per bundle
+ * (first slot, count); info->registers = registers of the bundled form,
+ * info->reserved = its output register. */
+TSI_API tsi_status tsi_compile_wide_gpu_instructions(const tsi_gpu_instruction *instr, uint32_t n, uint32_t *slots,
+                                                     uint32_t cap_slot_words, uint32_t *bundles,
+                                                     uint32_t cap_bundle_words, tsi_tape_info *info,
+                                                     uint32_t *n_bundles);
 /* Elementwise device f32 math, for the math tests: which = 0 sin(a),
  * 1 exp(a), 2 log(a), 3 atan2(a, b), 4 powi(a, (int)b), 5 min(a, b),
  * 6 max(a, b) (minimumNumber / maximumNumber), 7 fminf, 8 fmaxf. */
@@ -322,9 +333,12 @@ TSI_API tsi_status tsi_debug_math(tsi_ctx *ctx, int32_t which, uint32_t n, const
                                   float *out);
 /* Per-level profile of the context's last inversion: device ms of each
  * level's refinement launch (-1 unless TSI_PROFILE_LEVELS is set in the
- * environment when the context is created) and the 17 counters per level
- * (order of the tsi_stats fields from parents_expanded to prune_fallbacks,
- * without voxels_live and items_high_water). */
+ * environment when the context is created) and TSI_LEVEL_COUNTERS counters
+ * per level: the tsi_stats fields from parents_expanded to prune_fallbacks
+ * (without voxels_live and items_high_water), then SM clock cycles: wide
+ * items processed, their cycles (sum, max), the forward and reverse passes
+ * of their first cell (sums), narrow items' cycles (sum, max). */
+#define TSI_LEVEL_COUNTERS 24
 TSI_API tsi_status tsi_debug_level_profile(tsi_ctx *ctx, uint32_t max_levels, float *ms, uint64_t *counters,
                                            uint32_t *n_levels);
 

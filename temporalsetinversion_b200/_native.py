@@ -45,7 +45,8 @@ class Uniforms(C.Structure):  # uniforms.rs:8-17
 
 LEVEL_COUNTERS = ["parents", "evaluated", "reverse", "skipped", "ambiguous", "empty", "full", "enqueued", "reused",
                   "instr_fwd", "instr_rev", "instr_full", "fp32", "brick_alloc", "brick_free", "tape_words",
-                  "prune_fallback"]
+                  "prune_fallback", "wide_items", "cyc_wide", "cyc_wide_max", "cyc_wide_fwd", "cyc_wide_rev",
+                  "cyc_narrow", "cyc_narrow_max"]
 
 
 class Stats(C.Structure):
@@ -120,6 +121,8 @@ SIGNATURES = {
     "tsi_compile_gpu_instructions": (i32, [P(GPUInstruction), u32, P(u32), u32, P(TapeInfo)]),
     "tsi_debug_math": (i32, [C.c_void_p, i32, u32, P(f32), P(f32), P(f32)]),
     "tsi_debug_level_profile": (i32, [C.c_void_p, u32, P(f32), P(u64), P(u32)]),
+    "tsi_compile_wide_gpu_instructions": (i32, [P(GPUInstruction), u32, P(u32), u32, P(u32), u32, P(TapeInfo),
+                                                 P(u32)]),
     "tsi_tape_eval_boxes_static": (i32, [C.c_void_p, u32, C.c_void_p, i32, i32, C.c_void_p, C.c_void_p]),
     "tsi_static_scratch_bytes": (u64, []),
 }

@@ -101,7 +101,8 @@ struct tsi_tape {
   uint4 *d_wslots = nullptr;
   uint2 *d_wbundles = nullptr;
   uint32_t *d_wmm = nullptr;
-  uint32_t wbundles = 0, wregs = 0, wout = 0, wmin_len = 0xffffffffu;
+  uint32_t wbundles = 0, wregs = 0, wout = 0, wmin_len = 0xffffffffu, wcontrib = 0;
+  uint32_t warg_gbase[4] = {TSI_NONE, TSI_NONE, TSI_NONE, TSI_NONE}, warg_gcount[4] = {0, 0, 0, 0};
 };
 
 struct tsi_scene {
@@ -158,7 +159,6 @@ struct tsi_ctx {
   std::vector<cudaEvent_t> level_events;
   uint32_t last_levels = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
-  size_t smem_set = 0;
   // scratch for tsi_tape_eval_boxes
   void *d_scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -258,6 +258,11 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, Scene
   L.wide.nregs = s->tape->wregs;
   L.wide.out_reg = s->tape->wout;
   L.wide.min_len = s->tape->wmin_len;
+  L.wide.ncontrib = s->tape->wcontrib;
+  for (int q = 0; q < 4; ++q) {
+    L.wide.arg_gbase[q] = s->tape->warg_gbase[q];
+    L.wide.arg_gcount[q] = s->tape->warg_gcount[q];
+  }
   R.code = s->tape->d_code;
   R.len = s->tape->len;
   R.nregs = s->tape->nregs;
@@ -307,11 +312,14 @@ tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *tim
     }
   }
   const uint32_t rcap = (rmax + 3u) & ~3u;
-  const size_t smem = (size_t)kWarpsPerBlock * rcap * 32u * sizeof(float2);
-  if (smem > c->smem_set) {
-    CK(refine_set_smem(smem));
-    c->smem_set = smem;
-  }
+  size_t smem = (size_t)kWarpsPerBlock * rcap * 32u * sizeof(float2);
+  // the wide path's branch ballots and liveness flags go to shared memory
+  // after the register file when they take at most 64 KB and the block at
+  // most 160 KB
+  const size_t wide_bytes = (size_t)c->wide_dec_stride * sizeof(uint2) + c->wide_flag_stride;
+  const bool wide_smem = wide_bytes <= (64u << 10) && smem + wide_bytes <= (160u << 10);
+  if (wide_smem) smem += wide_bytes;
+  CK(refine_set_smem(smem));
   int bps = 0;
   CK(refine_occupancy(kBlock, smem, &bps));
   if (bps < 1) return set_err(TSI_ERR_TAPE_TOO_WIDE, "register file does not fit in shared memory");
@@ -322,8 +330,9 @@ tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *tim
   CK(cudaMemsetAsync(c->d_error, 0, sizeof(uint32_t), c->stream));
   CK(cudaMemsetAsync(c->d_stats, 0, ST_COUNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(c->d_level_stats, 0, (TSI_MAX_LEVELS + 1) * ST_COUNT * sizeof(unsigned long long), c->stream));
-  CK(cudaMemsetAsync(c->d_log_used, 0, sizeof(unsigned long long), c->stream));
-  const LaunchParams P = make_params(c, n);
+  CK(cudaMemsetAsync(c->d_log_used, 0, (TSI_MAX_LEVELS + 1) * sizeof(unsigned long long), c->stream));
+  LaunchParams P = make_params(c, n);
+  P.wide_smem = wide_smem ? 1u : 0u;
   CK(launch_frame_begin(P, c->stream));
   const bool prof = c->profile_levels && c->level_events.size() >= lmax + 1;
   for (uint32_t level = 0; level < lmax; ++level) {
@@ -623,6 +632,33 @@ TSI_API tsi_status tsi_compile_gpu_instructions(const tsi_gpu_instruction *instr
   return TSI_OK;
 }
 
+// host-only: the bundled form of a tape given in the ir.rs layout (tests)
+TSI_API tsi_status tsi_compile_wide_gpu_instructions(const tsi_gpu_instruction *instr, uint32_t n, uint32_t *slots,
+                                                     uint32_t cap_slot_words, uint32_t *bundles,
+                                                     uint32_t cap_bundle_words, tsi_tape_info *info,
+                                                     uint32_t *n_bundles) {
+  if (!instr || !info || !n_bundles) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  std::vector<IrInstr> ins;
+  tsi_status st = TSI_OK;
+  std::string why;
+  if (!ir_from_gpu(instr, n, ins, st, why)) return set_err(st, why);
+  PackedTape pt;
+  if (!compile_tape(ins, pt, st, why)) return set_err(st, why);
+  WideTape wt;
+  if (!compile_wide(ins, pt, wt, st, why)) return set_err(st, why);
+  info->instruction_count = pt.count;
+  info->registers = wt.nregs;
+  info->minmax_count = pt.n_minmax;
+  info->reserved = wt.out_reg;
+  *n_bundles = wt.nbundles;
+  if (slots)
+    for (uint32_t i = 0; i < std::min<uint32_t>(cap_slot_words, (uint32_t)wt.slots.size()); ++i) slots[i] = wt.slots[i];
+  if (bundles)
+    for (uint32_t i = 0; i < std::min<uint32_t>(cap_bundle_words, (uint32_t)wt.bundles.size()); ++i)
+      bundles[i] = wt.bundles[i];
+  return TSI_OK;
+}
+
 TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   if (!out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
   *out = nullptr;
@@ -665,7 +701,6 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   {
     const size_t smem_min = (size_t)kWarpsPerBlock * 4u * 32u * sizeof(float2);
     CKC(refine_set_smem(smem_min));
-    c->smem_set = smem_min;
     int bps = 0;
     CKC(refine_occupancy(kBlock, smem_min, &bps));
     c->max_warps = (uint32_t)std::max(1, bps) * (uint32_t)c->sm_count * kWarpsPerBlock;
@@ -692,7 +727,7 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   CKC(dalloc(&c->d_log, (size_t)c->max_warps * c->slice_len * 32u));
   CKC(dalloc(&c->d_dec, (size_t)c->max_warps * c->slice_len));
   CKC(dalloc(&c->d_log_overflow, c->log_overflow_cap));
-  CKC(dalloc(&c->d_log_used, 1));
+  CKC(dalloc(&c->d_log_used, TSI_MAX_LEVELS + 1));
   CKC(dalloc(&c->d_error, 1));
   CKC(dalloc(&c->d_stats, ST_COUNT));
   CKC(dalloc(&c->d_level_stats, (TSI_MAX_LEVELS + 1) * ST_COUNT));
@@ -812,6 +847,11 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
       t->wregs = wt.nregs;
       t->wout = wt.out_reg;
       t->wmin_len = std::max<uint32_t>(256u, 3u * wt.nbundles);
+      t->wcontrib = wt.ncontrib;
+      for (int q = 0; q < 4; ++q) {
+        t->warg_gbase[q] = wt.arg_gbase[q];
+        t->warg_gcount[q] = wt.arg_gcount[q];
+      }
     }
   }
   *out = t;
@@ -925,6 +965,7 @@ TSI_API tsi_status tsi_debug_math(tsi_ctx *c, int32_t which, uint32_t n, const f
   return TSI_OK;
 }
 
+static_assert(ST_COUNT == TSI_LEVEL_COUNTERS, "level counters of tsi.h");
 TSI_API tsi_status tsi_debug_level_profile(tsi_ctx *c, uint32_t max_levels, float *ms, uint64_t *counters,
                                            uint32_t *n_levels) {
   if (!c || !n_levels) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");

@@ -61,13 +61,16 @@ struct SceneCounters {
 // Bundled form of a scene's full tape (tape_compile.h WideTape), evaluated
 // with one warp per cell for items whose tape is long.
 struct WideDev {
-  const uint4 *slots;         // 2 x uint4 per slot
-  const uint2 *bundles;       // slot offset, count | max_round << 16
+  const uint4 *slots;         // 3 x uint4 per slot (tape_compile.h)
+  const uint2 *bundles;       // slot offset, count
   const uint32_t *narrow_mm;  // min/max ordinal per narrow instruction
   uint32_t nbundles;
   uint32_t nregs;
   uint32_t out_reg;           // wide register of the field
   uint32_t min_len;           // tapes at least this long go to the wide path
+  uint32_t ncontrib;          // reverse contribution records per cell
+  uint32_t arg_gbase[4];      // records of x, y, z, t (TSI_NONE: in its register)
+  uint32_t arg_gcount[4];
 };
 
 struct SceneLaunch {
@@ -116,7 +119,11 @@ struct WorkItem {
 enum tsi_stat_index {
   ST_PARENTS = 0, ST_EVAL, ST_REVERSE, ST_SKIPPED, ST_AMBIG, ST_EMPTY, ST_FULL, ST_ENQUEUED,
   ST_REUSED, ST_INSTR_FWD, ST_INSTR_REV, ST_INSTR_FULL, ST_FP32, ST_BRICK_ALLOC, ST_BRICK_FREE,
-  ST_TAPE_WORDS, ST_PRUNE_FALLBACK, ST_COUNT
+  ST_TAPE_WORDS, ST_PRUNE_FALLBACK,
+  // SM clock cycles (clock64): wide items (count, sum, max, and the forward
+  // and reverse passes of their first cell) and narrow items (sum, max)
+  ST_WIDE_ITEMS, ST_CYC_WIDE, ST_CYC_WIDE_MAX, ST_CYC_WIDE_FWD, ST_CYC_WIDE_REV, ST_CYC_NARROW,
+  ST_CYC_NARROW_MAX, ST_COUNT
 };
 
 struct LaunchParams {
@@ -136,6 +143,7 @@ struct LaunchParams {
   uint32_t *witem_cursor;  // [TSI_MAX_LEVELS + 1]
   uint2 *wide_dec;         // per block: branch ballots of the 8 cells, [wide_dec_stride]
   uint32_t wide_dec_stride;
+  uint32_t wide_smem;      // 1: ballots and flags in shared memory after the register file
   uint32_t wide_flag_stride;
   uint8_t *wide_flags;     // per block: liveness flags, [wide_flag_stride]
   uint32_t item_cap;
@@ -149,7 +157,9 @@ struct LaunchParams {
   uint32_t slice_len;
   uint32_t pad0;
   float4 *log_overflow;
-  unsigned long long *log_overflow_used;  // in float4 units
+  // [TSI_MAX_LEVELS + 1], in float4 units: a level's logs are dead once the
+  // next level starts, so every level fills the arena from its start
+  unsigned long long *log_overflow_used;
   unsigned long long log_overflow_cap;
   uint32_t *error;
   unsigned long long *stats;        // [ST_COUNT]

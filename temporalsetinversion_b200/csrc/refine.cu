@@ -31,6 +31,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "device_types.h"
 #include "interval.cuh"
 #include "opcost.h"
@@ -304,8 +306,8 @@ __device__ __forceinline__ float warp_max(float v) {
 
 // scratch for one item: operand log + decisions, in the warp's slice or the
 // shared overflow arena (long tapes)
-__device__ __forceinline__ bool item_scratch(const LaunchParams &P, uint32_t len, uint32_t lane, float4 *slice_log,
-                                             uint2 *slice_dec, float4 *&lg, uint2 *&dg) {
+__device__ __forceinline__ bool item_scratch(const LaunchParams &P, uint32_t level, uint32_t len, uint32_t lane,
+                                             float4 *slice_log, uint2 *slice_dec, float4 *&lg, uint2 *&dg) {
   if (len <= P.slice_len) {
     lg = slice_log;
     dg = slice_dec;
@@ -313,7 +315,7 @@ __device__ __forceinline__ bool item_scratch(const LaunchParams &P, uint32_t len
   }
   const unsigned long long need = (unsigned long long)len * 32ull + ((unsigned long long)len + 1ull) / 2ull;
   unsigned long long off = 0;
-  if (lane == 0) off = atomicAdd(P.log_overflow_used, need);
+  if (lane == 0) off = atomicAdd(P.log_overflow_used + level, need);
   off = __shfl_sync(FULL_MASK, off, 0);
   if (off + need > P.log_overflow_cap) {
     if (lane == 0) atomicOr(P.error, EB_LOG_OOM);
@@ -424,7 +426,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
       if (any_deriv || want_prune) {
         float4 *lgs = nullptr;
         uint2 *dgs = nullptr;
-        if (!item_scratch(P, TR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
+        if (!item_scratch(P, level, TR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
         lg = lgs;
         dg = want_prune ? dgs : nullptr;
       }
@@ -551,17 +553,34 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
       nh = -fm_inf();
     }
     const bool widen = enq && (nl < targ.lo || nh > targ.hi);
+    const uint32_t wb = __ballot_sync(FULL_MASK, widen);
     uint32_t prec = rec;  // record the group tapes are pruned from
     TapeRec PR = TR;
-    if (want_prune && __any_sync(FULL_MASK, widen)) {
+    bool handed = false;  // the group's children go to the wide path unpruned
+    if (want_prune && wb) {
       // decisions over the widened interval, from a tape valid there
       const float wl = warp_min(nl), wh = warp_max(nh);
-      find_valid(P, prec, PR, wl, wh);
-      want_prune = (flags & SF_PRUNING) && PR.len >= TSI_PRUNE_MIN_LEN && PR.nregs <= TSI_PRUNE_MAX_REGS;
-      if (want_prune) {
+      uint32_t wrec = rec;
+      TapeRec WR;
+      find_valid(P, wrec, WR, wl, wh);
+      if (WR.len >= S.wide.min_len) {
+        // A long tape: no pass over it on one warp.  A group with a widened
+        // child hands its children, with that tape's record, to the wide
+        // path; the other groups prune from the first pass's decisions.
+        if ((wb >> (g * 8u)) & 0xffu) {
+          prec = wrec;
+          PR = WR;
+          handed = true;
+        }
+      } else {
+        prec = wrec;
+        PR = WR;
+        want_prune = (flags & SF_PRUNING) && PR.len >= TSI_PRUNE_MIN_LEN && PR.nregs <= TSI_PRUNE_MAX_REGS;
+      }
+      if (want_prune && WR.len < S.wide.min_len) {
         float4 *lgs;
         uint2 *dgs;
-        if (!item_scratch(P, PR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
+        if (!item_scratch(P, level, PR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
         lg = lgs;
         dg = dgs;
         const Iv tw = enq ? Iv{nl, nh} : targ;
@@ -584,7 +603,8 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     }
     uint32_t cnt = 0, mmk = 0, fcost = 0, rcost = 0;
     bool pruned = false;
-    uint2 *tmp = (want_prune && lg != nullptr) ? reinterpret_cast<uint2 *>(lg) + (size_t)g * PR.len : nullptr;
+    uint2 *tmp =
+        (want_prune && !handed && lg != nullptr) ? reinterpret_cast<uint2 *>(lg) + (size_t)g * PR.len : nullptr;
     if (k == 0 && E != 0 && tmp != nullptr) {
       cnt = prune_scan(PR.code, PR.len, PR.n_minmax, PR.out_reg, dg, g, E, tmp, mmk, fcost, rcost);
       pruned = cnt < PR.len;
@@ -635,46 +655,42 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     if (k == 0 && E != 0 && next_len >= S.wide.min_len) {  // long tape: wide path, one item per child
       const uint32_t n = __popc(E);
       const uint32_t pos = atomicAdd(&P.witem_count[level + 1], n);
-      if (pos + n > P.item_cap) {
-        atomicOr(P.error, EB_QUEUE_FULL);
-      } else {
-        uint32_t e = E, j = 0;
-        while (e) {
-          const uint32_t bit = __ffs(e) - 1u;
-          e &= e - 1u;
-          WorkItem wi;
-          wi.scene = it.scene;
-          wi.rec = new_rec;
-          wi.n = 1;
-          wi.level = level + 1;
-          wi.parent[0] = wi.parent[1] = wi.parent[2] = wi.parent[3] = cb[bit];
-          P.witems[(level + 1) & 1][pos + j++] = wi;
-        }
+      // every reserved slot below the capacity is written (readers take
+      // min(count, capacity) entries); the rest are dropped and reported
+      if (pos + n > P.item_cap) atomicOr(P.error, EB_QUEUE_FULL);
+      uint32_t e = E, j = 0;
+      while (e && pos + j < P.item_cap) {
+        const uint32_t bit = __ffs(e) - 1u;
+        e &= e - 1u;
+        WorkItem wi;
+        wi.scene = it.scene;
+        wi.rec = new_rec;
+        wi.n = 1;
+        wi.level = level + 1;
+        wi.parent[0] = wi.parent[1] = wi.parent[2] = wi.parent[3] = cb[bit];
+        P.witems[(level + 1) & 1][pos + j++] = wi;
       }
     } else if (k == 0 && E != 0) {
       const uint32_t n = __popc(E);
       const uint32_t nitems = (n + 3u) >> 2;
       const uint32_t pos = atomicAdd(&P.item_count[level + 1], nitems);
-      if (pos + nitems > P.item_cap) {
-        atomicOr(P.error, EB_QUEUE_FULL);
-      } else {
-        WorkItem *dst = P.items[(level + 1) & 1];
-        uint32_t e = E;
-        for (uint32_t j = 0; j < nitems; ++j) {
-          WorkItem wi;
-          wi.scene = it.scene;
-          wi.rec = new_rec;
-          wi.level = level + 1;
-          uint32_t c = 0;
-          while (e && c < 4u) {
-            const uint32_t bit = __ffs(e) - 1u;
-            e &= e - 1u;
-            wi.parent[c++] = cb[bit];
-          }
-          wi.n = c;
-          for (uint32_t q = c; q < 4u; ++q) wi.parent[q] = wi.parent[0];
-          dst[pos + j] = wi;
+      if (pos + nitems > P.item_cap) atomicOr(P.error, EB_QUEUE_FULL);
+      WorkItem *dst = P.items[(level + 1) & 1];
+      uint32_t e = E;
+      for (uint32_t j = 0; j < nitems && pos + j < P.item_cap; ++j) {
+        WorkItem wi;
+        wi.scene = it.scene;
+        wi.rec = new_rec;
+        wi.level = level + 1;
+        uint32_t c = 0;
+        while (e && c < 4u) {
+          const uint32_t bit = __ffs(e) - 1u;
+          e &= e - 1u;
+          wi.parent[c++] = cb[bit];
         }
+        wi.n = c;
+        for (uint32_t q = c; q < 4u; ++q) wi.parent[q] = wi.parent[0];
+        dst[pos + j] = wi;
       }
     }
   }
@@ -744,19 +760,6 @@ __device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level,
 // sensitivity register in the sequential order (rounds), so the results
 // are those of the narrow path bit for bit.
 
-__device__ __forceinline__ void wide_slot(const WideDev &W, uint32_t si, uint32_t &h, uint32_t &fa, uint32_t &fb,
-                                          uint32_t &dst, uint32_t &a, uint32_t &b, uint32_t &round, float &lit) {
-  const uint4 s0 = W.slots[2u * si];
-  h = s0.x & 63u;
-  fa = (s0.x >> 6) & 1u;
-  fb = (s0.x >> 7) & 1u;
-  dst = s0.y & 0xffffu;
-  a = s0.y >> 16;
-  b = s0.z & 0xffffu;
-  round = s0.z >> 16;
-  lit = __uint_as_float(s0.w);
-}
-
 template <bool D>
 __device__ Iv wide_forward(const WideDev &W, float2 *rfw, uint32_t lane, Iv x, Iv y, Iv z, Iv t, float4 *lg,
                            uint2 *dec, uint32_t cellbit) {
@@ -767,19 +770,23 @@ __device__ Iv wide_forward(const WideDev &W, float2 *rfw, uint32_t lane, Iv x, I
     rfw[3] = make_float2(t.lo, t.hi);
   }
   __syncwarp();
+  // the tape's fields in registers (stores through rfw could alias them)
+  const uint2 *__restrict__ bundles = W.bundles;
+  const uint4 *__restrict__ slots = W.slots;
+  const uint32_t nb = W.nbundles, out_reg = W.out_reg;
   // descriptors and slots are fetched two bundles ahead of their use
-  uint2 bt0 = W.bundles[0];
-  uint2 bt1 = W.nbundles > 1 ? W.bundles[1] : bt0;
-  uint4 sl0 = lane < (bt0.y & 0xffffu) ? W.slots[2u * (bt0.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
-  uint4 sl1 = (W.nbundles > 1 && lane < (bt1.y & 0xffffu)) ? W.slots[2u * (bt1.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
-  for (uint32_t k = 0; k < W.nbundles; ++k) {
+  uint2 bt0 = bundles[0];
+  uint2 bt1 = nb > 1 ? bundles[1] : bt0;
+  uint4 sl0 = lane < (bt0.y & 0xffffu) ? slots[3u * (bt0.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
+  uint4 sl1 = (nb > 1 && lane < (bt1.y & 0xffffu)) ? slots[3u * (bt1.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
+  for (uint32_t k = 0; k < nb; ++k) {
     const uint2 bt = bt0;
     const uint4 sl = sl0;
     bt0 = bt1;
     sl0 = sl1;
-    if (k + 2 < W.nbundles) {
-      bt1 = W.bundles[k + 2];
-      sl1 = lane < (bt1.y & 0xffffu) ? W.slots[2u * (bt1.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
+    if (k + 2 < nb) {
+      bt1 = bundles[k + 2];
+      sl1 = lane < (bt1.y & 0xffffu) ? slots[3u * (bt1.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
     }
     const bool act = lane < (bt.y & 0xffffu);
     Iv r = iv(0.0f);
@@ -799,7 +806,7 @@ __device__ Iv wide_forward(const WideDev &W, float2 *rfw, uint32_t lane, Iv x, I
       r = op_forward<D>(h, A, B, lit);
       if (lg) lg[(size_t)k * 32u + lane] = make_float4(A.lo, A.hi, B.lo, B.hi);
       if (dec && TSI_H_IS_MINMAX(h)) {
-        const uint32_t mm = W.slots[2u * (bt.x + lane) + 1u].w;
+        const uint32_t mm = slots[3u * (bt.x + lane) + 1u].w;
         const bool amax = (h == H_MAX_II || h == H_MAX_IF);
         const bool a_below = A.hi < B.lo, b_below = B.hi < A.lo;
         if (amax ? b_below : a_below) atomicOr(&dec[mm].x, cellbit);
@@ -810,35 +817,56 @@ __device__ Iv wide_forward(const WideDev &W, float2 *rfw, uint32_t lane, Iv x, I
     if (act) rfw[dst] = make_float2(r.lo, r.hi);
     __syncwarp();
   }
-  const float2 f = rfw[W.out_reg];
+  const float2 f = rfw[out_reg];
   __syncwarp();
   return Iv{f.x, f.y};
 }
 
+// Sum of a value's contribution records, last user first, onto +0: the
+// accumulation order of the sequential reverse pass.
 template <bool D>
-__device__ void wide_reverse(const WideDev &W, float2 *rfw, uint32_t lane, const float4 *lg, Iv sens[4]) {
+__device__ __forceinline__ Iv gather_sens(const float2 *ctb, uint32_t base, uint32_t count) {
+  Iv S = iv(0.0f);
+  for (uint32_t i = 0; i < count; ++i) {
+    const float2 c = ctb[base + i];
+    S = IA<D>::add(Iv{c.x, c.y}, S);
+  }
+  return S;
+}
+
+// Reverse interval AD over the bundled tape (compute.wgsl:3786-3900), one
+// lane per slot.  A single-use operand accumulates in its register; an
+// operand with several users gets a contribution record (ctb), summed when
+// the reverse pass reaches the value.
+template <bool D>
+__device__ void wide_reverse(const WideDev &W, float2 *rfw, uint32_t lane, const float4 *lg, float2 *ctb,
+                             Iv sens[4]) {
   using I = IA<D>;
+  const uint2 *__restrict__ bundles = W.bundles;
+  const uint4 *__restrict__ slots = W.slots;
+  const int nb = (int)W.nbundles;
   for (uint32_t r = lane; r < W.nregs; r += 32u) rfw[r] = make_float2(0.0f, 0.0f);
   __syncwarp();
   if (lane == 0) rfw[W.out_reg] = make_float2(1.0f, 1.0f);
   __syncwarp();
-  const int nb = (int)W.nbundles;
-  uint2 btn = W.bundles[nb - 1];
-  uint4 sln = lane < (btn.y & 0xffffu) ? W.slots[2u * (btn.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
-  float4 Ln = lane < (btn.y & 0xffffu) ? lg[(size_t)(nb - 1) * 32u + lane] : make_float4(0, 0, 0, 0);
+  const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
+  uint2 btn = bundles[nb - 1];
+  bool an = lane < btn.y;
+  uint4 s0n = an ? slots[3u * (btn.x + lane)] : zero4;
+  uint4 s2n = an ? slots[3u * (btn.x + lane) + 2u] : zero4;
+  float4 Ln = an ? lg[(size_t)(nb - 1) * 32u + lane] : make_float4(0, 0, 0, 0);
   for (int k = nb - 1; k >= 0; --k) {
-    const uint2 bt = btn;
-    const uint4 sl = sln;
+    const bool act = an;
+    const uint4 sl = s0n, s2 = s2n;
     const float4 L = Ln;
     if (k > 0) {  // next (lower) bundle, fetched while this one runs
-      btn = W.bundles[k - 1];
-      const bool an = lane < (btn.y & 0xffffu);
-      sln = an ? W.slots[2u * (btn.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
+      btn = bundles[k - 1];
+      an = lane < btn.y;
+      s0n = an ? slots[3u * (btn.x + lane)] : zero4;
+      s2n = an ? slots[3u * (btn.x + lane) + 2u] : zero4;
       Ln = an ? lg[(size_t)(k - 1) * 32u + lane] : make_float4(0, 0, 0, 0);
     }
-    const bool act = lane < (bt.y & 0xffffu);
-    const uint32_t maxr = bt.y >> 16;
-    uint32_t h = H_CONST, fa = 0, fb = 0, dst = 0, a = 0, b = 0, round = 0;
+    uint32_t h = H_CONST, fa = 0, fb = 0, dst = 0, a = 0, b = 0;
     float lit = 0.0f;
     Iv A = iv(0.0f), B = iv(0.0f), s = iv(0.0f);
     if (act) {
@@ -848,56 +876,67 @@ __device__ void wide_reverse(const WideDev &W, float2 *rfw, uint32_t lane, const
       dst = sl.y & 0xffffu;
       a = sl.y >> 16;
       b = sl.z & 0xffffu;
-      round = sl.z >> 16;
       lit = __uint_as_float(sl.w);
       A = Iv{L.x, L.y};
       B = Iv{L.z, L.w};
-      const float2 sv = rfw[dst];
-      s = Iv{sv.x, sv.y};
+      if (s2.w) {
+        s = gather_sens<D>(ctb, s2.z, s2.w);
+      } else {
+        const float2 sv = rfw[dst];
+        s = Iv{sv.x, sv.y};
+      }
     }
     __syncwarp();
     if (act) rfw[dst] = make_float2(0.0f, 0.0f);
     __syncwarp();
-    const bool II = TSI_H_IS_II(h);
-    bool skip = false;
-    Iv c0 = iv(0.0f), c1 = iv(0.0f);
     if (act && h != H_CONST) {
+      const bool II = TSI_H_IS_II(h);
       const bool s0 = (s.lo == 0.0f && s.hi == 0.0f);
-      skip = II ? (s0 && fa && fb) : (s0 && fa);
+      const bool skip = II ? (s0 && fa && fb) : (s0 && fa);
+      Iv c0 = iv(0.0f), c1 = iv(0.0f);
       if (!skip) {
         Iv r0, r1;
         op_reverse_rule<D>(h, A, B, lit, r0, r1);
         c0 = I::mul(I::fix(r0), s);
         if (II) c1 = I::mul(I::fix(r1), s);
       }
-    }
-    for (uint32_t rd = 0; rd <= maxr; ++rd) {
-      if (act && h != H_CONST && round == rd) {
-        if (II) {
-          if (skip) {
-            rfw[a] = make_float2(0.0f, 0.0f);
-            rfw[b] = make_float2(0.0f, 0.0f);
-          } else {
-            const float2 pa = rfw[a], pb = rfw[b];
-            const Iv n0 = I::add(c0, Iv{pa.x, pa.y});
-            const Iv n1 = I::add(c1, Iv{pb.x, pb.y});
-            rfw[a] = make_float2(n0.lo, n0.hi);
-            rfw[b] = make_float2(n1.lo, n1.hi);
-          }
+      // both operands read before either is written (an instruction whose
+      // operands are one value keeps the second write)
+      const float2 pa = (s2.x == TSI_NONE && !skip) ? rfw[a] : make_float2(0.0f, 0.0f);
+      const float2 pb = (II && s2.y == TSI_NONE && !skip) ? rfw[b] : make_float2(0.0f, 0.0f);
+      if (s2.x != TSI_NONE) {
+        ctb[s2.x] = make_float2(c0.lo, c0.hi);
+      } else if (skip) {
+        rfw[a] = make_float2(0.0f, 0.0f);
+      } else {
+        const Iv n0 = I::add(c0, Iv{pa.x, pa.y});
+        rfw[a] = make_float2(n0.lo, n0.hi);
+      }
+      if (II) {
+        if (s2.y != TSI_NONE) {
+          ctb[s2.y] = make_float2(c1.lo, c1.hi);
         } else if (skip) {
-          rfw[a] = make_float2(0.0f, 0.0f);
+          rfw[b] = make_float2(0.0f, 0.0f);
         } else {
-          const float2 pa = rfw[a];
-          const Iv n0 = I::add(c0, Iv{pa.x, pa.y});
-          rfw[a] = make_float2(n0.lo, n0.hi);
+          const Iv n1 = I::add(c1, Iv{pb.x, pb.y});
+          rfw[b] = make_float2(n1.lo, n1.hi);
         }
       }
-      __syncwarp();
+    }
+    __syncwarp();
+  }
+  Iv g = iv(0.0f);
+  if (lane < 4u) {
+    const uint32_t gc = W.arg_gcount[lane];
+    if (gc) {
+      g = gather_sens<D>(ctb, W.arg_gbase[lane], gc);
+    } else {
+      const float2 v = rfw[lane];
+      g = Iv{v.x, v.y};
     }
   }
   for (int q = 0; q < 4; ++q) {
-    const float2 v = rfw[q];
-    sens[q] = Iv{v.x, v.y};
+    sens[q] = Iv{__shfl_sync(FULL_MASK, g.lo, q), __shfl_sync(FULL_MASK, g.hi, q)};
   }
   __syncwarp();
 }
@@ -1020,13 +1059,16 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
   Iv sens[4] = {iv(0.0f), iv(0.0f), iv(0.0f), iv(0.0f)};
   float4 *lg = nullptr;
   bool ok = true;
+  // operand log (32 float4 per bundle), then the contribution records
+  // (2 per float4)
+  const unsigned long long need =
+      (unsigned long long)W.nbundles * 32ull + ((unsigned long long)W.ncontrib + 1ull) / 2ull;
   if (take_deriv) {
-    if (W.nbundles <= P.slice_len) {
+    if (need <= (unsigned long long)P.slice_len * 32ull) {
       lg = slice_log;
     } else {
-      const unsigned long long need = (unsigned long long)W.nbundles * 32ull;
       unsigned long long off = 0;
-      if (lane == 0) off = atomicAdd(P.log_overflow_used, need);
+      if (lane == 0) off = atomicAdd(P.log_overflow_used + level, need);
       off = __shfl_sync(FULL_MASK, off, 0);
       if (off + need > P.log_overflow_cap) {
         if (lane == 0) atomicOr(P.error, EB_LOG_OOM);
@@ -1037,8 +1079,15 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
     }
   }
   if (evaluate && ok) {
+    const long long c0 = clock64();
     field = wide_forward<D>(W, rfw, lane, cx, cy, cz, targ, lg, want_prune ? dec : nullptr, 1u << k);
-    if (take_deriv) wide_reverse<D>(W, rfw, lane, lg, sens);
+    const long long c1 = clock64();
+    if (take_deriv)
+      wide_reverse<D>(W, rfw, lane, lg, reinterpret_cast<float2 *>(lg + (size_t)W.nbundles * 32u), sens);
+    if (threadIdx.x == 0) {
+      ws[ST_CYC_WIDE_FWD] += (unsigned long long)(c1 - c0);
+      ws[ST_CYC_WIDE_REV] += (unsigned long long)(clock64() - c1);
+    }
   }
 
   // ---- temporal error bound, fast flag, classification (3966-4045)
@@ -1153,15 +1202,26 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
     for (uint32_t i = threadIdx.x; i < root.len + 4u; i += blockDim.x) flags[i] = 0;
     __syncthreads();
     if (k == 0) {
+      const uint2 *__restrict__ bundles = W.bundles;
+      const uint4 *__restrict__ slots = W.slots;
       if (lane == 0) flags[root.len + 3u] = 1;
       __syncwarp();
-      for (int kb = (int)W.nbundles - 1; kb >= 0; --kb) {
-        const uint2 bt = W.bundles[kb];
-        if (lane < (bt.y & 0xffffu)) {
-          const uint32_t si = bt.x + lane;
-          const uint4 s1 = W.slots[2u * si + 1u];
+      // slots fetched one bundle ahead
+      int kb = (int)W.nbundles - 1;
+      uint2 btn = bundles[kb];
+      uint4 s1n = lane < btn.y ? slots[3u * (btn.x + lane) + 1u] : make_uint4(0u, 0u, 0u, 0u);
+      uint32_t hn = lane < btn.y ? (slots[3u * (btn.x + lane)].x & 63u) : 0u;
+      for (; kb >= 0; --kb) {
+        const uint2 bt = btn;
+        const uint4 s1 = s1n;
+        const uint32_t h = hn;
+        if (kb > 0) {
+          btn = bundles[kb - 1];
+          s1n = lane < btn.y ? slots[3u * (btn.x + lane) + 1u] : make_uint4(0u, 0u, 0u, 0u);
+          hn = lane < btn.y ? (slots[3u * (btn.x + lane)].x & 63u) : 0u;
+        }
+        if (lane < bt.y) {
           if (flags[s1.x]) {
-            const uint32_t h = W.slots[2u * si].x & 63u;
             bool la = s1.y != TSI_NONE, lb = s1.z != TSI_NONE;
             if (TSI_H_IS_MINMAX(h)) {
               const uint2 d = dec[s1.w];
@@ -1275,50 +1335,47 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
     const uint32_t n = __popc(E);
     if (len >= W.min_len) {  // stay on the wide path: one item per child
       const uint32_t pos = atomicAdd(&P.witem_count[level + 1], n);
-      if (pos + n > P.item_cap) {
-        atomicOr(P.error, EB_QUEUE_FULL);
-      } else {
-        uint32_t e = E, j = 0;
-        while (e) {
-          const uint32_t bit = __ffs(e) - 1u;
-          e &= e - 1u;
-          WorkItem wi;
-          wi.scene = it.scene;
-          wi.rec = new_rec;
-          wi.n = 1;
-          wi.level = level + 1;
-          wi.parent[0] = wi.parent[1] = wi.parent[2] = wi.parent[3] = base + bit;
-          P.witems[(level + 1) & 1][pos + j++] = wi;
-        }
+      // every reserved slot below the capacity is written; the rest are
+      // dropped and reported
+      if (pos + n > P.item_cap) atomicOr(P.error, EB_QUEUE_FULL);
+      uint32_t e = E, j = 0;
+      while (e && pos + j < P.item_cap) {
+        const uint32_t bit = __ffs(e) - 1u;
+        e &= e - 1u;
+        WorkItem wi;
+        wi.scene = it.scene;
+        wi.rec = new_rec;
+        wi.n = 1;
+        wi.level = level + 1;
+        wi.parent[0] = wi.parent[1] = wi.parent[2] = wi.parent[3] = base + bit;
+        P.witems[(level + 1) & 1][pos + j++] = wi;
       }
     } else {
       const uint32_t nitems = (n + 3u) >> 2;
       const uint32_t pos = atomicAdd(&P.item_count[level + 1], nitems);
-      if (pos + nitems > P.item_cap) {
-        atomicOr(P.error, EB_QUEUE_FULL);
-      } else {
-        uint32_t e = E;
-        for (uint32_t j = 0; j < nitems; ++j) {
-          WorkItem wi;
-          wi.scene = it.scene;
-          wi.rec = new_rec;
-          wi.level = level + 1;
-          uint32_t c = 0;
-          while (e && c < 4u) {
-            const uint32_t bit = __ffs(e) - 1u;
-            e &= e - 1u;
-            wi.parent[c++] = base + bit;
-          }
-          wi.n = c;
-          for (uint32_t q = c; q < 4u; ++q) wi.parent[q] = wi.parent[0];
-          P.items[(level + 1) & 1][pos + j] = wi;
+      if (pos + nitems > P.item_cap) atomicOr(P.error, EB_QUEUE_FULL);
+      uint32_t e = E;
+      for (uint32_t j = 0; j < nitems && pos + j < P.item_cap; ++j) {
+        WorkItem wi;
+        wi.scene = it.scene;
+        wi.rec = new_rec;
+        wi.level = level + 1;
+        uint32_t c = 0;
+        while (e && c < 4u) {
+          const uint32_t bit = __ffs(e) - 1u;
+          e &= e - 1u;
+          wi.parent[c++] = base + bit;
         }
+        wi.n = c;
+        for (uint32_t q = c; q < 4u; ++q) wi.parent[q] = wi.parent[0];
+        P.items[(level + 1) & 1][pos + j] = wi;
       }
     }
   }
 }
 
-__global__ void __launch_bounds__(256) refine_kernel(LaunchParams P, uint32_t level, uint32_t rcap) {
+__global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ LaunchParams P, uint32_t level,
+                                                     uint32_t rcap) {
   extern __shared__ float2 smem_regs[];
   __shared__ unsigned long long s_stats[kWarps][ST_COUNT];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
@@ -1337,18 +1394,29 @@ __global__ void __launch_bounds__(256) refine_kernel(LaunchParams P, uint32_t le
     const uint32_t n_w = min(P.witem_count[level], P.item_cap);
     uint2 *dec = P.wide_dec + (size_t)blockIdx.x * P.wide_dec_stride;
     uint8_t *flg = P.wide_flags + (size_t)blockIdx.x * P.wide_flag_stride;
+    if (P.wide_smem) {
+      dec = reinterpret_cast<uint2 *>(smem_regs + (size_t)kWarps * rcap * 32u);
+      flg = reinterpret_cast<uint8_t *>(dec + P.wide_dec_stride);
+    }
     while (true) {
       if (threadIdx.x == 0) s_idx = atomicAdd(&P.witem_cursor[level], 1u);
       __syncthreads();
       const uint32_t idx = s_idx;
       __syncthreads();
       if (idx >= n_w) break;
-      const WorkItem it = P.witems[level & 1][idx];
+      const WorkItem &it = P.witems[level & 1][idx];  // read in place (the next level writes the other list)
+      const long long c0 = clock64();
       if (P.scenes[it.scene].flags & SF_DIRECTED)
         process_wide<true>(P, it, level, rf, slice_log, dec, flg, sh, s_stats[0]);
       else
         process_wide<false>(P, it, level, rf, slice_log, dec, flg, sh, s_stats[0]);
       __syncthreads();
+      if (threadIdx.x == 0) {
+        const unsigned long long c = (unsigned long long)(clock64() - c0);
+        s_stats[0][ST_WIDE_ITEMS] += 1;
+        s_stats[0][ST_CYC_WIDE] += c;
+        s_stats[0][ST_CYC_WIDE_MAX] = max(s_stats[0][ST_CYC_WIDE_MAX], c);
+      }
     }
   }
 
@@ -1359,10 +1427,16 @@ __global__ void __launch_bounds__(256) refine_kernel(LaunchParams P, uint32_t le
     if (lane == 0) idx = atomicAdd(&P.item_cursor[level], 1u);
     idx = __shfl_sync(FULL_MASK, idx, 0);
     if (idx >= n_items) break;
-    const WorkItem it = items[idx];
+    const WorkItem &it = items[idx];
+    const long long c0 = clock64();
     if (P.scenes[it.scene].flags & SF_DIRECTED) process_item<true>(P, it, level, rf, slice_log, slice_dec, ws);
     else process_item<false>(P, it, level, rf, slice_log, slice_dec, ws);
     __syncwarp();
+    if (lane == 0) {
+      const unsigned long long c = (unsigned long long)(clock64() - c0);
+      ws[ST_CYC_NARROW] += c;
+      ws[ST_CYC_NARROW_MAX] = max(ws[ST_CYC_NARROW_MAX], c);
+    }
   }
   // deallocation items: 4 bricks per warp
   const uint32_t n_dealloc = min(P.dealloc_count[level], P.dealloc_cap);
@@ -1379,8 +1453,13 @@ __global__ void __launch_bounds__(256) refine_kernel(LaunchParams P, uint32_t le
   }
   __syncwarp();
   if (lane < ST_COUNT && ws[lane]) {
-    atomicAdd(&P.stats[lane], ws[lane]);
-    atomicAdd(&P.level_stats[level * ST_COUNT + lane], ws[lane]);
+    if (lane == ST_CYC_WIDE_MAX || lane == ST_CYC_NARROW_MAX) {
+      atomicMax(&P.stats[lane], ws[lane]);
+      atomicMax(&P.level_stats[level * ST_COUNT + lane], ws[lane]);
+    } else {
+      atomicAdd(&P.stats[lane], ws[lane]);
+      atomicAdd(&P.level_stats[level * ST_COUNT + lane], ws[lane]);
+    }
   }
 }
 
@@ -1410,8 +1489,11 @@ __global__ void frame_begin_kernel(LaunchParams P) {
     w.parent[0] = w.parent[1] = w.parent[2] = w.parent[3] = 0u;
     const SceneLaunch &S = P.scenes[s];
     const uint32_t len = P.recs[S.root_rec].len;
-    if (len >= S.wide.min_len) P.witems[0][atomicAdd(&P.witem_count[0], 1u)] = w;
-    else P.items[0][atomicAdd(&P.item_count[0], 1u)] = w;
+    uint32_t *count = len >= S.wide.min_len ? P.witem_count : P.item_count;
+    WorkItem *list = len >= S.wide.min_len ? P.witems[0] : P.items[0];
+    const uint32_t pos = atomicAdd(count, 1u);
+    if (pos < P.item_cap) list[pos] = w;
+    else atomicOr(P.error, EB_QUEUE_FULL);
   }
 }
 
@@ -1452,8 +1534,19 @@ cudaError_t launch_frame_end(const LaunchParams &P, cudaStream_t st) {
   frame_end_kernel<<<P.n_scenes, 256, 0, st>>>(P);
   return cudaGetLastError();
 }
+// The attribute belongs to the kernel on the current device, shared by every
+// context of the process: only ever raise it.
 cudaError_t refine_set_smem(size_t bytes) {
-  return cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  static std::mutex mu;
+  static size_t set_bytes[64] = {0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && bytes <= set_bytes[dev]) return cudaSuccess;
+  e = cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess && dev >= 0 && dev < 64) set_bytes[dev] = bytes;
+  return e;
 }
 cudaError_t refine_occupancy(int block, size_t smem, int *blocks_per_sm) {
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, refine_kernel, block, smem);

@@ -169,36 +169,76 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
       opa[j] = ins[j].rarg.reg;
     }
   }
-  // List scheduling in program order, width 32.  Users of one value keep
-  // their program order across bundles (a later user is never placed in an
-  // earlier bundle): the reverse pass accumulates into that value's
-  // sensitivity user by user, and the order fixes the rounding.
+  auto handler = [&](uint32_t j) { return TSI_W0_H(narrow.code[2 * (j - 4)]); };
+  // users of every value, in program order (an instruction reading one value
+  // through both operands is one user)
   std::vector<std::vector<uint32_t>> users(n);
   for (uint32_t j = 4; j < n; ++j) {
     if (opa[j] != TSI_NONE) users[opa[j]].push_back(j);
     if (opb[j] != TSI_NONE && opb[j] != opa[j]) users[opb[j]].push_back(j);
   }
-  std::vector<uint32_t> next_user(n, 0);  // index into users[v] of its first unscheduled user
+  // The reverse pass accumulates a value's sensitivity user by user, in
+  // reverse program order, and that order fixes the rounding.  A value with
+  // one user accumulates in its register; a value with several gets one
+  // contribution record per user, which the value sums in that order when
+  // the reverse pass reaches it.  The skip rule (zero sensitivity of a
+  // single-use operand) overwrites the register, so it needs the ir.rs use
+  // count to agree with the users found here.
+  for (uint32_t j = 4; j < n; ++j) {
+    const uint32_t w0 = narrow.code[2 * (j - 4)];
+    if ((TSI_W0_FA(w0) && opa[j] != TSI_NONE && users[opa[j]].size() != 1) ||
+        (TSI_W0_FB(w0) && opb[j] != TSI_NONE && users[opb[j]].size() != 1)) {
+      status = TSI_ERR_INVALID_ARGUMENT;
+      why = "single-use flag on a value with several users";
+      return false;
+    }
+  }
+  std::vector<uint32_t> gbase(n, TSI_NONE), rec_a(n, TSI_NONE), rec_b(n, TSI_NONE);
+  uint32_t ncontrib = 0;
+  for (uint32_t v = 0; v < n; ++v) {
+    if (users[v].size() < 2) continue;
+    gbase[v] = ncontrib;
+    for (size_t u = users[v].size(); u-- > 0;) {  // last user first
+      const uint32_t j = users[v][u];
+      if (opa[j] == v) rec_a[j] = ncontrib;
+      if (opb[j] == v) rec_b[j] = ncontrib;
+      ++ncontrib;
+    }
+  }
+  // List scheduling, width 32, one handler per bundle: a warp executes a
+  // bundle with one lane per slot, so a bundle of one handler runs without
+  // divergence.  Each bundle takes the handler with the most instructions
+  // ready (the oldest ready instruction's on a tie), oldest first.
   std::vector<int32_t> bundle_of(n, -1);
   for (uint32_t a = 0; a < 4; ++a) bundle_of[a] = -2;  // arguments: before everything
   std::vector<std::vector<uint32_t>> bundles;
   std::vector<uint32_t> pending;
   pending.reserve(n - 4);
   for (uint32_t j = 4; j < n; ++j) pending.push_back(j);
-  auto in_turn = [&](uint32_t v, uint32_t j) { return v == TSI_NONE || users[v][next_user[v]] == j; };
+  std::vector<uint32_t> ready_count(64, 0);
   while (!pending.empty()) {
-    std::vector<uint32_t> b;
     const int32_t k = int32_t(bundles.size());
-    std::vector<uint32_t> rest;
+    auto ready = [&](uint32_t j) {
+      return (opa[j] == TSI_NONE || (bundle_of[opa[j]] != -1 && bundle_of[opa[j]] < k)) &&
+             (opb[j] == TSI_NONE || (bundle_of[opb[j]] != -1 && bundle_of[opb[j]] < k));
+    };
+    std::fill(ready_count.begin(), ready_count.end(), 0u);
+    uint32_t hsel = 64, best = 0;
+    for (uint32_t j : pending) {
+      if (!ready(j)) continue;
+      const uint32_t c = ++ready_count[handler(j)];
+      if (c > best) {
+        best = c;
+        hsel = handler(j);
+      }
+      if (c == 32) break;
+    }
+    std::vector<uint32_t> b, rest;
     rest.reserve(pending.size());
     for (uint32_t j : pending) {
-      const bool deps = (opa[j] == TSI_NONE || (bundle_of[opa[j]] != -1 && bundle_of[opa[j]] < k)) &&
-                        (opb[j] == TSI_NONE || (bundle_of[opb[j]] != -1 && bundle_of[opb[j]] < k));
-      if (b.size() < 32 && deps && in_turn(opa[j], j) && in_turn(opb[j], j)) {
+      if (b.size() < 32 && handler(j) == hsel && ready(j)) {
         b.push_back(j);
         bundle_of[j] = k;
-        if (opa[j] != TSI_NONE) next_user[opa[j]]++;
-        if (opb[j] != TSI_NONE && opb[j] != opa[j]) next_user[opb[j]]++;
       } else {
         rest.push_back(j);
       }
@@ -251,7 +291,7 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
   }
   // slots
   const uint32_t nslots = n - 4;
-  out.slots.assign(size_t(nslots) * 8, 0);
+  out.slots.assign(size_t(nslots) * 12, 0);
   out.bundles.assign(size_t(nb) * 2, 0);
   out.narrow_mm.assign(nslots, TSI_NONE);
   {
@@ -264,48 +304,46 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
   uint32_t off = 0;
   for (uint32_t k = 0; k < nb; ++k) {
     const std::vector<uint32_t> &b = bundles[k];
-    // reverse rounds: descending slot order, a slot waits for every higher
-    // slot that accumulates into one of its target registers
-    std::vector<uint32_t> round(b.size(), 0);
-    uint32_t maxr = 0;
-    for (int s = int(b.size()) - 1; s >= 0; --s) {
-      const uint32_t j = b[size_t(s)];
-      uint32_t r = 0;
-      for (int t = int(b.size()) - 1; t > s; --t) {
-        const uint32_t q = b[size_t(t)];
-        bool share = false;
-        for (uint32_t x : {opa[j], opb[j]})
-          for (uint32_t y : {opa[q], opb[q]})
-            if (x != TSI_NONE && y != TSI_NONE && reg[x] == reg[y]) share = true;
-        if (share) r = std::max(r, round[size_t(t)] + 1);
-      }
-      round[size_t(s)] = r;
-      maxr = std::max(maxr, r);
-    }
-    if (maxr > 0xffffu) {
-      status = TSI_ERR_TAPE_TOO_WIDE;
-      why = "too many accumulation rounds in one bundle";
+    // registers accumulated into by this bundle's reverse step: single-use
+    // operands, distinct by construction (both live when the bundle reads)
+    std::vector<uint32_t> acc;
+    for (uint32_t j : b)
+      for (uint32_t v : {opa[j], opb[j]})
+        if (v != TSI_NONE && gbase[v] == TSI_NONE && !(v == opb[j] && opb[j] == opa[j])) acc.push_back(reg[v]);
+    std::sort(acc.begin(), acc.end());
+    if (std::adjacent_find(acc.begin(), acc.end()) != acc.end()) {
+      status = TSI_ERR_INVALID_ARGUMENT;
+      why = "two slots of one bundle accumulate into one register";
       return false;
     }
     for (size_t s = 0; s < b.size(); ++s) {
       const uint32_t j = b[s];
       const uint32_t w0 = narrow.code[2 * (j - 4)], w1 = narrow.code[2 * (j - 4) + 1];
       const uint32_t h = TSI_W0_H(w0);
-      uint32_t *S = &out.slots[size_t(off + s) * 8];
+      uint32_t *S = &out.slots[size_t(off + s) * 12];
       S[0] = h | (TSI_W0_FA(w0) << 6) | (TSI_W0_FB(w0) << 7);
       const uint32_t ra = opa[j] != TSI_NONE ? reg[opa[j]] : 0, rb = opb[j] != TSI_NONE ? reg[opb[j]] : 0;
       S[1] = reg[j] | (ra << 16);
-      S[2] = rb | (round[s] << 16);
+      S[2] = rb;
       S[3] = TSI_H_IS_II(h) ? 0u : w1;  // literal bits
       S[4] = j;
       S[5] = opa[j];
       S[6] = opb[j];
       S[7] = out.narrow_mm[j - 4];
+      S[8] = rec_a[j];
+      S[9] = rec_b[j];
+      S[10] = gbase[j];
+      S[11] = gbase[j] == TSI_NONE ? 0u : uint32_t(users[j].size());
     }
     out.bundles[2 * k] = off;
-    out.bundles[2 * k + 1] = uint32_t(b.size()) | (maxr << 16);
+    out.bundles[2 * k + 1] = uint32_t(b.size());
     off += uint32_t(b.size());
   }
+  for (uint32_t a = 0; a < 4; ++a) {
+    out.arg_gbase[a] = gbase[a];
+    out.arg_gcount[a] = gbase[a] == TSI_NONE ? 0u : uint32_t(users[a].size());
+  }
+  out.ncontrib = ncontrib;
   out.nregs = maxreg + 1;
   out.nbundles = nb;
   out.out_reg = reg[n - 1];

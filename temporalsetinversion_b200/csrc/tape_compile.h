@@ -21,22 +21,29 @@ struct PackedTape {
 };
 
 // Bundled ("wide") form of a full tape, for evaluating one cell with a whole
-// warp: instructions are list-scheduled, in program order, into bundles of
-// at most 32 mutually independent instructions (one per lane), and given
-// their own register allocation in which a bundle reads all its operands
-// before it writes any result.  Per slot (2 x uint4):
+// warp: instructions are list-scheduled into bundles of at most 32 mutually
+// independent instructions of one handler (one per lane), and given their
+// own register allocation in which a bundle reads all its operands before
+// it writes any result.  Per slot (3 x uint4):
 //   s0.x  handler | single-use A << 6 | single-use B << 7
 //   s0.y  dst register | A register << 16
-//   s0.z  B register | reverse round << 16
+//   s0.z  B register
 //   s0.w  f32 literal
 //   s1    SSA slot of dst, A, B (TSI_NONE if absent), min/max ordinal
-// The reverse round orders, within a bundle, the slots that accumulate into
-// the same sensitivity register: highest slot first, as the sequential
-// reverse pass (compute.wgsl:3786) does.
+//   s2    contribution record of A, of B (TSI_NONE: the operand has one
+//         user and accumulates in its register); first record and record
+//         count of dst (count 0: dst has at most one user)
+// A value with several users gets one contribution record per user, last
+// user first, and sums them in that order when the reverse pass reaches it:
+// the order of the sequential reverse pass (compute.wgsl:3786), whatever
+// bundles the users fall in.
 struct WideTape {
-  std::vector<uint32_t> slots;    // 8 words per slot
-  std::vector<uint32_t> bundles;  // 2 words per bundle: slot offset, count | max_round << 16
+  std::vector<uint32_t> slots;    // 12 words per slot
+  std::vector<uint32_t> bundles;  // 2 words per bundle: slot offset, count
   std::vector<uint32_t> narrow_mm;  // per narrow instruction: min/max ordinal or TSI_NONE
+  uint32_t arg_gbase[4] = {TSI_NONE, TSI_NONE, TSI_NONE, TSI_NONE};  // records of x, y, z, t
+  uint32_t arg_gcount[4] = {0, 0, 0, 0};
+  uint32_t ncontrib = 0;          // contribution records per cell
   uint32_t nregs = 0;
   uint32_t nbundles = 0;
   uint32_t out_reg = 0;
