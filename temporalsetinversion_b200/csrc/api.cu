@@ -101,7 +101,7 @@ struct tsi_tape {
   uint4 *d_wslots = nullptr;
   uint2 *d_wbundles = nullptr;
   uint32_t *d_wmm = nullptr;
-  uint32_t wbundles = 0, wregs = 0, wout = 0, wmin_len = 0xffffffffu, wcontrib = 0;
+  uint32_t wslots = 0, wbundles = 0, wvalues = 0, wmin_len = 0xffffffffu, wcontrib = 0;
   uint32_t warg_gbase[4] = {TSI_NONE, TSI_NONE, TSI_NONE, TSI_NONE}, warg_gcount[4] = {0, 0, 0, 0};
 };
 
@@ -136,9 +136,15 @@ struct tsi_ctx {
   uint32_t *d_item_count = nullptr, *d_item_cursor = nullptr;
   WorkItem *d_witems[2] = {nullptr, nullptr};
   uint32_t *d_witem_count = nullptr, *d_witem_cursor = nullptr;
-  uint2 *d_wide_dec = nullptr;
-  uint8_t *d_wide_flags = nullptr;
-  uint32_t wide_dec_stride = 0, wide_flag_stride = 0;
+  // wide path: per-cell hand-over to the group (per level parity) and, for
+  // tapes whose working set exceeds shared memory, per-block scratch
+  CellInfo *d_cell_info[2] = {nullptr, nullptr};
+  uint32_t *d_cell_bits[2] = {nullptr, nullptr};
+  size_t cell_arena_bytes = 0;  // of each parity's info + bits
+  uint32_t witem_cap = 0, bm_words = 0;
+  unsigned char *d_cell_scratch = nullptr;
+  size_t cell_scratch_bytes = 0;
+  uint32_t cell_bytes = 0, cell_smem = 0;
   uint2 *d_dealloc[2] = {nullptr, nullptr};
   uint32_t dealloc_cap = 0;
   uint32_t *d_dealloc_count = nullptr, *d_dealloc_cursor = nullptr;
@@ -201,10 +207,15 @@ LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes) {
   P.witems[1] = c->d_witems[1];
   P.witem_count = c->d_witem_count;
   P.witem_cursor = c->d_witem_cursor;
-  P.wide_dec = c->d_wide_dec;
-  P.wide_flags = c->d_wide_flags;
-  P.wide_dec_stride = c->wide_dec_stride;
-  P.wide_flag_stride = c->wide_flag_stride;
+  P.witem_cap = c->witem_cap;
+  P.bm_words = c->bm_words;
+  for (int q = 0; q < 2; ++q) {
+    P.cell_info[q] = c->d_cell_info[q];
+    P.cell_bits[q] = c->d_cell_bits[q];
+  }
+  P.cell_smem = c->cell_smem;
+  P.cell_bytes = c->cell_bytes;
+  P.cell_scratch = c->d_cell_scratch;
   P.dealloc_cap = c->dealloc_cap;
   P.dealloc[0] = c->d_dealloc[0];
   P.dealloc[1] = c->d_dealloc[1];
@@ -254,9 +265,9 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, Scene
   L.wide.slots = s->tape->d_wslots;
   L.wide.bundles = s->tape->d_wbundles;
   L.wide.narrow_mm = s->tape->d_wmm;
+  L.wide.nslots = s->tape->wslots;
   L.wide.nbundles = s->tape->wbundles;
-  L.wide.nregs = s->tape->wregs;
-  L.wide.out_reg = s->tape->wout;
+  L.wide.nvalues = s->tape->wvalues;
   L.wide.min_len = s->tape->wmin_len;
   L.wide.ncontrib = s->tape->wcontrib;
   for (int q = 0; q < 4; ++q) {
@@ -278,61 +289,99 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, Scene
   R.c_level = TSI_NONE;
 }
 
+// Launch geometry of one frame for n scenes.
+struct FramePlan {
+  uint32_t lmax = 0, rcap = 4;
+  size_t smem = 0;
+  int grid = 0;
+};
+
+// Sizes the launch for these scenes and grows the wide path's arenas (no
+// allocation when they are large enough, so a plan made once before stream
+// capture holds inside it).
+tsi_status plan_frame(tsi_ctx *c, tsi_scene *const *scenes, uint32_t n, FramePlan &fp) {
+  uint32_t rmax = 4, mm_max = 0, bm_words = 1;
+  size_t cell_bytes = 0;
+  bool any_wide = false;
+  fp.lmax = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const tsi_tape *t = scenes[i]->tape;
+    fp.lmax = std::max(fp.lmax, (uint32_t)scenes[i]->p.localsubdiv);
+    rmax = std::max(rmax, t->nregs);
+    if (t->d_wslots) {
+      any_wide = true;
+      mm_max = std::max(mm_max, t->n_minmax);
+    }
+  }
+  bm_words = std::max(1u, (mm_max + 15u) / 16u);
+  for (uint32_t i = 0; i < n; ++i) {  // the device's cell_layout, per scene
+    const tsi_tape *t = scenes[i]->tape;
+    if (!t->d_wslots) continue;
+    const size_t nv = t->wvalues;
+    const size_t bytes = 16 * nv + ((size_t(t->wcontrib) * 8 + 15) & ~size_t(15)) +
+                         ((size_t(bm_words) * 4 + 15) & ~size_t(15)) + ((nv + 15) & ~size_t(15));
+    cell_bytes = std::max(cell_bytes, bytes);
+  }
+  fp.rcap = (rmax + 3u) & ~3u;
+  const size_t regfile = (size_t)kWarpsPerBlock * fp.rcap * 32u * sizeof(float2);
+  // the wide cell's working set lives in shared memory when it fits
+  const bool cell_smem = any_wide && cell_bytes <= (160u << 10);
+  fp.smem = std::max(regfile, cell_smem ? cell_bytes : 0);
+  CK(refine_set_smem(fp.smem));
+  int bps = 0;
+  CK(refine_occupancy(kBlock, fp.smem, &bps));
+  if (bps < 1) return set_err(TSI_ERR_TAPE_TOO_WIDE, "register file does not fit in shared memory");
+  fp.grid = std::min<int>(bps * c->sm_count, (int)(c->max_warps / kWarpsPerBlock));
+  c->cell_smem = cell_smem ? 1u : 0u;
+  c->cell_bytes = (uint32_t)cell_bytes;
+  if (any_wide && !cell_smem) {
+    const size_t need = (size_t)fp.grid * cell_bytes;
+    if (need > c->cell_scratch_bytes) {
+      cudaFree(c->d_cell_scratch);
+      c->d_cell_scratch = nullptr;
+      c->cell_scratch_bytes = 0;
+      CK(dalloc(&c->d_cell_scratch, need));
+      c->cell_scratch_bytes = need;
+    }
+  }
+  // hand-over arenas: 64 MB per level parity, as many wide items as fit
+  const size_t per_item = 8 * (sizeof(CellInfo) + (size_t)bm_words * 4);
+  const size_t arena = std::max<size_t>(64u << 20, c->cell_arena_bytes);
+  if (arena > c->cell_arena_bytes || !c->d_cell_info[0]) {
+    for (int q = 0; q < 2; ++q) {
+      cudaFree(c->d_cell_info[q]);
+      c->d_cell_info[q] = nullptr;
+    }
+    c->cell_arena_bytes = 0;
+    for (int q = 0; q < 2; ++q) CK(dalloc((unsigned char **)&c->d_cell_info[q], arena));
+    c->cell_arena_bytes = arena;
+  }
+  c->bm_words = bm_words;
+  c->witem_cap = (uint32_t)std::min<size_t>(c->item_cap, c->cell_arena_bytes / per_item);
+  for (int q = 0; q < 2; ++q)
+    c->d_cell_bits[q] = reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(c->d_cell_info[q]) +
+                                                     (size_t)c->witem_cap * 8 * sizeof(CellInfo));
+  return TSI_OK;
+}
+
 // One frame of set inversion for n scenes, all levels in one launch sequence.
 tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *times, const float *t0s, uint32_t n) {
   if (n == 0) return TSI_OK;
   if (n > c->max_scenes) return set_err(TSI_ERR_INVALID_ARGUMENT, "too many scenes in one launch");
-  uint32_t lmax = 0, rmax = 4, mm_max = 1, slots_max = 8;
-  for (uint32_t i = 0; i < n; ++i) {
-    fill_launch(scenes[i], i, times[i], t0s[i], c->h_scenes[i], c->h_recs[i]);
-    lmax = std::max(lmax, (uint32_t)scenes[i]->p.localsubdiv);
-    rmax = std::max(rmax, scenes[i]->tape->nregs);
-    if (scenes[i]->tape->d_wslots) {
-      rmax = std::max(rmax, (scenes[i]->tape->wregs + 31u) / 32u);
-      mm_max = std::max(mm_max, scenes[i]->tape->n_minmax);
-      slots_max = std::max(slots_max, scenes[i]->tape->count);
-    }
-  }
-  {  // per-block scratch of the wide path
-    const uint32_t blocks = c->max_warps / kWarpsPerBlock;
-    const uint32_t dstride = (mm_max + 31u) & ~31u, fstride = (slots_max + 255u) & ~255u;
-    if (dstride > c->wide_dec_stride) {
-      cudaFree(c->d_wide_dec);
-      c->d_wide_dec = nullptr;
-      c->wide_dec_stride = 0;
-      CK(dalloc(&c->d_wide_dec, (size_t)blocks * dstride));
-      c->wide_dec_stride = dstride;
-    }
-    if (fstride > c->wide_flag_stride) {
-      cudaFree(c->d_wide_flags);
-      c->d_wide_flags = nullptr;
-      c->wide_flag_stride = 0;
-      CK(dalloc(&c->d_wide_flags, (size_t)blocks * fstride));
-      c->wide_flag_stride = fstride;
-    }
-  }
-  const uint32_t rcap = (rmax + 3u) & ~3u;
-  size_t smem = (size_t)kWarpsPerBlock * rcap * 32u * sizeof(float2);
-  // the wide path's branch ballots and liveness flags go to shared memory
-  // after the register file when they take at most 64 KB and the block at
-  // most 160 KB
-  const size_t wide_bytes = (size_t)c->wide_dec_stride * sizeof(uint2) + c->wide_flag_stride;
-  const bool wide_smem = wide_bytes <= (64u << 10) && smem + wide_bytes <= (160u << 10);
-  if (wide_smem) smem += wide_bytes;
-  CK(refine_set_smem(smem));
-  int bps = 0;
-  CK(refine_occupancy(kBlock, smem, &bps));
-  if (bps < 1) return set_err(TSI_ERR_TAPE_TOO_WIDE, "register file does not fit in shared memory");
-  int grid = bps * c->sm_count;
-  grid = std::min<int>(grid, (int)(c->max_warps / kWarpsPerBlock));
+  for (uint32_t i = 0; i < n; ++i) fill_launch(scenes[i], i, times[i], t0s[i], c->h_scenes[i], c->h_recs[i]);
+  FramePlan fp;
+  tsi_status pst = plan_frame(c, scenes, n, fp);
+  if (pst != TSI_OK) return pst;
+  const uint32_t lmax = fp.lmax, rcap = fp.rcap;
+  const size_t smem = fp.smem;
+  const int grid = fp.grid;
   CK(cudaMemcpyAsync(c->d_scenes, c->h_scenes, n * sizeof(SceneLaunch), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_recs, c->h_recs, n * sizeof(TapeRec), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->d_error, 0, sizeof(uint32_t), c->stream));
   CK(cudaMemsetAsync(c->d_stats, 0, ST_COUNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(c->d_level_stats, 0, (TSI_MAX_LEVELS + 1) * ST_COUNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(c->d_log_used, 0, (TSI_MAX_LEVELS + 1) * sizeof(unsigned long long), c->stream));
-  LaunchParams P = make_params(c, n);
-  P.wide_smem = wide_smem ? 1u : 0u;
+  const LaunchParams P = make_params(c, n);
   CK(launch_frame_begin(P, c->stream));
   const bool prof = c->profile_levels && c->level_events.size() >= lmax + 1;
   for (uint32_t level = 0; level < lmax; ++level) {
@@ -647,9 +696,9 @@ TSI_API tsi_status tsi_compile_wide_gpu_instructions(const tsi_gpu_instruction *
   WideTape wt;
   if (!compile_wide(ins, pt, wt, st, why)) return set_err(st, why);
   info->instruction_count = pt.count;
-  info->registers = wt.nregs;
+  info->registers = wt.nvalues;
   info->minmax_count = pt.n_minmax;
-  info->reserved = wt.out_reg;
+  info->reserved = wt.ncontrib;
   *n_bundles = wt.nbundles;
   if (slots)
     for (uint32_t i = 0; i < std::min<uint32_t>(cap_slot_words, (uint32_t)wt.slots.size()); ++i) slots[i] = wt.slots[i];
@@ -769,8 +818,8 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   cudaFree(c->d_witems[1]);
   cudaFree(c->d_witem_count);
   cudaFree(c->d_witem_cursor);
-  cudaFree(c->d_wide_dec);
-  cudaFree(c->d_wide_flags);
+  for (int q = 0; q < 2; ++q) cudaFree(c->d_cell_info[q]);
+  cudaFree(c->d_cell_scratch);
   cudaFree(c->d_dealloc[0]);
   cudaFree(c->d_dealloc[1]);
   cudaFree(c->d_dealloc_count);
@@ -828,12 +877,18 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
   // several times more instructions than bundles)
   if (t->len >= 256) {
     WideTape wt;
-    if (compile_wide(ins, pt, wt, st, why) && wt.nbundles > 0 && wt.nregs <= 32u * 255u) {
+    if (compile_wide(ins, pt, wt, st, why) && wt.nbundles > 0) {
+      // device layout: the three uint4 of every slot in three arrays
+      const size_t nsl = wt.slots.size() / 12;
+      std::vector<uint32_t> soa(wt.slots.size());
+      for (size_t i = 0; i < nsl; ++i)
+        for (size_t q = 0; q < 3; ++q)
+          for (size_t w = 0; w < 4; ++w) soa[(q * nsl + i) * 4 + w] = wt.slots[i * 12 + q * 4 + w];
       cudaError_t e = dalloc(&t->d_wslots, wt.slots.size() / 4);
       if (e == cudaSuccess) e = dalloc(&t->d_wbundles, wt.bundles.size() / 2);
       if (e == cudaSuccess) e = dalloc(&t->d_wmm, wt.narrow_mm.size());
       if (e == cudaSuccess)
-        e = cudaMemcpy(t->d_wslots, wt.slots.data(), wt.slots.size() * 4, cudaMemcpyHostToDevice);
+        e = cudaMemcpy(t->d_wslots, soa.data(), soa.size() * 4, cudaMemcpyHostToDevice);
       if (e == cudaSuccess)
         e = cudaMemcpy(t->d_wbundles, wt.bundles.data(), wt.bundles.size() * 4, cudaMemcpyHostToDevice);
       if (e == cudaSuccess)
@@ -843,9 +898,9 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
         tsi_tape_destroy(t);
         return TSI_ERR_CUDA;
       }
+      t->wslots = (uint32_t)nsl;
       t->wbundles = wt.nbundles;
-      t->wregs = wt.nregs;
-      t->wout = wt.out_reg;
+      t->wvalues = wt.nvalues;
       t->wmin_len = std::max<uint32_t>(256u, 3u * wt.nbundles);
       t->wcontrib = wt.ncontrib;
       for (int q = 0; q < 4; ++q) {
@@ -1255,7 +1310,18 @@ TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *c, tsi_request *reqs, uint32_
   g->ctx = c;
   g->reqs.assign(reqs, reqs + n);
   CK(cudaStreamSynchronize(c->stream));
-  // grow the shared-memory attribute and the frame buffers before capture
+  // grow the shared-memory attribute, the wide path's arenas and the frame
+  // buffers before capture
+  {
+    std::vector<tsi_scene *> sc(n);
+    for (uint32_t i = 0; i < n; ++i) sc[i] = reqs[i].scene;
+    FramePlan fp;
+    const tsi_status pst = plan_frame(c, sc.data(), n, fp);
+    if (pst != TSI_OK) {
+      delete g;
+      return pst;
+    }
+  }
   for (uint32_t i = 0; i < n; ++i)
     if (reqs[i].uniforms) {
       tsi_status st = ensure_image(reqs[i].scene, reqs[i].uniforms->resolution[0], reqs[i].uniforms->resolution[1]);

@@ -59,17 +59,17 @@ struct SceneCounters {
 };
 
 // Bundled form of a scene's full tape (tape_compile.h WideTape), evaluated
-// with one warp per cell for items whose tape is long.
+// with one block per cell for items whose tape is long.
 struct WideDev {
-  const uint4 *slots;         // 3 x uint4 per slot (tape_compile.h)
-  const uint2 *bundles;       // slot offset, count
+  const uint4 *slots;         // [3][nslots]: words 0-3, 4-7, 8-11 of each slot (tape_compile.h)
+  const uint2 *bundles;       // first slot, count | handler << 16
   const uint32_t *narrow_mm;  // min/max ordinal per narrow instruction
+  uint32_t nslots;
   uint32_t nbundles;
-  uint32_t nregs;
-  uint32_t out_reg;           // wide register of the field
+  uint32_t nvalues;           // SSA values (nslots + 4); the field is the last
   uint32_t min_len;           // tapes at least this long go to the wide path
   uint32_t ncontrib;          // reverse contribution records per cell
-  uint32_t arg_gbase[4];      // records of x, y, z, t (TSI_NONE: in its register)
+  uint32_t arg_gbase[4];      // records of x, y, z, t (TSI_NONE: one user)
   uint32_t arg_gcount[4];
 };
 
@@ -108,20 +108,32 @@ struct TapeRec {
   uint32_t c_level;
 };
 
+// A narrow item: up to four sibling parents evaluated by one warp.  A wide
+// item: one parent, its eight children evaluated by eight blocks; parent[1]
+// is the children's brick (allocated when the item was enqueued, TSI_NONE if
+// the pool was exhausted), parent[2] is 1 if that brick is new, parent[3]
+// counts the children done (the last one finishes the group).
 struct WorkItem {
   uint32_t scene;
   uint32_t rec;
-  uint32_t n;         // valid parents (1..4)
+  uint32_t n;         // valid parents (1..4; 1 for a wide item)
   uint32_t level;     // level of the parents
   uint32_t parent[4];
+};
+
+// What a wide item's child cell leaves for the block that finishes the group.
+struct CellInfo {
+  float nl, nh;       // time range its children will be evaluated over
+  uint32_t enq;       // 1: enqueued for subdivision
+  uint32_t pad;
 };
 
 enum tsi_stat_index {
   ST_PARENTS = 0, ST_EVAL, ST_REVERSE, ST_SKIPPED, ST_AMBIG, ST_EMPTY, ST_FULL, ST_ENQUEUED,
   ST_REUSED, ST_INSTR_FWD, ST_INSTR_REV, ST_INSTR_FULL, ST_FP32, ST_BRICK_ALLOC, ST_BRICK_FREE,
   ST_TAPE_WORDS, ST_PRUNE_FALLBACK,
-  // SM clock cycles (clock64): wide items (count, sum, max, and the forward
-  // and reverse passes of their first cell) and narrow items (sum, max)
+  // SM clock cycles (clock64): wide cells (count, sum, max, and their
+  // forward and reverse passes) and narrow items (sum, max)
   ST_WIDE_ITEMS, ST_CYC_WIDE, ST_CYC_WIDE_MAX, ST_CYC_WIDE_FWD, ST_CYC_WIDE_REV, ST_CYC_NARROW,
   ST_CYC_NARROW_MAX, ST_COUNT
 };
@@ -138,14 +150,19 @@ struct LaunchParams {
   WorkItem *items[2];
   uint32_t *item_count;    // [TSI_MAX_LEVELS + 1]
   uint32_t *item_cursor;   // [TSI_MAX_LEVELS + 1]
-  WorkItem *witems[2];     // wide items: one parent each, one block per item
+  WorkItem *witems[2];     // wide items: one parent each, one block per child cell
   uint32_t *witem_count;   // [TSI_MAX_LEVELS + 1]
-  uint32_t *witem_cursor;  // [TSI_MAX_LEVELS + 1]
-  uint2 *wide_dec;         // per block: branch ballots of the 8 cells, [wide_dec_stride]
-  uint32_t wide_dec_stride;
-  uint32_t wide_smem;      // 1: ballots and flags in shared memory after the register file
-  uint32_t wide_flag_stride;
-  uint8_t *wide_flags;     // per block: liveness flags, [wide_flag_stride]
+  uint32_t *witem_cursor;  // [TSI_MAX_LEVELS + 1], in child cells
+  uint32_t witem_cap;      // wide items per level; more go to the narrow list
+  uint32_t bm_words;       // branch-decision words per wide cell (2 bits per min/max)
+  CellInfo *cell_info[2];  // [witem_cap * 8] per level parity
+  uint32_t *cell_bits[2];  // [witem_cap * 8][bm_words] per level parity
+  // per-cell working set of the wide path (values, sensitivities,
+  // contribution records, decision bits, liveness flags): in shared memory
+  // when cell_smem, else cell_scratch + blockIdx.x * cell_bytes
+  uint32_t cell_smem;
+  uint32_t cell_bytes;
+  unsigned char *cell_scratch;
   uint32_t item_cap;
   uint32_t dealloc_cap;
   uint2 *dealloc[2];       // (scene, brick)

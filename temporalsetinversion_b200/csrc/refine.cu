@@ -295,6 +295,68 @@ __device__ __forceinline__ void find_valid(const LaunchParams &P, uint32_t &rec,
   }
 }
 
+// Next-level work for the enqueued children (mask E) of one parent, whose
+// cells are cells[0..7]; one thread.  `wide`: one wide item per child, its
+// own children's brick allocated here; children beyond the wide list's
+// capacity, or all of them when not `wide`, go to the narrow list in items
+// of up to four.  Every reserved list slot below the capacity is written
+// (readers take min(count, capacity) entries); narrow-list overflow is
+// dropped and reported.
+__device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint32_t scene, uint32_t rec,
+                              uint32_t level, uint32_t E, const uint32_t *cells, bool wide,
+                              unsigned long long *ws) {
+  uint32_t rest = E;
+  if (wide) {
+    const uint32_t n = __popc(E);
+    const uint32_t pos = atomicAdd(&P.witem_count[level + 1], n);
+    uint32_t j = 0;
+    while (rest && pos + j < P.witem_cap) {
+      const uint32_t bit = __ffs(rest) - 1u;
+      rest &= rest - 1u;
+      const uint32_t c = cells[bit];
+      uint32_t b = S.pool.child[c], fresh = 0;
+      if (b == TSI_NONE) {
+        b = alloc_brick(S, P.error);
+        if (b != TSI_NONE) {
+          S.pool.child[c] = b;
+          fresh = 1;
+          atomicAdd(&ws[ST_BRICK_ALLOC], 1ull);
+        }
+      }
+      WorkItem wi;
+      wi.scene = scene;
+      wi.rec = rec;
+      wi.n = 1;
+      wi.level = level + 1;
+      wi.parent[0] = c;
+      wi.parent[1] = b;
+      wi.parent[2] = fresh;
+      wi.parent[3] = 0;
+      P.witems[(level + 1) & 1][pos + j++] = wi;
+    }
+  }
+  if (rest == 0) return;
+  const uint32_t nitems = (__popc(rest) + 3u) >> 2;
+  const uint32_t pos = atomicAdd(&P.item_count[level + 1], nitems);
+  if (pos + nitems > P.item_cap) atomicOr(P.error, EB_QUEUE_FULL);
+  WorkItem *dst = P.items[(level + 1) & 1];
+  for (uint32_t j = 0; j < nitems && pos + j < P.item_cap; ++j) {
+    WorkItem wi;
+    wi.scene = scene;
+    wi.rec = rec;
+    wi.level = level + 1;
+    uint32_t c = 0;
+    while (rest && c < 4u) {
+      const uint32_t bit = __ffs(rest) - 1u;
+      rest &= rest - 1u;
+      wi.parent[c++] = cells[bit];
+    }
+    wi.n = c;
+    for (uint32_t q = c; q < 4u; ++q) wi.parent[q] = wi.parent[0];
+    dst[pos + j] = wi;
+  }
+}
+
 __device__ __forceinline__ float warp_min(float v) {
   for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(FULL_MASK, v, o));
   return v;
@@ -379,6 +441,10 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
   Iv cx = Iv{__fadd_rn(pxy.x, __fmul_rn(dx, kx)), __fadd_rn(pxy.x, __fmul_rn(dx, 1.0f + kx))};
   Iv cy = Iv{__fadd_rn(pxy.z, __fmul_rn(dy, ky)), __fadd_rn(pxy.z, __fmul_rn(dy, 1.0f + ky))};
   Iv cz = Iv{__fadd_rn(pz.x, __fmul_rn(dz, kz)), __fadd_rn(pz.x, __fmul_rn(dz, 1.0f + kz))};
+  // half extent of this cell's children, as they will compute it
+  const float child_width =
+      fm_max(__fdiv_rn(__fsub_rn(cx.hi, cx.lo), 2.0f),
+             fm_max(__fdiv_rn(__fsub_rn(cy.hi, cy.lo), 2.0f), __fdiv_rn(__fsub_rn(cz.hi, cz.lo), 2.0f)));
   const bool point_branch = new_voxel || pfast == 1.0f || width <= S.eps;
   Iv cur_t;
   if (point_branch) {
@@ -534,9 +600,12 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
   const uint32_t E = (em >> (g * 8u)) & 0xffu;
   uint32_t new_rec = rec;
   if (em) {
-    // time range the children will be evaluated over: [child.t, time]
+    // time range the children will be evaluated over: [child.t, time], or
+    // the point branch's range for children at most eps wide or of a fast
+    // cell
+    const bool child_point = child_width <= S.eps || c_fast == 1.0f;
     float nl = targ.lo, nh = targ.hi;
-    if (enq && old_child != TSI_NONE) {
+    if (enq && old_child != TSI_NONE && !child_point) {
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const float ct = pool.t[old_child + q];
@@ -647,52 +716,12 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     } else if (E != 0 && want_prune) {
       new_rec = prec;  // not pruned (or no arena room): the widened-valid tape
     }
-    // next-level work items: ceil(n/4) per group
+    // next-level work: wide items for a long tape, else narrow items
     uint32_t cb[8];
 #pragma unroll
     for (int b2 = 0; b2 < 8; ++b2) cb[b2] = __shfl_sync(FULL_MASK, C, gl0 + b2);
     const uint32_t next_len = (new_rec == prec) ? PR.len : ((new_rec == rec) ? TR.len : cnt);
-    if (k == 0 && E != 0 && next_len >= S.wide.min_len) {  // long tape: wide path, one item per child
-      const uint32_t n = __popc(E);
-      const uint32_t pos = atomicAdd(&P.witem_count[level + 1], n);
-      // every reserved slot below the capacity is written (readers take
-      // min(count, capacity) entries); the rest are dropped and reported
-      if (pos + n > P.item_cap) atomicOr(P.error, EB_QUEUE_FULL);
-      uint32_t e = E, j = 0;
-      while (e && pos + j < P.item_cap) {
-        const uint32_t bit = __ffs(e) - 1u;
-        e &= e - 1u;
-        WorkItem wi;
-        wi.scene = it.scene;
-        wi.rec = new_rec;
-        wi.n = 1;
-        wi.level = level + 1;
-        wi.parent[0] = wi.parent[1] = wi.parent[2] = wi.parent[3] = cb[bit];
-        P.witems[(level + 1) & 1][pos + j++] = wi;
-      }
-    } else if (k == 0 && E != 0) {
-      const uint32_t n = __popc(E);
-      const uint32_t nitems = (n + 3u) >> 2;
-      const uint32_t pos = atomicAdd(&P.item_count[level + 1], nitems);
-      if (pos + nitems > P.item_cap) atomicOr(P.error, EB_QUEUE_FULL);
-      WorkItem *dst = P.items[(level + 1) & 1];
-      uint32_t e = E;
-      for (uint32_t j = 0; j < nitems && pos + j < P.item_cap; ++j) {
-        WorkItem wi;
-        wi.scene = it.scene;
-        wi.rec = new_rec;
-        wi.level = level + 1;
-        uint32_t c = 0;
-        while (e && c < 4u) {
-          const uint32_t bit = __ffs(e) - 1u;
-          e &= e - 1u;
-          wi.parent[c++] = cb[bit];
-        }
-        wi.n = c;
-        for (uint32_t q = c; q < 4u; ++q) wi.parent[q] = wi.parent[0];
-        dst[pos + j] = wi;
-      }
-    }
+    if (k == 0 && E != 0) push_children(P, S, it.scene, new_rec, level, E, cb, next_len >= S.wide.min_len, ws);
   }
 
   // ---- counters
@@ -752,145 +781,139 @@ __device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level,
 }
 
 // ======================================================================
-// Wide path: one block per parent, one warp per child cell, one lane per
+// Wide path: one block per child cell of a wide item, one thread per
 // instruction of a bundle (tape_compile.h WideTape).  Long tapes at the top
 // of the octree leave the narrow path latency bound (few items, thousands of
-// dependent instructions each); here a cell takes one step per bundle.
-// The reverse pass applies, bundle by bundle, the accumulations into each
-// sensitivity register in the sequential order (rounds), so the results
-// are those of the narrow path bit for bit.
+// dependent instructions each); here a cell takes one block-wide step per
+// bundle.  Every SSA value has its own slot in the cell's working set, so
+// the reverse pass reads operands where the forward pass left them; values
+// with several users sum per-use contribution records in the sequential
+// order, so the results are those of the narrow path bit for bit.  The eight
+// cells of an item run on eight blocks; the last to finish prunes the
+// group's tape and enqueues its children.
 
+// Byte offsets of a cell's working set (values, sensitivities, contribution
+// records, decision bits, liveness flags); the host sizes it the same way.
+struct CellLayout {
+  uint32_t sens, rec, bits, flags;
+};
+__device__ __forceinline__ CellLayout cell_layout(const WideDev &W, uint32_t bm_words) {
+  CellLayout L;
+  L.sens = W.nvalues * 8u;
+  L.rec = L.sens + W.nvalues * 8u;
+  L.bits = L.rec + ((W.ncontrib * 8u + 15u) & ~15u);
+  L.flags = L.bits + ((bm_words * 4u + 15u) & ~15u);
+  return L;
+}
+
+__device__ __forceinline__ Iv ldv(const float2 *a, uint32_t i) {
+  const float2 v = a[i];
+  return Iv{v.x, v.y};
+}
+__device__ __forceinline__ void stv(float2 *a, uint32_t i, Iv v) { a[i] = make_float2(v.lo, v.hi); }
+
+// Forward pass over the bundles (compute.wgsl:3633-3772); returns the field.
+// `bits`: 2 bits per min/max of this cell (A always chosen, B always chosen).
 template <bool D>
-__device__ Iv wide_forward(const WideDev &W, float2 *rfw, uint32_t lane, Iv x, Iv y, Iv z, Iv t, float4 *lg,
-                           uint2 *dec, uint32_t cellbit) {
-  if (lane == 0) {
-    rfw[0] = make_float2(x.lo, x.hi);
-    rfw[1] = make_float2(y.lo, y.hi);
-    rfw[2] = make_float2(z.lo, z.hi);
-    rfw[3] = make_float2(t.lo, t.hi);
-  }
-  __syncwarp();
-  // the tape's fields in registers (stores through rfw could alias them)
+__device__ Iv cell_forward(const WideDev &W, float2 *V, uint32_t *bits, Iv x, Iv y, Iv z, Iv t) {
+  const uint32_t tid = threadIdx.x;
   const uint2 *__restrict__ bundles = W.bundles;
   const uint4 *__restrict__ slots = W.slots;
-  const uint32_t nb = W.nbundles, out_reg = W.out_reg;
-  // descriptors and slots are fetched two bundles ahead of their use
-  uint2 bt0 = bundles[0];
-  uint2 bt1 = nb > 1 ? bundles[1] : bt0;
-  uint4 sl0 = lane < (bt0.y & 0xffffu) ? slots[3u * (bt0.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
-  uint4 sl1 = (nb > 1 && lane < (bt1.y & 0xffffu)) ? slots[3u * (bt1.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
+  const uint32_t nb = W.nbundles, ns = W.nslots;
+  if (tid == 0) {
+    stv(V, 0, x);
+    stv(V, 1, y);
+    stv(V, 2, z);
+    stv(V, 3, t);
+  }
+  // descriptor and slot of the next bundle fetched while this one runs
+  uint2 btn = bundles[0];
+  uint4 sln = tid < (btn.y & 0xffffu) ? slots[btn.x + tid] : make_uint4(0u, 0u, 0u, 0u);
+  __syncthreads();
   for (uint32_t k = 0; k < nb; ++k) {
-    const uint2 bt = bt0;
-    const uint4 sl = sl0;
-    bt0 = bt1;
-    sl0 = sl1;
-    if (k + 2 < nb) {
-      bt1 = bundles[k + 2];
-      sl1 = lane < (bt1.y & 0xffffu) ? slots[3u * (bt1.x + lane)] : make_uint4(0u, 0u, 0u, 0u);
+    const uint2 bt = btn;
+    const uint4 sl = sln;
+    if (k + 1 < nb) {
+      btn = bundles[k + 1];
+      sln = tid < (btn.y & 0xffffu) ? slots[btn.x + tid] : make_uint4(0u, 0u, 0u, 0u);
     }
-    const bool act = lane < (bt.y & 0xffffu);
-    Iv r = iv(0.0f);
-    uint32_t dst = 0;
-    if (act) {
-      const uint32_t h = sl.x & 63u;
-      dst = sl.y & 0xffffu;
-      const uint32_t a = sl.y >> 16, b = sl.z & 0xffffu;
+    const uint32_t h = bt.y >> 16;
+    if (tid < (bt.y & 0xffffu)) {
       const float lit = __uint_as_float(sl.w);
-      const float2 av = rfw[a];
-      const Iv A = Iv{av.x, av.y};
-      Iv B = iv(lit);
-      if (TSI_H_IS_II(h)) {
-        const float2 bv = rfw[b];
-        B = Iv{bv.x, bv.y};
-      }
-      r = op_forward<D>(h, A, B, lit);
-      if (lg) lg[(size_t)k * 32u + lane] = make_float4(A.lo, A.hi, B.lo, B.hi);
-      if (dec && TSI_H_IS_MINMAX(h)) {
-        const uint32_t mm = slots[3u * (bt.x + lane) + 1u].w;
+      const Iv A = ldv(V, sl.y);
+      const Iv B = TSI_H_IS_II(h) ? ldv(V, sl.z) : iv(lit);
+      stv(V, sl.x >> 8, op_forward<D>(h, A, B, lit));
+      if (bits && TSI_H_IS_MINMAX(h)) {
+        const uint32_t mm = slots[ns + bt.x + tid].y;
         const bool amax = (h == H_MAX_II || h == H_MAX_IF);
         const bool a_below = A.hi < B.lo, b_below = B.hi < A.lo;
-        if (amax ? b_below : a_below) atomicOr(&dec[mm].x, cellbit);
-        if (amax ? a_below : b_below) atomicOr(&dec[mm].y, cellbit);
+        const uint32_t d = ((amax ? b_below : a_below) ? 1u : 0u) | ((amax ? a_below : b_below) ? 2u : 0u);
+        if (d) atomicOr(&bits[mm >> 4], d << (2u * (mm & 15u)));
       }
     }
-    __syncwarp();
-    if (act) rfw[dst] = make_float2(r.lo, r.hi);
-    __syncwarp();
+    __syncthreads();
   }
-  const float2 f = rfw[out_reg];
-  __syncwarp();
-  return Iv{f.x, f.y};
+  return ldv(V, W.nvalues - 1u);
 }
 
 // Sum of a value's contribution records, last user first, onto +0: the
 // accumulation order of the sequential reverse pass.
 template <bool D>
-__device__ __forceinline__ Iv gather_sens(const float2 *ctb, uint32_t base, uint32_t count) {
+__device__ __forceinline__ Iv gather_sens(const float2 *R, uint32_t base, uint32_t count) {
   Iv S = iv(0.0f);
-  for (uint32_t i = 0; i < count; ++i) {
-    const float2 c = ctb[base + i];
-    S = IA<D>::add(Iv{c.x, c.y}, S);
+  uint32_t i = 0;
+  for (; i + 4u <= count; i += 4u) {  // loads ahead of the dependent adds
+    const float2 c0 = R[base + i], c1 = R[base + i + 1u], c2 = R[base + i + 2u], c3 = R[base + i + 3u];
+    S = IA<D>::add(Iv{c0.x, c0.y}, S);
+    S = IA<D>::add(Iv{c1.x, c1.y}, S);
+    S = IA<D>::add(Iv{c2.x, c2.y}, S);
+    S = IA<D>::add(Iv{c3.x, c3.y}, S);
   }
+  for (; i < count; ++i) S = IA<D>::add(ldv(R, base + i), S);
   return S;
 }
 
-// Reverse interval AD over the bundled tape (compute.wgsl:3786-3900), one
-// lane per slot.  A single-use operand accumulates in its register; an
-// operand with several users gets a contribution record (ctb), summed when
-// the reverse pass reaches the value.
+// Reverse interval AD over the bundles (compute.wgsl:3786-3900).  A
+// single-use operand's sensitivity is written by its one user; an operand
+// with several users gets a contribution record per user (R), summed when
+// the reverse pass reaches the value.  sens_out: 4 floats x 2 in shared
+// memory for the arguments' sensitivities.
 template <bool D>
-__device__ void wide_reverse(const WideDev &W, float2 *rfw, uint32_t lane, const float4 *lg, float2 *ctb,
-                             Iv sens[4]) {
+__device__ void cell_reverse(const WideDev &W, const float2 *V, float2 *G, float2 *R, float2 *sens_out) {
   using I = IA<D>;
+  const uint32_t tid = threadIdx.x;
   const uint2 *__restrict__ bundles = W.bundles;
   const uint4 *__restrict__ slots = W.slots;
+  const uint32_t ns = W.nslots, nv = W.nvalues;
   const int nb = (int)W.nbundles;
-  for (uint32_t r = lane; r < W.nregs; r += 32u) rfw[r] = make_float2(0.0f, 0.0f);
-  __syncwarp();
-  if (lane == 0) rfw[W.out_reg] = make_float2(1.0f, 1.0f);
-  __syncwarp();
+  for (uint32_t v = tid; v < nv; v += blockDim.x) G[v] = make_float2(0.0f, 0.0f);
   const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
   uint2 btn = bundles[nb - 1];
-  bool an = lane < btn.y;
-  uint4 s0n = an ? slots[3u * (btn.x + lane)] : zero4;
-  uint4 s2n = an ? slots[3u * (btn.x + lane) + 2u] : zero4;
-  float4 Ln = an ? lg[(size_t)(nb - 1) * 32u + lane] : make_float4(0, 0, 0, 0);
+  bool an = tid < (btn.y & 0xffffu);
+  uint4 s0n = an ? slots[btn.x + tid] : zero4;
+  uint4 s2n = an ? slots[2u * ns + btn.x + tid] : zero4;
+  __syncthreads();
+  if (tid == 0) G[nv - 1u] = make_float2(1.0f, 1.0f);
+  __syncthreads();
   for (int k = nb - 1; k >= 0; --k) {
+    const uint2 bt = btn;
     const bool act = an;
     const uint4 sl = s0n, s2 = s2n;
-    const float4 L = Ln;
     if (k > 0) {  // next (lower) bundle, fetched while this one runs
       btn = bundles[k - 1];
-      an = lane < btn.y;
-      s0n = an ? slots[3u * (btn.x + lane)] : zero4;
-      s2n = an ? slots[3u * (btn.x + lane) + 2u] : zero4;
-      Ln = an ? lg[(size_t)(k - 1) * 32u + lane] : make_float4(0, 0, 0, 0);
+      an = tid < (btn.y & 0xffffu);
+      s0n = an ? slots[btn.x + tid] : zero4;
+      s2n = an ? slots[2u * ns + btn.x + tid] : zero4;
     }
-    uint32_t h = H_CONST, fa = 0, fb = 0, dst = 0, a = 0, b = 0;
-    float lit = 0.0f;
-    Iv A = iv(0.0f), B = iv(0.0f), s = iv(0.0f);
-    if (act) {
-      h = sl.x & 63u;
-      fa = (sl.x >> 6) & 1u;
-      fb = (sl.x >> 7) & 1u;
-      dst = sl.y & 0xffffu;
-      a = sl.y >> 16;
-      b = sl.z & 0xffffu;
-      lit = __uint_as_float(sl.w);
-      A = Iv{L.x, L.y};
-      B = Iv{L.z, L.w};
-      if (s2.w) {
-        s = gather_sens<D>(ctb, s2.z, s2.w);
-      } else {
-        const float2 sv = rfw[dst];
-        s = Iv{sv.x, sv.y};
-      }
-    }
-    __syncwarp();
-    if (act) rfw[dst] = make_float2(0.0f, 0.0f);
-    __syncwarp();
+    const uint32_t h = bt.y >> 16;
     if (act && h != H_CONST) {
       const bool II = TSI_H_IS_II(h);
+      const uint32_t fa = (sl.x >> 6) & 1u, fb = (sl.x >> 7) & 1u;
+      const uint32_t a = sl.y, b = sl.z;
+      const float lit = __uint_as_float(sl.w);
+      const Iv A = ldv(V, a);
+      const Iv B = II ? ldv(V, b) : iv(lit);
+      const Iv s = s2.w ? gather_sens<D>(R, s2.z, s2.w) : ldv(G, sl.x >> 8);
       const bool s0 = (s.lo == 0.0f && s.hi == 0.0f);
       const bool skip = II ? (s0 && fa && fb) : (s0 && fa);
       Iv c0 = iv(0.0f), c1 = iv(0.0f);
@@ -902,43 +925,22 @@ __device__ void wide_reverse(const WideDev &W, float2 *rfw, uint32_t lane, const
       }
       // both operands read before either is written (an instruction whose
       // operands are one value keeps the second write)
-      const float2 pa = (s2.x == TSI_NONE && !skip) ? rfw[a] : make_float2(0.0f, 0.0f);
-      const float2 pb = (II && s2.y == TSI_NONE && !skip) ? rfw[b] : make_float2(0.0f, 0.0f);
-      if (s2.x != TSI_NONE) {
-        ctb[s2.x] = make_float2(c0.lo, c0.hi);
-      } else if (skip) {
-        rfw[a] = make_float2(0.0f, 0.0f);
-      } else {
-        const Iv n0 = I::add(c0, Iv{pa.x, pa.y});
-        rfw[a] = make_float2(n0.lo, n0.hi);
-      }
+      const Iv pa = (s2.x == TSI_NONE && !skip) ? ldv(G, a) : iv(0.0f);
+      const Iv pb = (II && s2.y == TSI_NONE && !skip) ? ldv(G, b) : iv(0.0f);
+      if (s2.x != TSI_NONE) stv(R, s2.x, c0);
+      else stv(G, a, skip ? iv(0.0f) : I::add(c0, pa));
       if (II) {
-        if (s2.y != TSI_NONE) {
-          ctb[s2.y] = make_float2(c1.lo, c1.hi);
-        } else if (skip) {
-          rfw[b] = make_float2(0.0f, 0.0f);
-        } else {
-          const Iv n1 = I::add(c1, Iv{pb.x, pb.y});
-          rfw[b] = make_float2(n1.lo, n1.hi);
-        }
+        if (s2.y != TSI_NONE) stv(R, s2.y, c1);
+        else stv(G, b, skip ? iv(0.0f) : I::add(c1, pb));
       }
     }
-    __syncwarp();
+    __syncthreads();
   }
-  Iv g = iv(0.0f);
-  if (lane < 4u) {
-    const uint32_t gc = W.arg_gcount[lane];
-    if (gc) {
-      g = gather_sens<D>(ctb, W.arg_gbase[lane], gc);
-    } else {
-      const float2 v = rfw[lane];
-      g = Iv{v.x, v.y};
-    }
+  if (tid < 4u) {
+    const uint32_t gc = W.arg_gcount[tid];
+    stv(sens_out, tid, gc ? gather_sens<D>(R, W.arg_gbase[tid], gc) : ldv(G, tid));
   }
-  for (int q = 0; q < 4; ++q) {
-    sens[q] = Iv{__shfl_sync(FULL_MASK, g.lo, q), __shfl_sync(FULL_MASK, g.hi, q)};
-  }
-  __syncwarp();
+  __syncthreads();
 }
 
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *scratch, uint32_t &total) {
@@ -961,289 +963,100 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s
 }
 
 struct WideShared {
-  uint32_t base, is_new, E, widen, cnt, mmk, fcost, rcost, ri;
+  uint32_t last, E, cnt, mmk, fcost, rcost, ri;
   unsigned long long off;
-  float nl[kWarps], nh[kWarps];
+  float gl, gh, hl, hh;
   uint32_t scan[kWarps];
+  float2 sens[4];
 };
 
-template <bool D>
-__device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem &it, uint32_t level, float2 *rfw,
-                                          float4 *slice_log, uint2 *dec, uint8_t *flags, WideShared &sh,
-                                          unsigned long long *ws) {
-  using A = IA<D>;
-  const uint32_t lane = threadIdx.x & 31u, k = threadIdx.x >> 5;  // warp = octant
+// The last cell of a wide item to finish: prunes the full tape with the
+// branch decisions shared by all enqueued siblings and enqueues them.
+__device__ void finish_group(const LaunchParams &P, const WorkItem &it, uint32_t level, uint32_t unit0,
+                             unsigned char *cell, WideShared &sh, unsigned long long *ws) {
+  const uint32_t tid = threadIdx.x;
   const SceneLaunch &S = P.scenes[it.scene];
-  const VoxelPoolDev &pool = S.pool;
   const WideDev &W = S.wide;
-  const uint32_t flg = S.flags;
-  const bool swept = (flg & SF_SWEPT) != 0;
-  const uint32_t Pv = it.parent[0];
   const TapeRec root = P.recs[S.root_rec];
   const uint32_t n_narrow = root.len;
-
-  if (threadIdx.x == 0) {
-    ws[ST_PARENTS] += 1;  // every processed parent, as the narrow path counts it.n
-    const uint32_t pc = pool.child[Pv];
-    sh.is_new = pc == TSI_NONE;
-    sh.base = pc;
-    if (sh.is_new) {
-      sh.base = alloc_brick(S, P.error);
-      if (sh.base != TSI_NONE) {
-        pool.child[Pv] = sh.base;
-        ws[ST_BRICK_ALLOC]++;
-      }
-    }
-    sh.E = 0;
-    sh.widen = 0;
-  }
-  for (uint32_t i = threadIdx.x; i < root.n_minmax; i += blockDim.x) dec[i] = make_uint2(0u, 0u);
-  __syncthreads();
-  const uint32_t base = sh.base;
-  const bool new_voxel = sh.is_new != 0;
-  if (base == TSI_NONE) return;  // pool exhausted (error bit set)
-  const uint32_t C = base + k;
-
-  // ---- cell setup (compute.wgsl:3582-3626), uniform across the warp
-  const float4 pxy = pool.box_xy[Pv];
-  const float2 pz = pool.box_z[Pv];
-  const float pfast = pool.fast[Pv];
-  float c_t = 0.0f, c_f = 1.0f, c_te = 0.0f, c_fast = 0.0f;
-  uint32_t c_child = TSI_NONE;
-  if (!new_voxel) {
-    c_t = pool.t[C];
-    c_f = pool.f[C];
-    c_te = pool.time_err[C];
-    c_fast = pool.fast[C];
-    c_child = pool.child[C];
-  }
-  __syncwarp();
-  if (new_voxel && lane == 0) {
-    pool.child[C] = TSI_NONE;
-    pool.normal[C] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  }
-  const float dx = __fdiv_rn(__fsub_rn(pxy.y, pxy.x), 2.0f);
-  const float dy = __fdiv_rn(__fsub_rn(pxy.w, pxy.z), 2.0f);
-  const float dz = __fdiv_rn(__fsub_rn(pz.y, pz.x), 2.0f);
-  float width = fm_max(dx, fm_max(dy, dz));
-  const float kx = (float)(k & 1u), ky = (float)((k >> 1) & 1u), kz = (float)(k >> 2);
-  Iv cx = Iv{__fadd_rn(pxy.x, __fmul_rn(dx, kx)), __fadd_rn(pxy.x, __fmul_rn(dx, 1.0f + kx))};
-  Iv cy = Iv{__fadd_rn(pxy.z, __fmul_rn(dy, ky)), __fadd_rn(pxy.z, __fmul_rn(dy, 1.0f + ky))};
-  Iv cz = Iv{__fadd_rn(pz.x, __fmul_rn(dz, kz)), __fadd_rn(pz.x, __fmul_rn(dz, 1.0f + kz))};
-  const bool point_branch = new_voxel || pfast == 1.0f || width <= S.eps;
-  Iv cur_t;
-  if (point_branch) {
-    cur_t = swept ? Iv{S.t0, S.time} : iv(S.time);
-    c_fast = 0.0f;
-  } else {
-    cur_t = Iv{c_t, S.time};
-  }
-  if (lane == 0) {
-    pool.box_xy[C] = make_float4(cx.lo, cx.hi, cy.lo, cy.hi);
-    pool.box_z[C] = make_float2(cz.lo, cz.hi);
-    pool.t[C] = S.time;
-  }
-  if ((flg & SF_POINTSAMPLE) && width <= S.eps) {
-    cx = iv(__fdiv_rn(__fadd_rn(cx.lo, cx.hi), 2.0f));
-    cy = iv(__fdiv_rn(__fadd_rn(cy.lo, cy.hi), 2.0f));
-    cz = iv(__fdiv_rn(__fadd_rn(cz.lo, cz.hi), 2.0f));
-    width = 0.0f;
-  }
-  const Iv targ = Iv{fm_min(cur_t.lo, cur_t.hi), fm_max(cur_t.lo, cur_t.hi)};
-  const bool evaluate = new_voxel || c_f >= 0.0f || c_child == TSI_NONE;
-  const bool take_deriv = evaluate && ((cur_t.lo != cur_t.hi) || (flg & SF_ALWAYS_DERIV));
-  const bool want_prune = (flg & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS;
-
-  // ---- forward and reverse over the full tape, bundle by bundle
-  Iv field = iv(0.0f);
-  Iv sens[4] = {iv(0.0f), iv(0.0f), iv(0.0f), iv(0.0f)};
-  float4 *lg = nullptr;
-  bool ok = true;
-  // operand log (32 float4 per bundle), then the contribution records
-  // (2 per float4)
-  const unsigned long long need =
-      (unsigned long long)W.nbundles * 32ull + ((unsigned long long)W.ncontrib + 1ull) / 2ull;
-  if (take_deriv) {
-    if (need <= (unsigned long long)P.slice_len * 32ull) {
-      lg = slice_log;
-    } else {
-      unsigned long long off = 0;
-      if (lane == 0) off = atomicAdd(P.log_overflow_used + level, need);
-      off = __shfl_sync(FULL_MASK, off, 0);
-      if (off + need > P.log_overflow_cap) {
-        if (lane == 0) atomicOr(P.error, EB_LOG_OOM);
-        ok = false;
-      } else {
-        lg = P.log_overflow + off;
-      }
-    }
-  }
-  if (evaluate && ok) {
-    const long long c0 = clock64();
-    field = wide_forward<D>(W, rfw, lane, cx, cy, cz, targ, lg, want_prune ? dec : nullptr, 1u << k);
-    const long long c1 = clock64();
-    if (take_deriv)
-      wide_reverse<D>(W, rfw, lane, lg, reinterpret_cast<float2 *>(lg + (size_t)W.nbundles * 32u), sens);
-    if (threadIdx.x == 0) {
-      ws[ST_CYC_WIDE_FWD] += (unsigned long long)(c1 - c0);
-      ws[ST_CYC_WIDE_REV] += (unsigned long long)(clock64() - c1);
-    }
-  }
-
-  // ---- temporal error bound, fast flag, classification (3966-4045)
-  Iv df = iv(0.0f), df_dt = iv(0.0f);
-  const float delta = S.delta;
-  if (take_deriv && ok) {
-    const float nx = __fdiv_rn(__fadd_rn(sens[0].lo, sens[0].hi), 2.0f);
-    const float ny = __fdiv_rn(__fadd_rn(sens[1].lo, sens[1].hi), 2.0f);
-    const float nz = __fdiv_rn(__fadd_rn(sens[2].lo, sens[2].hi), 2.0f);
-    if (lane == 0) pool.normal[C] = make_float4(nx, ny, nz, 0.0f);
-    df_dt = sens[3];
-    const float dt = __fsub_rn(targ.hi, targ.lo);
-    df = A::mul_f(df_dt, dt);
-    const Iv Wd = A::mul_f(Iv{-1.0f, 1.0f}, __fsub_rn(field.hi, field.lo));
-    df = A::cap(df, Wd);
-    if ((flg & SF_LIPSCHITZ) && A::abs_(df).hi != 0.0f) {
-      const float lb =
-          A::abs_(A::sqrt_(A::add(A::sqr(sens[0]), A::add(A::sqr(sens[1]), A::sqr(sens[2]))))).lo;
-      if (!is_nan_f(lb)) df = A::div(df, iv(lb));
-    }
-    if (df.lo == -fm_inf() || df.hi == fm_inf() || is_nan_f(df.lo) || is_nan_f(df.hi)) df = iv(delta);
-    c_te = __fadd_rn(c_te, fm_min(fm_max(A::abs_(df).hi, 0.0f), delta));
-  }
-  if (evaluate && !swept && (flg & SF_FASTENABLED)) c_fast = (A::abs_(df).hi >= S.fast_thresh) ? 1.0f : 0.0f;
-  bool enq = false, dealloc = false, reused = false;
-  int cls = 3;
-  if (evaluate && ok) {
-    if (field.lo <= 0.0f && 0.0f <= field.hi) {
-      c_f = 0.0f;
-      cls = 0;
-      if (width > S.eps) {
-        if (new_voxel || is_nan_f(df_dt.lo) || is_nan_f(df_dt.hi) || fabsf(df_dt.lo) == fm_inf() ||
-            fabsf(df_dt.hi) == fm_inf() || pfast == 1.0f || cur_t.lo == cur_t.hi || c_te >= delta ||
-            c_child == TSI_NONE) {
-          c_te = 0.0f;
-          enq = true;
-        } else {
-          reused = true;
-        }
-      }
-    } else {
-      if (field.hi <= 0.0f) {
-        c_f = -1.0f;
-        cls = 2;
-      } else {
-        cls = 1;
-        if (!swept) c_f = 1.0f;
-      }
-      if (!swept && c_child != TSI_NONE) dealloc = true;
-    }
-  }
-  const uint32_t old_child = c_child;
-  if (dealloc) c_child = TSI_NONE;
-  if (lane == 0) {
-    pool.f[C] = c_f;
-    pool.time_err[C] = c_te;
-    pool.fast[C] = c_fast;
-    if (dealloc || new_voxel) pool.child[C] = c_child;
-    if (dealloc) {
-      const uint32_t pos = atomicAdd(&P.dealloc_count[level + 1], 1u);
-      if (pos < P.dealloc_cap) P.dealloc[(level + 1) & 1][pos] = make_uint2(it.scene, old_child >> 3);
-      else atomicOr(P.error, EB_QUEUE_FULL);
-    }
-    if (enq) atomicOr(&sh.E, 1u << k);
-    atomicAdd(&ws[ST_EVAL], evaluate ? 1ull : 0ull);
-    atomicAdd(&ws[ST_REVERSE], take_deriv ? 1ull : 0ull);
-    atomicAdd(&ws[ST_SKIPPED], evaluate ? 0ull : 1ull);
-    if (cls == 0) atomicAdd(&ws[ST_AMBIG], 1ull);
-    if (cls == 1) atomicAdd(&ws[ST_EMPTY], 1ull);
-    if (cls == 2) atomicAdd(&ws[ST_FULL], 1ull);
-    if (enq) atomicAdd(&ws[ST_ENQUEUED], 1ull);
-    if (reused) atomicAdd(&ws[ST_REUSED], 1ull);
-    if (evaluate) {
-      atomicAdd(&ws[ST_INSTR_FWD], (unsigned long long)n_narrow);
-      atomicAdd(&ws[ST_INSTR_FULL], (unsigned long long)S.full_len);
-      atomicAdd(&ws[ST_FP32], (unsigned long long)root.fwd_cost + (take_deriv ? root.rev_cost : 0u));
-    }
-    if (take_deriv) atomicAdd(&ws[ST_INSTR_REV], (unsigned long long)n_narrow);
-  }
-  // time range the children will be evaluated over
-  float nl = targ.lo, nh = targ.hi;
-  if (enq && old_child != TSI_NONE) {
+  const CellInfo *info = P.cell_info[level & 1] + unit0;
+  if (tid == 0) {
+    ws[ST_PARENTS] += 1;
+    uint32_t E = 0;
+    float gl = -fm_inf(), gh = fm_inf(), hl = fm_inf(), hh = -fm_inf();
     for (int q = 0; q < 8; ++q) {
-      const float ct = pool.t[old_child + q];
-      nl = fm_min(nl, fm_min(ct, S.time));
-      nh = fm_max(nh, fm_max(ct, S.time));
+      const CellInfo ci = info[q];
+      gl = fmaxf(gl, ci.nl);
+      gh = fminf(gh, ci.nh);
+      if (ci.enq) {
+        E |= 1u << q;
+        hl = fminf(hl, ci.nl);
+        hh = fmaxf(hh, ci.nh);
+      }
     }
-  }
-  if (enq && swept) {
-    nl = fm_min(nl, fm_min(S.t0, S.time));
-    nh = fm_max(nh, fm_max(S.t0, S.time));
-  }
-  if (lane == 0) {
-    sh.nl[k] = enq ? nl : -fm_inf();
-    sh.nh[k] = enq ? nh : fm_inf();
-    if (enq && (nl < targ.lo || nh > targ.hi)) atomicOr(&sh.widen, 1u);
+    sh.E = E;
+    sh.gl = gl;
+    sh.gh = gh;
+    sh.hl = hl;
+    sh.hh = hh;
   }
   __syncthreads();
   const uint32_t E = sh.E;
   if (E == 0) return;
-
+  const bool want_prune = (S.flags & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS;
   uint32_t new_rec = S.root_rec;
   if (want_prune) {
-    if (sh.widen) {  // decisions over the children's (wider) time range
-      for (uint32_t i = threadIdx.x; i < root.n_minmax; i += blockDim.x) dec[i] = make_uint2(0u, 0u);
-      __syncthreads();
-      if (enq) (void)wide_forward<D>(W, rfw, lane, cx, cy, cz, Iv{nl, nh}, nullptr, dec, 1u << k);
-      if (lane == 0 && enq) atomicAdd(&ws[ST_FP32], (unsigned long long)root.fwd_cost);
-      __syncthreads();
+    const CellLayout L = cell_layout(W, P.bm_words);
+    uint32_t *cb = reinterpret_cast<uint32_t *>(cell + L.bits);  // decisions shared by the enqueued cells
+    uint8_t *flags = cell + L.flags;
+    const uint32_t words = (root.n_minmax + 15u) >> 4;
+    const uint32_t *gbits = P.cell_bits[level & 1] + (size_t)unit0 * P.bm_words;
+    for (uint32_t w = tid; w < words; w += blockDim.x) {
+      uint32_t acc = 0xffffffffu;
+      for (int q = 0; q < 8; ++q)
+        if ((E >> q) & 1u) acc &= gbits[(size_t)q * P.bm_words + w];
+      cb[w] = acc;
     }
-    // liveness from the field backwards, by bundles (warp 0)
-    for (uint32_t i = threadIdx.x; i < root.len + 4u; i += blockDim.x) flags[i] = 0;
+    for (uint32_t i = tid; i < W.nvalues; i += blockDim.x) flags[i] = 0;
     __syncthreads();
-    if (k == 0) {
+    // liveness from the field backwards, bundle by bundle
+    {
       const uint2 *__restrict__ bundles = W.bundles;
       const uint4 *__restrict__ slots = W.slots;
-      if (lane == 0) flags[root.len + 3u] = 1;
-      __syncwarp();
-      // slots fetched one bundle ahead
+      const uint32_t ns = W.nslots;
+      if (tid == 0) flags[W.nvalues - 1u] = 1;
       int kb = (int)W.nbundles - 1;
       uint2 btn = bundles[kb];
-      uint4 s1n = lane < btn.y ? slots[3u * (btn.x + lane) + 1u] : make_uint4(0u, 0u, 0u, 0u);
-      uint32_t hn = lane < btn.y ? (slots[3u * (btn.x + lane)].x & 63u) : 0u;
+      uint4 s1n = tid < (btn.y & 0xffffu) ? slots[ns + btn.x + tid] : make_uint4(0u, 0u, 0u, 0u);
+      __syncthreads();
       for (; kb >= 0; --kb) {
         const uint2 bt = btn;
         const uint4 s1 = s1n;
-        const uint32_t h = hn;
         if (kb > 0) {
           btn = bundles[kb - 1];
-          s1n = lane < btn.y ? slots[3u * (btn.x + lane) + 1u] : make_uint4(0u, 0u, 0u, 0u);
-          hn = lane < btn.y ? (slots[3u * (btn.x + lane)].x & 63u) : 0u;
+          s1n = tid < (btn.y & 0xffffu) ? slots[ns + btn.x + tid] : make_uint4(0u, 0u, 0u, 0u);
         }
-        if (lane < bt.y) {
-          if (flags[s1.x]) {
-            bool la = s1.y != TSI_NONE, lb = s1.z != TSI_NONE;
-            if (TSI_H_IS_MINMAX(h)) {
-              const uint2 d = dec[s1.w];
-              if ((d.x & E) == E) lb = false;
-              else if ((d.y & E) == E) { la = false; }
-            }
-            if (la) flags[s1.y] = 1;
-            if (lb) flags[s1.z] = 1;
+        if (tid < (bt.y & 0xffffu) && flags[s1.x]) {
+          bool la = s1.z != TSI_NONE, lb = s1.w != TSI_NONE;
+          if (TSI_H_IS_MINMAX(bt.y >> 16)) {
+            const uint32_t d = (cb[s1.y >> 4] >> (2u * (s1.y & 15u))) & 3u;
+            if (d & 1u) lb = false;
+            else if (d & 2u) la = false;
           }
+          if (la) flags[s1.z] = 1;
+          if (lb) flags[s1.w] = 1;
         }
-        __syncwarp();
+        __syncthreads();
       }
     }
-    __syncthreads();
     // compaction of the narrow full tape in program order
     const uint32_t per = (n_narrow + blockDim.x - 1) / blockDim.x;
-    const uint32_t i0 = min(n_narrow, threadIdx.x * per), i1 = min(n_narrow, i0 + per);
+    const uint32_t i0 = min(n_narrow, tid * per), i1 = min(n_narrow, i0 + per);
     uint32_t mine = 0;
     for (uint32_t i = i0; i < i1; ++i) mine += flags[i + 4u];
     uint32_t total = 0;
     const uint32_t pos0 = block_exclusive_scan(mine, sh.scan, total);
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       sh.ri = TSI_NONE;
       sh.off = 0;
       sh.cnt = total;
@@ -1271,12 +1084,13 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
         uint2 out = w;
         uint32_t hk = h;
         if (TSI_H_IS_MINMAX(h)) {
-          const uint2 d = dec[W.narrow_mm[i]];
+          const uint32_t mm = W.narrow_mm[i];
+          const uint32_t d = (cb[mm >> 4] >> (2u * (mm & 15u))) & 3u;
           const uint32_t dd = TSI_W0_DST(w.x);
-          if ((d.x & E) == E) {
+          if (d & 1u) {
             out = make_uint2(TSI_W0(H_COPY, TSI_W0_FA(w.x), 0u, dd, TSI_W0_A(w.x)), 0u);
             hk = H_COPY;
-          } else if ((d.y & E) == E) {
+          } else if (d & 2u) {
             if (TSI_H_IS_II(h)) {
               out = make_uint2(TSI_W0(H_COPY, TSI_W0_FB(w.x), 0u, dd, w.y & 255u), 0u);
               hk = H_COPY;
@@ -1299,29 +1113,20 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
     }
     __syncthreads();
     if (sh.ri != TSI_NONE) {
-      if (threadIdx.x == 0) {
-        float gl = -fm_inf(), gh = fm_inf(), hl = fm_inf(), hh = -fm_inf();
-        for (int q = 0; q < kWarps; ++q) {
-          gl = fmaxf(gl, sh.nl[q]);
-          gh = fminf(gh, sh.nh[q]);
-          if ((E >> q) & 1u) {
-            hl = fminf(hl, sh.nl[q]);
-            hh = fmaxf(hh, sh.nh[q]);
-          }
-        }
+      if (tid == 0) {
         TapeRec nr;
         nr.code = P.code_arena + sh.off;
         nr.len = sh.cnt;
         nr.nregs = root.nregs;
         nr.out_reg = root.out_reg;
         nr.n_minmax = sh.mmk;
-        nr.t_lo = gl;
-        nr.t_hi = gh;
+        nr.t_lo = sh.gl;
+        nr.t_hi = sh.gh;
         nr.parent = S.root_rec;
         nr.fwd_cost = sh.fcost;
         nr.rev_cost = sh.rcost;
-        nr.c_lo = hl;
-        nr.c_hi = hh;
+        nr.c_lo = sh.hl;
+        nr.c_hi = sh.hh;
         nr.c_level = level + 1u;
         P.recs[sh.ri] = nr;
         ws[ST_TAPE_WORDS] += sh.cnt;
@@ -1329,49 +1134,238 @@ __device__ __noinline__ void process_wide(const LaunchParams &P, const WorkItem 
       new_rec = sh.ri;
     }
   }
-  // ---- next-level items for the enqueued children
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     const uint32_t len = (new_rec == S.root_rec) ? root.len : sh.cnt;
-    const uint32_t n = __popc(E);
-    if (len >= W.min_len) {  // stay on the wide path: one item per child
-      const uint32_t pos = atomicAdd(&P.witem_count[level + 1], n);
-      // every reserved slot below the capacity is written; the rest are
-      // dropped and reported
-      if (pos + n > P.item_cap) atomicOr(P.error, EB_QUEUE_FULL);
-      uint32_t e = E, j = 0;
-      while (e && pos + j < P.item_cap) {
-        const uint32_t bit = __ffs(e) - 1u;
-        e &= e - 1u;
-        WorkItem wi;
-        wi.scene = it.scene;
-        wi.rec = new_rec;
-        wi.n = 1;
-        wi.level = level + 1;
-        wi.parent[0] = wi.parent[1] = wi.parent[2] = wi.parent[3] = base + bit;
-        P.witems[(level + 1) & 1][pos + j++] = wi;
-      }
-    } else {
-      const uint32_t nitems = (n + 3u) >> 2;
-      const uint32_t pos = atomicAdd(&P.item_count[level + 1], nitems);
-      if (pos + nitems > P.item_cap) atomicOr(P.error, EB_QUEUE_FULL);
-      uint32_t e = E;
-      for (uint32_t j = 0; j < nitems && pos + j < P.item_cap; ++j) {
-        WorkItem wi;
-        wi.scene = it.scene;
-        wi.rec = new_rec;
-        wi.level = level + 1;
-        uint32_t c = 0;
-        while (e && c < 4u) {
-          const uint32_t bit = __ffs(e) - 1u;
-          e &= e - 1u;
-          wi.parent[c++] = base + bit;
-        }
-        wi.n = c;
-        for (uint32_t q = c; q < 4u; ++q) wi.parent[q] = wi.parent[0];
-        P.items[(level + 1) & 1][pos + j] = wi;
-      }
+    uint32_t cells[8];
+    for (int q = 0; q < 8; ++q) cells[q] = it.parent[1] + q;
+    push_children(P, S, it.scene, new_rec, level, E, cells, len >= W.min_len, ws);
+  }
+}
+
+// One child cell (octant k) of a wide item.  unit = item * 8 + k.
+template <bool D>
+__device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, uint32_t k, uint32_t unit,
+                                          uint32_t level, unsigned char *cell, WideShared &sh,
+                                          unsigned long long *ws) {
+  using A = IA<D>;
+  const uint32_t tid = threadIdx.x;
+  const WorkItem &it = *itp;
+  const SceneLaunch &S = P.scenes[it.scene];
+  const VoxelPoolDev &pool = S.pool;
+  const WideDev &W = S.wide;
+  const uint32_t flg = S.flags;
+  const bool swept = (flg & SF_SWEPT) != 0;
+  const uint32_t Pv = it.parent[0];
+  const uint32_t base = it.parent[1];
+  const bool new_voxel = it.parent[2] != 0;
+  if (base == TSI_NONE) return;  // pool exhausted when the item was enqueued (error bit set)
+  const TapeRec root = P.recs[S.root_rec];
+  const uint32_t n_narrow = root.len;
+  const uint32_t C = base + k;
+  const CellLayout L = cell_layout(W, P.bm_words);
+  float2 *V = reinterpret_cast<float2 *>(cell);
+  float2 *G = reinterpret_cast<float2 *>(cell + L.sens);
+  float2 *R = reinterpret_cast<float2 *>(cell + L.rec);
+  uint32_t *bits = reinterpret_cast<uint32_t *>(cell + L.bits);
+
+  // ---- cell setup (compute.wgsl:3582-3626), uniform across the block
+  const float4 pxy = pool.box_xy[Pv];
+  const float2 pz = pool.box_z[Pv];
+  const float pfast = pool.fast[Pv];
+  float c_t = 0.0f, c_f = 1.0f, c_te = 0.0f, c_fast = 0.0f;
+  uint32_t c_child = TSI_NONE;
+  if (!new_voxel) {
+    c_t = pool.t[C];
+    c_f = pool.f[C];
+    c_te = pool.time_err[C];
+    c_fast = pool.fast[C];
+    c_child = pool.child[C];
+  }
+  const float dx = __fdiv_rn(__fsub_rn(pxy.y, pxy.x), 2.0f);
+  const float dy = __fdiv_rn(__fsub_rn(pxy.w, pxy.z), 2.0f);
+  const float dz = __fdiv_rn(__fsub_rn(pz.y, pz.x), 2.0f);
+  float width = fm_max(dx, fm_max(dy, dz));
+  const float kx = (float)(k & 1u), ky = (float)((k >> 1) & 1u), kz = (float)(k >> 2);
+  Iv cx = Iv{__fadd_rn(pxy.x, __fmul_rn(dx, kx)), __fadd_rn(pxy.x, __fmul_rn(dx, 1.0f + kx))};
+  Iv cy = Iv{__fadd_rn(pxy.z, __fmul_rn(dy, ky)), __fadd_rn(pxy.z, __fmul_rn(dy, 1.0f + ky))};
+  Iv cz = Iv{__fadd_rn(pz.x, __fmul_rn(dz, kz)), __fadd_rn(pz.x, __fmul_rn(dz, 1.0f + kz))};
+  // half extent of this cell's children, as they will compute it
+  const float child_width =
+      fm_max(__fdiv_rn(__fsub_rn(cx.hi, cx.lo), 2.0f),
+             fm_max(__fdiv_rn(__fsub_rn(cy.hi, cy.lo), 2.0f), __fdiv_rn(__fsub_rn(cz.hi, cz.lo), 2.0f)));
+  const bool point_branch = new_voxel || pfast == 1.0f || width <= S.eps;
+  Iv cur_t;
+  if (point_branch) {
+    cur_t = swept ? Iv{S.t0, S.time} : iv(S.time);
+    c_fast = 0.0f;
+  } else {
+    cur_t = Iv{c_t, S.time};
+  }
+  if ((flg & SF_POINTSAMPLE) && width <= S.eps) {
+    const Iv ox = cx, oy = cy, oz = cz;
+    cx = iv(__fdiv_rn(__fadd_rn(ox.lo, ox.hi), 2.0f));
+    cy = iv(__fdiv_rn(__fadd_rn(oy.lo, oy.hi), 2.0f));
+    cz = iv(__fdiv_rn(__fadd_rn(oz.lo, oz.hi), 2.0f));
+    width = 0.0f;
+    if (tid == 0) {
+      pool.box_xy[C] = make_float4(ox.lo, ox.hi, oy.lo, oy.hi);
+      pool.box_z[C] = make_float2(oz.lo, oz.hi);
+    }
+  } else if (tid == 0) {
+    pool.box_xy[C] = make_float4(cx.lo, cx.hi, cy.lo, cy.hi);
+    pool.box_z[C] = make_float2(cz.lo, cz.hi);
+  }
+  if (tid == 0) {
+    pool.t[C] = S.time;
+    if (new_voxel) {
+      pool.child[C] = TSI_NONE;
+      pool.normal[C] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
   }
+  const Iv targ = Iv{fm_min(cur_t.lo, cur_t.hi), fm_max(cur_t.lo, cur_t.hi)};
+  const bool evaluate = new_voxel || c_f >= 0.0f || c_child == TSI_NONE;
+  const bool take_deriv = evaluate && ((cur_t.lo != cur_t.hi) || (flg & SF_ALWAYS_DERIV));
+  const bool want_prune = (flg & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS;
+  const uint32_t words = (root.n_minmax + 15u) >> 4;
+
+  // ---- forward and reverse over the full tape, bundle by bundle
+  Iv field = iv(0.0f);
+  Iv sens[4] = {iv(0.0f), iv(0.0f), iv(0.0f), iv(0.0f)};
+  if (evaluate) {
+    if (want_prune)
+      for (uint32_t w = tid; w < words; w += blockDim.x) bits[w] = 0u;
+    const long long c0 = clock64();
+    field = cell_forward<D>(W, V, want_prune ? bits : nullptr, cx, cy, cz, targ);
+    const long long c1 = clock64();
+    if (take_deriv) {
+      cell_reverse<D>(W, V, G, R, sh.sens);
+      for (int q = 0; q < 4; ++q) sens[q] = ldv(sh.sens, q);
+    }
+    if (tid == 0) {
+      ws[ST_CYC_WIDE_FWD] += (unsigned long long)(c1 - c0);
+      ws[ST_CYC_WIDE_REV] += (unsigned long long)(clock64() - c1);
+    }
+  }
+
+  // ---- temporal error bound, fast flag, classification (3966-4045)
+  Iv df = iv(0.0f), df_dt = iv(0.0f);
+  const float delta = S.delta;
+  if (take_deriv) {
+    const float nx = __fdiv_rn(__fadd_rn(sens[0].lo, sens[0].hi), 2.0f);
+    const float ny = __fdiv_rn(__fadd_rn(sens[1].lo, sens[1].hi), 2.0f);
+    const float nz = __fdiv_rn(__fadd_rn(sens[2].lo, sens[2].hi), 2.0f);
+    if (tid == 0) pool.normal[C] = make_float4(nx, ny, nz, 0.0f);
+    df_dt = sens[3];
+    const float dt = __fsub_rn(targ.hi, targ.lo);
+    df = A::mul_f(df_dt, dt);
+    const Iv Wd = A::mul_f(Iv{-1.0f, 1.0f}, __fsub_rn(field.hi, field.lo));
+    df = A::cap(df, Wd);
+    if ((flg & SF_LIPSCHITZ) && A::abs_(df).hi != 0.0f) {
+      const float lb =
+          A::abs_(A::sqrt_(A::add(A::sqr(sens[0]), A::add(A::sqr(sens[1]), A::sqr(sens[2]))))).lo;
+      if (!is_nan_f(lb)) df = A::div(df, iv(lb));
+    }
+    if (df.lo == -fm_inf() || df.hi == fm_inf() || is_nan_f(df.lo) || is_nan_f(df.hi)) df = iv(delta);
+    c_te = __fadd_rn(c_te, fm_min(fm_max(A::abs_(df).hi, 0.0f), delta));
+  }
+  if (evaluate && !swept && (flg & SF_FASTENABLED)) c_fast = (A::abs_(df).hi >= S.fast_thresh) ? 1.0f : 0.0f;
+  bool enq = false, dealloc = false, reused = false;
+  int cls = 3;
+  if (evaluate) {
+    if (field.lo <= 0.0f && 0.0f <= field.hi) {
+      c_f = 0.0f;
+      cls = 0;
+      if (width > S.eps) {
+        if (new_voxel || is_nan_f(df_dt.lo) || is_nan_f(df_dt.hi) || fabsf(df_dt.lo) == fm_inf() ||
+            fabsf(df_dt.hi) == fm_inf() || pfast == 1.0f || cur_t.lo == cur_t.hi || c_te >= delta ||
+            c_child == TSI_NONE) {
+          c_te = 0.0f;
+          enq = true;
+        } else {
+          reused = true;
+        }
+      }
+    } else {
+      if (field.hi <= 0.0f) {
+        c_f = -1.0f;
+        cls = 2;
+      } else {
+        cls = 1;
+        if (!swept) c_f = 1.0f;
+      }
+      if (!swept && c_child != TSI_NONE) dealloc = true;
+    }
+  }
+  const uint32_t old_child = c_child;
+  if (dealloc) c_child = TSI_NONE;
+  if (tid == 0) {
+    pool.f[C] = c_f;
+    pool.time_err[C] = c_te;
+    pool.fast[C] = c_fast;
+    if (dealloc || new_voxel) pool.child[C] = c_child;
+    if (dealloc) {
+      const uint32_t pos = atomicAdd(&P.dealloc_count[level + 1], 1u);
+      if (pos < P.dealloc_cap) P.dealloc[(level + 1) & 1][pos] = make_uint2(it.scene, old_child >> 3);
+      else atomicOr(P.error, EB_QUEUE_FULL);
+    }
+    ws[ST_EVAL] += evaluate ? 1ull : 0ull;
+    ws[ST_REVERSE] += take_deriv ? 1ull : 0ull;
+    ws[ST_SKIPPED] += evaluate ? 0ull : 1ull;
+    if (cls == 0) ws[ST_AMBIG] += 1ull;
+    if (cls == 1) ws[ST_EMPTY] += 1ull;
+    if (cls == 2) ws[ST_FULL] += 1ull;
+    if (enq) ws[ST_ENQUEUED] += 1ull;
+    if (reused) ws[ST_REUSED] += 1ull;
+    if (evaluate) {
+      ws[ST_INSTR_FWD] += (unsigned long long)n_narrow;
+      ws[ST_INSTR_FULL] += (unsigned long long)S.full_len;
+      ws[ST_FP32] += (unsigned long long)root.fwd_cost + (take_deriv ? root.rev_cost : 0u);
+    }
+    if (take_deriv) ws[ST_INSTR_REV] += (unsigned long long)n_narrow;
+  }
+  // time range the children will be evaluated over: [child.t, time], or
+  // the point branch's range for children at most eps wide or of a fast cell
+  const bool child_point = child_width <= S.eps || c_fast == 1.0f;
+  float nl = targ.lo, nh = targ.hi;
+  if (enq && old_child != TSI_NONE && !child_point) {
+    for (int q = 0; q < 8; ++q) {
+      const float ct = pool.t[old_child + q];
+      nl = fm_min(nl, fm_min(ct, S.time));
+      nh = fm_max(nh, fm_max(ct, S.time));
+    }
+  }
+  if (enq && swept) {
+    nl = fm_min(nl, fm_min(S.t0, S.time));
+    nh = fm_max(nh, fm_max(S.t0, S.time));
+  }
+  if (want_prune && enq && (nl < targ.lo || nh > targ.hi)) {
+    // decisions over the children's (wider) time range
+    __syncthreads();
+    for (uint32_t w = tid; w < words; w += blockDim.x) bits[w] = 0u;
+    (void)cell_forward<D>(W, V, bits, cx, cy, cz, Iv{nl, nh});
+    if (tid == 0) ws[ST_FP32] += (unsigned long long)root.fwd_cost;
+  }
+  // ---- hand over to the group: decision bits and time range, then count in
+  __syncthreads();
+  if (want_prune && enq) {
+    uint32_t *dst = P.cell_bits[level & 1] + (size_t)unit * P.bm_words;
+    for (uint32_t w = tid; w < words; w += blockDim.x) dst[w] = bits[w];
+  }
+  if (tid == 0) {
+    CellInfo ci;
+    ci.nl = enq ? nl : -fm_inf();
+    ci.nh = enq ? nh : fm_inf();
+    ci.enq = enq ? 1u : 0u;
+    ci.pad = 0;
+    P.cell_info[level & 1][unit] = ci;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) sh.last = atomicAdd(&itp->parent[3], 1u) == 7u ? 1u : 0u;
+  __syncthreads();
+  if (!sh.last) return;
+  __threadfence();
+  finish_group(P, it, level, unit & ~7u, cell, sh, ws);
 }
 
 __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ LaunchParams P, uint32_t level,
@@ -1387,29 +1381,25 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
   if (lane < ST_COUNT) ws[lane] = 0;
   __syncwarp();
 
-  // wide items: the whole block per parent
+  // wide items: one block per child cell
   {
     __shared__ WideShared sh;
     __shared__ uint32_t s_idx;
-    const uint32_t n_w = min(P.witem_count[level], P.item_cap);
-    uint2 *dec = P.wide_dec + (size_t)blockIdx.x * P.wide_dec_stride;
-    uint8_t *flg = P.wide_flags + (size_t)blockIdx.x * P.wide_flag_stride;
-    if (P.wide_smem) {
-      dec = reinterpret_cast<uint2 *>(smem_regs + (size_t)kWarps * rcap * 32u);
-      flg = reinterpret_cast<uint8_t *>(dec + P.wide_dec_stride);
-    }
+    const uint32_t n_units = min(P.witem_count[level], P.witem_cap) * 8u;
+    unsigned char *cell = P.cell_smem ? reinterpret_cast<unsigned char *>(smem_regs)
+                                      : P.cell_scratch + (size_t)blockIdx.x * P.cell_bytes;
     while (true) {
       if (threadIdx.x == 0) s_idx = atomicAdd(&P.witem_cursor[level], 1u);
       __syncthreads();
-      const uint32_t idx = s_idx;
+      const uint32_t u = s_idx;
       __syncthreads();
-      if (idx >= n_w) break;
-      const WorkItem &it = P.witems[level & 1][idx];  // read in place (the next level writes the other list)
+      if (u >= n_units) break;
+      WorkItem *itp = P.witems[level & 1] + (u >> 3);
       const long long c0 = clock64();
-      if (P.scenes[it.scene].flags & SF_DIRECTED)
-        process_wide<true>(P, it, level, rf, slice_log, dec, flg, sh, s_stats[0]);
+      if (P.scenes[itp->scene].flags & SF_DIRECTED)
+        process_cell<true>(P, itp, u & 7u, u, level, cell, sh, s_stats[0]);
       else
-        process_wide<false>(P, it, level, rf, slice_log, dec, flg, sh, s_stats[0]);
+        process_cell<false>(P, itp, u & 7u, u, level, cell, sh, s_stats[0]);
       __syncthreads();
       if (threadIdx.x == 0) {
         const unsigned long long c = (unsigned long long)(clock64() - c0);
@@ -1489,10 +1479,28 @@ __global__ void frame_begin_kernel(LaunchParams P) {
     w.parent[0] = w.parent[1] = w.parent[2] = w.parent[3] = 0u;
     const SceneLaunch &S = P.scenes[s];
     const uint32_t len = P.recs[S.root_rec].len;
-    uint32_t *count = len >= S.wide.min_len ? P.witem_count : P.item_count;
-    WorkItem *list = len >= S.wide.min_len ? P.witems[0] : P.items[0];
-    const uint32_t pos = atomicAdd(count, 1u);
-    if (pos < P.item_cap) list[pos] = w;
+    if (len >= S.wide.min_len) {  // wide item: the root's children brick now
+      const uint32_t pos = atomicAdd(P.witem_count, 1u);
+      if (pos < P.witem_cap) {
+        uint32_t b = S.pool.child[0], fresh = 0;
+        if (b == TSI_NONE) {
+          b = alloc_brick(S, P.error);
+          if (b != TSI_NONE) {
+            S.pool.child[0] = b;
+            fresh = 1;
+            atomicAdd(&P.stats[ST_BRICK_ALLOC], 1ull);
+            atomicAdd(&P.level_stats[ST_BRICK_ALLOC], 1ull);
+          }
+        }
+        w.parent[1] = b;
+        w.parent[2] = fresh;
+        w.parent[3] = 0;
+        P.witems[0][pos] = w;
+        continue;
+      }
+    }
+    const uint32_t pos = atomicAdd(P.item_count, 1u);
+    if (pos < P.item_cap) P.items[0][pos] = w;
     else atomicOr(P.error, EB_QUEUE_FULL);
   }
 }

@@ -156,6 +156,11 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
   const uint32_t n = uint32_t(ins.size());
   out = WideTape{};
   if (n <= 4) return true;
+  if (n >= (1u << 24)) {
+    status = TSI_ERR_TAPE_TOO_WIDE;
+    why = "bundled tape limited to 2^24 slots";
+    return false;
+  }
   // operands of every slot
   std::vector<uint32_t> opa(n, TSI_NONE), opb(n, TSI_NONE);
   for (uint32_t j = 4; j < n; ++j) {
@@ -179,11 +184,11 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
   }
   // The reverse pass accumulates a value's sensitivity user by user, in
   // reverse program order, and that order fixes the rounding.  A value with
-  // one user accumulates in its register; a value with several gets one
+  // one user receives it directly; a value with several gets one
   // contribution record per user, which the value sums in that order when
   // the reverse pass reaches it.  The skip rule (zero sensitivity of a
-  // single-use operand) overwrites the register, so it needs the ir.rs use
-  // count to agree with the users found here.
+  // single-use operand) relies on the ir.rs use count agreeing with the
+  // users found here.
   for (uint32_t j = 4; j < n; ++j) {
     const uint32_t w0 = narrow.code[2 * (j - 4)];
     if ((TSI_W0_FA(w0) && opa[j] != TSI_NONE && users[opa[j]].size() != 1) ||
@@ -205,10 +210,11 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
       ++ncontrib;
     }
   }
-  // List scheduling, width 32, one handler per bundle: a warp executes a
-  // bundle with one lane per slot, so a bundle of one handler runs without
+  // List scheduling, one handler per bundle: the block executes a bundle
+  // with one thread per slot, so a bundle of one handler runs without
   // divergence.  Each bundle takes the handler with the most instructions
   // ready (the oldest ready instruction's on a tie), oldest first.
+  const uint32_t width = WideTape::kWidth;
   std::vector<int32_t> bundle_of(n, -1);
   for (uint32_t a = 0; a < 4; ++a) bundle_of[a] = -2;  // arguments: before everything
   std::vector<std::vector<uint32_t>> bundles;
@@ -231,12 +237,12 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
         best = c;
         hsel = handler(j);
       }
-      if (c == 32) break;
+      if (c == width) break;
     }
     std::vector<uint32_t> b, rest;
     rest.reserve(pending.size());
     for (uint32_t j : pending) {
-      if (b.size() < 32 && handler(j) == hsel && ready(j)) {
+      if (b.size() < width && handler(j) == hsel && ready(j)) {
         b.push_back(j);
         bundle_of[j] = k;
       } else {
@@ -252,44 +258,6 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
     pending.swap(rest);
   }
   const uint32_t nb = uint32_t(bundles.size());
-  // last bundle reading each value; the field lives to the end
-  std::vector<int64_t> last(n, -1);
-  for (uint32_t j = 4; j < n; ++j) {
-    if (opa[j] != TSI_NONE) last[opa[j]] = std::max<int64_t>(last[opa[j]], bundle_of[j]);
-    if (opb[j] != TSI_NONE) last[opb[j]] = std::max<int64_t>(last[opb[j]], bundle_of[j]);
-  }
-  last[n - 1] = int64_t(nb) + 1;
-  // register allocation: a bundle reads before it writes
-  std::vector<uint32_t> reg(n, 0);
-  std::vector<uint8_t> used(64, 0);
-  for (uint32_t a = 0; a < 4; ++a) {
-    reg[a] = a;
-    used[a] = last[a] >= 0 ? 1 : 0;
-  }
-  uint32_t maxreg = 3;
-  for (uint32_t k = 0; k < nb; ++k) {
-    for (uint32_t j : bundles[k]) {  // operands whose last read is this bundle
-      if (opa[j] != TSI_NONE && last[opa[j]] == int64_t(k)) used[reg[opa[j]]] = 0;
-      if (opb[j] != TSI_NONE && last[opb[j]] == int64_t(k)) used[reg[opb[j]]] = 0;
-    }
-    std::vector<uint32_t> dead;
-    for (uint32_t j : bundles[k]) {
-      uint32_t d = 0;
-      while (d < used.size() && used[d]) ++d;
-      if (d == used.size()) used.push_back(0);
-      if (d >= 65535u) {
-        status = TSI_ERR_TAPE_TOO_WIDE;
-        why = "bundled tape needs more than 65535 registers";
-        return false;
-      }
-      reg[j] = d;
-      used[d] = 1;
-      if (last[j] < 0) dead.push_back(d);
-      maxreg = std::max(maxreg, d);
-    }
-    for (uint32_t d : dead) used[d] = 0;
-  }
-  // slots
   const uint32_t nslots = n - 4;
   out.slots.assign(size_t(nslots) * 12, 0);
   out.bundles.assign(size_t(nb) * 2, 0);
@@ -304,39 +272,26 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
   uint32_t off = 0;
   for (uint32_t k = 0; k < nb; ++k) {
     const std::vector<uint32_t> &b = bundles[k];
-    // registers accumulated into by this bundle's reverse step: single-use
-    // operands, distinct by construction (both live when the bundle reads)
-    std::vector<uint32_t> acc;
-    for (uint32_t j : b)
-      for (uint32_t v : {opa[j], opb[j]})
-        if (v != TSI_NONE && gbase[v] == TSI_NONE && !(v == opb[j] && opb[j] == opa[j])) acc.push_back(reg[v]);
-    std::sort(acc.begin(), acc.end());
-    if (std::adjacent_find(acc.begin(), acc.end()) != acc.end()) {
-      status = TSI_ERR_INVALID_ARGUMENT;
-      why = "two slots of one bundle accumulate into one register";
-      return false;
-    }
     for (size_t s = 0; s < b.size(); ++s) {
       const uint32_t j = b[s];
       const uint32_t w0 = narrow.code[2 * (j - 4)], w1 = narrow.code[2 * (j - 4) + 1];
       const uint32_t h = TSI_W0_H(w0);
       uint32_t *S = &out.slots[size_t(off + s) * 12];
-      S[0] = h | (TSI_W0_FA(w0) << 6) | (TSI_W0_FB(w0) << 7);
-      const uint32_t ra = opa[j] != TSI_NONE ? reg[opa[j]] : 0, rb = opb[j] != TSI_NONE ? reg[opb[j]] : 0;
-      S[1] = reg[j] | (ra << 16);
-      S[2] = rb;
+      S[0] = h | (TSI_W0_FA(w0) << 6) | (TSI_W0_FB(w0) << 7) | (j << 8);
+      S[1] = opa[j] != TSI_NONE ? opa[j] : 0u;
+      S[2] = opb[j] != TSI_NONE ? opb[j] : 0u;
       S[3] = TSI_H_IS_II(h) ? 0u : w1;  // literal bits
       S[4] = j;
-      S[5] = opa[j];
-      S[6] = opb[j];
-      S[7] = out.narrow_mm[j - 4];
+      S[5] = out.narrow_mm[j - 4];
+      S[6] = opa[j];
+      S[7] = opb[j];
       S[8] = rec_a[j];
       S[9] = rec_b[j];
       S[10] = gbase[j];
       S[11] = gbase[j] == TSI_NONE ? 0u : uint32_t(users[j].size());
     }
     out.bundles[2 * k] = off;
-    out.bundles[2 * k + 1] = uint32_t(b.size());
+    out.bundles[2 * k + 1] = uint32_t(b.size()) | (TSI_W0_H(narrow.code[2 * (b[0] - 4)]) << 16);
     off += uint32_t(b.size());
   }
   for (uint32_t a = 0; a < 4; ++a) {
@@ -344,9 +299,8 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
     out.arg_gcount[a] = gbase[a] == TSI_NONE ? 0u : uint32_t(users[a].size());
   }
   out.ncontrib = ncontrib;
-  out.nregs = maxreg + 1;
+  out.nvalues = n;
   out.nbundles = nb;
-  out.out_reg = reg[n - 1];
   return true;
 }
 

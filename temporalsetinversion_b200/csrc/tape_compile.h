@@ -21,32 +21,31 @@ struct PackedTape {
 };
 
 // Bundled ("wide") form of a full tape, for evaluating one cell with a whole
-// warp: instructions are list-scheduled into bundles of at most 32 mutually
-// independent instructions of one handler (one per lane), and given their
-// own register allocation in which a bundle reads all its operands before
-// it writes any result.  Per slot (3 x uint4):
-//   s0.x  handler | single-use A << 6 | single-use B << 7
-//   s0.y  dst register | A register << 16
-//   s0.z  B register
+// block: instructions are list-scheduled into bundles of at most kWidth
+// mutually independent instructions of one handler (one per thread).  Every
+// SSA value keeps its own slot (no register reuse), so the reverse pass
+// reads operands where the forward pass left them.  Per slot (3 x uint4):
+//   s0.x  handler | single-use A << 6 | single-use B << 7 | dst SSA << 8
+//   s0.y  A SSA (0 if absent)     s0.z  B SSA (0 if absent)
 //   s0.w  f32 literal
-//   s1    SSA slot of dst, A, B (TSI_NONE if absent), min/max ordinal
+//   s1    dst SSA, min/max ordinal, A SSA, B SSA (TSI_NONE if absent)
 //   s2    contribution record of A, of B (TSI_NONE: the operand has one
-//         user and accumulates in its register); first record and record
-//         count of dst (count 0: dst has at most one user)
+//         user, which writes its sensitivity directly); first record and
+//         record count of dst (count 0: dst has at most one user)
 // A value with several users gets one contribution record per user, last
 // user first, and sums them in that order when the reverse pass reaches it:
 // the order of the sequential reverse pass (compute.wgsl:3786), whatever
 // bundles the users fall in.
 struct WideTape {
+  static constexpr uint32_t kWidth = 256;  // threads of the evaluating block
   std::vector<uint32_t> slots;    // 12 words per slot
-  std::vector<uint32_t> bundles;  // 2 words per bundle: slot offset, count
+  std::vector<uint32_t> bundles;  // 2 words per bundle: first slot, count | handler << 16
   std::vector<uint32_t> narrow_mm;  // per narrow instruction: min/max ordinal or TSI_NONE
   uint32_t arg_gbase[4] = {TSI_NONE, TSI_NONE, TSI_NONE, TSI_NONE};  // records of x, y, z, t
   uint32_t arg_gcount[4] = {0, 0, 0, 0};
   uint32_t ncontrib = 0;          // contribution records per cell
-  uint32_t nregs = 0;
+  uint32_t nvalues = 0;           // SSA values (the 4 arguments included)
   uint32_t nbundles = 0;
-  uint32_t out_reg = 0;
 };
 
 bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, WideTape &out, tsi_status &status,

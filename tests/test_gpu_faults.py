@@ -58,11 +58,22 @@ def test_bad_opcode_and_bad_tapes_rejected(device):
     assert s.invert(0.0).cells_evaluated > 0
 
 
+def _serial_chain(n: int) -> str:
+    """A sphere followed by a chain of n dependent multiply-adds: a long tape
+    with no parallelism, which stays on the one-warp path."""
+    b = scenes.IRBuilder()
+    v = b.add(b.add(b.mul(b.X, b.X), b.mul(b.Y, b.Y)), b.mul(b.Z, b.Z))
+    v = b.add(v, b.mul(b.T, 0.1))
+    for _ in range(n):
+        v = b.sub(b.mul(v, 1.0001), 0.0001)
+    return b.text(b.sub(v, 0.25))
+
+
 @pytest.mark.gpu
 def test_log_arena_exhaustion_is_reported():
     with Device(log_arena_bytes=1 << 16) as dev:
-        # 37.5k slots in ~1.2k bundles: the reverse-AD log outgrows a warp's slice
-        text = scenes.csg(2048, 7)
+        # ~1.2k dependent instructions: the operand log outgrows a warp's slice
+        text = _serial_chain(600)
         s = Scene(dev, Tape.from_llvm_ir(dev, text), api.default_params(localsubdiv=3))
         with pytest.raises(N.TsiError) as e:
             for t in (0.0, 0.02):  # the second frame runs reverse AD on the long root tape
