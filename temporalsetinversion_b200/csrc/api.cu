@@ -142,9 +142,7 @@ struct tsi_ctx {
   uint32_t *d_cell_bits[2] = {nullptr, nullptr};
   size_t cell_arena_bytes = 0;  // of each parity's info + bits
   uint32_t witem_cap = 0, bm_words = 0;
-  unsigned char *d_cell_scratch = nullptr;
-  size_t cell_scratch_bytes = 0;
-  uint32_t cell_bytes = 0, cell_smem = 0;
+
   uint2 *d_dealloc[2] = {nullptr, nullptr};
   uint32_t dealloc_cap = 0;
   uint32_t *d_dealloc_count = nullptr, *d_dealloc_cursor = nullptr;
@@ -213,9 +211,7 @@ LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes) {
     P.cell_info[q] = c->d_cell_info[q];
     P.cell_bits[q] = c->d_cell_bits[q];
   }
-  P.cell_smem = c->cell_smem;
-  P.cell_bytes = c->cell_bytes;
-  P.cell_scratch = c->d_cell_scratch;
+
   P.dealloc_cap = c->dealloc_cap;
   P.dealloc[0] = c->d_dealloc[0];
   P.dealloc[1] = c->d_dealloc[1];
@@ -289,6 +285,18 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, Scene
   R.c_level = TSI_NONE;
 }
 
+// Shared-memory working set of one wide cell (the device's cell_layout):
+// values and sensitivities (8 bytes per SSA value each), contribution
+// records, decision bits, liveness flags.
+size_t wide_cell_bytes(size_t nvalues, size_t ncontrib, size_t bm_words) {
+  return 16 * nvalues + ((ncontrib * 8 + 15) & ~size_t(15)) + ((bm_words * 4 + 15) & ~size_t(15)) +
+         ((nvalues + 15) & ~size_t(15));
+}
+// Tapes whose cell working set exceeds this stay on the narrow path (the
+// block also needs its static shared memory and room for a second block's
+// decision bits is kept).
+constexpr size_t kWideCellMaxBytes = 192u << 10;
+
 // Launch geometry of one frame for n scenes.
 struct FramePlan {
   uint32_t lmax = 0, rcap = 4;
@@ -302,48 +310,27 @@ struct FramePlan {
 tsi_status plan_frame(tsi_ctx *c, tsi_scene *const *scenes, uint32_t n, FramePlan &fp) {
   uint32_t rmax = 4, mm_max = 0, bm_words = 1;
   size_t cell_bytes = 0;
-  bool any_wide = false;
   fp.lmax = 0;
   for (uint32_t i = 0; i < n; ++i) {
     const tsi_tape *t = scenes[i]->tape;
     fp.lmax = std::max(fp.lmax, (uint32_t)scenes[i]->p.localsubdiv);
     rmax = std::max(rmax, t->nregs);
-    if (t->d_wslots) {
-      any_wide = true;
-      mm_max = std::max(mm_max, t->n_minmax);
-    }
+    if (t->d_wslots) mm_max = std::max(mm_max, t->n_minmax);
   }
   bm_words = std::max(1u, (mm_max + 15u) / 16u);
-  for (uint32_t i = 0; i < n; ++i) {  // the device's cell_layout, per scene
-    const tsi_tape *t = scenes[i]->tape;
-    if (!t->d_wslots) continue;
-    const size_t nv = t->wvalues;
-    const size_t bytes = 16 * nv + ((size_t(t->wcontrib) * 8 + 15) & ~size_t(15)) +
-                         ((size_t(bm_words) * 4 + 15) & ~size_t(15)) + ((nv + 15) & ~size_t(15));
-    cell_bytes = std::max(cell_bytes, bytes);
-  }
+  for (uint32_t i = 0; i < n; ++i)
+    if (scenes[i]->tape->d_wslots)
+      cell_bytes = std::max(cell_bytes, wide_cell_bytes(scenes[i]->tape->wvalues, scenes[i]->tape->wcontrib, bm_words));
   fp.rcap = (rmax + 3u) & ~3u;
   const size_t regfile = (size_t)kWarpsPerBlock * fp.rcap * 32u * sizeof(float2);
-  // the wide cell's working set lives in shared memory when it fits
-  const bool cell_smem = any_wide && cell_bytes <= (160u << 10);
-  fp.smem = std::max(regfile, cell_smem ? cell_bytes : 0);
+  // the wide cell's working set and the narrow register files share the
+  // dynamic shared memory (the phases run one after the other)
+  fp.smem = std::max(regfile, cell_bytes);
   CK(refine_set_smem(fp.smem));
   int bps = 0;
   CK(refine_occupancy(kBlock, fp.smem, &bps));
   if (bps < 1) return set_err(TSI_ERR_TAPE_TOO_WIDE, "register file does not fit in shared memory");
   fp.grid = std::min<int>(bps * c->sm_count, (int)(c->max_warps / kWarpsPerBlock));
-  c->cell_smem = cell_smem ? 1u : 0u;
-  c->cell_bytes = (uint32_t)cell_bytes;
-  if (any_wide && !cell_smem) {
-    const size_t need = (size_t)fp.grid * cell_bytes;
-    if (need > c->cell_scratch_bytes) {
-      cudaFree(c->d_cell_scratch);
-      c->d_cell_scratch = nullptr;
-      c->cell_scratch_bytes = 0;
-      CK(dalloc(&c->d_cell_scratch, need));
-      c->cell_scratch_bytes = need;
-    }
-  }
   // hand-over arenas: 64 MB per level parity, as many wide items as fit
   const size_t per_item = 8 * (sizeof(CellInfo) + (size_t)bm_words * 4);
   const size_t arena = std::max<size_t>(64u << 20, c->cell_arena_bytes);
@@ -819,7 +806,6 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   cudaFree(c->d_witem_count);
   cudaFree(c->d_witem_cursor);
   for (int q = 0; q < 2; ++q) cudaFree(c->d_cell_info[q]);
-  cudaFree(c->d_cell_scratch);
   cudaFree(c->d_dealloc[0]);
   cudaFree(c->d_dealloc[1]);
   cudaFree(c->d_dealloc_count);
@@ -877,7 +863,8 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
   // several times more instructions than bundles)
   if (t->len >= 256) {
     WideTape wt;
-    if (compile_wide(ins, pt, wt, st, why) && wt.nbundles > 0) {
+    if (compile_wide(ins, pt, wt, st, why) && wt.nbundles > 0 &&
+        wide_cell_bytes(wt.nvalues, wt.ncontrib, (pt.n_minmax + 15) / 16) + 4096 <= kWideCellMaxBytes) {
       // device layout: the three uint4 of every slot in three arrays
       const size_t nsl = wt.slots.size() / 12;
       std::vector<uint32_t> soa(wt.slots.size());

@@ -157,12 +157,6 @@ struct LaunchParams {
   uint32_t bm_words;       // branch-decision words per wide cell (2 bits per min/max)
   CellInfo *cell_info[2];  // [witem_cap * 8] per level parity
   uint32_t *cell_bits[2];  // [witem_cap * 8][bm_words] per level parity
-  // per-cell working set of the wide path (values, sensitivities,
-  // contribution records, decision bits, liveness flags): in shared memory
-  // when cell_smem, else cell_scratch + blockIdx.x * cell_bytes
-  uint32_t cell_smem;
-  uint32_t cell_bytes;
-  unsigned char *cell_scratch;
   uint32_t item_cap;
   uint32_t dealloc_cap;
   uint2 *dealloc[2];       // (scene, brick)

@@ -780,6 +780,10 @@ __device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level,
   if (lane == 0) ws[ST_BRICK_FREE] += __popc(fm);
 }
 
+// Dynamic shared memory of refine_kernel: the narrow path's register files,
+// or the working set of the wide path's cell.
+extern __shared__ __align__(16) unsigned char tsi_dyn_smem[];
+
 // ======================================================================
 // Wide path: one block per child cell of a wide item, one thread per
 // instruction of a bundle (tape_compile.h WideTape).  Long tapes at the top
@@ -812,31 +816,52 @@ __device__ __forceinline__ Iv ldv(const float2 *a, uint32_t i) {
 }
 __device__ __forceinline__ void stv(float2 *a, uint32_t i, Iv v) { a[i] = make_float2(v.lo, v.hi); }
 
+constexpr uint32_t kSmemBundles = 512;  // bundle descriptors held in shared memory
+
+struct WideShared {
+  uint32_t last, E, cnt, mmk, fcost, rcost, ri;
+  unsigned long long off;
+  float gl, gh, hl, hh;
+  uint32_t scan[kWarps];
+  float2 sens[4];
+  uint2 bt[kSmemBundles];  // the tape's bundle descriptors when they fit
+};
+
+// Bundle descriptors: the shared copy when the tape has few enough bundles.
+__device__ __forceinline__ const uint2 *bundle_table(const WideDev &W, const WideShared &sh) {
+  return W.nbundles <= kSmemBundles ? sh.bt : W.bundles;
+}
+
 // Forward pass over the bundles (compute.wgsl:3633-3772); returns the field.
 // `bits`: 2 bits per min/max of this cell (A always chosen, B always chosen).
 template <bool D>
-__device__ Iv cell_forward(const WideDev &W, float2 *V, uint32_t *bits, Iv x, Iv y, Iv z, Iv t) {
+__device__ __forceinline__ Iv cell_forward(const WideDev &W, const uint2 *bt_tab, float2 *V, uint32_t *bits, Iv x, Iv y, Iv z,
+                           Iv t) {
   const uint32_t tid = threadIdx.x;
-  const uint2 *__restrict__ bundles = W.bundles;
   const uint4 *__restrict__ slots = W.slots;
   const uint32_t nb = W.nbundles, ns = W.nslots;
+  const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
+  // slots fetched three bundles ahead of their use (an L2 round trip spans
+  // several bundle steps)
+  auto fetch = [&](uint32_t kk) -> uint4 {
+    if (kk >= nb) return zero4;
+    const uint2 b = bt_tab[kk];
+    return tid < (b.y & 0xffffu) ? slots[b.x + tid] : zero4;
+  };
   if (tid == 0) {
     stv(V, 0, x);
     stv(V, 1, y);
     stv(V, 2, z);
     stv(V, 3, t);
   }
-  // descriptor and slot of the next bundle fetched while this one runs
-  uint2 btn = bundles[0];
-  uint4 sln = tid < (btn.y & 0xffffu) ? slots[btn.x + tid] : make_uint4(0u, 0u, 0u, 0u);
+  uint4 q0 = fetch(0), q1 = fetch(1), q2 = fetch(2);
   __syncthreads();
   for (uint32_t k = 0; k < nb; ++k) {
-    const uint2 bt = btn;
-    const uint4 sl = sln;
-    if (k + 1 < nb) {
-      btn = bundles[k + 1];
-      sln = tid < (btn.y & 0xffffu) ? slots[btn.x + tid] : make_uint4(0u, 0u, 0u, 0u);
-    }
+    const uint4 sl = q0;
+    q0 = q1;
+    q1 = q2;
+    q2 = fetch(k + 3u);
+    const uint2 bt = bt_tab[k];
     const uint32_t h = bt.y >> 16;
     if (tid < (bt.y & 0xffffu)) {
       const float lit = __uint_as_float(sl.w);
@@ -879,34 +904,40 @@ __device__ __forceinline__ Iv gather_sens(const float2 *R, uint32_t base, uint32
 // the reverse pass reaches the value.  sens_out: 4 floats x 2 in shared
 // memory for the arguments' sensitivities.
 template <bool D>
-__device__ void cell_reverse(const WideDev &W, const float2 *V, float2 *G, float2 *R, float2 *sens_out) {
+__device__ __forceinline__ void cell_reverse(const WideDev &W, const uint2 *bt_tab, const float2 *V, float2 *G, float2 *R,
+                             float2 *sens_out) {
   using I = IA<D>;
   const uint32_t tid = threadIdx.x;
-  const uint2 *__restrict__ bundles = W.bundles;
   const uint4 *__restrict__ slots = W.slots;
   const uint32_t ns = W.nslots, nv = W.nvalues;
   const int nb = (int)W.nbundles;
-  for (uint32_t v = tid; v < nv; v += blockDim.x) G[v] = make_float2(0.0f, 0.0f);
   const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
-  uint2 btn = bundles[nb - 1];
-  bool an = tid < (btn.y & 0xffffu);
-  uint4 s0n = an ? slots[btn.x + tid] : zero4;
-  uint4 s2n = an ? slots[2u * ns + btn.x + tid] : zero4;
+  // words 0-3 and 8-11 of this thread's slot, two bundles ahead
+  auto fetch = [&](int kk, uint4 &s0, uint4 &s2) {
+    s0 = zero4;
+    s2 = zero4;
+    if (kk < 0) return;
+    const uint2 b = bt_tab[kk];
+    if (tid < (b.y & 0xffffu)) {
+      s0 = slots[b.x + tid];
+      s2 = slots[2u * ns + b.x + tid];
+    }
+  };
+  for (uint32_t v = tid; v < nv; v += blockDim.x) G[v] = make_float2(0.0f, 0.0f);
+  uint4 a0, a2, b0, b2;
+  fetch(nb - 1, a0, a2);
+  fetch(nb - 2, b0, b2);
   __syncthreads();
   if (tid == 0) G[nv - 1u] = make_float2(1.0f, 1.0f);
   __syncthreads();
   for (int k = nb - 1; k >= 0; --k) {
-    const uint2 bt = btn;
-    const bool act = an;
-    const uint4 sl = s0n, s2 = s2n;
-    if (k > 0) {  // next (lower) bundle, fetched while this one runs
-      btn = bundles[k - 1];
-      an = tid < (btn.y & 0xffffu);
-      s0n = an ? slots[btn.x + tid] : zero4;
-      s2n = an ? slots[2u * ns + btn.x + tid] : zero4;
-    }
+    const uint4 sl = a0, s2 = a2;
+    a0 = b0;
+    a2 = b2;
+    fetch(k - 2, b0, b2);
+    const uint2 bt = bt_tab[k];
     const uint32_t h = bt.y >> 16;
-    if (act && h != H_CONST) {
+    if (tid < (bt.y & 0xffffu) && h != H_CONST) {
       const bool II = TSI_H_IS_II(h);
       const uint32_t fa = (sl.x >> 6) & 1u, fb = (sl.x >> 7) & 1u;
       const uint32_t a = sl.y, b = sl.z;
@@ -962,18 +993,13 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s
   return base + x - v;
 }
 
-struct WideShared {
-  uint32_t last, E, cnt, mmk, fcost, rcost, ri;
-  unsigned long long off;
-  float gl, gh, hl, hh;
-  uint32_t scan[kWarps];
-  float2 sens[4];
-};
+
 
 // The last cell of a wide item to finish: prunes the full tape with the
 // branch decisions shared by all enqueued siblings and enqueues them.
-__device__ void finish_group(const LaunchParams &P, const WorkItem &it, uint32_t level, uint32_t unit0,
-                             unsigned char *cell, WideShared &sh, unsigned long long *ws) {
+__device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkItem &it, uint32_t level,
+                                             uint32_t unit0, WideShared &sh, unsigned long long *ws) {
+  unsigned char *cell = tsi_dyn_smem;
   const uint32_t tid = threadIdx.x;
   const SceneLaunch &S = P.scenes[it.scene];
   const WideDev &W = S.wide;
@@ -1021,21 +1047,24 @@ __device__ void finish_group(const LaunchParams &P, const WorkItem &it, uint32_t
     __syncthreads();
     // liveness from the field backwards, bundle by bundle
     {
-      const uint2 *__restrict__ bundles = W.bundles;
+      const uint2 *bt_tab = bundle_table(W, sh);
       const uint4 *__restrict__ slots = W.slots;
       const uint32_t ns = W.nslots;
+      const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
+      auto fetch = [&](int kk) -> uint4 {
+        if (kk < 0) return zero4;
+        const uint2 b = bt_tab[kk];
+        return tid < (b.y & 0xffffu) ? slots[ns + b.x + tid] : zero4;
+      };
       if (tid == 0) flags[W.nvalues - 1u] = 1;
       int kb = (int)W.nbundles - 1;
-      uint2 btn = bundles[kb];
-      uint4 s1n = tid < (btn.y & 0xffffu) ? slots[ns + btn.x + tid] : make_uint4(0u, 0u, 0u, 0u);
+      uint4 q0 = fetch(kb), q1 = fetch(kb - 1);
       __syncthreads();
       for (; kb >= 0; --kb) {
-        const uint2 bt = btn;
-        const uint4 s1 = s1n;
-        if (kb > 0) {
-          btn = bundles[kb - 1];
-          s1n = tid < (btn.y & 0xffffu) ? slots[ns + btn.x + tid] : make_uint4(0u, 0u, 0u, 0u);
-        }
+        const uint2 bt = bt_tab[kb];
+        const uint4 s1 = q0;
+        q0 = q1;
+        q1 = fetch(kb - 2);
         if (tid < (bt.y & 0xffffu) && flags[s1.x]) {
           bool la = s1.z != TSI_NONE, lb = s1.w != TSI_NONE;
           if (TSI_H_IS_MINMAX(bt.y >> 16)) {
@@ -1145,8 +1174,8 @@ __device__ void finish_group(const LaunchParams &P, const WorkItem &it, uint32_t
 // One child cell (octant k) of a wide item.  unit = item * 8 + k.
 template <bool D>
 __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, uint32_t k, uint32_t unit,
-                                          uint32_t level, unsigned char *cell, WideShared &sh,
-                                          unsigned long long *ws) {
+                                          uint32_t level, WideShared &sh, unsigned long long *ws) {
+  unsigned char *cell = tsi_dyn_smem;  // the cell's working set (shared memory)
   using A = IA<D>;
   const uint32_t tid = threadIdx.x;
   const WorkItem &it = *itp;
@@ -1167,6 +1196,10 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   float2 *G = reinterpret_cast<float2 *>(cell + L.sens);
   float2 *R = reinterpret_cast<float2 *>(cell + L.rec);
   uint32_t *bits = reinterpret_cast<uint32_t *>(cell + L.bits);
+  if (W.nbundles <= kSmemBundles)
+    for (uint32_t i = tid; i < W.nbundles; i += blockDim.x) sh.bt[i] = W.bundles[i];
+  const uint2 *bt_tab = bundle_table(W, sh);
+  __syncthreads();
 
   // ---- cell setup (compute.wgsl:3582-3626), uniform across the block
   const float4 pxy = pool.box_xy[Pv];
@@ -1235,10 +1268,10 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
     if (want_prune)
       for (uint32_t w = tid; w < words; w += blockDim.x) bits[w] = 0u;
     const long long c0 = clock64();
-    field = cell_forward<D>(W, V, want_prune ? bits : nullptr, cx, cy, cz, targ);
+    field = cell_forward<D>(W, bt_tab, V, want_prune ? bits : nullptr, cx, cy, cz, targ);
     const long long c1 = clock64();
     if (take_deriv) {
-      cell_reverse<D>(W, V, G, R, sh.sens);
+      cell_reverse<D>(W, bt_tab, V, G, R, sh.sens);
       for (int q = 0; q < 4; ++q) sens[q] = ldv(sh.sens, q);
     }
     if (tid == 0) {
@@ -1342,7 +1375,7 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
     // decisions over the children's (wider) time range
     __syncthreads();
     for (uint32_t w = tid; w < words; w += blockDim.x) bits[w] = 0u;
-    (void)cell_forward<D>(W, V, bits, cx, cy, cz, Iv{nl, nh});
+    (void)cell_forward<D>(W, bt_tab, V, bits, cx, cy, cz, Iv{nl, nh});
     if (tid == 0) ws[ST_FP32] += (unsigned long long)root.fwd_cost;
   }
   // ---- hand over to the group: decision bits and time range, then count in
@@ -1365,12 +1398,12 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   __syncthreads();
   if (!sh.last) return;
   __threadfence();
-  finish_group(P, it, level, unit & ~7u, cell, sh, ws);
+  finish_group(P, it, level, unit & ~7u, sh, ws);
 }
 
 __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ LaunchParams P, uint32_t level,
                                                      uint32_t rcap) {
-  extern __shared__ float2 smem_regs[];
+  float2 *smem_regs = reinterpret_cast<float2 *>(tsi_dyn_smem);
   __shared__ unsigned long long s_stats[kWarps][ST_COUNT];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -1386,8 +1419,6 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
     __shared__ WideShared sh;
     __shared__ uint32_t s_idx;
     const uint32_t n_units = min(P.witem_count[level], P.witem_cap) * 8u;
-    unsigned char *cell = P.cell_smem ? reinterpret_cast<unsigned char *>(smem_regs)
-                                      : P.cell_scratch + (size_t)blockIdx.x * P.cell_bytes;
     while (true) {
       if (threadIdx.x == 0) s_idx = atomicAdd(&P.witem_cursor[level], 1u);
       __syncthreads();
@@ -1397,9 +1428,9 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
       WorkItem *itp = P.witems[level & 1] + (u >> 3);
       const long long c0 = clock64();
       if (P.scenes[itp->scene].flags & SF_DIRECTED)
-        process_cell<true>(P, itp, u & 7u, u, level, cell, sh, s_stats[0]);
+        process_cell<true>(P, itp, u & 7u, u, level, sh, s_stats[0]);
       else
-        process_cell<false>(P, itp, u & 7u, u, level, cell, sh, s_stats[0]);
+        process_cell<false>(P, itp, u & 7u, u, level, sh, s_stats[0]);
       __syncthreads();
       if (threadIdx.x == 0) {
         const unsigned long long c = (unsigned long long)(clock64() - c0);

@@ -63,7 +63,7 @@ __device__ __forceinline__ void node_box(const VoxelPoolDev &pool, uint32_t v, F
   p1 = f3(a.y, a.w, b.y);
 }
 
-__global__ void __launch_bounds__(256) trace_kernel(TraceParams T) {
+__global__ void __launch_bounds__(256, 4) trace_kernel(TraceParams T) {
   const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t py = blockIdx.y * blockDim.y + threadIdx.y;
   const bool valid = px < T.W && py < T.H;
@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(256) trace_kernel(TraceParams T) {
   rd.y = ((T.m[1] * d.x + T.m[5] * d.y) + T.m[9] * d.z) + T.m[13] * 0.0f;
   rd.z = ((T.m[2] * d.x + T.m[6] * d.y) + T.m[10] * d.z) + T.m[14] * 0.0f;
   const F3 ro = f3(T.eye[0], T.eye[1], T.eye[2]);
+  const F3 inv = rcp3(rd);  // the slab tests' reciprocal direction, once per ray
 
   F3 c = f3(1.0f, 1.0f, 1.0f);
   F3 nrm = f3(0.0f, 0.0f, 0.0f);
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(256) trace_kernel(TraceParams T) {
     uint32_t region = 0u;
     F3 p0, p1;
     node_box(pool, region, p0, p1);
-    F3 hit = slabs(p0, p1, ro2, rcp3(rd));
+    F3 hit = slabs(p0, p1, ro2, inv);
     bool done = (hit.x == 0.0f);
     float spheremarch = 0.0f;
     for (uint32_t iter = 0; iter < 5000u && !done; ++iter) {
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(256) trace_kernel(TraceParams T) {
       if (hit.x == 0.0f) {
         if (sp == 0) continue;
         node_box(pool, stack[sp - 1], p0, p1);
-        hit = slabs(p0, p1, ro2, rcp3(rd));
+        hit = slabs(p0, p1, ro2, inv);
         continue;
       }
       const F3 two = f3(2.0f, 2.0f, 2.0f);
@@ -126,11 +127,11 @@ __global__ void __launch_bounds__(256) trace_kernel(TraceParams T) {
       float sd2 = ((s2 * ((float)mp2 - rol.z) + s2 * 0.5f) + 0.5f) * dd2;
       float m0 = 0.0f, m1 = 0.0f, m2 = 0.0f;
       const F3 old_ro2 = ro2;
+      // per node: the darkening of every DDA step and the children's brick
+      const bool darken = !T.normal_viz && fm_max(p1.x - p0.x, fm_max(p1.y - p0.y, p1.z - p0.z)) < 1.0f;
+      const uint32_t cbase = pool.child[region];
       for (int i = 0; i < 32; ++i) {
-        if (!T.normal_viz) {
-          const float ext = fm_max(p1.x - p0.x, fm_max(p1.y - p0.y, p1.z - p0.z));
-          if (ext < 1.0f) c = muls(c, T.darken);
-        }
+        if (darken) c = muls(c, T.darken);
         const F3 mv = f3(m0 * (sd0 - dd0), m1 * (sd1 - dd1), m2 * (sd2 - dd2));
         const float t = ((len3(mv) + hit.y) + TEPS) + spheremarch;
         ro2 = old_ro2 + muls(rd, t);
@@ -142,12 +143,11 @@ __global__ void __launch_bounds__(256) trace_kernel(TraceParams T) {
             break;
           }
           node_box(pool, stack[sp - 1], p0, p1);
-          hit = slabs(p0, p1, ro2, rcp3(rd));
+          hit = slabs(p0, p1, ro2, inv);
           break;
         }
         const int ci = mp0 + 2 * mp1 + 4 * mp2;
         if (ci < 0 || ci >= 8) break;
-        const uint32_t cbase = pool.child[region];
         const uint32_t child = cbase + (uint32_t)ci;
         if (cbase != TSI_NONE) ++visits;
         if (cbase != TSI_NONE && pool.f[child] <= 0.0f) {
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(256) trace_kernel(TraceParams T) {
           node_box(pool, child, q0, q1);
           const F3 tp0 = f3(q0.x - TEPS, q0.y - TEPS, q0.z - TEPS);
           const F3 tp1 = f3(q1.x + TEPS, q1.y + TEPS, q1.z + TEPS);
-          const F3 th = slabs(tp0, tp1, ro2, rcp3(rd));
+          const F3 th = slabs(tp0, tp1, ro2, inv);
           if (th.x == 1.0f) {
             if (pool.child[child] != TSI_NONE) {
               if (sp < 32) stack[sp++] = region;
