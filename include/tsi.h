@@ -335,10 +335,14 @@ TSI_API tsi_status tsi_debug_math(tsi_ctx *ctx, int32_t which, uint32_t n, const
  * level's refinement launch (-1 unless TSI_PROFILE_LEVELS is set in the
  * environment when the context is created) and TSI_LEVEL_COUNTERS counters
  * per level: the tsi_stats fields from parents_expanded to prune_fallbacks
- * (without voxels_live and items_high_water), then SM clock cycles: wide
- * items processed, their cycles (sum, max), the forward and reverse passes
- * of their first cell (sums), narrow items' cycles (sum, max). */
-#define TSI_LEVEL_COUNTERS 24
+ * (without voxels_live and items_high_water), then wide cells processed
+ * and SM clock cycles: wide cells (sum, max), their forward and reverse
+ * passes (sums), narrow items (sum, max); then narrow
+ * items on a tape at least the wide path's threshold long, and the longest
+ * tape a narrow item ran; then narrow items' cycles in the first forward
+ * pass, the reverse pass and the pruning scan, and the instructions of the
+ * first forward pass. */
+#define TSI_LEVEL_COUNTERS 30
 TSI_API tsi_status tsi_debug_level_profile(tsi_ctx *ctx, uint32_t max_levels, float *ms, uint64_t *counters,
                                            uint32_t *n_levels);
 

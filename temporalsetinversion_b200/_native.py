@@ -46,7 +46,8 @@ class Uniforms(C.Structure):  # uniforms.rs:8-17
 LEVEL_COUNTERS = ["parents", "evaluated", "reverse", "skipped", "ambiguous", "empty", "full", "enqueued", "reused",
                   "instr_fwd", "instr_rev", "instr_full", "fp32", "brick_alloc", "brick_free", "tape_words",
                   "prune_fallback", "wide_items", "cyc_wide", "cyc_wide_max", "cyc_wide_fwd", "cyc_wide_rev",
-                  "cyc_narrow", "cyc_narrow_max"]
+                  "cyc_narrow", "cyc_narrow_max", "narrow_long", "narrow_len_max",
+                  "cyc_n_fwd", "cyc_n_rev", "cyc_n_prune", "n_fwd_instr"]
 
 
 class Stats(C.Structure):

@@ -135,7 +135,12 @@ enum tsi_stat_index {
   // SM clock cycles (clock64): wide cells (count, sum, max, and their
   // forward and reverse passes) and narrow items (sum, max)
   ST_WIDE_ITEMS, ST_CYC_WIDE, ST_CYC_WIDE_MAX, ST_CYC_WIDE_FWD, ST_CYC_WIDE_REV, ST_CYC_NARROW,
-  ST_CYC_NARROW_MAX, ST_COUNT
+  ST_CYC_NARROW_MAX,
+  // narrow items: on a tape at least the wide threshold long, longest tape
+  ST_NARROW_LONG, ST_NARROW_LEN_MAX,
+  // narrow items: SM cycles of the first forward pass, the reverse pass and
+  // the pruning scan, and the instructions of the first forward pass
+  ST_CYC_N_FWD, ST_CYC_N_REV, ST_CYC_N_PRUNE, ST_N_FWD_INSTR, ST_COUNT
 };
 
 struct LaunchParams {

@@ -34,238 +34,91 @@
 #include <mutex>
 
 #include "device_types.h"
+#include "interp.cuh"
+#include "wide_interp.cuh"
 #include "interval.cuh"
 #include "opcost.h"
 
 namespace tsi {
-
-#define FULL_MASK 0xffffffffu
 
 __constant__ uint32_t c_cost_fwd[H_COUNT] = TSI_OPCOST_FWD_INIT;
 __constant__ uint32_t c_cost_rr[H_COUNT] = TSI_OPCOST_RR_INIT;
 
 constexpr int kWarps = 8;  // warps per block (block of 256)
 
-__device__ __forceinline__ bool finite2(Iv a) { return isfinite(a.lo) && isfinite(a.hi); }
+// Dynamic shared memory of refine_kernel: the narrow path's register files,
+// or the working set of the wide path's cell.
+extern __shared__ __align__(16) unsigned char tsi_dyn_smem[];
 
-__device__ __forceinline__ Iv ld_reg(const float2 *rf, uint32_t r, uint32_t lane) {
-  const float2 v = rf[r * 32u + lane];
-  return Iv{v.x, v.y};
-}
-__device__ __forceinline__ void st_reg(float2 *rf, uint32_t r, uint32_t lane, Iv v) {
-  rf[r * 32u + lane] = make_float2(v.lo, v.hi);
-}
-
-// ---------------------------------------------------------------- handlers
-// Rare handlers live out of line so the interpreter loop stays small.
-template <bool D>
-__device__ __noinline__ Iv cold_forward(uint32_t h, Iv A, Iv B, float lit) {
-  return IA<D>::forward(h, A, B, lit);
-}
-
-template <bool D>
-__device__ __forceinline__ Iv op_forward(uint32_t h, Iv A, Iv B, float lit) {
-  using I = IA<D>;
-  Iv v;
-  switch (h) {
-    case H_CONST: v = iv(lit); break;
-    case H_COPY: v = A; break;
-    case H_ADD_II: v = I::add(A, B); break;
-    case H_SUB_II: v = I::sub(A, B); break;
-    case H_MUL_II: v = I::mul(A, B); break;
-    case H_MIN_II: v = I::min_(A, B); break;
-    case H_MAX_II: v = I::max_(A, B); break;
-    case H_ADD_IF: v = I::add_f(A, lit); break;
-    case H_SUB_IF: v = I::sub_f(A, lit); break;
-    case H_MUL_IF: v = I::mul_f(A, lit); break;
-    case H_MIN_IF: v = Iv{fm_min(A.lo, lit), fm_min(A.hi, lit)}; break;
-    case H_MAX_IF: v = Iv{fm_max(A.lo, lit), fm_max(A.hi, lit)}; break;
-    case H_SQR: v = I::sqr(A); break;
-    case H_SQRT: v = I::sqrt_(A); break;
-    case H_NEG: v = I::neg(A); break;
-    case H_ABS: v = I::abs_(A); break;
-    case H_SUB_FI: v = I::sub(iv(lit), A); break;
-    default: return cold_forward<D>(h, A, B, lit);  // fixed inside
-  }
-  return I::fix(v);
-}
-
-template <bool D>
-__device__ __noinline__ int cold_reverse_rule(uint32_t h, Iv A, Iv B, float lit, Iv &r0, Iv &r1) {
-  return IA<D>::reverse_rule(h, A, B, lit, r0, r1);
-}
-
-template <bool D>
-__device__ __forceinline__ void op_reverse_rule(uint32_t h, Iv A, Iv B, float lit, Iv &r0, Iv &r1) {
-  using I = IA<D>;
-  switch (h) {
-    case H_COPY: r0 = iv(1.0f); break;
-    case H_ADD_II: r0 = iv(1.0f); r1 = iv(1.0f); break;
-    case H_SUB_II: r0 = iv(1.0f); r1 = iv(-1.0f); break;
-    case H_MUL_II: r0 = B; r1 = A; break;
-    case H_MIN_II: I::min_rr(A, B, r0, r1); break;
-    case H_MAX_II: I::max_rr(A, B, r0, r1); break;
-    case H_ADD_IF: r0 = iv(1.0f); break;
-    case H_SUB_IF: r0 = iv(1.0f); break;
-    case H_MUL_IF: r0 = iv(lit); break;
-    case H_SQR: r0 = I::mul_f(A, 2.0f); break;
-    case H_NEG: r0 = iv(-1.0f); break;
-    case H_ABS: r0 = I::abs_rr(A); break;
-    case H_SUB_FI: r0 = iv(-1.0f); break;
-    case H_MIN_IF: { Iv t; I::min_rr(A, iv(lit), r0, t); break; }
-    case H_MAX_IF: { Iv t; I::max_rr(A, iv(lit), r0, t); break; }
-    default: cold_reverse_rule<D>(h, A, B, lit, r0, r1); break;
-  }
-}
-
-// ---------------------------------------------------------------- passes
-// Forward pass over `len` instructions (compute.wgsl:3633-3772).  Writes the
-// operand log when `lg` is set and the min/max branch ballots when `dg` is
-// set.  Returns the output register's value.
-template <bool D>
-__device__ __forceinline__ Iv forward_pass(const uint2 *__restrict__ code, uint32_t len, uint32_t out_reg, float2 *rf,
-                                           uint32_t lane, Iv x, Iv y, Iv z, Iv t, float4 *lg, uint2 *dg) {
-  st_reg(rf, 0, lane, x);
-  st_reg(rf, 1, lane, y);
-  st_reg(rf, 2, lane, z);
-  st_reg(rf, 3, lane, t);
-  uint32_t mm = 0;
-  uint2 w = len ? code[0] : make_uint2(0u, 0u);
-  for (uint32_t i = 0; i < len; ++i) {
-    const uint2 wn = (i + 1 < len) ? code[i + 1] : w;  // fetched while this one executes
-    const uint32_t h = TSI_W0_H(w.x);
-    const float lit = __uint_as_float(w.y);
-    const Iv Av = ld_reg(rf, TSI_W0_A(w.x), lane);
-    const Iv Bv = TSI_H_IS_II(h) ? ld_reg(rf, w.y & 255u, lane) : iv(lit);
-    const Iv r = op_forward<D>(h, Av, Bv, lit);
-    if (lg) lg[(size_t)i * 32u + lane] = make_float4(Av.lo, Av.hi, Bv.lo, Bv.hi);
-    if (dg && TSI_H_IS_MINMAX(h)) {
-      const bool amax = (h == H_MAX_II || h == H_MAX_IF);
-      const bool a_below = Av.hi < Bv.lo, b_below = Bv.hi < Av.lo;
-      const uint32_t ua = __ballot_sync(FULL_MASK, amax ? b_below : a_below);
-      const uint32_t ub = __ballot_sync(FULL_MASK, amax ? a_below : b_below);
-      if (lane == 0) dg[mm] = make_uint2(ua, ub);
-      ++mm;
-    }
-    st_reg(rf, TSI_W0_DST(w.x), lane, r);
-    w = wn;
-  }
-  return ld_reg(rf, out_reg, lane);
-}
-
-// Reverse pass (compute.wgsl:3785-3964): sensitivities reuse the register
-// file; a register's accumulator is consumed and cleared at the definition
-// it holds.  `bad` collects non-finite sensitivities.
-template <bool D>
-__device__ __forceinline__ void reverse_pass(const uint2 *__restrict__ code, uint32_t len, uint32_t nregs,
-                                             uint32_t out_reg, float2 *rf, uint32_t lane, const float4 *lg,
-                                             bool take, Iv sens[4], bool &bad) {
-  using I = IA<D>;
-  for (uint32_t r = 0; r < nregs; ++r) st_reg(rf, r, lane, iv(0.0f));
-  st_reg(rf, out_reg, lane, iv(1.0f));
-  if (len) {
-    uint2 w = code[len - 1];
-    float4 L = lg[(size_t)(len - 1) * 32u + lane];
-    for (int i = (int)len - 1; i >= 0; --i) {
-      uint2 wn = w;
-      float4 Ln = L;
-      if (i > 0) {
-        wn = code[i - 1];
-        Ln = lg[(size_t)(i - 1) * 32u + lane];
-      }
-      const uint32_t h = TSI_W0_H(w.x);
-      const uint32_t d = TSI_W0_DST(w.x), a = TSI_W0_A(w.x), b = w.y & 255u;
-      const float lit = __uint_as_float(w.y);
-      const Iv Av = Iv{L.x, L.y}, Bv = Iv{L.z, L.w};
-      const Iv s = ld_reg(rf, d, lane);
-      st_reg(rf, d, lane, iv(0.0f));
-      if (take && h != H_CONST) {
-        bad |= !finite2(s);
-        const bool s0 = (s.lo == 0.0f && s.hi == 0.0f);
-        if (TSI_H_IS_II(h)) {
-          if (s0 && TSI_W0_FA(w.x) && TSI_W0_FB(w.x)) {
-            st_reg(rf, a, lane, iv(0.0f));
-            st_reg(rf, b, lane, iv(0.0f));
-          } else {
-            Iv r0, r1;
-            op_reverse_rule<D>(h, Av, Bv, lit, r0, r1);
-            r0 = I::mul(I::fix(r0), s);
-            r1 = I::mul(I::fix(r1), s);
-            const Iv n0 = I::add(r0, ld_reg(rf, a, lane));
-            const Iv n1 = I::add(r1, ld_reg(rf, b, lane));
-            st_reg(rf, a, lane, n0);
-            st_reg(rf, b, lane, n1);
-            bad |= !finite2(n0) || !finite2(n1);
-          }
-        } else if (s0 && TSI_W0_FA(w.x)) {
-          st_reg(rf, a, lane, iv(0.0f));
-        } else {
-          Iv r0, r1;
-          op_reverse_rule<D>(h, Av, Bv, lit, r0, r1);
-          r0 = I::mul(I::fix(r0), s);
-          const Iv n0 = I::add(r0, ld_reg(rf, a, lane));
-          st_reg(rf, a, lane, n0);
-          bad |= !finite2(n0);
-        }
-      } else if (take) {
-        bad |= !finite2(s);
-      }
-      w = wn;
-      L = Ln;
-    }
-  }
-  for (int q = 0; q < 4; ++q) sens[q] = ld_reg(rf, q, lane);
-}
-
-// Backward liveness scan of one sibling group (lane 8g): decided min/max
-// become copies/constants, dead instructions vanish.  The kept instructions
-// are written in reverse order to `tmp`; returns their count.
+// Backward liveness scan of one sibling group, run by the whole warp with the
+// group leaders (lane 8g, `active`) doing the work: decided min/max become
+// copies/constants, dead instructions vanish.  The kept instructions are
+// written in reverse order to `tmp`; returns their count.  The tape and the
+// branch ballots arrive 32 per coalesced load.
 __device__ uint32_t prune_scan(const uint2 *__restrict__ code, uint32_t len, uint32_t n_minmax, uint32_t out_reg,
-                               const uint2 *dg, uint32_t g, uint32_t E, uint2 *tmp, uint32_t &mm_kept,
-                               uint32_t &fwd_cost, uint32_t &rev_cost) {
+                               const uint2 *dg, uint32_t g, uint32_t E, uint2 *tmp, bool active, uint32_t lane,
+                               uint32_t &mm_kept, uint32_t &fwd_cost, uint32_t &rev_cost) {
   unsigned long long live = 1ull << out_reg;
-  uint32_t m = n_minmax, cnt = 0;
+  uint32_t cnt = 0;
   mm_kept = 0;
   fwd_cost = 0;
   rev_cost = 0;
-  for (int i = (int)len - 1; i >= 0; --i) {
-    const uint2 w = code[i];
-    const uint32_t h = TSI_W0_H(w.x);
-    const uint32_t d = TSI_W0_DST(w.x), a = TSI_W0_A(w.x), b = w.y & 255u;
-    const bool mmx = TSI_H_IS_MINMAX(h);
-    uint2 dd = make_uint2(0u, 0u);
-    if (mmx) dd = dg[--m];
-    if (!((live >> d) & 1ull)) continue;
-    live &= ~(1ull << d);
-    uint2 out = w;
-    uint32_t hk = h;
-    if (mmx) {
-      const uint32_t ga = (dd.x >> (g * 8u)) & 0xffu, gb = (dd.y >> (g * 8u)) & 0xffu;
-      if ((ga & E) == E) {
-        out = make_uint2(TSI_W0(H_COPY, TSI_W0_FA(w.x), 0u, d, a), 0u);
-        hk = H_COPY;
-        live |= 1ull << a;
-      } else if ((gb & E) == E) {
-        if (TSI_H_IS_II(h)) {
-          out = make_uint2(TSI_W0(H_COPY, TSI_W0_FB(w.x), 0u, d, b), 0u);
+  const int nch = (int)((len + 31u) / 32u);
+  uint2 cur = load_chunk(code, len, nch - 1, lane), nxt = load_chunk(code, len, nch - 2, lane);
+  // ballots: chunk km holds min/max ordinals [32 km, 32 km + 32)
+  int m = (int)n_minmax;
+  int km = (m - 1) / 32;
+  uint2 dcur = load_chunk(dg, n_minmax, m > 0 ? km : -1, lane);
+  for (int k = nch - 1; k >= 0; --k) {
+    const int c0 = 32 * k;
+    for (int j = min(32, (int)len - c0) - 1; j >= 0; --j) {
+      const uint2 w = chunk_word(cur, (uint32_t)j);
+      const uint32_t h = TSI_W0_H(w.x);
+      const uint32_t d = TSI_W0_DST(w.x), a = TSI_W0_A(w.x), b = w.y & 255u;
+      const bool mmx = TSI_H_IS_MINMAX(h);
+      uint2 dd = make_uint2(0u, 0u);
+      if (mmx) {  // uniform across the warp
+        --m;
+        if (m < 32 * km) {
+          km = m / 32;
+          dcur = load_chunk(dg, n_minmax, km, lane);
+        }
+        dd = chunk_word(dcur, (uint32_t)(m - 32 * km));
+      }
+      if (!active || !((live >> d) & 1ull)) continue;
+      live &= ~(1ull << d);
+      uint2 out = w;
+      uint32_t hk = h;
+      if (mmx) {
+        const uint32_t ga = (dd.x >> (g * 8u)) & 0xffu, gb = (dd.y >> (g * 8u)) & 0xffu;
+        if ((ga & E) == E) {
+          out = make_uint2(TSI_W0(H_COPY, TSI_W0_FA(w.x), 0u, d, a), 0u);
           hk = H_COPY;
-          live |= 1ull << b;
+          live |= 1ull << a;
+        } else if ((gb & E) == E) {
+          if (TSI_H_IS_II(h)) {
+            out = make_uint2(TSI_W0(H_COPY, TSI_W0_FB(w.x), 0u, d, b), 0u);
+            hk = H_COPY;
+            live |= 1ull << b;
+          } else {
+            out = make_uint2(TSI_W0(H_CONST, 0u, 0u, d, 0u), w.y);
+            hk = H_CONST;
+          }
         } else {
-          out = make_uint2(TSI_W0(H_CONST, 0u, 0u, d, 0u), w.y);
-          hk = H_CONST;
+          live |= 1ull << a;
+          if (TSI_H_IS_II(h)) live |= 1ull << b;
+          ++mm_kept;
         }
       } else {
-        live |= 1ull << a;
+        if (h != H_CONST) live |= 1ull << a;
         if (TSI_H_IS_II(h)) live |= 1ull << b;
-        ++mm_kept;
       }
-    } else {
-      if (h != H_CONST) live |= 1ull << a;
-      if (TSI_H_IS_II(h)) live |= 1ull << b;
+      fwd_cost += c_cost_fwd[hk] + TSI_FIX_COST;
+      rev_cost += c_cost_rr[hk] + TSI_REV_OPERAND_COST * TSI_H_NREG(hk);
+      tmp[cnt++] = out;
     }
-    fwd_cost += c_cost_fwd[hk] + TSI_FIX_COST;
-    rev_cost += c_cost_rr[hk] + TSI_REV_OPERAND_COST * TSI_H_NREG(hk);
-    tmp[cnt++] = out;
+    cur = nxt;
+    nxt = load_chunk(code, len, k - 2, lane);
   }
   return cnt;
 }
@@ -389,8 +242,9 @@ __device__ __forceinline__ bool item_scratch(const LaunchParams &P, uint32_t lev
 }
 
 template <bool D>
-__device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t level, float2 *rf,
+__device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t level, uint32_t rf_off,
                                           float4 *slice_log, uint2 *slice_dec, unsigned long long *ws) {
+  float2 *rf = reinterpret_cast<float2 *>(tsi_dyn_smem) + rf_off;  // this warp's register file
   using A = IA<D>;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t g = lane >> 3, k = lane & 7u;
@@ -487,6 +341,10 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     if (!(TR.c_level == level && TR.c_lo <= tl && th <= TR.c_hi)) find_valid(P, rec, TR, tl, th);
     for (int attempt = 0; attempt < 2; ++attempt) {
       want_prune = (flags & SF_PRUNING) && TR.len >= TSI_PRUNE_MIN_LEN && TR.nregs <= TSI_PRUNE_MAX_REGS;
+      if (lane == 0 && attempt == 0) {
+        if (TR.len >= S.wide.min_len) ws[ST_NARROW_LONG] += 1;
+        ws[ST_NARROW_LEN_MAX] = max(ws[ST_NARROW_LEN_MAX], (unsigned long long)TR.len);
+      }
       lg = nullptr;
       dg = nullptr;
       if (any_deriv || want_prune) {
@@ -496,9 +354,16 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
         lg = lgs;
         dg = want_prune ? dgs : nullptr;
       }
+      const long long q0 = clock64();
       field = forward_pass<D>(TR.code, TR.len, TR.out_reg, rf, lane, cx, cy, cz, targ, any_deriv ? lg : nullptr, dg);
+      const long long q1 = clock64();
       bool bad = false;
       if (any_deriv) reverse_pass<D>(TR.code, TR.len, TR.nregs, TR.out_reg, rf, lane, lg, take_deriv, sens, bad);
+      if (lane == 0 && attempt == 0) {
+        ws[ST_CYC_N_FWD] += (unsigned long long)(q1 - q0);
+        ws[ST_N_FWD_INSTR] += TR.len;
+        ws[ST_CYC_N_REV] += (unsigned long long)(clock64() - q1);
+      }
       // a pruned tape whose sensitivities overflowed: redo on the full tape
       const bool redo = __any_sync(FULL_MASK, bad) && TR.parent != TSI_NONE;
       if (!redo) break;
@@ -674,9 +539,23 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     bool pruned = false;
     uint2 *tmp =
         (want_prune && !handed && lg != nullptr) ? reinterpret_cast<uint2 *>(lg) + (size_t)g * PR.len : nullptr;
-    if (k == 0 && E != 0 && tmp != nullptr) {
-      cnt = prune_scan(PR.code, PR.len, PR.n_minmax, PR.out_reg, dg, g, E, tmp, mmk, fcost, rcost);
-      pruned = cnt < PR.len;
+    const uint32_t actm = __ballot_sync(FULL_MASK, k == 0 && E != 0 && tmp != nullptr);
+    if (actm) {
+      // every pruning group scans the same tape; lanes of other groups (a
+      // group handed to the wide path holds another record) follow the
+      // scan on that tape, so the warp's shuffles stay uniform
+      const int src = __ffs(actm) - 1;
+      const uint2 *pcode = reinterpret_cast<const uint2 *>(
+          __shfl_sync(FULL_MASK, reinterpret_cast<unsigned long long>(PR.code), src));
+      const uint32_t plen = __shfl_sync(FULL_MASK, PR.len, src);
+      const uint32_t pmm = __shfl_sync(FULL_MASK, PR.n_minmax, src);
+      const uint32_t pout = __shfl_sync(FULL_MASK, PR.out_reg, src);
+      const bool act = (actm >> lane) & 1u;
+      const long long q0 = clock64();
+      cnt = prune_scan(pcode, plen, pmm, pout, dg, g, E, tmp, act, lane, mmk, fcost, rcost);
+      if (lane == 0) ws[ST_CYC_N_PRUNE] += (unsigned long long)(clock64() - q0);
+      pruned = act && cnt < PR.len;
+      if (!act) cnt = 0;
     }
     // reserve arena space and a record (lane 8g), then copy with the group
     unsigned long long off = 0;
@@ -780,10 +659,6 @@ __device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level,
   if (lane == 0) ws[ST_BRICK_FREE] += __popc(fm);
 }
 
-// Dynamic shared memory of refine_kernel: the narrow path's register files,
-// or the working set of the wide path's cell.
-extern __shared__ __align__(16) unsigned char tsi_dyn_smem[];
-
 // ======================================================================
 // Wide path: one block per child cell of a wide item, one thread per
 // instruction of a bundle (tape_compile.h WideTape).  Long tapes at the top
@@ -810,12 +685,6 @@ __device__ __forceinline__ CellLayout cell_layout(const WideDev &W, uint32_t bm_
   return L;
 }
 
-__device__ __forceinline__ Iv ldv(const float2 *a, uint32_t i) {
-  const float2 v = a[i];
-  return Iv{v.x, v.y};
-}
-__device__ __forceinline__ void stv(float2 *a, uint32_t i, Iv v) { a[i] = make_float2(v.lo, v.hi); }
-
 constexpr uint32_t kSmemBundles = 512;  // bundle descriptors held in shared memory
 
 struct WideShared {
@@ -830,148 +699,6 @@ struct WideShared {
 // Bundle descriptors: the shared copy when the tape has few enough bundles.
 __device__ __forceinline__ const uint2 *bundle_table(const WideDev &W, const WideShared &sh) {
   return W.nbundles <= kSmemBundles ? sh.bt : W.bundles;
-}
-
-// Forward pass over the bundles (compute.wgsl:3633-3772); returns the field.
-// `bits`: 2 bits per min/max of this cell (A always chosen, B always chosen).
-template <bool D>
-__device__ __forceinline__ Iv cell_forward(const WideDev &W, const uint2 *bt_tab, float2 *V, uint32_t *bits, Iv x, Iv y, Iv z,
-                           Iv t) {
-  const uint32_t tid = threadIdx.x;
-  const uint4 *__restrict__ slots = W.slots;
-  const uint32_t nb = W.nbundles, ns = W.nslots;
-  const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
-  // slots fetched three bundles ahead of their use (an L2 round trip spans
-  // several bundle steps)
-  auto fetch = [&](uint32_t kk) -> uint4 {
-    if (kk >= nb) return zero4;
-    const uint2 b = bt_tab[kk];
-    return tid < (b.y & 0xffffu) ? slots[b.x + tid] : zero4;
-  };
-  if (tid == 0) {
-    stv(V, 0, x);
-    stv(V, 1, y);
-    stv(V, 2, z);
-    stv(V, 3, t);
-  }
-  uint4 q0 = fetch(0), q1 = fetch(1), q2 = fetch(2);
-  __syncthreads();
-  for (uint32_t k = 0; k < nb; ++k) {
-    const uint4 sl = q0;
-    q0 = q1;
-    q1 = q2;
-    q2 = fetch(k + 3u);
-    const uint2 bt = bt_tab[k];
-    const uint32_t h = bt.y >> 16;
-    if (tid < (bt.y & 0xffffu)) {
-      const float lit = __uint_as_float(sl.w);
-      const Iv A = ldv(V, sl.y);
-      const Iv B = TSI_H_IS_II(h) ? ldv(V, sl.z) : iv(lit);
-      stv(V, sl.x >> 8, op_forward<D>(h, A, B, lit));
-      if (bits && TSI_H_IS_MINMAX(h)) {
-        const uint32_t mm = slots[ns + bt.x + tid].y;
-        const bool amax = (h == H_MAX_II || h == H_MAX_IF);
-        const bool a_below = A.hi < B.lo, b_below = B.hi < A.lo;
-        const uint32_t d = ((amax ? b_below : a_below) ? 1u : 0u) | ((amax ? a_below : b_below) ? 2u : 0u);
-        if (d) atomicOr(&bits[mm >> 4], d << (2u * (mm & 15u)));
-      }
-    }
-    __syncthreads();
-  }
-  return ldv(V, W.nvalues - 1u);
-}
-
-// Sum of a value's contribution records, last user first, onto +0: the
-// accumulation order of the sequential reverse pass.
-template <bool D>
-__device__ __forceinline__ Iv gather_sens(const float2 *R, uint32_t base, uint32_t count) {
-  Iv S = iv(0.0f);
-  uint32_t i = 0;
-  for (; i + 4u <= count; i += 4u) {  // loads ahead of the dependent adds
-    const float2 c0 = R[base + i], c1 = R[base + i + 1u], c2 = R[base + i + 2u], c3 = R[base + i + 3u];
-    S = IA<D>::add(Iv{c0.x, c0.y}, S);
-    S = IA<D>::add(Iv{c1.x, c1.y}, S);
-    S = IA<D>::add(Iv{c2.x, c2.y}, S);
-    S = IA<D>::add(Iv{c3.x, c3.y}, S);
-  }
-  for (; i < count; ++i) S = IA<D>::add(ldv(R, base + i), S);
-  return S;
-}
-
-// Reverse interval AD over the bundles (compute.wgsl:3786-3900).  A
-// single-use operand's sensitivity is written by its one user; an operand
-// with several users gets a contribution record per user (R), summed when
-// the reverse pass reaches the value.  sens_out: 4 floats x 2 in shared
-// memory for the arguments' sensitivities.
-template <bool D>
-__device__ __forceinline__ void cell_reverse(const WideDev &W, const uint2 *bt_tab, const float2 *V, float2 *G, float2 *R,
-                             float2 *sens_out) {
-  using I = IA<D>;
-  const uint32_t tid = threadIdx.x;
-  const uint4 *__restrict__ slots = W.slots;
-  const uint32_t ns = W.nslots, nv = W.nvalues;
-  const int nb = (int)W.nbundles;
-  const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
-  // words 0-3 and 8-11 of this thread's slot, two bundles ahead
-  auto fetch = [&](int kk, uint4 &s0, uint4 &s2) {
-    s0 = zero4;
-    s2 = zero4;
-    if (kk < 0) return;
-    const uint2 b = bt_tab[kk];
-    if (tid < (b.y & 0xffffu)) {
-      s0 = slots[b.x + tid];
-      s2 = slots[2u * ns + b.x + tid];
-    }
-  };
-  for (uint32_t v = tid; v < nv; v += blockDim.x) G[v] = make_float2(0.0f, 0.0f);
-  uint4 a0, a2, b0, b2;
-  fetch(nb - 1, a0, a2);
-  fetch(nb - 2, b0, b2);
-  __syncthreads();
-  if (tid == 0) G[nv - 1u] = make_float2(1.0f, 1.0f);
-  __syncthreads();
-  for (int k = nb - 1; k >= 0; --k) {
-    const uint4 sl = a0, s2 = a2;
-    a0 = b0;
-    a2 = b2;
-    fetch(k - 2, b0, b2);
-    const uint2 bt = bt_tab[k];
-    const uint32_t h = bt.y >> 16;
-    if (tid < (bt.y & 0xffffu) && h != H_CONST) {
-      const bool II = TSI_H_IS_II(h);
-      const uint32_t fa = (sl.x >> 6) & 1u, fb = (sl.x >> 7) & 1u;
-      const uint32_t a = sl.y, b = sl.z;
-      const float lit = __uint_as_float(sl.w);
-      const Iv A = ldv(V, a);
-      const Iv B = II ? ldv(V, b) : iv(lit);
-      const Iv s = s2.w ? gather_sens<D>(R, s2.z, s2.w) : ldv(G, sl.x >> 8);
-      const bool s0 = (s.lo == 0.0f && s.hi == 0.0f);
-      const bool skip = II ? (s0 && fa && fb) : (s0 && fa);
-      Iv c0 = iv(0.0f), c1 = iv(0.0f);
-      if (!skip) {
-        Iv r0, r1;
-        op_reverse_rule<D>(h, A, B, lit, r0, r1);
-        c0 = I::mul(I::fix(r0), s);
-        if (II) c1 = I::mul(I::fix(r1), s);
-      }
-      // both operands read before either is written (an instruction whose
-      // operands are one value keeps the second write)
-      const Iv pa = (s2.x == TSI_NONE && !skip) ? ldv(G, a) : iv(0.0f);
-      const Iv pb = (II && s2.y == TSI_NONE && !skip) ? ldv(G, b) : iv(0.0f);
-      if (s2.x != TSI_NONE) stv(R, s2.x, c0);
-      else stv(G, a, skip ? iv(0.0f) : I::add(c0, pa));
-      if (II) {
-        if (s2.y != TSI_NONE) stv(R, s2.y, c1);
-        else stv(G, b, skip ? iv(0.0f) : I::add(c1, pb));
-      }
-    }
-    __syncthreads();
-  }
-  if (tid < 4u) {
-    const uint32_t gc = W.arg_gcount[tid];
-    stv(sens_out, tid, gc ? gather_sens<D>(R, W.arg_gbase[tid], gc) : ldv(G, tid));
-  }
-  __syncthreads();
 }
 
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *scratch, uint32_t &total) {
@@ -1403,21 +1130,20 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
 
 __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ LaunchParams P, uint32_t level,
                                                      uint32_t rcap) {
-  float2 *smem_regs = reinterpret_cast<float2 *>(tsi_dyn_smem);
   __shared__ unsigned long long s_stats[kWarps][ST_COUNT];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
-  float2 *rf = smem_regs + (size_t)wib * rcap * 32u;
+  const uint32_t rf_off = wib * rcap * 32u;  // this warp's register file in tsi_dyn_smem (float2 units)
   float4 *slice_log = P.log_slices + (size_t)gw * P.slice_len * 32u;
   uint2 *slice_dec = P.dec_slices + (size_t)gw * P.slice_len;
   unsigned long long *ws = s_stats[wib];
   if (lane < ST_COUNT) ws[lane] = 0;
   __syncwarp();
 
+  __shared__ WideShared sh;
+  __shared__ uint32_t s_idx;
   // wide items: one block per child cell
-  {
-    __shared__ WideShared sh;
-    __shared__ uint32_t s_idx;
+  auto wide_phase = [&]() {
     const uint32_t n_units = min(P.witem_count[level], P.witem_cap) * 8u;
     while (true) {
       if (threadIdx.x == 0) s_idx = atomicAdd(&P.witem_cursor[level], 1u);
@@ -1439,25 +1165,36 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
         s_stats[0][ST_CYC_WIDE_MAX] = max(s_stats[0][ST_CYC_WIDE_MAX], c);
       }
     }
-  }
-
-  const uint32_t n_items = min(P.item_count[level], P.item_cap);
-  const WorkItem *items = P.items[level & 1];
-  while (true) {
-    uint32_t idx = 0;
-    if (lane == 0) idx = atomicAdd(&P.item_cursor[level], 1u);
-    idx = __shfl_sync(FULL_MASK, idx, 0);
-    if (idx >= n_items) break;
-    const WorkItem &it = items[idx];
-    const long long c0 = clock64();
-    if (P.scenes[it.scene].flags & SF_DIRECTED) process_item<true>(P, it, level, rf, slice_log, slice_dec, ws);
-    else process_item<false>(P, it, level, rf, slice_log, slice_dec, ws);
-    __syncwarp();
-    if (lane == 0) {
-      const unsigned long long c = (unsigned long long)(clock64() - c0);
-      ws[ST_CYC_NARROW] += c;
-      ws[ST_CYC_NARROW_MAX] = max(ws[ST_CYC_NARROW_MAX], c);
+  };
+  // narrow items: one warp per item
+  auto narrow_phase = [&]() {
+    const uint32_t n_items = min(P.item_count[level], P.item_cap);
+    const WorkItem *items = P.items[level & 1];
+    while (true) {
+      uint32_t idx = 0;
+      if (lane == 0) idx = atomicAdd(&P.item_cursor[level], 1u);
+      idx = __shfl_sync(FULL_MASK, idx, 0);
+      if (idx >= n_items) break;
+      const WorkItem &it = items[idx];
+      const long long c0 = clock64();
+      if (P.scenes[it.scene].flags & SF_DIRECTED) process_item<true>(P, it, level, rf_off, slice_log, slice_dec, ws);
+      else process_item<false>(P, it, level, rf_off, slice_log, slice_dec, ws);
+      __syncwarp();
+      if (lane == 0) {
+        const unsigned long long c = (unsigned long long)(clock64() - c0);
+        ws[ST_CYC_NARROW] += c;
+        ws[ST_CYC_NARROW_MAX] = max(ws[ST_CYC_NARROW_MAX], c);
+      }
     }
+  };
+  // half of the blocks drain the narrow list first, so both lists start
+  // draining at once
+  if (blockIdx.x & 1u) {
+    narrow_phase();
+    wide_phase();
+  } else {
+    wide_phase();
+    narrow_phase();
   }
   // deallocation items: 4 bricks per warp
   const uint32_t n_dealloc = min(P.dealloc_count[level], P.dealloc_cap);
@@ -1474,7 +1211,7 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
   }
   __syncwarp();
   if (lane < ST_COUNT && ws[lane]) {
-    if (lane == ST_CYC_WIDE_MAX || lane == ST_CYC_NARROW_MAX) {
+    if (lane == ST_CYC_WIDE_MAX || lane == ST_CYC_NARROW_MAX || lane == ST_NARROW_LEN_MAX) {
       atomicMax(&P.stats[lane], ws[lane]);
       atomicMax(&P.level_stats[level * ST_COUNT + lane], ws[lane]);
     } else {

@@ -278,9 +278,12 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
       const uint32_t h = TSI_W0_H(w0);
       uint32_t *S = &out.slots[size_t(off + s) * 12];
       S[0] = h | (TSI_W0_FA(w0) << 6) | (TSI_W0_FB(w0) << 7) | (j << 8);
+      // the min/max ordinal sits in the word the handler does not use: the
+      // literal's for two registers, B's for a register and a literal
+      const uint32_t mmo = TSI_H_IS_MINMAX(h) ? out.narrow_mm[j - 4] : 0u;
       S[1] = opa[j] != TSI_NONE ? opa[j] : 0u;
-      S[2] = opb[j] != TSI_NONE ? opb[j] : 0u;
-      S[3] = TSI_H_IS_II(h) ? 0u : w1;  // literal bits
+      S[2] = opb[j] != TSI_NONE ? opb[j] : (TSI_H_IS_II(h) ? 0u : mmo);
+      S[3] = TSI_H_IS_II(h) ? mmo : w1;  // literal bits
       S[4] = j;
       S[5] = out.narrow_mm[j - 4];
       S[6] = opa[j];

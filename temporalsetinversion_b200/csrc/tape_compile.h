@@ -26,8 +26,9 @@ struct PackedTape {
 // SSA value keeps its own slot (no register reuse), so the reverse pass
 // reads operands where the forward pass left them.  Per slot (3 x uint4):
 //   s0.x  handler | single-use A << 6 | single-use B << 7 | dst SSA << 8
-//   s0.y  A SSA (0 if absent)     s0.z  B SSA (0 if absent)
-//   s0.w  f32 literal
+//   s0.y  A SSA (0 if absent)
+//   s0.z  B SSA; for a register-literal min/max its min/max ordinal
+//   s0.w  f32 literal; for a two-register min/max its min/max ordinal
 //   s1    dst SSA, min/max ordinal, A SSA, B SSA (TSI_NONE if absent)
 //   s2    contribution record of A, of B (TSI_NONE: the operand has one
 //         user, which writes its sensitivity directly); first record and

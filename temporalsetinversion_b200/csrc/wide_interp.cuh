@@ -1,0 +1,165 @@
+// wide_interp.cuh — the block-wide interpreter of the bundled tape
+// (tape_compile.h WideTape): one cell per block, one thread per slot of a
+// bundle, every SSA value in its own shared-memory slot.
+//
+// cell_forward follows compute.wgsl:3633-3772, cell_reverse
+// compute.wgsl:3786-3900 with per-use contribution records for values with
+// several users (their sensitivities are summed in the sequential order).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_types.h"
+#include "interp.cuh"
+
+namespace tsi {
+
+__device__ __forceinline__ Iv ldv(const float2 *a, uint32_t i) {
+  const float2 v = a[i];
+  return Iv{v.x, v.y};
+}
+__device__ __forceinline__ void stv(float2 *a, uint32_t i, Iv v) { a[i] = make_float2(v.lo, v.hi); }
+
+// Forward pass over the bundles (compute.wgsl:3633-3772); returns the field.
+// `bits`: 2 bits per min/max of this cell (A always chosen, B always chosen).
+template <bool D>
+__device__ __forceinline__ Iv cell_forward(const WideDev &W, const uint2 *bt_tab, float2 *V, uint32_t *bits, Iv x, Iv y, Iv z,
+                           Iv t) {
+  const uint32_t tid = threadIdx.x;
+  const uint4 *__restrict__ slots = W.slots;
+  const uint32_t nb = W.nbundles;
+  const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
+  // slots fetched three bundles ahead of their use (an L2 round trip spans
+  // several bundle steps)
+  auto fetch = [&](uint32_t kk) -> uint4 {
+    if (kk >= nb) return zero4;
+    const uint2 b = bt_tab[kk];
+    return tid < (b.y & 0xffffu) ? slots[b.x + tid] : zero4;
+  };
+  if (tid == 0) {
+    stv(V, 0, x);
+    stv(V, 1, y);
+    stv(V, 2, z);
+    stv(V, 3, t);
+  }
+  uint4 q0 = fetch(0), q1 = fetch(1), q2 = fetch(2);
+  __syncthreads();
+  for (uint32_t k = 0; k < nb; ++k) {
+    const uint4 sl = q0;
+    q0 = q1;
+    q1 = q2;
+    q2 = fetch(k + 3u);
+    const uint2 bt = bt_tab[k];
+    const uint32_t h = bt.y >> 16;
+    if (tid < (bt.y & 0xffffu)) {
+      const float lit = __uint_as_float(sl.w);
+      const Iv A = ldv(V, sl.y);
+      const Iv B = TSI_H_IS_II(h) ? ldv(V, sl.z) : iv(lit);
+      stv(V, sl.x >> 8, op_forward<D>(h, A, B, lit));
+      if (bits && TSI_H_IS_MINMAX(h)) {
+        const uint32_t mm = TSI_H_IS_II(h) ? sl.w : sl.z;
+        const bool amax = (h == H_MAX_II || h == H_MAX_IF);
+        const bool a_below = A.hi < B.lo, b_below = B.hi < A.lo;
+        const uint32_t d = ((amax ? b_below : a_below) ? 1u : 0u) | ((amax ? a_below : b_below) ? 2u : 0u);
+        if (d) atomicOr(&bits[mm >> 4], d << (2u * (mm & 15u)));
+      }
+    }
+    __syncthreads();
+  }
+  return ldv(V, W.nvalues - 1u);
+}
+
+// Sum of a value's contribution records, last user first, onto +0: the
+// accumulation order of the sequential reverse pass.
+template <bool D>
+__device__ __forceinline__ Iv gather_sens(const float2 *R, uint32_t base, uint32_t count) {
+  Iv S = iv(0.0f);
+  uint32_t i = 0;
+  for (; i + 4u <= count; i += 4u) {  // loads ahead of the dependent adds
+    const float2 c0 = R[base + i], c1 = R[base + i + 1u], c2 = R[base + i + 2u], c3 = R[base + i + 3u];
+    S = IA<D>::add(Iv{c0.x, c0.y}, S);
+    S = IA<D>::add(Iv{c1.x, c1.y}, S);
+    S = IA<D>::add(Iv{c2.x, c2.y}, S);
+    S = IA<D>::add(Iv{c3.x, c3.y}, S);
+  }
+  for (; i < count; ++i) S = IA<D>::add(ldv(R, base + i), S);
+  return S;
+}
+
+// Reverse interval AD over the bundles (compute.wgsl:3786-3900).  A
+// single-use operand's sensitivity is written by its one user; an operand
+// with several users gets a contribution record per user (R), summed when
+// the reverse pass reaches the value.  sens_out: 4 floats x 2 in shared
+// memory for the arguments' sensitivities.
+template <bool D>
+__device__ __forceinline__ void cell_reverse(const WideDev &W, const uint2 *bt_tab, const float2 *V, float2 *G, float2 *R,
+                             float2 *sens_out) {
+  using I = IA<D>;
+  const uint32_t tid = threadIdx.x;
+  const uint4 *__restrict__ slots = W.slots;
+  const uint32_t ns = W.nslots, nv = W.nvalues;
+  const int nb = (int)W.nbundles;
+  const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
+  // words 0-3 and 8-11 of this thread's slot, two bundles ahead
+  auto fetch = [&](int kk, uint4 &s0, uint4 &s2) {
+    s0 = zero4;
+    s2 = zero4;
+    if (kk < 0) return;
+    const uint2 b = bt_tab[kk];
+    if (tid < (b.y & 0xffffu)) {
+      s0 = slots[b.x + tid];
+      s2 = slots[2u * ns + b.x + tid];
+    }
+  };
+  for (uint32_t v = tid; v < nv; v += blockDim.x) G[v] = make_float2(0.0f, 0.0f);
+  uint4 a0, a2, b0, b2;
+  fetch(nb - 1, a0, a2);
+  fetch(nb - 2, b0, b2);
+  __syncthreads();
+  if (tid == 0) G[nv - 1u] = make_float2(1.0f, 1.0f);
+  __syncthreads();
+  for (int k = nb - 1; k >= 0; --k) {
+    const uint4 sl = a0, s2 = a2;
+    a0 = b0;
+    a2 = b2;
+    fetch(k - 2, b0, b2);
+    const uint2 bt = bt_tab[k];
+    const uint32_t h = bt.y >> 16;
+    if (tid < (bt.y & 0xffffu) && h != H_CONST) {
+      const bool II = TSI_H_IS_II(h);
+      const uint32_t fa = (sl.x >> 6) & 1u, fb = (sl.x >> 7) & 1u;
+      const uint32_t a = sl.y, b = sl.z;
+      const float lit = __uint_as_float(sl.w);
+      const Iv A = ldv(V, a);
+      const Iv B = II ? ldv(V, b) : iv(lit);
+      const Iv s = s2.w ? gather_sens<D>(R, s2.z, s2.w) : ldv(G, sl.x >> 8);
+      const bool s0 = (s.lo == 0.0f && s.hi == 0.0f);
+      const bool skip = II ? (s0 && fa && fb) : (s0 && fa);
+      Iv c0 = iv(0.0f), c1 = iv(0.0f);
+      if (!skip) {
+        Iv r0, r1;
+        op_reverse_rule<D>(h, A, B, lit, r0, r1);
+        c0 = I::mul(I::fix(r0), s);
+        if (II) c1 = I::mul(I::fix(r1), s);
+      }
+      // both operands read before either is written (an instruction whose
+      // operands are one value keeps the second write)
+      const Iv pa = (s2.x == TSI_NONE && !skip) ? ldv(G, a) : iv(0.0f);
+      const Iv pb = (II && s2.y == TSI_NONE && !skip) ? ldv(G, b) : iv(0.0f);
+      if (s2.x != TSI_NONE) stv(R, s2.x, c0);
+      else stv(G, a, skip ? iv(0.0f) : I::add(c0, pa));
+      if (II) {
+        if (s2.y != TSI_NONE) stv(R, s2.y, c1);
+        else stv(G, b, skip ? iv(0.0f) : I::add(c1, pb));
+      }
+    }
+    __syncthreads();
+  }
+  if (tid < 4u) {
+    const uint32_t gc = W.arg_gcount[tid];
+    stv(sens_out, tid, gc ? gather_sens<D>(R, W.arg_gbase[tid], gc) : ldv(G, tid));
+  }
+  __syncthreads();
+}
+
+}  // namespace tsi

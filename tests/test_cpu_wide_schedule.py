@@ -66,7 +66,12 @@ def test_wide_schedule_invariants(case):
     users, rec = {}, {}
     for s in slots:
         j, a, b = int(s[4]), int(s[6]), int(s[7])
-        assert int(s[1]) == (a if a != NONE else 0) and int(s[2]) == (b if b != NONE else 0)
+        h = int(s[0]) & 63
+        assert int(s[1]) == (a if a != NONE else 0)
+        if b != NONE:
+            assert int(s[2]) == b
+        if int(s[5]) != NONE:  # min/max: ordinal in the word the handler does not use
+            assert int(s[3]) == int(s[5]) if b != NONE else int(s[2]) == int(s[5])
         for v in {a, b} - {NONE}:
             assert bundle_of[v] < bundle_of[j], "slot %d runs before its operand %d" % (j, v)
             users.setdefault(v, []).append(j)
