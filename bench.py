@@ -342,6 +342,12 @@ def run_gpu(args, rank, world, local, dist) -> None:
         try:
             cb = cpu_sample(text, params, view, frames=2)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            cores = cb["cores"]
+            one = cpu_sample(text, params, view, frames=2, threads=1)  # the same frames on one core
+            line["cpu_baseline"]["single_thread"] = {"value": one["value"], "unit": "frames/s", "cores": 1,
+                                                     "sample": one["sample"]}
+            import oracle
+            oracle.set_threads(cores)
         except Exception as e:  # the oracle needs g++ on the host
             line["cpu_baseline"] = {"value": None, "unit": "frames/s", "cores": 0, "kind": "port",
                                     "sample": "unavailable: %s" % e}

@@ -253,6 +253,13 @@ TSI_API tsi_status tsi_scene_image_device(tsi_scene *scene, tsi_image_device *ou
  * With out == NULL only the count is returned. */
 TSI_API tsi_status tsi_scene_readback_cells(tsi_scene *scene, tsi_cell *out, uint64_t cap,
                                             uint64_t *n);
+/* Keys of the leaves the tracer can hit (compute.wgsl:4302, 4313): cells
+ * with f <= 0 and no children, depth-first order.  With out == NULL only
+ * the count is returned. */
+typedef struct tsi_leaf {
+  uint32_t level, ix, iy, iz;
+} tsi_leaf;
+TSI_API tsi_status tsi_scene_readback_leaves(tsi_scene *scene, tsi_leaf *out, uint64_t cap, uint64_t *n);
 TSI_API tsi_status tsi_scene_get_params(const tsi_scene *scene, tsi_params *out);
 TSI_API uint64_t tsi_scene_device_bytes(const tsi_scene *scene);
 

@@ -111,6 +111,7 @@ SIGNATURES = {
     "tsi_scene_trace": (i32, [C.c_void_p, P(Uniforms), P(Image), P(Stats)]),
     "tsi_scene_image_device": (i32, [C.c_void_p, P(ImageDevice)]),
     "tsi_scene_readback_cells": (i32, [C.c_void_p, P(Cell), u64, P(u64)]),
+    "tsi_scene_readback_leaves": (i32, [C.c_void_p, P(u32), u64, P(u64)]),
     "tsi_scene_get_params": (i32, [C.c_void_p, P(Params)]),
     "tsi_scene_device_bytes": (u64, [C.c_void_p]),
     "tsi_batch_run": (i32, [C.c_void_p, P(Request), u32]),

@@ -239,6 +239,16 @@ class Scene:
                                              C.byref(n)), "tsi_scene_readback_cells")
         return arr
 
+    def leaves(self) -> np.ndarray:
+        """(level, ix, iy, iz) of the cells the tracer can hit, one row each."""
+        lib = self.device.lib
+        n = C.c_uint64(0)
+        N.check(lib.tsi_scene_readback_leaves(self.handle, None, 0, C.byref(n)), "tsi_scene_readback_leaves")
+        arr = np.zeros((n.value, 4), dtype=np.uint32)
+        N.check(lib.tsi_scene_readback_leaves(self.handle, arr.ctypes.data_as(C.POINTER(C.c_uint32)), n.value,
+                                              C.byref(n)), "tsi_scene_readback_leaves")
+        return arr
+
     def close(self) -> None:
         if getattr(self, "handle", None) and getattr(self.device, "handle", None):
             self.device.lib.tsi_scene_destroy(self.handle)

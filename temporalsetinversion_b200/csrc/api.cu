@@ -1230,6 +1230,24 @@ TSI_API tsi_status tsi_scene_readback_cells(tsi_scene *s, tsi_cell *out, uint64_
   return (out && cap < cnt) ? TSI_ERR_BUFFER_TOO_SMALL : TSI_OK;
 }
 
+TSI_API tsi_status tsi_scene_readback_leaves(tsi_scene *s, tsi_leaf *out, uint64_t cap, uint64_t *n) {
+  if (!s || !n) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  uint64_t nc = 0;
+  tsi_status st = tsi_scene_readback_cells(s, nullptr, 0, &nc);
+  if (st != TSI_OK) return st;
+  std::vector<tsi_cell> cells(nc);
+  st = tsi_scene_readback_cells(s, cells.data(), nc, &nc);
+  if (st != TSI_OK) return st;
+  uint64_t cnt = 0;
+  for (const tsi_cell &c : cells) {
+    if (c.has_children || !(c.f <= 0.0f)) continue;
+    if (out && cnt < cap) out[cnt] = tsi_leaf{c.level, c.ix, c.iy, c.iz};
+    ++cnt;
+  }
+  *n = cnt;
+  return TSI_OK;
+}
+
 TSI_API tsi_status tsi_scene_get_params(const tsi_scene *s, tsi_params *out) {
   if (!s || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
   *out = s->p;

@@ -104,3 +104,23 @@ def test_pruning_reduces_work(device):
     assert s_on.instr_forward * 2 < s_off.instr_forward
     assert s_off.instr_forward == s_off.instr_full_equiv
     assert_cells_equal(on.cells(), off.cells())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["spheres16_L6", "csg64_reuse", "sponza_L6"])
+def test_leaf_keys_match_oracle(device, case):
+    """The leaf key set (cells with f <= 0 and no children, what the tracer
+    can hit) equals the oracle's after every frame."""
+    src, params, times = CASES[case]
+    tape = tape_of(src)
+    p = api.default_params(**params)
+    gs = Scene(device, Tape.upload(device, tape), p)
+    os_ = oracle.Scene(tape, p)
+    for t in times:
+        gs.invert(t)
+        os_.invert(t)
+        oc = os_.cells()
+        want = oc[(oc["has_children"] == 0) & (oc["f"] <= 0)]
+        want = {(int(c["level"]), int(c["ix"]), int(c["iy"]), int(c["iz"])) for c in want}
+        got = {tuple(int(v) for v in row) for row in gs.leaves()}
+        assert got == want, "t=%g: %d leaves, oracle %d" % (t, len(got), len(want))

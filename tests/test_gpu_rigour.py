@@ -1,0 +1,56 @@
+"""Rigour of the directed-rounding mode at the octree level: no cell the
+GPU classifies as empty (f = +1) or full (f = -1) may contain a sign change
+of f, checked by dense float64 point sampling (tests/point_eval.py) of the
+same tape.  Point sampling is off, so every classification rests on an
+interval enclosure.  Only cells evaluated in the current frame are checked:
+a cell carried over from an earlier frame is only guaranteed up to the
+temporal tolerance delta (compute.wgsl:3996), not exactly."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from point_eval import evaluate
+from temporalsetinversion_b200 import Scene, Tape, api, scenes
+
+CASES = {
+    "spheres16": (lambda: scenes.spheres16(0), 6),
+    "csg24": (lambda: scenes.csg(24, 3, 0.9), 6),
+    "csg64": (lambda: scenes.csg(64, 5, 0.85), 6),
+}
+
+
+def _samples(cells: np.ndarray, rng, n_random: int = 24):
+    """Corners, centre and random interior points of every cell box."""
+    lo = np.stack([cells["x"][:, 0], cells["y"][:, 0], cells["z"][:, 0]], axis=1).astype(np.float64)
+    hi = np.stack([cells["x"][:, 1], cells["y"][:, 1], cells["z"][:, 1]], axis=1).astype(np.float64)
+    corners = np.array([[(k >> 0) & 1, (k >> 1) & 1, (k >> 2) & 1] for k in range(8)], np.float64)
+    u = np.concatenate([corners, [[0.5, 0.5, 0.5]], rng.uniform(size=(n_random, 3))], axis=0)
+    return lo[:, None, :] + u[None, :, :] * (hi - lo)[:, None, :]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_directed_octree_is_rigorous(device, case):
+    make, levels = CASES[case]
+    text = make()
+    tape = api.IR.new(text).gpu_instructions
+    p = api.default_params(localsubdiv=levels, pointsample=0, rounding_mode=1)
+    s = Scene(device, Tape.upload(device, tape), p)
+    rng = np.random.default_rng(11)
+    checked = 0
+    for t in (0.0, 0.05, 0.1):
+        s.invert(t)
+        cells = s.cells()
+        now = cells[(cells["t"] == np.float32(t)) & (cells["f"] != 0)]
+        for sign in (1.0, -1.0):
+            sel = now[now["f"] == sign]
+            if len(sel) == 0:
+                continue
+            pts = _samples(sel, rng)
+            f = evaluate(tape, pts[..., 0], pts[..., 1], pts[..., 2], np.float64(np.float32(t)))
+            bad = np.nonzero(np.any(sign * f <= -1e-9, axis=1))[0]
+            assert len(bad) == 0, "%s t=%g: %d cells classified %+d contain f of the other sign, e.g. key %s" % (
+                case, t, len(bad), sign, tuple(int(sel[bad[0]][k]) for k in ("level", "ix", "iy", "iz")))
+            checked += len(sel)
+    assert checked > 100
