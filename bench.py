@@ -222,6 +222,84 @@ def run_reference(args, rank, world, dist) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ served leg
+SERVED = dict(scenes=8, rate_rps=400.0, seconds=2.0, seed=1000)
+
+
+def served_leg(local: int) -> dict:
+    """Open-loop Poisson arrivals over SERVED["scenes"] animations of the
+    workload's kind (each request: the next frame of one scene, inverted and
+    traced at 1920x1080 with the frame left on the device) through the
+    serving layer, against the plain path's per-frame latency on one scene."""
+    import threading
+
+    from temporalsetinversion_b200 import Device, Scene, Server, Tape, api
+
+    W, H, F = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["frames"]
+    dev = Device(local)
+    try:
+        work = [build_workload(WORKLOAD["seed"] + 1 + k) for k in range(SERVED["scenes"])]
+        sc = [Scene(dev, Tape.from_llvm_ir(dev, t), p) for t, p, _ in work]
+        # plain path: one scene, one synchronous call pair per frame
+        lat_plain = []
+        for i in range(24):
+            t = frame_time(i, F)
+            u = api.make_uniforms(work[0][2], (W, H), t)
+            t0 = time.perf_counter()
+            sc[0].invert(t)
+            sc[0].trace(u, rgba=False, depth=False, normal=False)
+            dev.lib.tsi_synchronize(dev.handle)
+            lat_plain.append((time.perf_counter() - t0) * 1000.0)
+        for s in sc:
+            s.reset()
+        rng = np.random.default_rng(SERVED["seed"])
+        n = int(SERVED["rate_rps"] * SERVED["seconds"])
+        arrivals = np.cumsum(rng.exponential(1.0 / SERVED["rate_rps"], n))
+        which = rng.integers(0, SERVED["scenes"], n)
+        frame = [0] * SERVED["scenes"]
+        with Server(dev) as srv:
+            tickets = []
+            done = threading.Event()
+            lats = []
+
+            def collect():
+                i = 0
+                while i < n:
+                    if i >= len(tickets):
+                        time.sleep(0.0002)
+                        continue
+                    r = srv.poll(tickets[i], 1000)
+                    if r is not None:
+                        lats.append(r[1])
+                        i += 1
+                done.set()
+
+            th = threading.Thread(target=collect, daemon=True)
+            th.start()
+            start = time.perf_counter()
+            for k in range(n):
+                delay = start + arrivals[k] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                j = int(which[k])
+                t = frame_time(frame[j], F)
+                frame[j] += 1
+                tickets.append(srv.submit(sc[j], t, uniforms=api.make_uniforms(work[j][2], (W, H), t)))
+            done.wait(120.0)
+            wall = time.perf_counter() - start
+            st = srv.stats()
+        lats = np.sort(np.asarray(lats))
+        return {"scenes": SERVED["scenes"], "rate_rps": SERVED["rate_rps"], "requests": int(len(lats)),
+                "throughput_rps": len(lats) / wall, "p50_ms": float(np.percentile(lats, 50)),
+                "p99_ms": float(np.percentile(lats, 99)), "max_ms": float(lats[-1]),
+                "mean_batch": st["mean_batch"], "plain_p50_ms": float(np.percentile(lat_plain, 50)),
+                "plain_p99_ms": float(np.percentile(lat_plain, 99)),
+                "note": "Poisson arrivals, next frame of a random scene, invert + 1080p trace, frame kept on device; "
+                        "plain = one scene, tsi_scene_invert + tsi_scene_trace per frame"}
+    finally:
+        dev.close()
+
+
 # ------------------------------------------------------------------ GPU leg
 def run_gpu(args, rank, world, local, dist) -> None:
     import ctypes as C
@@ -351,8 +429,13 @@ def run_gpu(args, rank, world, local, dist) -> None:
         except Exception as e:  # the oracle needs g++ on the host
             line["cpu_baseline"] = {"value": None, "unit": "frames/s", "cores": 0, "kind": "port",
                                     "sample": "unavailable: %s" % e}
-    print(json.dumps(line), flush=True)
     dev.close()
+    if world == 1 and not args.no_served:
+        try:
+            line["served"] = served_leg(local)
+        except Exception as e:
+            line["served"] = {"unavailable": str(e)}
+    print(json.dumps(line), flush=True)
 
 
 def main() -> None:
@@ -363,6 +446,7 @@ def main() -> None:
     ap.add_argument("--impl", default="tsi", choices=["tsi", "reference"])
     ap.add_argument("--voxels", type=int, default=64 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-latency leg")
     ap.add_argument("--small-arenas", action="store_true",
                     help="small work-item, tape and log arenas (use with --voxels 4194304 under a profiler)")
     args = ap.parse_args()

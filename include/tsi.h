@@ -286,6 +286,39 @@ TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *ctx, tsi_request *reqs, uint3
 TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g);
 TSI_API void tsi_batch_graph_destroy(tsi_batch_graph *g);
 
+/* ---------------- serving ---------------- */
+/* No counterpart in the reference (its frames are driven by the window's
+ * event loop, main.rs:978-1063).  A server owns a worker thread that drains
+ * a queue of requests on one context, fusing the pending requests of
+ * distinct scenes into one tsi_batch_run (requests for one scene run in
+ * submission order, one per batch).  While a server exists only the server
+ * uses its context.  A request's uniforms, image and stats pointers must
+ * stay valid until its ticket completes. */
+typedef struct tsi_server tsi_server;
+typedef struct tsi_server_opts {
+  uint32_t max_batch;       /* scenes fused per launch (0: the context's maximum) */
+  uint32_t reserved;
+} tsi_server_opts;
+typedef struct tsi_server_stats {
+  uint64_t completed;       /* requests finished */
+  uint64_t batches;         /* fused launches run */
+  float mean_batch;         /* requests per launch */
+  float p50_ms, p99_ms;     /* submit-to-completion latency of finished requests */
+  float max_ms;
+} tsi_server_stats;
+TSI_API tsi_status tsi_server_create(tsi_ctx *ctx, const tsi_server_opts *opts, tsi_server **out);
+/* Queues one request; *ticket identifies it for tsi_server_poll. */
+TSI_API tsi_status tsi_server_submit(tsi_server *s, const tsi_request *req, uint64_t *ticket);
+/* The request's status once it has completed (its stats are filled in and
+ * the ticket is released); TSI_ERR_BUSY if it is still pending after
+ * waiting up to wait_ms milliseconds; TSI_ERR_NOT_FOUND for an unknown
+ * ticket.  latency_ms (may be NULL) receives its submit-to-completion time. */
+TSI_API tsi_status tsi_server_poll(tsi_server *s, uint64_t ticket, uint32_t wait_ms, float *latency_ms);
+TSI_API tsi_status tsi_server_stats_get(tsi_server *s, tsi_server_stats *out);
+/* Stops the worker after the running batch; requests still queued complete
+ * with TSI_ERR_SHUTDOWN. */
+TSI_API void tsi_server_destroy(tsi_server *s);
+
 /* ---------------- allocation-free evaluation ---------------- */
 /* No counterpart in the reference.  tsi_tape_eval_boxes allocates device
  * scratch with cudaMalloc; callers that cannot allocate at call time (a

@@ -4,7 +4,8 @@ implicits, temporal error bound, per-cell tape pruning, octree ray tracing).
 The compute path is libtsi.so (CUDA, sm_100a) behind the C ABI of
 include/tsi.h; this package is its Python host.
 """
-from .api import CELL_DTYPE, IR, Device, Scene, State, Tape, default_params, make_uniforms  # noqa: F401
+from .api import CELL_DTYPE, IR, Device, Scene, Server, State, Tape, default_params, make_uniforms  # noqa: F401
 from . import scenes  # noqa: F401
 
-__all__ = ["IR", "Device", "Tape", "Scene", "State", "default_params", "make_uniforms", "scenes", "CELL_DTYPE"]
+__all__ = ["IR", "Device", "Tape", "Scene", "Server", "State", "default_params", "make_uniforms", "scenes",
+           "CELL_DTYPE"]

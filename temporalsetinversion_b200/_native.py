@@ -67,6 +67,15 @@ class Cell(C.Structure):
                 ("y", f32 * 2), ("z", f32 * 2)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("max_batch", u32), ("reserved", u32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", u64), ("batches", u64), ("mean_batch", f32), ("p50_ms", f32), ("p99_ms", f32),
+                ("max_ms", f32)]
+
+
 class Image(C.Structure):
     _fields_ = [("width", u32), ("height", u32), ("rgba", P(f32)), ("depth", P(f32)), ("normal", P(f32))]
 
@@ -115,6 +124,11 @@ SIGNATURES = {
     "tsi_scene_get_params": (i32, [C.c_void_p, P(Params)]),
     "tsi_scene_device_bytes": (u64, [C.c_void_p]),
     "tsi_batch_run": (i32, [C.c_void_p, P(Request), u32]),
+    "tsi_server_create": (i32, [C.c_void_p, P(ServerOpts), P(C.c_void_p)]),
+    "tsi_server_submit": (i32, [C.c_void_p, P(Request), P(u64)]),
+    "tsi_server_poll": (i32, [C.c_void_p, u64, u32, P(f32)]),
+    "tsi_server_stats_get": (i32, [C.c_void_p, P(ServerStats)]),
+    "tsi_server_destroy": (None, [C.c_void_p]),
     "tsi_batch_graph_create": (i32, [C.c_void_p, P(Request), u32, P(C.c_void_p)]),
     "tsi_batch_graph_launch": (i32, [C.c_void_p]),
     "tsi_batch_graph_destroy": (None, [C.c_void_p]),

@@ -317,3 +317,66 @@ def run_batch(device: Device, requests: list, graph: bool = False) -> list:
         outs.append(out)
     N.check(device.lib.tsi_batch_run(device.handle, reqs, n), "tsi_batch_run")
     return outs
+
+
+class Server:
+    """A worker thread on one device that fuses the pending requests of
+    distinct scenes into one launch sequence (tsi_server_*).  While it
+    exists, only the server uses the device."""
+
+    def __init__(self, device: Device, max_batch: int = 0):
+        self.device = device
+        h = C.c_void_p()
+        N.check(device.lib.tsi_server_create(device.handle, C.byref(N.ServerOpts(max_batch, 0)), C.byref(h)),
+                "tsi_server_create")
+        self.handle = h
+        self._keep = {}  # request structs and buffers alive until the ticket completes
+
+    def submit(self, scene: "Scene", time: float, t0: float = float("nan"), uniforms=None,
+               image: bool = False) -> int:
+        req = N.Request()
+        req.scene = scene.handle
+        req.time = float(time)
+        req.t0_or_nan = float(t0)
+        st = N.Stats()
+        req.stats = C.pointer(st)
+        keep = {"req": req, "stats": st}
+        if uniforms is not None:
+            keep["uniforms"] = uniforms
+            req.uniforms = C.pointer(uniforms)
+            if image:
+                w, hgt = uniforms.resolution[0], uniforms.resolution[1]
+                keep["rgba"] = np.empty((hgt, w, 4), np.float32)
+                img = N.Image(w, hgt, _fptr(keep["rgba"]), None, None)
+                keep["img"] = img
+                req.out = C.pointer(img)
+        ticket = C.c_uint64(0)
+        N.check(self.device.lib.tsi_server_submit(self.handle, C.byref(req), C.byref(ticket)), "tsi_server_submit")
+        self._keep[ticket.value] = keep
+        return ticket.value
+
+    def poll(self, ticket: int, wait_ms: int = 60000):
+        """(stats, latency ms, rgba or None) once done; None while pending."""
+        lat = C.c_float(0.0)
+        status = self.device.lib.tsi_server_poll(self.handle, ticket, wait_ms, C.byref(lat))
+        if status == 11:  # TSI_ERR_BUSY
+            return None
+        keep = self._keep.pop(ticket, {})
+        N.check(status, "tsi_server_poll")
+        return keep.get("stats"), lat.value, keep.get("rgba")
+
+    def stats(self) -> dict:
+        st = N.ServerStats()
+        N.check(self.device.lib.tsi_server_stats_get(self.handle, C.byref(st)), "tsi_server_stats_get")
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.device.lib.tsi_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -982,6 +982,8 @@ tsi_status tsi_internal_tape_view(const tsi_tape *t, TsiTapeView *v) {
   return TSI_OK;
 }
 void tsi_internal_set_error(const char *msg) { g_last_error = msg; }
+tsi_ctx *tsi_internal_scene_ctx(const tsi_scene *s) { return s ? s->ctx : nullptr; }
+uint32_t tsi_internal_max_scenes(const tsi_ctx *c) { return c ? c->max_scenes : 0u; }
 
 extern "C" {
 

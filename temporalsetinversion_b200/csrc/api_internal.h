@@ -17,3 +17,6 @@ struct TsiTapeView {
 tsi_status tsi_internal_tape_view(const tsi_tape *t, TsiTapeView *v);
 // Sets the message tsi_last_error returns on this thread.
 void tsi_internal_set_error(const char *msg);
+// Context of a scene, and the most scenes one fused launch takes.
+tsi_ctx *tsi_internal_scene_ctx(const tsi_scene *s);
+uint32_t tsi_internal_max_scenes(const tsi_ctx *c);
