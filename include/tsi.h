@@ -260,6 +260,15 @@ typedef struct tsi_leaf {
   uint32_t level, ix, iy, iz;
 } tsi_leaf;
 TSI_API tsi_status tsi_scene_readback_leaves(tsi_scene *scene, tsi_leaf *out, uint64_t cap, uint64_t *n);
+/* Resident-octree snapshot for eviction and restore (no counterpart in the
+ * reference, whose octree lives in one wgpu buffer for the process): the
+ * voxel pool up to its high-water mark, the free list and the allocation
+ * counters, as one host blob.  Taken between frames.  Restore needs a scene
+ * with the same tape and parameters and a pool at least as large; the
+ * scene then continues exactly where the snapshot's scene was. */
+TSI_API tsi_status tsi_scene_snapshot_size(tsi_scene *scene, uint64_t *bytes);
+TSI_API tsi_status tsi_scene_snapshot(tsi_scene *scene, void *host, uint64_t cap, uint64_t *bytes);
+TSI_API tsi_status tsi_scene_restore(tsi_scene *scene, const void *host, uint64_t bytes);
 TSI_API tsi_status tsi_scene_get_params(const tsi_scene *scene, tsi_params *out);
 TSI_API uint64_t tsi_scene_device_bytes(const tsi_scene *scene);
 

@@ -121,6 +121,9 @@ SIGNATURES = {
     "tsi_scene_image_device": (i32, [C.c_void_p, P(ImageDevice)]),
     "tsi_scene_readback_cells": (i32, [C.c_void_p, P(Cell), u64, P(u64)]),
     "tsi_scene_readback_leaves": (i32, [C.c_void_p, P(u32), u64, P(u64)]),
+    "tsi_scene_snapshot_size": (i32, [C.c_void_p, P(u64)]),
+    "tsi_scene_snapshot": (i32, [C.c_void_p, C.c_void_p, u64, P(u64)]),
+    "tsi_scene_restore": (i32, [C.c_void_p, C.c_void_p, u64]),
     "tsi_scene_get_params": (i32, [C.c_void_p, P(Params)]),
     "tsi_scene_device_bytes": (u64, [C.c_void_p]),
     "tsi_batch_run": (i32, [C.c_void_p, P(Request), u32]),

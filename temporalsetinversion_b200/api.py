@@ -239,6 +239,18 @@ class Scene:
                                              C.byref(n)), "tsi_scene_readback_cells")
         return arr
 
+    def snapshot(self) -> bytes:
+        """The resident octree as a host blob (tsi_scene_snapshot)."""
+        lib = self.device.lib
+        n = C.c_uint64(0)
+        N.check(lib.tsi_scene_snapshot_size(self.handle, C.byref(n)), "tsi_scene_snapshot_size")
+        buf = C.create_string_buffer(n.value)
+        N.check(lib.tsi_scene_snapshot(self.handle, buf, n.value, C.byref(n)), "tsi_scene_snapshot")
+        return buf.raw[:n.value]
+
+    def restore(self, blob: bytes) -> None:
+        N.check(self.device.lib.tsi_scene_restore(self.handle, blob, len(blob)), "tsi_scene_restore")
+
     def leaves(self) -> np.ndarray:
         """(level, ix, iy, iz) of the cells the tracer can hit, one row each."""
         lib = self.device.lib

@@ -1232,6 +1232,103 @@ TSI_API tsi_status tsi_scene_readback_cells(tsi_scene *s, tsi_cell *out, uint64_
   return (out && cap < cnt) ? TSI_ERR_BUFFER_TOO_SMALL : TSI_OK;
 }
 
+}  // extern "C"
+
+// Snapshot blob: header, then the pool arrays over [0, bump * 8) voxels
+// in VoxelPoolDev order, then the free list [0, free_count).
+namespace {
+struct SnapshotHeader {
+  uint32_t magic, version;
+  uint32_t bump, free_count, live_bricks, tape_len;
+  uint64_t params_hash;
+};
+constexpr uint32_t kSnapMagic = 0x54534931u;  // "TSI1"
+constexpr size_t kVoxelBytes = sizeof(float4) + sizeof(float2) + 4 * sizeof(float) + sizeof(uint32_t) + sizeof(float4);
+
+uint64_t params_hash(const tsi_params &p) {  // FNV-1a over the bytes of the parameters
+  const unsigned char *b = reinterpret_cast<const unsigned char *>(&p);
+  uint64_t h = 1469598103934665603ull;
+  for (size_t i = 0; i < sizeof(p); ++i) h = (h ^ b[i]) * 1099511628211ull;
+  return h;
+}
+
+template <typename T>
+tsi_status copy_part(T *dev, unsigned char *&host, size_t n, bool to_host) {
+  const size_t bytes = n * sizeof(T);
+  const cudaError_t e = to_host ? cudaMemcpy(host, dev, bytes, cudaMemcpyDeviceToHost)
+                                : cudaMemcpy(dev, host, bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return set_err(TSI_ERR_CUDA, cudaGetErrorString(e));
+  host += bytes;
+  return TSI_OK;
+}
+
+tsi_status snapshot_io(tsi_scene *s, unsigned char *p, uint32_t bump, uint32_t free_count, bool to_host) {
+  const size_t nv = (size_t)bump * 8;
+  tsi_status st = TSI_OK;
+  if ((st = copy_part(s->pool.box_xy, p, nv, to_host)) != TSI_OK) return st;
+  if ((st = copy_part(s->pool.box_z, p, nv, to_host)) != TSI_OK) return st;
+  if ((st = copy_part(s->pool.t, p, nv, to_host)) != TSI_OK) return st;
+  if ((st = copy_part(s->pool.time_err, p, nv, to_host)) != TSI_OK) return st;
+  if ((st = copy_part(s->pool.f, p, nv, to_host)) != TSI_OK) return st;
+  if ((st = copy_part(s->pool.fast, p, nv, to_host)) != TSI_OK) return st;
+  if ((st = copy_part(s->pool.child, p, nv, to_host)) != TSI_OK) return st;
+  if ((st = copy_part(s->pool.normal, p, nv, to_host)) != TSI_OK) return st;
+  return copy_part(s->pool.free_list, p, free_count, to_host);
+}
+}  // namespace
+
+extern "C" {
+
+TSI_API tsi_status tsi_scene_snapshot_size(tsi_scene *s, uint64_t *bytes) {
+  if (!s || !bytes) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  CK(cudaSetDevice(s->ctx->device));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  SceneCounters ctr;
+  tsi_status st = read_counters(s, ctr);
+  if (st != TSI_OK) return st;
+  const uint32_t bump = std::min(ctr.bump, s->cap_bricks);
+  *bytes = sizeof(SnapshotHeader) + (uint64_t)bump * 8 * kVoxelBytes + (uint64_t)std::max(ctr.free_count, 0) * 4;
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_scene_snapshot(tsi_scene *s, void *host, uint64_t cap, uint64_t *bytes) {
+  if (!s || !host || !bytes) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  uint64_t need = 0;
+  tsi_status st = tsi_scene_snapshot_size(s, &need);
+  if (st != TSI_OK) return st;
+  *bytes = need;
+  if (cap < need) return set_err(TSI_ERR_BUFFER_TOO_SMALL, "snapshot buffer too small");
+  SceneCounters ctr;
+  if ((st = read_counters(s, ctr)) != TSI_OK) return st;
+  if (ctr.pending_count != 0) return set_err(TSI_ERR_BUSY, "snapshot taken inside a frame");
+  SnapshotHeader h{kSnapMagic, 1u, std::min(ctr.bump, s->cap_bricks), (uint32_t)std::max(ctr.free_count, 0),
+                   ctr.live_bricks, s->tape->len, params_hash(s->p)};
+  unsigned char *p = static_cast<unsigned char *>(host);
+  memcpy(p, &h, sizeof(h));
+  return snapshot_io(s, p + sizeof(h), h.bump, h.free_count, true);
+}
+
+TSI_API tsi_status tsi_scene_restore(tsi_scene *s, const void *host, uint64_t bytes) {
+  if (!s || !host) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  if (bytes < sizeof(SnapshotHeader)) return set_err(TSI_ERR_INVALID_ARGUMENT, "snapshot too short");
+  SnapshotHeader h;
+  memcpy(&h, host, sizeof(h));
+  if (h.magic != kSnapMagic || h.version != 1u) return set_err(TSI_ERR_INVALID_ARGUMENT, "not a scene snapshot");
+  if (h.tape_len != s->tape->len || h.params_hash != params_hash(s->p))
+    return set_err(TSI_ERR_INVALID_ARGUMENT, "snapshot of a scene with another tape or other parameters");
+  if (h.bump > s->cap_bricks) return set_err(TSI_ERR_BUFFER_TOO_SMALL, "voxel pool smaller than the snapshot's");
+  if (bytes != sizeof(h) + (uint64_t)h.bump * 8 * kVoxelBytes + (uint64_t)h.free_count * 4)
+    return set_err(TSI_ERR_INVALID_ARGUMENT, "snapshot size does not match its header");
+  CK(cudaSetDevice(s->ctx->device));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  unsigned char *p = const_cast<unsigned char *>(static_cast<const unsigned char *>(host)) + sizeof(h);
+  tsi_status st = snapshot_io(s, p, h.bump, h.free_count, false);
+  if (st != TSI_OK) return st;
+  SceneCounters ctr{(int32_t)h.free_count, h.bump, 0u, h.live_bricks};
+  CK(cudaMemcpy(s->d_ctr, &ctr, sizeof(ctr), cudaMemcpyHostToDevice));
+  return TSI_OK;
+}
+
 TSI_API tsi_status tsi_scene_readback_leaves(tsi_scene *s, tsi_leaf *out, uint64_t cap, uint64_t *n) {
   if (!s || !n) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
   uint64_t nc = 0;

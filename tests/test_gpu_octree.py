@@ -124,3 +124,27 @@ def test_leaf_keys_match_oracle(device, case):
         want = {(int(c["level"]), int(c["ix"]), int(c["iy"]), int(c["iz"])) for c in want}
         got = {tuple(int(v) for v in row) for row in gs.leaves()}
         assert got == want, "t=%g: %d leaves, oracle %d" % (t, len(got), len(want))
+
+
+@pytest.mark.gpu
+def test_snapshot_restore_continues_exactly(device):
+    """A scene restored from a snapshot into a fresh scene (same tape and
+    parameters) continues frame for frame like the original."""
+    src, params, times = CASES["csg64_reuse"]
+    tape = tape_of(src)
+    p = api.default_params(**params)
+    a = Scene(device, Tape.upload(device, tape), p)
+    for t in times[:3]:
+        a.invert(t)
+    blob = a.snapshot()
+    b = Scene(device, Tape.upload(device, tape), p)
+    b.restore(blob)
+    assert_cells_equal(b.cells(), a.cells())
+    for t in times[3:]:
+        sa, sb = a.invert(t).as_dict(), b.invert(t).as_dict()
+        for k in COUNTERS:
+            assert sa[k] == sb[k]
+        assert_cells_equal(b.cells(), a.cells())
+    other = Scene(device, Tape.upload(device, tape), api.default_params(**dict(params, delta=0.02)))
+    with pytest.raises(Exception):
+        other.restore(blob)  # other parameters
