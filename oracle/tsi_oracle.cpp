@@ -737,6 +737,29 @@ struct TraceOut {
 
 const float TEPS = 0.0001f; /* compute.wgsl:4141 */
 
+/* finite_diff_normal (compute.wgsl:4143-4184) for any tape: the tetrahedron
+   of points p + k h, h = 0.01, k in {(1,-1,-1), (-1,-1,1), (-1,1,-1),
+   (1,1,1)}, with f evaluated by the tape on point boxes, normalised as
+   v / |v| (the reference pastes a per-scene function here). */
+V3 tape_normal(const Scene &S, V3 p, float t) {
+  static thread_local Scratch sc;
+  const float h = 0.01f;
+  const float kx[4] = {1.0f, -1.0f, -1.0f, 1.0f}, ky[4] = {-1.0f, -1.0f, 1.0f, 1.0f};
+  const float kz[4] = {-1.0f, 1.0f, -1.0f, 1.0f};
+  float f[4];
+  for (int q = 0; q < 4; ++q) {
+    const float ax = p.x + kx[q] * h, ay = p.y + ky[q] * h, az = p.z + kz[q] * h;
+    const I args[4] = {{ax, ax}, {ay, ay}, {az, az}, {t, t}};
+    EvalOut o;
+    eval_cell(S.tape.data(), (uint32_t)S.tape.size(), args, false, sc, o);
+    f[q] = o.field.lo;
+  }
+  V3 v = v3(kx[0] * f[0], ky[0] * f[0], kz[0] * f[0]);
+  for (int q = 1; q < 4; ++q) v = add(v, v3(kx[q] * f[q], ky[q] * f[q], kz[q] * f[q]));
+  const float l = len3(v);
+  return v3(v.x / l, v.y / l, v.z / l);
+}
+
 void trace(const Scene &S, V3 ro, V3 rd, float time, TraceOut &out) { /* 4189-4403 */
   const Params &p = S.p;
   uint32_t stack[32];
@@ -832,6 +855,8 @@ void trace(const Scene &S, V3 ro, V3 rd, float time, TraceOut &out) { /* 4189-44
           } else {
             intersected = true;
             normal_at_hit = v3(cv.dx, cv.dy, cv.dz);
+            if (p.fast_normals) /* 4337-4342 */
+              normal_at_hit = tape_normal(S, ro2, p.swept_volume ? vx[region].t : time);
             float timesince = time - cv.t;
             V3 movement = v3(1.0f, 0.0f, 0.0f);
             V3 base = v3(1.0f, 1.0f, 1.0f);

@@ -23,6 +23,7 @@
 #include "device_types.h"
 #include "ir_lower.h"
 #include "tape_compile.h"
+#include "trace_params.h"
 #include "tsi.h"
 
 namespace tsi {
@@ -37,23 +38,6 @@ cudaError_t launch_evalbox(bool directed, const uint2 *code, uint32_t len, uint3
                            cudaStream_t st);
 cudaError_t launch_math(int which, uint32_t n, const float *a, const float *b, float *out, cudaStream_t st);
 
-struct TraceParams {
-  float eye[3];
-  float m[16];
-  float zdist;
-  float yshift;
-  uint32_t W, H;
-  float time;
-  float rendermode;
-  uint32_t normal_viz;
-  float darken;
-  VoxelPoolDev pool;
-  float4 *rgba;
-  float *depth;
-  float *normal;
-  unsigned long long *visits;
-};
-cudaError_t launch_trace(const TraceParams &T, cudaStream_t st);
 }  // namespace tsi
 
 using namespace tsi;
@@ -518,6 +502,15 @@ tsi_status enqueue_trace(tsi_scene *s, const tsi_uniforms *u) {
   T.depth = s->d_depth;
   T.normal = s->d_normal;
   T.visits = c->d_visits;
+  T.swept = s->p.swept_volume ? 1u : 0u;
+  if (s->p.fast_normals) {  // normals by finite differences of the full tape
+    if (s->tape->nregs > 96u)
+      return set_err(TSI_ERR_TAPE_TOO_WIDE, "fast normals need a tape of at most 96 interval registers");
+    T.code = s->tape->d_code;
+    T.len = s->tape->len;
+    T.nregs = s->tape->nregs;
+    T.out_reg = s->tape->out_reg;
+  }
   if (T.W == 0 || T.H == 0) return TSI_OK;
   CK(launch_trace(T, c->stream));
   return TSI_OK;

@@ -12,27 +12,14 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "device_types.h"
 #include "fmath.cuh"
+#include "interp.cuh"
+#include "trace_params.h"
 
 namespace tsi {
-
-struct TraceParams {
-  float eye[3];
-  float m[16];        // view matrix after the scene rotation, column major
-  float zdist;        // res.y / tan(radians(fov) / 2)
-  float yshift;       // scene 0 shift of the pixel row (compute.wgsl:4681-4683)
-  uint32_t W, H;
-  float time;
-  float rendermode;
-  uint32_t normal_viz;
-  float darken;       // octree_darken_factor
-  VoxelPoolDev pool;
-  float4 *rgba;
-  float *depth;
-  float *normal;      // 3 floats per pixel
-  unsigned long long *visits;
-};
 
 struct F3 {
   float x, y, z;
@@ -63,6 +50,36 @@ __device__ __forceinline__ void node_box(const VoxelPoolDev &pool, uint32_t v, F
   p1 = f3(a.y, a.w, b.y);
 }
 
+// Dynamic shared memory of trace_kernel: with fast normals, one interval
+// register file per warp for the point evaluations.
+extern __shared__ __align__(16) unsigned char trace_smem[];
+
+// finite_diff_normal (compute.wgsl:4143-4184) for any tape: the tetrahedron
+// of points p + k h (h = 0.01, k in {(1,-1,-1), (-1,-1,1), (-1,1,-1),
+// (1,1,1)}) with f evaluated by the tape on point boxes (round to nearest),
+// normalised as v / |v|.  The reference pastes a per-scene function here;
+// the tape makes it work for every scene.  Called by the whole warp; lanes
+// without a hit evaluate a point too and discard it.
+__device__ __noinline__ F3 tape_normal(const TraceParams &T, uint32_t lane, uint32_t warp, F3 p, float t) {
+  float2 *rf = reinterpret_cast<float2 *>(trace_smem) + (size_t)warp * T.nregs * 32u;
+  const float h = 0.01f;
+  const float kx[4] = {1.0f, -1.0f, -1.0f, 1.0f}, ky[4] = {-1.0f, -1.0f, 1.0f, 1.0f};
+  const float kz[4] = {-1.0f, 1.0f, -1.0f, 1.0f};
+  float f[4];
+  for (int q = 0; q < 4; ++q) {
+    const Iv r = forward_pass<false>(T.code, T.len, T.out_reg, rf, lane, iv(p.x + kx[q] * h), iv(p.y + ky[q] * h),
+                                     iv(p.z + kz[q] * h), iv(t), nullptr, nullptr);
+    f[q] = r.lo;
+  }
+  F3 v = f3(kx[0] * f[0], ky[0] * f[0], kz[0] * f[0]);
+  for (int q = 1; q < 4; ++q) v = v + f3(kx[q] * f[q], ky[q] * f[q], kz[q] * f[q]);
+  const float l = len3(v);
+  return f3(v.x / l, v.y / l, v.z / l);
+}
+
+// FAST: normals by finite differences of the tape (a separate instance, so
+// the plain tracer carries no point-evaluation code).
+template <bool FAST>
 __global__ void __launch_bounds__(256, 4) trace_kernel(TraceParams T) {
   const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t py = blockIdx.y * blockDim.y + threadIdx.y;
@@ -90,6 +107,9 @@ __global__ void __launch_bounds__(256, 4) trace_kernel(TraceParams T) {
   float dist = -1.0f;
   uint32_t visits = 0;
   bool intersected = false;
+  F3 hit_point = ro;       // where the ray met its leaf
+  float hit_since = 0.0f;  // time since the leaf was evaluated
+  float hit_t = T.time;    // time of the finite-difference normal
 
   if (valid && T.rendermode == 0.0f) {
     uint32_t stack[32];
@@ -165,21 +185,13 @@ __global__ void __launch_bounds__(256, 4) trace_kernel(TraceParams T) {
               hit = th;
               break;
             }
+            // the leaf's colour is set after the walk (the fast normal is
+            // evaluated by the whole warp there)
             intersected = true;
             const float4 nv = pool.normal[child];
             nrm = f3(nv.x, nv.y, nv.z);
-            const float timesince = T.time - pool.t[child];
-            if (T.normal_viz) {
-              const float nl = len3(nrm);
-              c = f3(nrm.x / nl * 0.5f + 0.5f, nrm.y / nl * 0.5f + 0.5f, nrm.z / nl * 0.5f + 0.5f);
-            } else {
-              // c - mix(1 - movement, 1 - base, clamp(60 t, 0, 1)), movement (1,0,0), base (1,1,1)
-              const float tt = fm_min(fm_max(timesince * 60.0f, 0.0f), 1.0f);
-              const F3 a = f3(0.0f, 1.0f, 1.0f), b = f3(0.0f, 0.0f, 0.0f);
-              const F3 lerp = f3(a.x * (1.0f - tt) + b.x * tt, a.y * (1.0f - tt) + b.y * tt,
-                                 a.z * (1.0f - tt) + b.z * tt);
-              c = c - lerp;
-            }
+            hit_since = T.time - pool.t[child];
+            if (T.swept) hit_t = pool.t[region];  // compute.wgsl:4339-4341
             break;
           }
         }
@@ -198,9 +210,29 @@ __global__ void __launch_bounds__(256, 4) trace_kernel(TraceParams T) {
         mp2 = mp2 + (int)m2 * st2;
       }
     }
+    hit_point = ro2;
+  }
+  if (FAST) {  // fast normals (compute.wgsl:4337-4342)
+    const uint32_t tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (__any_sync(0xffffffffu, intersected)) {
+      const F3 n = tape_normal(T, tid & 31u, tid >> 5, hit_point, hit_t);
+      if (intersected) nrm = n;
+    }
+  }
+  if (valid && T.rendermode == 0.0f) {
     if (intersected) {
+      if (T.normal_viz) {
+        const float nl = len3(nrm);
+        c = f3(nrm.x / nl * 0.5f + 0.5f, nrm.y / nl * 0.5f + 0.5f, nrm.z / nl * 0.5f + 0.5f);
+      } else {
+        // c - mix(1 - movement, 1 - base, clamp(60 t, 0, 1)), movement (1,0,0), base (1,1,1)
+        const float tt = fm_min(fm_max(hit_since * 60.0f, 0.0f), 1.0f);
+        const F3 a = f3(0.0f, 1.0f, 1.0f), b = f3(0.0f, 0.0f, 0.0f);
+        const F3 lerp = f3(a.x * (1.0f - tt) + b.x * tt, a.y * (1.0f - tt) + b.y * tt, a.z * (1.0f - tt) + b.z * tt);
+        c = c - lerp;
+      }
       c = f3(fm_max(fm_min(c.x, 1.0f), 0.0f), fm_max(fm_min(c.y, 1.0f), 0.0f), fm_max(fm_min(c.z, 1.0f), 0.0f));
-      dist = fabsf(len3(ro2 - ro));
+      dist = fabsf(len3(hit_point - ro));
     } else {
       c = f3(fm_max(fm_min(c.x, 1.0f), 0.0f), fm_max(fm_min(c.y, 1.0f), 0.0f), fm_max(fm_min(c.z, 1.0f), 0.0f));
     }
@@ -228,10 +260,28 @@ __global__ void __launch_bounds__(256, 4) trace_kernel(TraceParams T) {
   }
 }
 
+// Shared memory of one block with fast normals: 8 warps' register files.
+size_t trace_smem_bytes(const TraceParams &T) { return T.code ? (size_t)8 * T.nregs * 32 * sizeof(float2) : 0; }
+
 cudaError_t launch_trace(const TraceParams &T, cudaStream_t st) {
+  const size_t smem = trace_smem_bytes(T);
+  if (smem > (48u << 10)) {  // the attribute is per kernel and device: only ever raise it
+    static std::mutex mu;
+    static size_t set_bytes[64] = {0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= 64 || smem > set_bytes[dev]) {
+      e = cudaFuncSetAttribute(trace_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) set_bytes[dev] = smem;
+    }
+  }
   dim3 block(16, 16);
   dim3 grid((T.W + 15) / 16, (T.H + 15) / 16);
-  trace_kernel<<<grid, block, 0, st>>>(T);
+  if (T.code) trace_kernel<true><<<grid, block, smem, st>>>(T);
+  else trace_kernel<false><<<grid, block, 0, st>>>(T);
   return cudaGetLastError();
 }
 

@@ -34,6 +34,10 @@ def _compare(g, o):
     ("spheres16", "spheres16", dict(localsubdiv=7, pointsample=0), (0.3, 0.6, 2.5)),
     ("csg48", "csg48", dict(localsubdiv=7), (-1.5, 1.0, 2.0)),
     ("sponza", "sponza", dict(localsubdiv=6, normal_viz=1), (0.0, 0.0, 8.0)),
+    # normals by finite differences of the tape (compute.wgsl:4143-4184 for any scene)
+    ("sponza_fast", "sponza", dict(localsubdiv=6, normal_viz=1, fast_normals=1), (0.0, 0.0, 8.0)),
+    ("spheres16_fast", "spheres16", dict(localsubdiv=7, pointsample=0, normal_viz=1, fast_normals=1),
+     (0.3, 0.6, 2.5)),
 ])
 def test_trace_matches_oracle(device, name, src, params, eye):
     if src == "spheres16":
