@@ -249,6 +249,10 @@ TSI_API tsi_status tsi_scene_invert(tsi_scene *scene, float time, float t0_or_na
 TSI_API tsi_status tsi_scene_trace(tsi_scene *scene, const tsi_uniforms *u, tsi_image *out,
                                    tsi_stats *stats);
 TSI_API tsi_status tsi_scene_image_device(tsi_scene *scene, tsi_image_device *out);
+/* Copies the scene's last rendered frame (e.g. from a graph replay or the
+ * server, which keep frames on the device) into host buffers; out's size
+ * must match the frame. */
+TSI_API tsi_status tsi_scene_image_copy(tsi_scene *scene, tsi_image *out);
 /* Octree as cells keyed by (level, ix, iy, iz), depth-first order.
  * With out == NULL only the count is returned. */
 TSI_API tsi_status tsi_scene_readback_cells(tsi_scene *scene, tsi_cell *out, uint64_t cap,
@@ -288,7 +292,10 @@ typedef struct tsi_request {
 TSI_API tsi_status tsi_batch_run(tsi_ctx *ctx, tsi_request *reqs, uint32_t n);
 
 /* Captures tsi_batch_run for a fixed request set into a CUDA graph and
- * replays it; times and cameras are re-read from the requests each replay. */
+ * replays it.  The request array must stay valid while the graph exists:
+ * every launch waits for the previous replay, then re-reads each request's
+ * time, t0 and uniforms (camera, time) from it; scenes and image sizes must
+ * stay as captured.  Images stay on the device (tsi_scene_image_device). */
 typedef struct tsi_batch_graph tsi_batch_graph;
 TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *ctx, tsi_request *reqs, uint32_t n,
                                           tsi_batch_graph **out);

@@ -133,6 +133,7 @@ SIGNATURES = {
     "tsi_server_stats_get": (i32, [C.c_void_p, P(ServerStats)]),
     "tsi_server_destroy": (None, [C.c_void_p]),
     "tsi_batch_graph_create": (i32, [C.c_void_p, P(Request), u32, P(C.c_void_p)]),
+    "tsi_scene_image_copy": (i32, [C.c_void_p, P(Image)]),
     "tsi_batch_graph_launch": (i32, [C.c_void_p]),
     "tsi_batch_graph_destroy": (None, [C.c_void_p]),
     "tsi_last_error": (C.c_char_p, []),

@@ -239,6 +239,15 @@ class Scene:
                                              C.byref(n)), "tsi_scene_readback_cells")
         return arr
 
+    def image(self, width: int, height: int) -> dict:
+        """The last rendered frame (kept on the device by graph replays and
+        the server) copied to host arrays."""
+        out = {"rgba": np.empty((height, width, 4), np.float32), "depth": np.empty((height, width), np.float32),
+               "normal": np.empty((height, width, 3), np.float32)}
+        img = N.Image(width, height, _fptr(out["rgba"]), _fptr(out["depth"]), _fptr(out["normal"]))
+        N.check(self.device.lib.tsi_scene_image_copy(self.handle, C.byref(img)), "tsi_scene_image_copy")
+        return out
+
     def snapshot(self) -> bytes:
         """The resident octree as a host blob (tsi_scene_snapshot)."""
         lib = self.device.lib
@@ -392,3 +401,41 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class BatchGraph:
+    """tsi_batch_run for a fixed set of distinct scenes captured into a CUDA
+    graph; each launch re-reads the requests' times and cameras."""
+
+    def __init__(self, device: Device, requests: list):
+        """requests: list of (scene, time, t0, uniforms or None)."""
+        self.device = device
+        n = len(requests)
+        self.reqs = (N.Request * n)()
+        self._keep = []
+        for i, (scene, time, t0, uni) in enumerate(requests):
+            self.reqs[i].scene = scene.handle
+            self.reqs[i].time = float(time)
+            self.reqs[i].t0_or_nan = float(t0)
+            if uni is not None:
+                u = N.Uniforms()
+                C.memmove(C.byref(u), C.byref(uni), C.sizeof(u))
+                self._keep.append(u)
+                self.reqs[i].uniforms = C.pointer(u)
+            else:
+                self._keep.append(None)
+        h = C.c_void_p()
+        N.check(device.lib.tsi_batch_graph_create(device.handle, self.reqs, n, C.byref(h)), "tsi_batch_graph_create")
+        self.handle = h
+
+    def launch(self, times: list, uniforms: list | None = None) -> None:
+        for i, t in enumerate(times):
+            self.reqs[i].time = float(t)
+            if uniforms is not None and uniforms[i] is not None:
+                C.memmove(C.byref(self._keep[i]), C.byref(uniforms[i]), C.sizeof(N.Uniforms))
+        N.check(self.device.lib.tsi_batch_graph_launch(self.handle), "tsi_batch_graph_launch")
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.device.lib.tsi_batch_graph_destroy(self.handle)
+            self.handle = None

@@ -51,6 +51,7 @@ thread_local std::string g_last_error;
     cudaError_t e_ = (call);                                                         \
     if (e_ != cudaSuccess) {                                                         \
       g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);             \
+      cudaGetLastError(); /* clear it, or the next launch check reports it again */  \
       return TSI_ERR_CUDA;                                                           \
     }                                                                                \
   } while (0)
@@ -100,6 +101,9 @@ struct tsi_scene {
   float4 *d_rgba = nullptr;
   float *d_depth = nullptr;
   float *d_normal = nullptr;
+  // the tracer's arguments: written on the host, uploaded before each trace
+  // (a captured upload reads the pinned copy when the graph replays)
+  TraceParams *h_trace = nullptr, *d_trace = nullptr;
   uint64_t bytes = 0;
 };
 
@@ -158,7 +162,8 @@ struct tsi_ctx {
 
 struct tsi_batch_graph {
   tsi_ctx *ctx = nullptr;
-  std::vector<tsi_request> reqs;
+  const tsi_request *user = nullptr;  // the caller's requests, re-read at every replay
+  std::vector<tsi_request> reqs;      // as captured
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -491,11 +496,13 @@ tsi_status ensure_image(tsi_scene *s, uint32_t w, uint32_t h) {
   return TSI_OK;
 }
 
-tsi_status enqueue_trace(tsi_scene *s, const tsi_uniforms *u) {
+// The tracer's arguments for these uniforms, into the scene's pinned copy.
+tsi_status fill_trace(tsi_scene *s, const tsi_uniforms *u) {
   tsi_ctx *c = s->ctx;
   const tsi_status st = ensure_image(s, u->resolution[0], u->resolution[1]);
   if (st != TSI_OK) return st;
-  TraceParams T{};
+  TraceParams &T = *s->h_trace;
+  T = TraceParams{};
   make_camera(s->p, *u, T);
   T.pool = s->pool;
   T.rgba = s->d_rgba;
@@ -511,8 +518,18 @@ tsi_status enqueue_trace(tsi_scene *s, const tsi_uniforms *u) {
     T.nregs = s->tape->nregs;
     T.out_reg = s->tape->out_reg;
   }
+  (void)c;
+  return TSI_OK;
+}
+
+tsi_status enqueue_trace(tsi_scene *s, const tsi_uniforms *u) {
+  tsi_ctx *c = s->ctx;
+  tsi_status st = fill_trace(s, u);
+  if (st != TSI_OK) return st;
+  const TraceParams &T = *s->h_trace;
   if (T.W == 0 || T.H == 0) return TSI_OK;
-  CK(launch_trace(T, c->stream));
+  CK(cudaMemcpyAsync(s->d_trace, s->h_trace, sizeof(TraceParams), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_trace(T, s->d_trace, c->stream));
   return TSI_OK;
 }
 
@@ -1060,6 +1077,8 @@ TSI_API tsi_status tsi_scene_create(tsi_ctx *c, const tsi_tape *tape, const tsi_
   A(dalloc(&s->pool.free_list, bricks));
   A(dalloc(&s->pool.pending, bricks));
   A(dalloc(&s->d_ctr, 1));
+  A(dalloc(&s->d_trace, 1));
+  A(cudaMallocHost((void **)&s->h_trace, sizeof(TraceParams)));
   s->pool.cap_bricks = s->cap_bricks;
   s->bytes = nv * (16 + 8 + 4 * 5 + 16) + bricks * 8 + sizeof(SceneCounters);
   if (e != cudaSuccess) {
@@ -1093,6 +1112,8 @@ TSI_API void tsi_scene_destroy(tsi_scene *s) {
   cudaFree(s->pool.normal);
   cudaFree(s->pool.free_list);
   cudaFree(s->pool.pending);
+  cudaFreeHost(s->h_trace);
+  cudaFree(s->d_trace);
   cudaFree(s->d_ctr);
   cudaFree(s->d_rgba);
   cudaFree(s->d_depth);
@@ -1149,6 +1170,16 @@ TSI_API tsi_status tsi_scene_trace(tsi_scene *s, const tsi_uniforms *u, tsi_imag
     stats->device_ms = ms;
     stats->reserved = (float)c->h_rb->visits;
   }
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_scene_image_copy(tsi_scene *s, tsi_image *out) {
+  if (!s || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  CK(cudaSetDevice(s->ctx->device));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  const tsi_status st = copy_image_out(s, out);
+  if (st != TSI_OK) return st;
+  CK(cudaStreamSynchronize(s->ctx->stream));
   return TSI_OK;
 }
 
@@ -1405,6 +1436,7 @@ TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *c, tsi_request *reqs, uint32_
   CK(cudaSetDevice(c->device));
   tsi_batch_graph *g = new tsi_batch_graph();
   g->ctx = c;
+  g->user = reqs;
   g->reqs.assign(reqs, reqs + n);
   CK(cudaStreamSynchronize(c->stream));
   // grow the shared-memory attribute, the wide path's arenas and the frame
@@ -1433,6 +1465,7 @@ TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *c, tsi_request *reqs, uint32_
   cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
   if (st != TSI_OK || e != cudaSuccess) {
     if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();  // a failed capture leaves an error behind
     delete g;
     if (st != TSI_OK) return st;
     return set_err(TSI_ERR_CUDA, cudaGetErrorString(e));
@@ -1452,11 +1485,21 @@ TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g) {
   if (!g) return set_err(TSI_ERR_INVALID_ARGUMENT, "null graph");
   tsi_ctx *c = g->ctx;
   CK(cudaSetDevice(c->device));
-  // the captured uploads read the pinned launch descriptors: refresh times
+  // the previous replay has read the pinned descriptors before they change
+  CK(cudaStreamSynchronize(c->stream));
+  // the captured uploads read the pinned descriptors: refresh them from the
+  // caller's requests (same scenes, same image sizes as captured)
   const uint32_t n = (uint32_t)g->reqs.size();
   for (uint32_t i = 0; i < n; ++i) {
-    const tsi_request &r = g->reqs[i];
+    const tsi_request &r = g->user[i], &cap = g->reqs[i];
+    if (r.scene != cap.scene || (r.uniforms == nullptr) != (cap.uniforms == nullptr) ||
+        (r.uniforms && (r.uniforms->resolution[0] != r.scene->img_w || r.uniforms->resolution[1] != r.scene->img_h)))
+      return set_err(TSI_ERR_INVALID_ARGUMENT, "requests differ from the captured ones (scene or image size)");
     fill_launch(r.scene, i, r.time, r.t0_or_nan, c->h_scenes[i], c->h_recs[i]);
+    if (r.uniforms) {
+      const tsi_status st = fill_trace(r.scene, r.uniforms);
+      if (st != TSI_OK) return st;
+    }
   }
   CK(cudaGraphLaunch(g->exec, c->stream));
   return TSI_OK;

@@ -80,7 +80,8 @@ __device__ __noinline__ F3 tape_normal(const TraceParams &T, uint32_t lane, uint
 // FAST: normals by finite differences of the tape (a separate instance, so
 // the plain tracer carries no point-evaluation code).
 template <bool FAST>
-__global__ void __launch_bounds__(256, 4) trace_kernel(TraceParams T) {
+__global__ void __launch_bounds__(256, 4) trace_kernel(const TraceParams *__restrict__ Tp) {
+  const TraceParams &T = *Tp;
   const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t py = blockIdx.y * blockDim.y + threadIdx.y;
   const bool valid = px < T.W && py < T.H;
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__(256, 4) trace_kernel(TraceParams T) {
 // Shared memory of one block with fast normals: 8 warps' register files.
 size_t trace_smem_bytes(const TraceParams &T) { return T.code ? (size_t)8 * T.nregs * 32 * sizeof(float2) : 0; }
 
-cudaError_t launch_trace(const TraceParams &T, cudaStream_t st) {
+cudaError_t launch_trace(const TraceParams &T, const TraceParams *Tdev, cudaStream_t st) {
   const size_t smem = trace_smem_bytes(T);
   if (smem > (48u << 10)) {  // the attribute is per kernel and device: only ever raise it
     static std::mutex mu;
@@ -280,8 +281,8 @@ cudaError_t launch_trace(const TraceParams &T, cudaStream_t st) {
   }
   dim3 block(16, 16);
   dim3 grid((T.W + 15) / 16, (T.H + 15) / 16);
-  if (T.code) trace_kernel<true><<<grid, block, smem, st>>>(T);
-  else trace_kernel<false><<<grid, block, 0, st>>>(T);
+  if (T.code) trace_kernel<true><<<grid, block, smem, st>>>(Tdev);
+  else trace_kernel<false><<<grid, block, 0, st>>>(Tdev);
   return cudaGetLastError();
 }
 

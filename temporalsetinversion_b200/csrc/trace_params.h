@@ -29,6 +29,7 @@ struct TraceParams {
   unsigned long long *visits;
 };
 
-cudaError_t launch_trace(const TraceParams &T, cudaStream_t st);
+// T: the host copy (grid size, variant); Tdev: the same in device memory, read by the kernel.
+cudaError_t launch_trace(const TraceParams &T, const TraceParams *Tdev, cudaStream_t st);
 
 }  // namespace tsi

@@ -42,3 +42,30 @@ def test_batch_equals_alone(device):
             assert_cells_equal(mixed[i].cells(), s.cells())
             assert np.array_equal(res[i]["depth"], img["depth"])
             assert np.array_equal(res[i]["rgba"], img["rgba"])
+
+
+@pytest.mark.gpu
+def test_graph_replays_equal_plain_frames(device):
+    """A captured batch replayed over several frames (new times and cameras
+    each launch) gives the plain path's octrees and images."""
+    alone = _make(device, SPECS[:3])
+    graphed = _make(device, SPECS[:3])
+    res = (96, 64)
+    eyes = [(0.4, 0.8, 2.4), (0.5, 0.7, 2.3), (0.6, 0.6, 2.2)]
+    times = [[0.0, 0.2, 0.9], [0.05, 0.25, 0.8], [0.1, 0.3, 0.7]]
+    reqs = [(s, times[0][i], math.nan, api.make_uniforms(scenes.camera_look_at(eyes[0]), res, times[0][i]))
+            for i, s in enumerate(graphed)]
+    g = api.BatchGraph(device, reqs)
+    try:
+        for f in range(3):
+            unis = [api.make_uniforms(scenes.camera_look_at(eyes[f]), res, times[f][i]) for i in range(3)]
+            g.launch(times[f], unis)
+            for i, s in enumerate(alone):
+                s.invert(times[f][i])
+                want = s.trace(unis[i])
+                got = graphed[i].image(*res)
+                assert_cells_equal(graphed[i].cells(), s.cells())
+                assert np.array_equal(got["depth"], want["depth"])
+                assert np.array_equal(got["rgba"], want["rgba"])
+    finally:
+        g.close()
