@@ -24,6 +24,10 @@ temporally reused frames, like one run of the animation.
           FP32 rate, plus the tracer's node traffic against measured HBM
   cpu_baseline: the CPU oracle (C++ restatement of compute.wgsl, OpenMP)
           on a bounded sample of the same animation
+  served : open-loop Poisson requests through the serving layer, p50/p99
+          latency beside the plain path's per-frame latency
+  batched: 32 scenes (8..2048 primitives, localsubdiv 7..10, 1024x1024)
+          per step, as 32 sequential plain calls and as one CUDA-graph replay
 
 --impl reference times the CPU restatement (the reference itself is WGSL
 under wgpu/Vulkan: no Vulkan driver or Rust toolchain exists on these
@@ -300,6 +304,107 @@ def served_leg(local: int) -> dict:
         dev.close()
 
 
+# ------------------------------------------------------------------ batched leg
+BATCHED = dict(scenes=32, prims=(8, 2048), levels=(7, 10), res=1024, seed=3000, warmup=3, steps=6)
+
+
+def batched_specs() -> list:
+    """32 scenes of the workload's kind: primitive counts log-uniform in
+    [8, 2048], localsubdiv uniform in {7..10}, a random start time in [0, 1]
+    and a random camera on the radius-2.5 sphere looking at the origin."""
+    from temporalsetinversion_b200 import scenes
+    rng = np.random.default_rng(BATCHED["seed"])
+    lo, hi = BATCHED["prims"]
+    out = []
+    for i in range(BATCHED["scenes"]):
+        n = int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
+        L = int(rng.integers(BATCHED["levels"][0], BATCHED["levels"][1] + 1))
+        t = float(rng.uniform(0.0, 1.0))
+        out.append((scenes.csg(n, BATCHED["seed"] + i), L, t, scenes.camera_on_sphere(rng, 2.5)))
+    return out
+
+
+def batched_leg(local: int) -> dict:
+    """The 32 scenes rendered frame after frame (each scene advances by
+    1/60 per step, images kept on the device) two ways on the same scenes:
+    32 sequential plain calls (tsi_scene_invert + tsi_scene_trace each) per
+    step, and one replay of a CUDA graph of tsi_batch_run per step."""
+    import ctypes as C
+
+    from temporalsetinversion_b200 import Device, Scene, Tape, _native as N, api
+
+    R = BATCHED["res"]
+    dev = Device(local, tape_arena_words=512 << 20)
+    try:
+        specs = batched_specs()
+        sc, unis0, slots = [], [], []
+        for text, L, t, view in specs:
+            p = api.default_params(localsubdiv=L, delta=WORKLOAD["delta"],
+                                   lipschitz_corrected=WORKLOAD["lipschitz_corrected"],
+                                   pointsample=WORKLOAD["pointsample"], fast_normals=WORKLOAD["fast_normals"])
+            tape = Tape.from_llvm_ir(dev, text)
+            slots.append(tape.instruction_count)
+            sc.append(Scene(dev, tape, p, voxel_capacity=(16 << 20) if L >= 10 else (4 << 20)))
+
+        def times(k):
+            return [(t + k / 60.0) % 1.0 for _, _, t, _ in specs]
+
+        # per-tape wide threshold, timed on each scene's first frames
+        t_tune = time.perf_counter()
+        tuned = []
+        for s, (_, _, t, _) in zip(sc, specs):
+            tuned.append(s.autotune([t, (t + 1 / 60.0) % 1.0], reps=1)["wide_threshold"])
+        t_tune = time.perf_counter() - t_tune
+
+        def uniforms(k):
+            return [api.make_uniforms(v, (R, R), tk) for (_, _, _, v), tk in zip(specs, times(k))]
+
+        W, K = BATCHED["warmup"], BATCHED["steps"]
+        # plain: 32 synchronous call pairs per step
+        plain_ms = []
+        for k in range(W + K):
+            ts, us = times(k), uniforms(k)
+            t0 = time.perf_counter()
+            for s, t, u in zip(sc, ts, us):
+                st = N.Stats()
+                N.check(dev.lib.tsi_scene_invert(s.handle, t, math.nan, C.byref(st)), "tsi_scene_invert")
+                N.check(dev.lib.tsi_scene_trace(s.handle, C.byref(u), None, None), "tsi_scene_trace")
+            if k >= W:
+                plain_ms.append((time.perf_counter() - t0) * 1000.0)
+        for s in sc:
+            s.reset()
+        # graph: one replay per step
+        g = api.BatchGraph(dev, [(s, t, math.nan, u) for s, t, u in zip(sc, times(0), uniforms(0))])
+        graph_ms, graph_dev_ms = [], []
+        try:
+            for k in range(W + K):
+                t0 = time.perf_counter()
+                g.launch(times(k), uniforms(k))
+                st = g.wait()
+                if k >= W:
+                    graph_ms.append((time.perf_counter() - t0) * 1000.0)
+                    graph_dev_ms.append(st.device_ms)
+        finally:
+            g.close()
+        n = BATCHED["scenes"]
+        plain_fps = n * K / (sum(plain_ms) / 1000.0)
+        graph_fps = n * K / (sum(graph_ms) / 1000.0)
+        return {"scenes": n, "resolution": "%dx%d" % (R, R), "steps": K, "warmup": W,
+                "tape_slots_min": int(min(slots)), "tape_slots_max": int(max(slots)),
+                "tape_slots_total": int(sum(slots)),
+                "levels": {str(L): sum(1 for _, l, _, _ in specs if l == L) for L in range(7, 11)},
+                "plain_frames_per_s": plain_fps, "graph_frames_per_s": graph_fps,
+                "graph_vs_plain": graph_fps / plain_fps,
+                "plain_ms_per_step": sum(plain_ms) / K, "graph_ms_per_step": sum(graph_ms) / K,
+                "graph_device_ms_per_step": sum(graph_dev_ms) / K,
+                "autotune_s": t_tune, "wide_thresholds": tuned,
+                "note": "wall clock per step (all 32 scenes advance by 1/60); plain = 32 x (tsi_scene_invert + "
+                        "tsi_scene_trace), graph = one tsi_batch_graph_launch + tsi_batch_graph_wait; frames on "
+                        "the device; warm-up steps include every scene's first_eval frame"}
+    finally:
+        dev.close()
+
+
 # ------------------------------------------------------------------ GPU leg
 def run_gpu(args, rank, world, local, dist) -> None:
     import ctypes as C
@@ -435,6 +540,11 @@ def run_gpu(args, rank, world, local, dist) -> None:
             line["served"] = served_leg(local)
         except Exception as e:
             line["served"] = {"unavailable": str(e)}
+    if world == 1 and not args.no_batched:
+        try:
+            line["batched"] = batched_leg(local)
+        except Exception as e:
+            line["batched"] = {"unavailable": str(e)}
     print(json.dumps(line), flush=True)
 
 
@@ -447,6 +557,7 @@ def main() -> None:
     ap.add_argument("--voxels", type=int, default=64 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the served-latency leg")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 32-scene batched leg")
     ap.add_argument("--small-arenas", action="store_true",
                     help="small work-item, tape and log arenas (use with --voxels 4194304 under a profiler)")
     args = ap.parse_args()

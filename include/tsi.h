@@ -249,6 +249,30 @@ TSI_API tsi_status tsi_scene_invert(tsi_scene *scene, float time, float t0_or_na
 TSI_API tsi_status tsi_scene_trace(tsi_scene *scene, const tsi_uniforms *u, tsi_image *out,
                                    tsi_stats *stats);
 TSI_API tsi_status tsi_scene_image_device(tsi_scene *scene, tsi_image_device *out);
+
+/* No counterpart in the reference (its workgroup shape is fixed at
+ * compute.wgsl:3513).  Child cells whose pruned tape is at least the tape's
+ * wide threshold are evaluated one cell per 256-thread block from the
+ * tape's bundled SSA form; shorter ones one warp per 8-cell group.  Results
+ * are identical for every threshold; only the speed changes.  Tapes whose
+ * SSA form does not fit in shared memory report UINT32_MAX (narrow only)
+ * and ignore a new value. */
+TSI_API uint32_t tsi_tape_wide_threshold(const tsi_tape *tape);
+TSI_API tsi_status tsi_tape_set_wide_threshold(tsi_tape *tape, uint32_t min_len);
+
+#define TSI_AUTOTUNE_MAX 16
+typedef struct tsi_autotune_result {
+  uint32_t wide_threshold;          /* chosen, now set on the scene's tape */
+  uint32_t candidates;              /* thresholds tried (0: narrow-only tape) */
+  uint32_t threshold[TSI_AUTOTUNE_MAX];
+  float ms[TSI_AUTOTUNE_MAX];       /* best of `reps` runs over `times`, device ms */
+} tsi_autotune_result;
+/* Times the scene's inversion over the frames `times` (the first from a
+ * reset octree, the rest carried over) for each candidate wide threshold,
+ * best of `reps`, and keeps the fastest on the scene's tape (shared by every
+ * scene of that tape).  The scene is left reset. */
+TSI_API tsi_status tsi_scene_autotune(tsi_scene *scene, const float *times, uint32_t ntimes, uint32_t reps,
+                                      tsi_autotune_result *out);
 /* Copies the scene's last rendered frame (e.g. from a graph replay or the
  * server, which keep frames on the device) into host buffers; out's size
  * must match the frame. */
@@ -300,6 +324,12 @@ typedef struct tsi_batch_graph tsi_batch_graph;
 TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *ctx, tsi_request *reqs, uint32_t n,
                                           tsi_batch_graph **out);
 TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g);
+/* Waits for the last replay and reports it: the status from its device
+ * error word (voxel pool, work list, log arena, watchdog) and, when stats is
+ * not NULL, its counters summed over the batch with device_ms = the replay's
+ * device time.  Plain calls on the same context between the launch and the
+ * wait overwrite what it reads. */
+TSI_API tsi_status tsi_batch_graph_wait(tsi_batch_graph *g, tsi_stats *stats);
 TSI_API void tsi_batch_graph_destroy(tsi_batch_graph *g);
 
 /* ---------------- serving ---------------- */

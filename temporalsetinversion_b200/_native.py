@@ -67,6 +67,14 @@ class Cell(C.Structure):
                 ("y", f32 * 2), ("z", f32 * 2)]
 
 
+AUTOTUNE_MAX = 16
+
+
+class AutotuneResult(C.Structure):
+    _fields_ = [("wide_threshold", u32), ("candidates", u32), ("threshold", u32 * AUTOTUNE_MAX),
+                ("ms", f32 * AUTOTUNE_MAX)]
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("max_batch", u32), ("reserved", u32)]
 
@@ -135,6 +143,10 @@ SIGNATURES = {
     "tsi_batch_graph_create": (i32, [C.c_void_p, P(Request), u32, P(C.c_void_p)]),
     "tsi_scene_image_copy": (i32, [C.c_void_p, P(Image)]),
     "tsi_batch_graph_launch": (i32, [C.c_void_p]),
+    "tsi_batch_graph_wait": (i32, [C.c_void_p, P(Stats)]),
+    "tsi_tape_wide_threshold": (u32, [C.c_void_p]),
+    "tsi_tape_set_wide_threshold": (i32, [C.c_void_p, u32]),
+    "tsi_scene_autotune": (i32, [C.c_void_p, P(f32), u32, u32, P(AutotuneResult)]),
     "tsi_batch_graph_destroy": (None, [C.c_void_p]),
     "tsi_last_error": (C.c_char_p, []),
     "tsi_ir_tape_info": (i32, [C.c_char_p, C.c_size_t, P(TapeInfo), P(u32), u32]),

@@ -179,6 +179,16 @@ class Tape:
                                                     rounding_mode, int(reverse), _fptr(out)), "tsi_tape_eval_boxes")
         return out
 
+    @property
+    def wide_threshold(self) -> int:
+        """Pruned-tape length from which child cells take the wide path
+        (0xffffffff: narrow only)."""
+        return int(self.device.lib.tsi_tape_wide_threshold(self.handle))
+
+    @wide_threshold.setter
+    def wide_threshold(self, v: int) -> None:
+        N.check(self.device.lib.tsi_tape_set_wide_threshold(self.handle, int(v)), "tsi_tape_set_wide_threshold")
+
     def close(self) -> None:
         if getattr(self, "handle", None) and getattr(self.device, "handle", None):
             self.device.lib.tsi_tape_destroy(self.handle)
@@ -204,6 +214,16 @@ class Scene:
 
     def reset(self) -> None:
         N.check(self.device.lib.tsi_scene_reset(self.handle), "tsi_scene_reset")
+
+    def autotune(self, times: list, reps: int = 2) -> dict:
+        """Picks the tape's wide threshold by timing inversions over
+        `times` (tsi_scene_autotune); the scene is left reset."""
+        arr = (C.c_float * len(times))(*[float(t) for t in times])
+        r = N.AutotuneResult()
+        N.check(self.device.lib.tsi_scene_autotune(self.handle, arr, len(times), int(reps), C.byref(r)),
+                "tsi_scene_autotune")
+        return {"wide_threshold": int(r.wide_threshold),
+                "trials": [(int(r.threshold[k]), float(r.ms[k])) for k in range(r.candidates)]}
 
     def invert(self, time: float, t0: float = math.nan) -> N.Stats:
         st = N.Stats()
@@ -434,6 +454,13 @@ class BatchGraph:
             if uniforms is not None and uniforms[i] is not None:
                 C.memmove(C.byref(self._keep[i]), C.byref(uniforms[i]), C.sizeof(N.Uniforms))
         N.check(self.device.lib.tsi_batch_graph_launch(self.handle), "tsi_batch_graph_launch")
+
+    def wait(self) -> N.Stats:
+        """Waits for the last launch; raises on its device error word and
+        returns its counters (summed over the batch) and device time."""
+        st = N.Stats()
+        N.check(self.device.lib.tsi_batch_graph_wait(self.handle, C.byref(st)), "tsi_batch_graph_wait")
+        return st
 
     def close(self) -> None:
         if getattr(self, "handle", None):

@@ -166,6 +166,7 @@ struct tsi_batch_graph {
   std::vector<tsi_request> reqs;      // as captured
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  bool launched = false;
 };
 
 namespace {
@@ -1183,6 +1184,70 @@ TSI_API tsi_status tsi_scene_image_copy(tsi_scene *s, tsi_image *out) {
   return TSI_OK;
 }
 
+TSI_API uint32_t tsi_tape_wide_threshold(const tsi_tape *t) { return t ? t->wmin_len : 0xffffffffu; }
+
+TSI_API tsi_status tsi_tape_set_wide_threshold(tsi_tape *t, uint32_t min_len) {
+  if (!t) return set_err(TSI_ERR_INVALID_ARGUMENT, "null tape");
+  if (t->d_wslots) t->wmin_len = min_len;
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_scene_autotune(tsi_scene *s, const float *times, uint32_t ntimes, uint32_t reps,
+                                      tsi_autotune_result *out) {
+  if (!s || !times || ntimes == 0 || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  memset(out, 0, sizeof(*out));
+  // the tape belongs to the caller's context; its threshold is the tunable
+  tsi_tape *t = const_cast<tsi_tape *>(s->tape);
+  if (!t->d_wslots) {
+    out->wide_threshold = t->wmin_len;
+    return tsi_scene_reset(s);
+  }
+  const uint32_t nb = t->wbundles, keep = t->wmin_len;
+  std::vector<uint32_t> cand = {std::max(128u, nb), std::max(128u, 2 * nb), 3 * nb, 4 * nb, 6 * nb,
+                                256u, 512u, 1024u, 2048u, keep};
+  cand.erase(std::remove_if(cand.begin(), cand.end(), [&](uint32_t v) { return v > t->len; }), cand.end());
+  cand.push_back(0xffffffffu);  // narrow only
+  std::sort(cand.begin(), cand.end());
+  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+  if (cand.size() > TSI_AUTOTUNE_MAX) cand.erase(cand.begin(), cand.end() - TSI_AUTOTUNE_MAX);
+  if (reps == 0) reps = 1;
+  float best = INFINITY;
+  uint32_t pick = keep;
+  for (size_t k = 0; k < cand.size(); ++k) {
+    t->wmin_len = cand[k];
+    float bk = INFINITY;
+    for (uint32_t r = 0; r < reps; ++r) {
+      tsi_status st = tsi_scene_reset(s);
+      float ms = 0.0f;
+      for (uint32_t i = 0; i < ntimes && st == TSI_OK; ++i) {
+        tsi_stats fs;
+        st = tsi_scene_invert(s, times[i], NAN, &fs);
+        ms += fs.device_ms;
+      }
+      if (st == TSI_ERR_QUEUE_FULL || st == TSI_ERR_OOM) {  // this threshold does not fit the arenas
+        bk = INFINITY;
+        break;
+      }
+      if (st != TSI_OK) {
+        t->wmin_len = keep;
+        tsi_scene_reset(s);
+        return st;
+      }
+      bk = std::min(bk, ms);
+    }
+    out->threshold[k] = cand[k];
+    out->ms[k] = bk;
+    if (bk < best) {
+      best = bk;
+      pick = cand[k];
+    }
+  }
+  out->candidates = (uint32_t)cand.size();
+  out->wide_threshold = pick;
+  t->wmin_len = pick;
+  return tsi_scene_reset(s);
+}
+
 TSI_API tsi_status tsi_scene_image_device(tsi_scene *s, tsi_image_device *out) {
   if (!s || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
   out->width = s->img_w;
@@ -1460,7 +1525,15 @@ TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *c, tsi_request *reqs, uint32_
       }
     }
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  tsi_status st = batch_enqueue(c, g->reqs.data(), n);
+  // the replay records its own timing events and reads back its error word
+  // and counters (tsi_batch_graph_wait reports them)
+  tsi_status st = TSI_OK;
+  if (cudaEventRecordWithFlags(c->ev0, c->stream, cudaEventRecordExternal) != cudaSuccess)
+    st = set_err(TSI_ERR_CUDA, "event record in capture");
+  if (st == TSI_OK) st = batch_enqueue(c, g->reqs.data(), n);
+  if (st == TSI_OK && cudaEventRecordWithFlags(c->ev1, c->stream, cudaEventRecordExternal) != cudaSuccess)
+    st = set_err(TSI_ERR_CUDA, "event record in capture");
+  if (st == TSI_OK) st = enqueue_readback(c);
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
   if (st != TSI_OK || e != cudaSuccess) {
@@ -1502,7 +1575,23 @@ TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g) {
     }
   }
   CK(cudaGraphLaunch(g->exec, c->stream));
+  g->launched = true;
   return TSI_OK;
+}
+
+TSI_API tsi_status tsi_batch_graph_wait(tsi_batch_graph *g, tsi_stats *stats) {
+  if (!g) return set_err(TSI_ERR_INVALID_ARGUMENT, "null graph");
+  tsi_ctx *c = g->ctx;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  if (!g->launched) return set_err(TSI_ERR_INVALID_ARGUMENT, "graph not launched");
+  if (stats) {
+    fill_stats(*c->h_rb, stats, 0);
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    stats->device_ms = ms;
+  }
+  return status_from_error_bits(c->h_rb->error);
 }
 
 TSI_API void tsi_batch_graph_destroy(tsi_batch_graph *g) {

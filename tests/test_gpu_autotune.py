@@ -1,0 +1,61 @@
+"""The wide-path threshold is a speed knob only: every threshold gives the
+same octrees and images, and the autotuner keeps one of the thresholds it
+timed."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import assert_cells_equal
+from temporalsetinversion_b200 import Scene, Tape, api, scenes
+
+NARROW_ONLY = 0xFFFFFFFF
+
+
+def _frames(device, text, L, threshold, times, res=(96, 64)):
+    tape = Tape.from_llvm_ir(device, text)
+    if threshold is not None:
+        tape.wide_threshold = threshold
+    s = Scene(device, tape, api.default_params(localsubdiv=L))
+    cam = scenes.camera_look_at((0.5, 0.9, 2.3))
+    out = []
+    for t in times:
+        st = s.invert(t)
+        assert st.error_flags == 0
+        img = s.trace(api.make_uniforms(cam, res, t))
+        out.append((s.cells(), img["depth"], img["rgba"]))
+    return tape, out
+
+
+@pytest.mark.gpu
+def test_thresholds_give_identical_frames(device):
+    text = scenes.csg(40, 11, 0.8)
+    times = [0.0, 1 / 60, 2 / 60, 0.5]
+    tape, want = _frames(device, text, 7, NARROW_ONLY, times)
+    assert tape.wide_threshold == NARROW_ONLY
+    for thr in (16, 128, None):
+        _, got = _frames(device, text, 7, thr, times)
+        for (wc, wd, wr), (gc, gd, gr) in zip(want, got):
+            assert_cells_equal(gc, wc)
+            assert np.array_equal(gd, wd)
+            assert np.array_equal(gr, wr)
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_a_timed_threshold(device):
+    text = scenes.csg(64, 12, 0.7)
+    tape = Tape.from_llvm_ir(device, text)
+    s = Scene(device, tape, api.default_params(localsubdiv=7))
+    times = [0.1, 0.1 + 1 / 60, 0.1 + 2 / 60]
+    r = s.autotune(times, reps=1)
+    tried = [thr for thr, _ in r["trials"]]
+    assert r["wide_threshold"] in tried and NARROW_ONLY in tried
+    assert tape.wide_threshold == r["wide_threshold"]
+    ms = dict(r["trials"])
+    assert ms[r["wide_threshold"]] == min(ms.values())
+    # left reset: the next frames match a fresh scene's
+    fresh = Scene(device, Tape.from_llvm_ir(device, text), api.default_params(localsubdiv=7))
+    for t in times:
+        s.invert(t)
+        fresh.invert(t)
+        assert_cells_equal(s.cells(), fresh.cells())

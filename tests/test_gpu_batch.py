@@ -60,6 +60,8 @@ def test_graph_replays_equal_plain_frames(device):
         for f in range(3):
             unis = [api.make_uniforms(scenes.camera_look_at(eyes[f]), res, times[f][i]) for i in range(3)]
             g.launch(times[f], unis)
+            st = g.wait()
+            assert st.error_flags == 0 and st.device_ms > 0.0 and st.cells_evaluated > 0
             for i, s in enumerate(alone):
                 s.invert(times[f][i])
                 want = s.trace(unis[i])
