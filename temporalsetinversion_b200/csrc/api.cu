@@ -87,6 +87,7 @@ struct tsi_tape {
   uint2 *d_wbundles = nullptr;
   uint32_t *d_wmm = nullptr;
   uint32_t wslots = 0, wbundles = 0, wvalues = 0, wmin_len = 0xffffffffu, wcontrib = 0;
+  uint32_t wglobal = 0;  // the cell working set exceeds shared memory: global scratch
   uint32_t warg_gbase[4] = {TSI_NONE, TSI_NONE, TSI_NONE, TSI_NONE}, warg_gcount[4] = {0, 0, 0, 0};
 };
 
@@ -130,6 +131,8 @@ struct tsi_ctx {
   uint32_t *d_cell_bits[2] = {nullptr, nullptr};
   size_t cell_arena_bytes = 0;  // of each parity's info + bits
   uint32_t witem_cap = 0, bm_words = 0;
+  unsigned char *d_wscratch = nullptr;
+  size_t wscratch_bytes = 0, wscratch_stride = 0;
 
   uint2 *d_dealloc[2] = {nullptr, nullptr};
   uint32_t dealloc_cap = 0;
@@ -197,6 +200,8 @@ LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes) {
   P.witem_cursor = c->d_witem_cursor;
   P.witem_cap = c->witem_cap;
   P.bm_words = c->bm_words;
+  P.wscratch = c->d_wscratch;
+  P.wscratch_stride = c->wscratch_stride;
   for (int q = 0; q < 2; ++q) {
     P.cell_info[q] = c->d_cell_info[q];
     P.cell_bits[q] = c->d_cell_bits[q];
@@ -256,6 +261,7 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, Scene
   L.wide.nvalues = s->tape->wvalues;
   L.wide.min_len = s->tape->wmin_len;
   L.wide.ncontrib = s->tape->wcontrib;
+  L.wide.global = s->tape->wglobal;
   for (int q = 0; q < 4; ++q) {
     L.wide.arg_gbase[q] = s->tape->warg_gbase[q];
     L.wide.arg_gcount[q] = s->tape->warg_gcount[q];
@@ -286,6 +292,8 @@ size_t wide_cell_bytes(size_t nvalues, size_t ncontrib, size_t bm_words) {
 // block also needs its static shared memory and room for a second block's
 // decision bits is kept).
 constexpr size_t kWideCellMaxBytes = 192u << 10;
+// Beyond this a tape has no wide form (global scratch per block of the grid).
+constexpr size_t kWideCellMaxGlobalBytes = 8u << 20;
 
 // Launch geometry of one frame for n scenes.
 struct FramePlan {
@@ -308,9 +316,14 @@ tsi_status plan_frame(tsi_ctx *c, tsi_scene *const *scenes, uint32_t n, FramePla
     if (t->d_wslots) mm_max = std::max(mm_max, t->n_minmax);
   }
   bm_words = std::max(1u, (mm_max + 15u) / 16u);
-  for (uint32_t i = 0; i < n; ++i)
-    if (scenes[i]->tape->d_wslots)
-      cell_bytes = std::max(cell_bytes, wide_cell_bytes(scenes[i]->tape->wvalues, scenes[i]->tape->wcontrib, bm_words));
+  size_t gm_bytes = 0;  // largest working set kept in the global scratch
+  for (uint32_t i = 0; i < n; ++i) {
+    const tsi_tape *t = scenes[i]->tape;
+    if (!t->d_wslots) continue;
+    const size_t b = wide_cell_bytes(t->wvalues, t->wcontrib, bm_words);
+    if (t->wglobal) gm_bytes = std::max(gm_bytes, b);
+    else cell_bytes = std::max(cell_bytes, b);
+  }
   fp.rcap = (rmax + 3u) & ~3u;
   const size_t regfile = (size_t)kWarpsPerBlock * fp.rcap * 32u * sizeof(float2);
   // the wide cell's working set and the narrow register files share the
@@ -321,6 +334,19 @@ tsi_status plan_frame(tsi_ctx *c, tsi_scene *const *scenes, uint32_t n, FramePla
   CK(refine_occupancy(kBlock, fp.smem, &bps));
   if (bps < 1) return set_err(TSI_ERR_TAPE_TOO_WIDE, "register file does not fit in shared memory");
   fp.grid = std::min<int>(bps * c->sm_count, (int)(c->max_warps / kWarpsPerBlock));
+  // one working-set slice per block of the persistent grid
+  if (gm_bytes) {
+    const size_t stride = (gm_bytes + 255) & ~size_t(255);
+    const size_t need = stride * (size_t)fp.grid;
+    if (need > c->wscratch_bytes) {
+      cudaFree(c->d_wscratch);
+      c->d_wscratch = nullptr;
+      c->wscratch_bytes = 0;
+      CK(dalloc(&c->d_wscratch, need));
+      c->wscratch_bytes = need;
+    }
+    c->wscratch_stride = stride;
+  }
   // hand-over arenas: 64 MB per level parity, as many wide items as fit
   const size_t per_item = 8 * (sizeof(CellInfo) + (size_t)bm_words * 4);
   const size_t arena = std::max<size_t>(64u << 20, c->cell_arena_bytes);
@@ -817,6 +843,7 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   cudaFree(c->d_witem_count);
   cudaFree(c->d_witem_cursor);
   for (int q = 0; q < 2; ++q) cudaFree(c->d_cell_info[q]);
+  cudaFree(c->d_wscratch);
   cudaFree(c->d_dealloc[0]);
   cudaFree(c->d_dealloc[1]);
   cudaFree(c->d_dealloc_count);
@@ -871,11 +898,13 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
     }
   }
   // bundled form for long tapes (the wide path pays off once a tape has
-  // several times more instructions than bundles)
+  // several times more instructions than bundles); a working set beyond
+  // shared memory lives in the per-block global scratch
   if (t->len >= 256) {
     WideTape wt;
+    size_t wbytes = 0;
     if (compile_wide(ins, pt, wt, st, why) && wt.nbundles > 0 &&
-        wide_cell_bytes(wt.nvalues, wt.ncontrib, (pt.n_minmax + 15) / 16) + 4096 <= kWideCellMaxBytes) {
+        (wbytes = wide_cell_bytes(wt.nvalues, wt.ncontrib, (pt.n_minmax + 15) / 16)) <= kWideCellMaxGlobalBytes) {
       // device layout: the three uint4 of every slot in three arrays
       const size_t nsl = wt.slots.size() / 12;
       std::vector<uint32_t> soa(wt.slots.size());
@@ -900,6 +929,7 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
       t->wbundles = wt.nbundles;
       t->wvalues = wt.nvalues;
       t->wmin_len = std::max<uint32_t>(256u, 3u * wt.nbundles);
+      t->wglobal = wbytes + 4096 > kWideCellMaxBytes ? 1u : 0u;
       t->wcontrib = wt.ncontrib;
       for (int q = 0; q < 4; ++q) {
         t->warg_gbase[q] = wt.arg_gbase[q];

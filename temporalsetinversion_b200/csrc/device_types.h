@@ -69,6 +69,8 @@ struct WideDev {
   uint32_t nvalues;           // SSA values (nslots + 4); the field is the last
   uint32_t min_len;           // tapes at least this long go to the wide path
   uint32_t ncontrib;          // reverse contribution records per cell
+  uint32_t global;            // 1: the cell working set lives in the block's slice of
+                              // LaunchParams::wscratch (too large for shared memory)
   uint32_t arg_gbase[4];      // records of x, y, z, t (TSI_NONE: one user)
   uint32_t arg_gcount[4];
 };
@@ -161,6 +163,8 @@ struct LaunchParams {
   uint32_t witem_cap;      // wide items per level; more go to the narrow list
   uint32_t bm_words;       // branch-decision words per wide cell (2 bits per min/max)
   CellInfo *cell_info[2];  // [witem_cap * 8] per level parity
+  unsigned char *wscratch;               // [grid][wscratch_stride]: wide cell working sets
+  unsigned long long wscratch_stride;    // of tapes with WideDev::global set
   uint32_t *cell_bits[2];  // [witem_cap * 8][bm_words] per level parity
   uint32_t item_cap;
   uint32_t dealloc_cap;

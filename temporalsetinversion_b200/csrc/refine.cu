@@ -687,6 +687,15 @@ __device__ __forceinline__ CellLayout cell_layout(const WideDev &W, uint32_t bm_
 
 constexpr uint32_t kSmemBundles = 512;  // bundle descriptors held in shared memory
 
+// Base of the block's cell working set: dynamic shared memory, or for tapes
+// too large for it the block's slice of the global scratch (each block of
+// the persistent grid owns one slice; L2 keeps the active slices).
+template <bool GM>
+__device__ __forceinline__ unsigned char *cell_base(const LaunchParams &P) {
+  if constexpr (GM) return P.wscratch + (size_t)blockIdx.x * P.wscratch_stride;
+  else return tsi_dyn_smem;
+}
+
 struct WideShared {
   uint32_t last, E, cnt, mmk, fcost, rcost, ri;
   unsigned long long off;
@@ -724,9 +733,10 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s
 
 // The last cell of a wide item to finish: prunes the full tape with the
 // branch decisions shared by all enqueued siblings and enqueues them.
+template <bool GM>
 __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkItem &it, uint32_t level,
                                              uint32_t unit0, WideShared &sh, unsigned long long *ws) {
-  unsigned char *cell = tsi_dyn_smem;
+  unsigned char *cell = cell_base<GM>(P);
   const uint32_t tid = threadIdx.x;
   const SceneLaunch &S = P.scenes[it.scene];
   const WideDev &W = S.wide;
@@ -899,10 +909,10 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
 }
 
 // One child cell (octant k) of a wide item.  unit = item * 8 + k.
-template <bool D>
+template <bool D, bool GM>
 __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, uint32_t k, uint32_t unit,
                                           uint32_t level, WideShared &sh, unsigned long long *ws) {
-  unsigned char *cell = tsi_dyn_smem;  // the cell's working set (shared memory)
+  unsigned char *cell = cell_base<GM>(P);  // the cell's working set
   using A = IA<D>;
   const uint32_t tid = threadIdx.x;
   const WorkItem &it = *itp;
@@ -1125,7 +1135,7 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   __syncthreads();
   if (!sh.last) return;
   __threadfence();
-  finish_group(P, it, level, unit & ~7u, sh, ws);
+  finish_group<GM>(P, it, level, unit & ~7u, sh, ws);
 }
 
 __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ LaunchParams P, uint32_t level,
@@ -1153,10 +1163,15 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
       if (u >= n_units) break;
       WorkItem *itp = P.witems[level & 1] + (u >> 3);
       const long long c0 = clock64();
-      if (P.scenes[itp->scene].flags & SF_DIRECTED)
-        process_cell<true>(P, itp, u & 7u, u, level, sh, s_stats[0]);
-      else
-        process_cell<false>(P, itp, u & 7u, u, level, sh, s_stats[0]);
+      const SceneLaunch &S = P.scenes[itp->scene];
+      const bool directed = (S.flags & SF_DIRECTED) != 0;
+      if (S.wide.global) {
+        if (directed) process_cell<true, true>(P, itp, u & 7u, u, level, sh, s_stats[0]);
+        else process_cell<false, true>(P, itp, u & 7u, u, level, sh, s_stats[0]);
+      } else {
+        if (directed) process_cell<true, false>(P, itp, u & 7u, u, level, sh, s_stats[0]);
+        else process_cell<false, false>(P, itp, u & 7u, u, level, sh, s_stats[0]);
+      }
       __syncthreads();
       if (threadIdx.x == 0) {
         const unsigned long long c = (unsigned long long)(clock64() - c0);

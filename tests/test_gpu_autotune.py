@@ -59,3 +59,21 @@ def test_autotune_keeps_a_timed_threshold(device):
         s.invert(t)
         fresh.invert(t)
         assert_cells_equal(s.cells(), fresh.cells())
+
+
+@pytest.mark.gpu
+def test_global_working_set_matches_narrow(device):
+    """A tape whose wide working set exceeds shared memory (about 12k
+    slots) runs its wide cells from global scratch, with the narrow path's
+    results."""
+    text = scenes.csg(700, 13, 0.7)
+    times = [0.2, 0.2 + 1 / 60, 0.6]
+    tape, want = _frames(device, text, 6, NARROW_ONLY, times)
+    assert tape.instruction_count > 12000
+    for thr in (None, 256):
+        t2, got = _frames(device, text, 6, thr, times)
+        assert t2.wide_threshold != NARROW_ONLY
+        for (wc, wd, wr), (gc, gd, gr) in zip(want, got):
+            assert_cells_equal(gc, wc)
+            assert np.array_equal(gd, wd)
+            assert np.array_equal(gr, wr)
