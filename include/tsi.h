@@ -180,6 +180,8 @@ typedef struct tsi_device_opts {
   uint64_t log_arena_bytes;     /* reverse-AD operand log (0 = default) */
   uint32_t watchdog_iters;      /* bound on every device wait (0 = default) */
   uint32_t max_scenes_per_launch; /* batch width (0 = default 64) */
+  uint32_t wide_smem_bytes;     /* shared memory a wide cell's working set may take; larger ones run
+                                 * from global scratch (0 = what keeps the narrow path's occupancy) */
 } tsi_device_opts;
 
 typedef struct tsi_ctx tsi_ctx;
@@ -254,9 +256,10 @@ TSI_API tsi_status tsi_scene_image_device(tsi_scene *scene, tsi_image_device *ou
  * compute.wgsl:3513).  Child cells whose pruned tape is at least the tape's
  * wide threshold are evaluated one cell per 256-thread block from the
  * tape's bundled SSA form; shorter ones one warp per 8-cell group.  Results
- * are identical for every threshold; only the speed changes.  Tapes whose
- * SSA form does not fit in shared memory report UINT32_MAX (narrow only)
- * and ignore a new value. */
+ * are identical for every threshold; only the speed changes.  Tapes shorter
+ * than 256 instructions, or whose wide working set would exceed 8 MiB per
+ * cell, have no bundled form: they report UINT32_MAX (narrow only) and
+ * ignore a new value. */
 TSI_API uint32_t tsi_tape_wide_threshold(const tsi_tape *tape);
 TSI_API tsi_status tsi_tape_set_wide_threshold(tsi_tape *tape, uint32_t min_len);
 

@@ -95,7 +95,7 @@ class ImageDevice(C.Structure):
 
 class DeviceOpts(C.Structure):
     _fields_ = [("device", i32), ("work_item_capacity", u64), ("tape_arena_words", u64), ("log_arena_bytes", u64),
-                ("watchdog_iters", u32), ("max_scenes_per_launch", u32)]
+                ("watchdog_iters", u32), ("max_scenes_per_launch", u32), ("wide_smem_bytes", u32)]
 
 
 class TapeInfo(C.Structure):

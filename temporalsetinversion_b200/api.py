@@ -94,9 +94,10 @@ class Device:
     """A tsi_ctx on one CUDA device (fails with TSI_ERR_NO_DEVICE without one)."""
 
     def __init__(self, device: int = 0, work_item_capacity: int = 0, tape_arena_words: int = 0,
-                 log_arena_bytes: int = 0, max_scenes_per_launch: int = 0):
+                 log_arena_bytes: int = 0, max_scenes_per_launch: int = 0, wide_smem_bytes: int = 0):
         self.lib = N.load()
-        opts = N.DeviceOpts(device, work_item_capacity, tape_arena_words, log_arena_bytes, 0, max_scenes_per_launch)
+        opts = N.DeviceOpts(device, work_item_capacity, tape_arena_words, log_arena_bytes, 0, max_scenes_per_launch,
+                            wide_smem_bytes)
         h = C.c_void_p()
         N.check(self.lib.tsi_create(C.byref(opts), C.byref(h)), "tsi_create")
         self.handle = h

@@ -33,6 +33,7 @@ cudaError_t launch_frame_begin(const LaunchParams &P, cudaStream_t st);
 cudaError_t launch_frame_end(const LaunchParams &P, cudaStream_t st);
 cudaError_t refine_set_smem(size_t bytes);
 cudaError_t refine_occupancy(int block, size_t smem, int *blocks_per_sm);
+cudaError_t refine_static_smem(size_t *bytes);
 cudaError_t launch_evalbox(bool directed, const uint2 *code, uint32_t len, uint32_t nregs, uint32_t out_reg,
                            uint32_t n, const float *boxes, int reverse, float *out, float2 *regs, float4 *log,
                            cudaStream_t st);
@@ -87,7 +88,6 @@ struct tsi_tape {
   uint2 *d_wbundles = nullptr;
   uint32_t *d_wmm = nullptr;
   uint32_t wslots = 0, wbundles = 0, wvalues = 0, wmin_len = 0xffffffffu, wcontrib = 0;
-  uint32_t wglobal = 0;  // the cell working set exceeds shared memory: global scratch
   uint32_t warg_gbase[4] = {TSI_NONE, TSI_NONE, TSI_NONE, TSI_NONE}, warg_gcount[4] = {0, 0, 0, 0};
 };
 
@@ -111,6 +111,7 @@ struct tsi_scene {
 struct tsi_ctx {
   int device = 0;
   int sm_count = 0;
+  size_t smem_per_sm = 0, smem_reserved = 0;  // shared memory of an SM, reserved per block
   cudaStream_t stream = nullptr;
   uint32_t max_scenes = 64;
   SceneLaunch *d_scenes = nullptr, *h_scenes = nullptr;
@@ -133,6 +134,7 @@ struct tsi_ctx {
   uint32_t witem_cap = 0, bm_words = 0;
   unsigned char *d_wscratch = nullptr;
   size_t wscratch_bytes = 0, wscratch_stride = 0;
+  size_t wide_smem_bytes = 0;  // shared-memory budget of a wide cell (0: keep the narrow occupancy)
 
   uint2 *d_dealloc[2] = {nullptr, nullptr};
   uint32_t dealloc_cap = 0;
@@ -170,6 +172,7 @@ struct tsi_batch_graph {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool launched = false;
+  std::vector<uint8_t> global;  // per request: wide cells in the global scratch
 };
 
 namespace {
@@ -179,7 +182,7 @@ tsi_status set_err(tsi_status s, const std::string &msg) {
   return s;
 }
 
-LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes) {
+LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes, size_t dyn_smem) {
   LaunchParams P{};
   P.scenes = c->d_scenes;
   P.n_scenes = n_scenes;
@@ -202,6 +205,7 @@ LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes) {
   P.bm_words = c->bm_words;
   P.wscratch = c->d_wscratch;
   P.wscratch_stride = c->wscratch_stride;
+  P.dyn_smem = (uint32_t)dyn_smem;
   for (int q = 0; q < 2; ++q) {
     P.cell_info[q] = c->d_cell_info[q];
     P.cell_bits[q] = c->d_cell_bits[q];
@@ -229,10 +233,12 @@ tsi_status status_from_error_bits(uint32_t e) {
   if (e & EB_LOG_OOM) return set_err(TSI_ERR_OOM, "reverse-AD log arena exhausted");
   if (e & EB_QUEUE_FULL) return set_err(TSI_ERR_QUEUE_FULL, "work list capacity exceeded");
   if (e & EB_WATCHDOG) return set_err(TSI_ERR_WATCHDOG, "bounded device wait expired");
+  if (e & EB_SMEM) return set_err(TSI_ERR_TAPE_TOO_WIDE, "wide cell larger than the launch's shared memory");
   return TSI_OK;
 }
 
-void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, SceneLaunch &L, TapeRec &R) {
+void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, bool wide_global, SceneLaunch &L,
+                 TapeRec &R) {
   const tsi_params &p = s->p;
   L.pool = s->pool;
   L.ctr = s->d_ctr;
@@ -261,7 +267,7 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, Scene
   L.wide.nvalues = s->tape->wvalues;
   L.wide.min_len = s->tape->wmin_len;
   L.wide.ncontrib = s->tape->wcontrib;
-  L.wide.global = s->tape->wglobal;
+  L.wide.global = wide_global ? 1u : 0u;
   for (int q = 0; q < 4; ++q) {
     L.wide.arg_gbase[q] = s->tape->warg_gbase[q];
     L.wide.arg_gcount[q] = s->tape->warg_gcount[q];
@@ -300,6 +306,7 @@ struct FramePlan {
   uint32_t lmax = 0, rcap = 4;
   size_t smem = 0;
   int grid = 0;
+  std::vector<uint8_t> global;  // per scene: wide cells in the global scratch
 };
 
 // Sizes the launch for these scenes and grows the wide path's arenas (no
@@ -316,16 +323,36 @@ tsi_status plan_frame(tsi_ctx *c, tsi_scene *const *scenes, uint32_t n, FramePla
     if (t->d_wslots) mm_max = std::max(mm_max, t->n_minmax);
   }
   bm_words = std::max(1u, (mm_max + 15u) / 16u);
+  fp.rcap = (rmax + 3u) & ~3u;
+  const size_t regfile = (size_t)kWarpsPerBlock * fp.rcap * 32u * sizeof(float2);
+  // A wide cell keeps its working set in shared memory when it fits the
+  // budget: by default what leaves the narrow path's blocks per SM as the
+  // register files alone allow; larger working sets use the global scratch.
+  size_t budget = c->wide_smem_bytes;
+  if (budget == 0) {
+    CK(refine_set_smem(regfile));
+    int bps0 = 0;
+    CK(refine_occupancy(kBlock, regfile, &bps0));
+    if (bps0 < 1) return set_err(TSI_ERR_TAPE_TOO_WIDE, "register file does not fit in shared memory");
+    size_t stat = 0;
+    CK(refine_static_smem(&stat));
+    const size_t per_block = c->smem_per_sm / (size_t)bps0;
+    budget = per_block > stat + c->smem_reserved ? ((per_block - stat - c->smem_reserved) & ~size_t(127)) : 0;
+  }
+  budget = std::min(budget, kWideCellMaxBytes);
   size_t gm_bytes = 0;  // largest working set kept in the global scratch
+  fp.global.assign(n, 0);
   for (uint32_t i = 0; i < n; ++i) {
     const tsi_tape *t = scenes[i]->tape;
     if (!t->d_wslots) continue;
     const size_t b = wide_cell_bytes(t->wvalues, t->wcontrib, bm_words);
-    if (t->wglobal) gm_bytes = std::max(gm_bytes, b);
-    else cell_bytes = std::max(cell_bytes, b);
+    if (b > budget) {
+      fp.global[i] = 1;
+      gm_bytes = std::max(gm_bytes, b);
+    } else {
+      cell_bytes = std::max(cell_bytes, b);
+    }
   }
-  fp.rcap = (rmax + 3u) & ~3u;
-  const size_t regfile = (size_t)kWarpsPerBlock * fp.rcap * 32u * sizeof(float2);
   // the wide cell's working set and the narrow register files share the
   // dynamic shared memory (the phases run one after the other)
   fp.smem = std::max(regfile, cell_bytes);
@@ -371,10 +398,11 @@ tsi_status plan_frame(tsi_ctx *c, tsi_scene *const *scenes, uint32_t n, FramePla
 tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *times, const float *t0s, uint32_t n) {
   if (n == 0) return TSI_OK;
   if (n > c->max_scenes) return set_err(TSI_ERR_INVALID_ARGUMENT, "too many scenes in one launch");
-  for (uint32_t i = 0; i < n; ++i) fill_launch(scenes[i], i, times[i], t0s[i], c->h_scenes[i], c->h_recs[i]);
   FramePlan fp;
   tsi_status pst = plan_frame(c, scenes, n, fp);
   if (pst != TSI_OK) return pst;
+  for (uint32_t i = 0; i < n; ++i)
+    fill_launch(scenes[i], i, times[i], t0s[i], fp.global[i] != 0, c->h_scenes[i], c->h_recs[i]);
   const uint32_t lmax = fp.lmax, rcap = fp.rcap;
   const size_t smem = fp.smem;
   const int grid = fp.grid;
@@ -384,7 +412,7 @@ tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *tim
   CK(cudaMemsetAsync(c->d_stats, 0, ST_COUNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(c->d_level_stats, 0, (TSI_MAX_LEVELS + 1) * ST_COUNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(c->d_log_used, 0, (TSI_MAX_LEVELS + 1) * sizeof(unsigned long long), c->stream));
-  const LaunchParams P = make_params(c, n);
+  const LaunchParams P = make_params(c, n, fp.smem);
   CK(launch_frame_begin(P, c->stream));
   const bool prof = c->profile_levels && c->level_events.size() >= lmax + 1;
   for (uint32_t level = 0; level < lmax; ++level) {
@@ -749,6 +777,8 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   tsi_ctx *c = new tsi_ctx();
   c->device = dev;
   c->sm_count = prop.multiProcessorCount;
+  c->smem_per_sm = prop.sharedMemPerMultiprocessor;
+  c->smem_reserved = prop.reservedSharedMemPerBlock;
   auto fail = [&](tsi_status s) {
     tsi_destroy(c);
     return s;
@@ -763,6 +793,7 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   } while (0)
   CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   c->max_scenes = (opts && opts->max_scenes_per_launch) ? opts->max_scenes_per_launch : 64u;
+  c->wide_smem_bytes = opts ? opts->wide_smem_bytes : 0u;
   c->item_cap = (opts && opts->work_item_capacity) ? (uint32_t)opts->work_item_capacity : (4u << 20);
   c->dealloc_cap = c->item_cap * 2u;
   c->rec_cap = c->item_cap * 2u;
@@ -902,9 +933,8 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
   // shared memory lives in the per-block global scratch
   if (t->len >= 256) {
     WideTape wt;
-    size_t wbytes = 0;
     if (compile_wide(ins, pt, wt, st, why) && wt.nbundles > 0 &&
-        (wbytes = wide_cell_bytes(wt.nvalues, wt.ncontrib, (pt.n_minmax + 15) / 16)) <= kWideCellMaxGlobalBytes) {
+        wide_cell_bytes(wt.nvalues, wt.ncontrib, (pt.n_minmax + 15) / 16) <= kWideCellMaxGlobalBytes) {
       // device layout: the three uint4 of every slot in three arrays
       const size_t nsl = wt.slots.size() / 12;
       std::vector<uint32_t> soa(wt.slots.size());
@@ -929,7 +959,6 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
       t->wbundles = wt.nbundles;
       t->wvalues = wt.nvalues;
       t->wmin_len = std::max<uint32_t>(256u, 3u * wt.nbundles);
-      t->wglobal = wbytes + 4096 > kWideCellMaxBytes ? 1u : 0u;
       t->wcontrib = wt.ncontrib;
       for (int q = 0; q < 4; ++q) {
         t->warg_gbase[q] = wt.arg_gbase[q];
@@ -1545,6 +1574,7 @@ TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *c, tsi_request *reqs, uint32_
       delete g;
       return pst;
     }
+    g->global = fp.global;  // the captured launches' choice, re-applied at every replay
   }
   for (uint32_t i = 0; i < n; ++i)
     if (reqs[i].uniforms) {
@@ -1598,7 +1628,7 @@ TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g) {
     if (r.scene != cap.scene || (r.uniforms == nullptr) != (cap.uniforms == nullptr) ||
         (r.uniforms && (r.uniforms->resolution[0] != r.scene->img_w || r.uniforms->resolution[1] != r.scene->img_h)))
       return set_err(TSI_ERR_INVALID_ARGUMENT, "requests differ from the captured ones (scene or image size)");
-    fill_launch(r.scene, i, r.time, r.t0_or_nan, c->h_scenes[i], c->h_recs[i]);
+    fill_launch(r.scene, i, r.time, r.t0_or_nan, g->global[i] != 0, c->h_scenes[i], c->h_recs[i]);
     if (r.uniforms) {
       const tsi_status st = fill_trace(r.scene, r.uniforms);
       if (st != TSI_OK) return st;

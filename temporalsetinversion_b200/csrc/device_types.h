@@ -34,6 +34,7 @@ enum tsi_error_bits {
   EB_QUEUE_FULL = 1u << 1,
   EB_WATCHDOG = 1u << 2,
   EB_LOG_OOM = 1u << 3,
+  EB_SMEM = 1u << 4,  // a wide cell's working set did not fit the launch's dynamic shared memory
 };
 
 struct VoxelPoolDev {
@@ -165,6 +166,7 @@ struct LaunchParams {
   CellInfo *cell_info[2];  // [witem_cap * 8] per level parity
   unsigned char *wscratch;               // [grid][wscratch_stride]: wide cell working sets
   unsigned long long wscratch_stride;    // of tapes with WideDev::global set
+  uint32_t dyn_smem;                     // dynamic shared memory of the launch, bytes
   uint32_t *cell_bits[2];  // [witem_cap * 8][bm_words] per level parity
   uint32_t item_cap;
   uint32_t dealloc_cap;

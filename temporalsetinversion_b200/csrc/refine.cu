@@ -929,6 +929,12 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   const uint32_t n_narrow = root.len;
   const uint32_t C = base + k;
   const CellLayout L = cell_layout(W, P.bm_words);
+  if constexpr (!GM) {  // the host sized the launch for this cell; never write past it
+    if (L.flags + ((W.nvalues + 15u) & ~15u) > P.dyn_smem) {
+      if (tid == 0) atomicOr(P.error, EB_SMEM);
+      return;
+    }
+  }
   float2 *V = reinterpret_cast<float2 *>(cell);
   float2 *G = reinterpret_cast<float2 *>(cell + L.sens);
   float2 *R = reinterpret_cast<float2 *>(cell + L.rec);
@@ -1341,6 +1347,12 @@ cudaError_t refine_set_smem(size_t bytes) {
 }
 cudaError_t refine_occupancy(int block, size_t smem, int *blocks_per_sm) {
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, refine_kernel, block, smem);
+}
+cudaError_t refine_static_smem(size_t *bytes) {
+  cudaFuncAttributes fa;
+  const cudaError_t e = cudaFuncGetAttributes(&fa, refine_kernel);
+  *bytes = e == cudaSuccess ? fa.sharedSizeBytes : 0;
+  return e;
 }
 
 }  // namespace tsi
