@@ -430,8 +430,10 @@ TSI_API tsi_status tsi_debug_math(tsi_ctx *ctx, int32_t which, uint32_t n, const
  * items on a tape at least the wide path's threshold long, and the longest
  * tape a narrow item ran; then narrow items' cycles in the first forward
  * pass, the reverse pass and the pruning scan, and the instructions of the
- * first forward pass. */
-#define TSI_LEVEL_COUNTERS 30
+ * first forward pass; then wide items' group finishes (count) and their
+ * cycles in the liveness pass, up to the end of compaction, and in
+ * enqueueing the children. */
+#define TSI_LEVEL_COUNTERS 34
 TSI_API tsi_status tsi_debug_level_profile(tsi_ctx *ctx, uint32_t max_levels, float *ms, uint64_t *counters,
                                            uint32_t *n_levels);
 

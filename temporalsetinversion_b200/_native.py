@@ -47,7 +47,8 @@ LEVEL_COUNTERS = ["parents", "evaluated", "reverse", "skipped", "ambiguous", "em
                   "instr_fwd", "instr_rev", "instr_full", "fp32", "brick_alloc", "brick_free", "tape_words",
                   "prune_fallback", "wide_items", "cyc_wide", "cyc_wide_max", "cyc_wide_fwd", "cyc_wide_rev",
                   "cyc_narrow", "cyc_narrow_max", "narrow_long", "narrow_len_max",
-                  "cyc_n_fwd", "cyc_n_rev", "cyc_n_prune", "n_fwd_instr"]
+                  "cyc_n_fwd", "cyc_n_rev", "cyc_n_prune", "n_fwd_instr",
+                  "wide_fin", "cyc_fin_live", "cyc_fin_compact", "cyc_fin_push"]
 
 
 class Stats(C.Structure):

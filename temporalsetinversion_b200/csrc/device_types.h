@@ -143,7 +143,10 @@ enum tsi_stat_index {
   ST_NARROW_LONG, ST_NARROW_LEN_MAX,
   // narrow items: SM cycles of the first forward pass, the reverse pass and
   // the pruning scan, and the instructions of the first forward pass
-  ST_CYC_N_FWD, ST_CYC_N_REV, ST_CYC_N_PRUNE, ST_N_FWD_INSTR, ST_COUNT
+  ST_CYC_N_FWD, ST_CYC_N_REV, ST_CYC_N_PRUNE, ST_N_FWD_INSTR,
+  // wide items' group finishes: count, SM cycles of the liveness pass, of
+  // liveness + compaction + record, and of enqueueing the children
+  ST_WIDE_FIN, ST_CYC_FIN_LIVE, ST_CYC_FIN_COMPACT, ST_CYC_FIN_PUSH, ST_COUNT
 };
 
 struct LaunchParams {

@@ -210,6 +210,52 @@ __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint3
   }
 }
 
+// push_children for the eight children of one wide item (cells base..base+7),
+// by one warp: lanes 0-7 take a child each, so the wide list's entries and
+// the brick allocations proceed in parallel; the first wide-list slots go
+// to the lowest enqueued octants, as in push_children.
+__device__ __forceinline__ void push_children_warp(const LaunchParams &P, const SceneLaunch &S, uint32_t scene,
+                                                   uint32_t rec, uint32_t level, uint32_t E, uint32_t base,
+                                                   bool wide, unsigned long long *ws, uint32_t lane) {
+  uint32_t rest = E;
+  if (wide && E) {
+    uint32_t pos = 0;
+    if (lane == 0) pos = atomicAdd(&P.witem_count[level + 1], (uint32_t)__popc(E));
+    pos = __shfl_sync(FULL_MASK, pos, 0);
+    const uint32_t avail = pos < P.witem_cap ? P.witem_cap - pos : 0u;
+    const uint32_t j = __popc(E & ((1u << lane) - 1u));
+    const bool take = lane < 8u && ((E >> lane) & 1u) && j < avail;
+    if (take) {
+      const uint32_t c = base + lane;
+      uint32_t b = S.pool.child[c], fresh = 0;
+      if (b == TSI_NONE) {
+        b = alloc_brick(S, P.error);
+        if (b != TSI_NONE) {
+          S.pool.child[c] = b;
+          fresh = 1;
+          atomicAdd(&ws[ST_BRICK_ALLOC], 1ull);
+        }
+      }
+      WorkItem wi;
+      wi.scene = scene;
+      wi.rec = rec;
+      wi.n = 1;
+      wi.level = level + 1;
+      wi.parent[0] = c;
+      wi.parent[1] = b;
+      wi.parent[2] = fresh;
+      wi.parent[3] = 0;
+      P.witems[(level + 1) & 1][pos + j] = wi;
+    }
+    rest = E & ~__ballot_sync(FULL_MASK, take);
+  }
+  if (lane == 0 && rest) {
+    uint32_t cells[8];
+    for (int q = 0; q < 8; ++q) cells[q] = base + q;
+    push_children(P, S, scene, rec, level, rest, cells, false, ws);
+  }
+}
+
 __device__ __forceinline__ float warp_min(float v) {
   for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(FULL_MASK, v, o));
   return v;
@@ -743,8 +789,10 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
   const TapeRec root = P.recs[S.root_rec];
   const uint32_t n_narrow = root.len;
   const CellInfo *info = P.cell_info[level & 1] + unit0;
+  const long long f0 = clock64();
   if (tid == 0) {
     ws[ST_PARENTS] += 1;
+    ws[ST_WIDE_FIN] += 1;
     uint32_t E = 0;
     float gl = -fm_inf(), gh = fm_inf(), hl = fm_inf(), hh = -fm_inf();
     for (int q = 0; q < 8; ++q) {
@@ -815,13 +863,15 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
         __syncthreads();
       }
     }
-    // compaction of the narrow full tape in program order
-    const uint32_t per = (n_narrow + blockDim.x - 1) / blockDim.x;
-    const uint32_t i0 = min(n_narrow, tid * per), i1 = min(n_narrow, i0 + per);
+    const long long f1 = clock64();
+    if (tid == 0) ws[ST_CYC_FIN_LIVE] += (unsigned long long)(f1 - f0);
+    // compaction of the narrow full tape in program order, one instruction
+    // per thread a step: live instructions by ballot, output positions from
+    // the warps' counts (coalesced reads of the tape)
     uint32_t mine = 0;
-    for (uint32_t i = i0; i < i1; ++i) mine += flags[i + 4u];
+    for (uint32_t i = tid; i < n_narrow; i += blockDim.x) mine += flags[i + 4u];
     uint32_t total = 0;
-    const uint32_t pos0 = block_exclusive_scan(mine, sh.scan, total);
+    (void)block_exclusive_scan(mine, sh.scan, total);
     if (tid == 0) {
       sh.ri = TSI_NONE;
       sh.off = 0;
@@ -829,7 +879,9 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
       sh.mmk = 0;
       sh.fcost = 0;
       sh.rcost = 0;
-      if (total < n_narrow) {
+      // a pruned record only for children that go to the narrow path (the
+      // wide path evaluates the full tape)
+      if (total < n_narrow && total < W.min_len) {
         const unsigned long long off = atomicAdd(P.code_count, (unsigned long long)total);
         if (off + total <= P.code_cap) {
           const uint32_t ri = atomicAdd(P.rec_count, 1u);
@@ -842,36 +894,65 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
     }
     __syncthreads();
     if (sh.ri != TSI_NONE) {
-      uint32_t p = pos0, mmk = 0, fc = 0, rc = 0;
-      for (uint32_t i = i0; i < i1; ++i) {
-        if (!flags[i + 4u]) continue;
-        const uint2 w = root.code[i];
-        const uint32_t h = TSI_W0_H(w.x);
-        uint2 out = w;
-        uint32_t hk = h;
-        if (TSI_H_IS_MINMAX(h)) {
-          const uint32_t mm = W.narrow_mm[i];
-          const uint32_t d = (cb[mm >> 4] >> (2u * (mm & 15u))) & 3u;
-          const uint32_t dd = TSI_W0_DST(w.x);
-          if (d & 1u) {
-            out = make_uint2(TSI_W0(H_COPY, TSI_W0_FA(w.x), 0u, dd, TSI_W0_A(w.x)), 0u);
-            hk = H_COPY;
-          } else if (d & 2u) {
-            if (TSI_H_IS_II(h)) {
-              out = make_uint2(TSI_W0(H_COPY, TSI_W0_FB(w.x), 0u, dd, w.y & 255u), 0u);
-              hk = H_COPY;
-            } else {
-              out = make_uint2(TSI_W0(H_CONST, 0u, 0u, dd, 0u), w.y);
-              hk = H_CONST;
-            }
-          } else {
-            ++mmk;
-          }
+      const uint32_t lane = tid & 31u, wib = tid >> 5, nw = blockDim.x >> 5;
+      const unsigned long long off = sh.off;
+      uint32_t base = 0, mmk = 0, fc = 0, rc = 0;
+      // this thread's instruction of a step, read one step ahead
+      auto fetch = [&](uint32_t i, uint2 &w, uint32_t &mm) {
+        w = make_uint2(0u, 0u);
+        mm = TSI_NONE;
+        if (i < n_narrow) {
+          w = root.code[i];
+          mm = W.narrow_mm[i];
         }
-        fc += c_cost_fwd[hk] + TSI_FIX_COST;
-        rc += c_cost_rr[hk] + TSI_REV_OPERAND_COST * TSI_H_NREG(hk);
-        P.code_arena[sh.off + p] = out;
-        ++p;
+      };
+      uint2 wn;
+      uint32_t mmn;
+      fetch(tid, wn, mmn);
+      for (uint32_t c0 = 0; c0 < n_narrow; c0 += blockDim.x) {
+        const uint32_t i = c0 + tid;
+        const uint2 w = wn;
+        const uint32_t mm = mmn;
+        fetch(i + blockDim.x, wn, mmn);
+        const bool live = i < n_narrow && flags[i + 4u];
+        const uint32_t bal = __ballot_sync(FULL_MASK, live);
+        if (lane == 0) sh.scan[wib] = __popc(bal);
+        __syncthreads();
+        uint32_t woff = 0, ctot = 0;
+        for (uint32_t q = 0; q < nw; ++q) {
+          const uint32_t v = sh.scan[q];
+          if (q < wib) woff += v;
+          ctot += v;
+        }
+        __syncthreads();  // the counts are read before the next step writes them
+        if (live) {
+          const uint32_t p = base + woff + __popc(bal & ((1u << lane) - 1u));
+          const uint32_t h = TSI_W0_H(w.x);
+          uint2 out = w;
+          uint32_t hk = h;
+          if (TSI_H_IS_MINMAX(h)) {
+            const uint32_t d = (cb[mm >> 4] >> (2u * (mm & 15u))) & 3u;
+            const uint32_t dd = TSI_W0_DST(w.x);
+            if (d & 1u) {
+              out = make_uint2(TSI_W0(H_COPY, TSI_W0_FA(w.x), 0u, dd, TSI_W0_A(w.x)), 0u);
+              hk = H_COPY;
+            } else if (d & 2u) {
+              if (TSI_H_IS_II(h)) {
+                out = make_uint2(TSI_W0(H_COPY, TSI_W0_FB(w.x), 0u, dd, w.y & 255u), 0u);
+                hk = H_COPY;
+              } else {
+                out = make_uint2(TSI_W0(H_CONST, 0u, 0u, dd, 0u), w.y);
+                hk = H_CONST;
+              }
+            } else {
+              ++mmk;
+            }
+          }
+          fc += c_cost_fwd[hk] + TSI_FIX_COST;
+          rc += c_cost_rr[hk] + TSI_REV_OPERAND_COST * TSI_H_NREG(hk);
+          P.code_arena[off + p] = out;
+        }
+        base += ctot;
       }
       atomicAdd(&sh.mmk, mmk);
       atomicAdd(&sh.fcost, fc);
@@ -900,11 +981,15 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
       new_rec = sh.ri;
     }
   }
-  if (tid == 0) {
+  const long long f2 = clock64();
+  if (tid < 32u) {
     const uint32_t len = (new_rec == S.root_rec) ? root.len : sh.cnt;
-    uint32_t cells[8];
-    for (int q = 0; q < 8; ++q) cells[q] = it.parent[1] + q;
-    push_children(P, S, it.scene, new_rec, level, E, cells, len >= W.min_len, ws);
+    push_children_warp(P, S, it.scene, new_rec, level, E, it.parent[1], len >= W.min_len, ws, tid);
+  }
+  if (tid == 0) {
+    const long long f3 = clock64();
+    ws[ST_CYC_FIN_COMPACT] += (unsigned long long)(f2 - f0);
+    ws[ST_CYC_FIN_PUSH] += (unsigned long long)(f3 - f2);
   }
 }
 
@@ -1153,7 +1238,7 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
   float4 *slice_log = P.log_slices + (size_t)gw * P.slice_len * 32u;
   uint2 *slice_dec = P.dec_slices + (size_t)gw * P.slice_len;
   unsigned long long *ws = s_stats[wib];
-  if (lane < ST_COUNT) ws[lane] = 0;
+  for (uint32_t i = lane; i < ST_COUNT; i += 32u) ws[i] = 0;
   __syncwarp();
 
   __shared__ WideShared sh;
@@ -1231,15 +1316,17 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
     dealloc_brick(P, item, level, valid, ws);
   }
   __syncwarp();
-  if (lane < ST_COUNT && ws[lane]) {
-    if (lane == ST_CYC_WIDE_MAX || lane == ST_CYC_NARROW_MAX || lane == ST_NARROW_LEN_MAX) {
-      atomicMax(&P.stats[lane], ws[lane]);
-      atomicMax(&P.level_stats[level * ST_COUNT + lane], ws[lane]);
+  for (uint32_t i = lane; i < ST_COUNT; i += 32u) {
+    if (!ws[i]) continue;
+    if (i == ST_CYC_WIDE_MAX || i == ST_CYC_NARROW_MAX || i == ST_NARROW_LEN_MAX) {
+      atomicMax(&P.stats[i], ws[i]);
+      atomicMax(&P.level_stats[level * ST_COUNT + i], ws[i]);
     } else {
-      atomicAdd(&P.stats[lane], ws[lane]);
-      atomicAdd(&P.level_stats[level * ST_COUNT + lane], ws[lane]);
+      atomicAdd(&P.stats[i], ws[i]);
+      atomicAdd(&P.level_stats[level * ST_COUNT + i], ws[i]);
     }
   }
+
 }
 
 // Per frame: reset level lists and the tape arena, seed the root of every
