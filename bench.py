@@ -227,14 +227,17 @@ def run_reference(args, rank, world, dist) -> None:
 
 
 # ------------------------------------------------------------------ served leg
-SERVED = dict(scenes=8, rate_rps=400.0, seconds=2.0, seed=1000)
+SERVED = dict(scenes=8, rates_rps=(400.0, 1600.0), seconds=1.5, seed=1000)
 
 
 def served_leg(local: int) -> dict:
-    """Open-loop Poisson arrivals over SERVED["scenes"] animations of the
-    workload's kind (each request: the next frame of one scene, inverted and
-    traced at 1920x1080 with the frame left on the device) through the
-    serving layer, against the plain path's per-frame latency on one scene."""
+    """Open-loop Poisson arrivals over SERVED["scenes"] concurrent runs of the
+    workload's animation (scene k starts at frame 15 k; each request: the
+    next frame of one scene, inverted and traced at 1920x1080 with the frame
+    left on the device) through the serving layer at each rate of
+    SERVED["rates_rps"], against the plain path's per-frame latency and
+    frames/s on one scene (one synchronous tsi_scene_invert +
+    tsi_scene_trace per frame)."""
     import threading
 
     from temporalsetinversion_b200 import Device, Scene, Server, Tape, api
@@ -242,64 +245,71 @@ def served_leg(local: int) -> dict:
     W, H, F = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["frames"]
     dev = Device(local)
     try:
-        work = [build_workload(WORKLOAD["seed"] + 1 + k) for k in range(SERVED["scenes"])]
+        work = [build_workload(WORKLOAD["seed"]) for k in range(SERVED["scenes"])]
         sc = [Scene(dev, Tape.from_llvm_ir(dev, t), p) for t, p, _ in work]
         # plain path: one scene, one synchronous call pair per frame
         lat_plain = []
-        for i in range(24):
+        for i in range(40):
             t = frame_time(i, F)
             u = api.make_uniforms(work[0][2], (W, H), t)
             t0 = time.perf_counter()
             sc[0].invert(t)
             sc[0].trace(u, rgba=False, depth=False, normal=False)
             dev.lib.tsi_synchronize(dev.handle)
-            lat_plain.append((time.perf_counter() - t0) * 1000.0)
-        for s in sc:
-            s.reset()
+            if i >= 4:  # after the first_eval frame
+                lat_plain.append((time.perf_counter() - t0) * 1000.0)
+        plain = {"p50_ms": float(np.percentile(lat_plain, 50)), "p99_ms": float(np.percentile(lat_plain, 99)),
+                 "frames_per_s": 1000.0 * len(lat_plain) / float(np.sum(lat_plain))}
         rng = np.random.default_rng(SERVED["seed"])
-        n = int(SERVED["rate_rps"] * SERVED["seconds"])
-        arrivals = np.cumsum(rng.exponential(1.0 / SERVED["rate_rps"], n))
-        which = rng.integers(0, SERVED["scenes"], n)
-        frame = [0] * SERVED["scenes"]
+        frame = [15 * k for k in range(SERVED["scenes"])]
+        runs = []
         with Server(dev) as srv:
-            tickets = []
-            done = threading.Event()
-            lats = []
+            for rate in SERVED["rates_rps"]:
+                n = int(rate * SERVED["seconds"])
+                arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+                which = rng.integers(0, SERVED["scenes"], n)
+                tickets = []
+                done = threading.Event()
+                lats = []
+                b0 = srv.stats()
 
-            def collect():
-                i = 0
-                while i < n:
-                    if i >= len(tickets):
-                        time.sleep(0.0002)
-                        continue
-                    r = srv.poll(tickets[i], 1000)
-                    if r is not None:
-                        lats.append(r[1])
-                        i += 1
-                done.set()
+                def collect():
+                    i = 0
+                    while i < n:
+                        if i >= len(tickets):
+                            time.sleep(0.0002)
+                            continue
+                        r = srv.poll(tickets[i], 1000)
+                        if r is not None:
+                            lats.append(r[1])
+                            i += 1
+                    done.set()
 
-            th = threading.Thread(target=collect, daemon=True)
-            th.start()
-            start = time.perf_counter()
-            for k in range(n):
-                delay = start + arrivals[k] - time.perf_counter()
-                if delay > 0:
-                    time.sleep(delay)
-                j = int(which[k])
-                t = frame_time(frame[j], F)
-                frame[j] += 1
-                tickets.append(srv.submit(sc[j], t, uniforms=api.make_uniforms(work[j][2], (W, H), t)))
-            done.wait(120.0)
-            wall = time.perf_counter() - start
-            st = srv.stats()
-        lats = np.sort(np.asarray(lats))
-        return {"scenes": SERVED["scenes"], "rate_rps": SERVED["rate_rps"], "requests": int(len(lats)),
-                "throughput_rps": len(lats) / wall, "p50_ms": float(np.percentile(lats, 50)),
-                "p99_ms": float(np.percentile(lats, 99)), "max_ms": float(lats[-1]),
-                "mean_batch": st["mean_batch"], "plain_p50_ms": float(np.percentile(lat_plain, 50)),
-                "plain_p99_ms": float(np.percentile(lat_plain, 99)),
-                "note": "Poisson arrivals, next frame of a random scene, invert + 1080p trace, frame kept on device; "
-                        "plain = one scene, tsi_scene_invert + tsi_scene_trace per frame"}
+                th = threading.Thread(target=collect, daemon=True)
+                th.start()
+                start = time.perf_counter()
+                for k in range(n):
+                    delay = start + arrivals[k] - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                    j = int(which[k])
+                    t = frame_time(frame[j], F)
+                    frame[j] += 1
+                    tickets.append(srv.submit(sc[j], t, uniforms=api.make_uniforms(work[j][2], (W, H), t)))
+                done.wait(120.0)
+                wall = time.perf_counter() - start
+                th.join(5.0)
+                b1 = srv.stats()
+                lats = np.sort(np.asarray(lats))
+                nb = max(1, b1["batches"] - b0["batches"])
+                runs.append({"rate_rps": rate, "requests": int(len(lats)), "frames_per_s": len(lats) / wall,
+                             "vs_plain_frames_per_s": len(lats) / wall / plain["frames_per_s"],
+                             "p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
+                             "max_ms": float(lats[-1]), "p99_vs_plain_p50": float(np.percentile(lats, 99)) / plain["p50_ms"],
+                             "mean_batch": (b1["completed"] - b0["completed"]) / nb})
+        return {"scenes": SERVED["scenes"], "plain": plain, "runs": runs,
+                "note": "Poisson arrivals, next frame of a random scene (8 runs of the workload's animation), "
+                        "invert + 1080p trace, frame kept on device; latency from submit to completion"}
     finally:
         dev.close()
 
@@ -362,13 +372,15 @@ def batched_leg(local: int) -> dict:
         W, K = BATCHED["warmup"], BATCHED["steps"]
         # plain: 32 synchronous call pairs per step
         plain_ms = []
+        cells = [0] * len(sc)
         for k in range(W + K):
             ts, us = times(k), uniforms(k)
             t0 = time.perf_counter()
-            for s, t, u in zip(sc, ts, us):
+            for i, (s, t, u) in enumerate(zip(sc, ts, us)):
                 st = N.Stats()
                 N.check(dev.lib.tsi_scene_invert(s.handle, t, math.nan, C.byref(st)), "tsi_scene_invert")
                 N.check(dev.lib.tsi_scene_trace(s.handle, C.byref(u), None, None), "tsi_scene_trace")
+                cells[i] = st.cells_evaluated
             if k >= W:
                 plain_ms.append((time.perf_counter() - t0) * 1000.0)
         for s in sc:
@@ -398,6 +410,8 @@ def batched_leg(local: int) -> dict:
                 "plain_ms_per_step": sum(plain_ms) / K, "graph_ms_per_step": sum(graph_ms) / K,
                 "graph_device_ms_per_step": sum(graph_dev_ms) / K,
                 "autotune_s": t_tune, "wide_thresholds": tuned,
+                "empty_scenes": sum(1 for c in cells if c <= 8),  # a max of disjoint subtrees at the root
+                "cells_per_step": int(sum(cells)),
                 "note": "wall clock per step (all 32 scenes advance by 1/60); plain = 32 x (tsi_scene_invert + "
                         "tsi_scene_trace), graph = one tsi_batch_graph_launch + tsi_batch_graph_wait; frames on "
                         "the device; warm-up steps include every scene's first_eval frame"}
