@@ -99,11 +99,99 @@ pub struct tsi_device_opts {
     pub log_arena_bytes: u64,
     pub watchdog_iters: u32,
     pub max_scenes_per_launch: u32,
+    pub wide_smem_bytes: u32,
+}
+
+#[repr(C)]
+#[derive(Debug, Copy, Clone, Default)]
+pub struct tsi_tape_info {
+    pub instruction_count: u32,
+    pub registers: u32,
+    pub minmax_count: u32,
+    pub reserved: u32,
+}
+
+#[repr(C)]
+pub struct tsi_image_device {
+    pub width: u32,
+    pub height: u32,
+    pub rgba: *const c_float,
+    pub depth: *const c_float,
+    pub normal: *const c_float,
+}
+
+#[repr(C)]
+#[derive(Debug, Copy, Clone, Default)]
+pub struct tsi_cell {
+    pub level: u32,
+    pub ix: u32,
+    pub iy: u32,
+    pub iz: u32,
+    pub f: f32,
+    pub t: f32,
+    pub time_err: f32,
+    pub fast: f32,
+    pub dx: f32,
+    pub dy: f32,
+    pub dz: f32,
+    pub has_children: u32,
+    pub x: [f32; 2],
+    pub y: [f32; 2],
+    pub z: [f32; 2],
+}
+
+#[repr(C)]
+#[derive(Debug, Copy, Clone, Default)]
+pub struct tsi_leaf {
+    pub level: u32,
+    pub ix: u32,
+    pub iy: u32,
+    pub iz: u32,
+}
+
+pub const TSI_AUTOTUNE_MAX: usize = 16;
+#[repr(C)]
+#[derive(Debug, Copy, Clone, Default)]
+pub struct tsi_autotune_result {
+    pub wide_threshold: u32,
+    pub candidates: u32,
+    pub threshold: [u32; TSI_AUTOTUNE_MAX],
+    pub ms: [f32; TSI_AUTOTUNE_MAX],
+}
+
+#[repr(C)]
+pub struct tsi_request {
+    pub scene: *mut tsi_scene,
+    pub time: f32,
+    pub t0_or_nan: f32,
+    pub uniforms: *const Uniforms,
+    pub out: *mut tsi_image,
+    pub stats: *mut tsi_stats,
+}
+
+#[repr(C)]
+#[derive(Debug, Copy, Clone, Default)]
+pub struct tsi_server_opts {
+    pub max_batch: u32,
+    pub reserved: u32,
+}
+
+#[repr(C)]
+#[derive(Debug, Copy, Clone, Default)]
+pub struct tsi_server_stats {
+    pub completed: u64,
+    pub batches: u64,
+    pub mean_batch: f32,
+    pub p50_ms: f32,
+    pub p99_ms: f32,
+    pub max_ms: f32,
 }
 
 pub enum tsi_ctx {}
 pub enum tsi_tape {}
 pub enum tsi_scene {}
+pub enum tsi_batch_graph {}
+pub enum tsi_server {}
 
 extern "C" {
     pub fn tsi_version() -> u32;
@@ -121,6 +209,39 @@ extern "C" {
     pub fn tsi_scene_reset(s: *mut tsi_scene) -> tsi_status;
     pub fn tsi_scene_invert(s: *mut tsi_scene, time: f32, t0_or_nan: f32, stats: *mut tsi_stats) -> tsi_status;
     pub fn tsi_scene_trace(s: *mut tsi_scene, u: *const Uniforms, out: *mut tsi_image, stats: *mut tsi_stats) -> tsi_status;
+    pub fn tsi_synchronize(ctx: *mut tsi_ctx) -> tsi_status;
+    pub fn tsi_ir_lower(text: *const c_char, len: usize, time: f32, out: *mut GPUInstruction, cap: u32, n: *mut u32)
+                        -> tsi_status;
+    pub fn tsi_tape_info_get(t: *const tsi_tape, info: *mut tsi_tape_info) -> tsi_status;
+    pub fn tsi_tape_eval_boxes(ctx: *mut tsi_ctx, t: *const tsi_tape, n: u32, boxes: *const f32, rounding_mode: i32,
+                               reverse: i32, out: *mut f32) -> tsi_status;
+    pub fn tsi_scene_image_device(s: *mut tsi_scene, out: *mut tsi_image_device) -> tsi_status;
+    pub fn tsi_scene_image_copy(s: *mut tsi_scene, out: *mut tsi_image) -> tsi_status;
+    pub fn tsi_tape_wide_threshold(t: *const tsi_tape) -> u32;
+    pub fn tsi_tape_set_wide_threshold(t: *mut tsi_tape, min_len: u32) -> tsi_status;
+    pub fn tsi_scene_autotune(s: *mut tsi_scene, times: *const f32, ntimes: u32, reps: u32,
+                              out: *mut tsi_autotune_result) -> tsi_status;
+    pub fn tsi_scene_readback_cells(s: *mut tsi_scene, out: *mut tsi_cell, cap: u64, n: *mut u64) -> tsi_status;
+    pub fn tsi_scene_readback_leaves(s: *mut tsi_scene, out: *mut tsi_leaf, cap: u64, n: *mut u64) -> tsi_status;
+    pub fn tsi_scene_snapshot_size(s: *mut tsi_scene, bytes: *mut u64) -> tsi_status;
+    pub fn tsi_scene_snapshot(s: *mut tsi_scene, host: *mut c_void, cap: u64, bytes: *mut u64) -> tsi_status;
+    pub fn tsi_scene_restore(s: *mut tsi_scene, host: *const c_void, bytes: u64) -> tsi_status;
+    pub fn tsi_scene_get_params(s: *const tsi_scene, out: *mut tsi_params) -> tsi_status;
+    pub fn tsi_scene_device_bytes(s: *const tsi_scene) -> u64;
+    pub fn tsi_batch_run(ctx: *mut tsi_ctx, reqs: *mut tsi_request, n: u32) -> tsi_status;
+    pub fn tsi_batch_graph_create(ctx: *mut tsi_ctx, reqs: *mut tsi_request, n: u32, out: *mut *mut tsi_batch_graph)
+                                  -> tsi_status;
+    pub fn tsi_batch_graph_launch(g: *mut tsi_batch_graph) -> tsi_status;
+    pub fn tsi_batch_graph_wait(g: *mut tsi_batch_graph, stats: *mut tsi_stats) -> tsi_status;
+    pub fn tsi_batch_graph_destroy(g: *mut tsi_batch_graph);
+    pub fn tsi_server_create(ctx: *mut tsi_ctx, opts: *const tsi_server_opts, out: *mut *mut tsi_server) -> tsi_status;
+    pub fn tsi_server_submit(s: *mut tsi_server, req: *const tsi_request, ticket: *mut u64) -> tsi_status;
+    pub fn tsi_server_poll(s: *mut tsi_server, ticket: u64, wait_ms: u32, latency_ms: *mut f32) -> tsi_status;
+    pub fn tsi_server_stats_get(s: *mut tsi_server, out: *mut tsi_server_stats) -> tsi_status;
+    pub fn tsi_server_destroy(s: *mut tsi_server);
+    pub fn tsi_tape_eval_boxes_static(t: *const tsi_tape, n: u32, boxes_dev: *const f32, rounding_mode: i32,
+                                      reverse: i32, out_dev: *mut f32, stream: *mut c_void) -> tsi_status;
+    pub fn tsi_static_scratch_bytes() -> u64;
 }
 
 /// Convenience used by `State::compute`: one frame, returns device ms.
