@@ -251,6 +251,17 @@ TSI_API tsi_status tsi_scene_invert(tsi_scene *scene, float time, float t0_or_na
 TSI_API tsi_status tsi_scene_trace(tsi_scene *scene, const tsi_uniforms *u, tsi_image *out,
                                    tsi_stats *stats);
 TSI_API tsi_status tsi_scene_image_device(tsi_scene *scene, tsi_image_device *out);
+/* tsi_scene_trace into host buffers without waiting for the frame: the
+ * trace is queued behind the scene's earlier work and the frame's copy to
+ * `out` runs on the context's copy stream, overlapping the caller's next
+ * device work (the next tsi_scene_invert, say).  `out`'s buffers should be
+ * pinned host memory (else the copy is not asynchronous) and must stay
+ * valid and unread until tsi_scene_trace_wait returns; the scene's next
+ * trace waits on the device for this copy to finish. */
+TSI_API tsi_status tsi_scene_trace_async(tsi_scene *scene, const tsi_uniforms *u, tsi_image *out);
+/* Waits until the frame of the scene's last tsi_scene_trace_async is in
+ * host memory. */
+TSI_API tsi_status tsi_scene_trace_wait(tsi_scene *scene);
 
 /* No counterpart in the reference (its workgroup shape is fixed at
  * compute.wgsl:3513).  Child cells whose pruned tape is at least the tape's

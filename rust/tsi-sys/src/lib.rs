@@ -217,6 +217,8 @@ extern "C" {
                                reverse: i32, out: *mut f32) -> tsi_status;
     pub fn tsi_scene_image_device(s: *mut tsi_scene, out: *mut tsi_image_device) -> tsi_status;
     pub fn tsi_scene_image_copy(s: *mut tsi_scene, out: *mut tsi_image) -> tsi_status;
+    pub fn tsi_scene_trace_async(s: *mut tsi_scene, u: *const Uniforms, out: *mut tsi_image) -> tsi_status;
+    pub fn tsi_scene_trace_wait(s: *mut tsi_scene) -> tsi_status;
     pub fn tsi_tape_wide_threshold(t: *const tsi_tape) -> u32;
     pub fn tsi_tape_set_wide_threshold(t: *mut tsi_tape, min_len: u32) -> tsi_status;
     pub fn tsi_scene_autotune(s: *mut tsi_scene, times: *const f32, ntimes: u32, reps: u32,

@@ -251,6 +251,29 @@ class Scene:
         out["visits"] = st.reserved
         return out
 
+    def trace_async(self, uniforms: N.Uniforms, rgba, depth=None, normal=None) -> None:
+        """tsi_scene_trace_async: queue the trace and the frame's copy into
+        the given host arrays (float32, C-contiguous; pinned memory, e.g. a
+        pinned torch tensor's numpy view, makes the copy asynchronous).  The
+        arrays must stay untouched until trace_wait()."""
+        w, h = uniforms.resolution[0], uniforms.resolution[1]
+        img = N.Image(w, h, None, None, None)
+        keep = []
+        for name, arr, n in (("rgba", rgba, 4), ("depth", depth, 1), ("normal", normal, 3)):
+            if arr is None:
+                continue
+            if arr.dtype != np.float32 or not arr.flags.c_contiguous or arr.size != w * h * n:
+                raise ValueError("%s must be a C-contiguous float32 array of %d values" % (name, w * h * n))
+            setattr(img, name, _fptr(arr))
+            keep.append(arr)
+        N.check(self.device.lib.tsi_scene_trace_async(self.handle, C.byref(uniforms), C.byref(img)),
+                "tsi_scene_trace_async")
+        self._async_keep = (keep, uniforms)
+
+    def trace_wait(self) -> None:
+        N.check(self.device.lib.tsi_scene_trace_wait(self.handle), "tsi_scene_trace_wait")
+        self._async_keep = None
+
     def cells(self) -> np.ndarray:
         lib = self.device.lib
         n = C.c_uint64(0)

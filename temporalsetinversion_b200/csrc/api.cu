@@ -105,6 +105,10 @@ struct tsi_scene {
   // the tracer's arguments: written on the host, uploaded before each trace
   // (a captured upload reads the pinned copy when the graph replays)
   TraceParams *h_trace = nullptr, *d_trace = nullptr;
+  // asynchronous frame read-back (tsi_scene_trace_async): the trace's end,
+  // the copy's end on the context's copy stream, and the upload of h_trace
+  cudaEvent_t traced = nullptr, copy_done = nullptr, trace_up = nullptr;
+  bool copy_pending = false, trace_up_pending = false;
   uint64_t bytes = 0;
 };
 
@@ -113,6 +117,7 @@ struct tsi_ctx {
   int sm_count = 0;
   size_t smem_per_sm = 0, smem_reserved = 0;  // shared memory of an SM, reserved per block
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // frame read-back of tsi_scene_trace_async
   uint32_t max_scenes = 64;
   SceneLaunch *d_scenes = nullptr, *h_scenes = nullptr;
   TapeRec *d_recs = nullptr, *h_recs = nullptr;
@@ -534,8 +539,28 @@ void make_camera(const tsi_params &p, const tsi_uniforms &u, TraceParams &T) {
   T.darken = p.octree_darken_factor;
 }
 
+// Whether the context's stream is being captured into a graph (no host
+// waits and no outside events then).
+bool capturing(tsi_ctx *c) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(c->stream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+// Host wait for the scene's pending asynchronous frame copy.
+tsi_status drain_copy(tsi_scene *s) {
+  if (s->copy_pending) {
+    CK(cudaEventSynchronize(s->copy_done));
+    s->copy_pending = false;
+  }
+  return TSI_OK;
+}
+
 tsi_status ensure_image(tsi_scene *s, uint32_t w, uint32_t h) {
   if (s->img_w == w && s->img_h == h && s->d_rgba) return TSI_OK;
+  if (s->copy_pending) {
+    const tsi_status st = drain_copy(s);
+    if (st != TSI_OK) return st;
+  }
   cudaFree(s->d_rgba);
   cudaFree(s->d_depth);
   cudaFree(s->d_normal);
@@ -554,6 +579,11 @@ tsi_status ensure_image(tsi_scene *s, uint32_t w, uint32_t h) {
 // The tracer's arguments for these uniforms, into the scene's pinned copy.
 tsi_status fill_trace(tsi_scene *s, const tsi_uniforms *u) {
   tsi_ctx *c = s->ctx;
+  // the previous upload of the pinned descriptor has been read
+  if (s->trace_up_pending && !capturing(c)) {
+    CK(cudaEventSynchronize(s->trace_up));
+    s->trace_up_pending = false;
+  }
   const tsi_status st = ensure_image(s, u->resolution[0], u->resolution[1]);
   if (st != TSI_OK) return st;
   TraceParams &T = *s->h_trace;
@@ -583,22 +613,29 @@ tsi_status enqueue_trace(tsi_scene *s, const tsi_uniforms *u) {
   if (st != TSI_OK) return st;
   const TraceParams &T = *s->h_trace;
   if (T.W == 0 || T.H == 0) return TSI_OK;
+  const bool cap = capturing(c);
   CK(cudaMemcpyAsync(s->d_trace, s->h_trace, sizeof(TraceParams), cudaMemcpyHostToDevice, c->stream));
+  if (!cap) {
+    CK(cudaEventRecord(s->trace_up, c->stream));
+    s->trace_up_pending = true;
+    // the frame buffers are free once the last asynchronous copy read them
+    if (s->copy_pending) CK(cudaStreamWaitEvent(c->stream, s->copy_done, 0));
+  }
   CK(launch_trace(T, s->d_trace, c->stream));
   return TSI_OK;
 }
 
-tsi_status copy_image_out(tsi_scene *s, tsi_image *out) {
-  tsi_ctx *c = s->ctx;
+tsi_status copy_image_out(tsi_scene *s, tsi_image *out, cudaStream_t st) {
   if (!out) return TSI_OK;
   if (out->width != s->img_w || out->height != s->img_h)
     return set_err(TSI_ERR_BUFFER_TOO_SMALL, "tsi_image size does not match the uniforms' resolution");
   const size_t np = (size_t)s->img_w * s->img_h;
-  if (out->rgba) CK(cudaMemcpyAsync(out->rgba, s->d_rgba, np * 16, cudaMemcpyDeviceToHost, c->stream));
-  if (out->depth) CK(cudaMemcpyAsync(out->depth, s->d_depth, np * 4, cudaMemcpyDeviceToHost, c->stream));
-  if (out->normal) CK(cudaMemcpyAsync(out->normal, s->d_normal, np * 12, cudaMemcpyDeviceToHost, c->stream));
+  if (out->rgba) CK(cudaMemcpyAsync(out->rgba, s->d_rgba, np * 16, cudaMemcpyDeviceToHost, st));
+  if (out->depth) CK(cudaMemcpyAsync(out->depth, s->d_depth, np * 4, cudaMemcpyDeviceToHost, st));
+  if (out->normal) CK(cudaMemcpyAsync(out->normal, s->d_normal, np * 12, cudaMemcpyDeviceToHost, st));
   return TSI_OK;
 }
+tsi_status copy_image_out(tsi_scene *s, tsi_image *out) { return copy_image_out(s, out, s->ctx->stream); }
 
 tsi_status reset_scene(tsi_scene *s) {
   tsi_ctx *c = s->ctx;
@@ -792,6 +829,7 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
     }                                                                      \
   } while (0)
   CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CKC(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
   c->max_scenes = (opts && opts->max_scenes_per_launch) ? opts->max_scenes_per_launch : 64u;
   c->wide_smem_bytes = opts ? opts->wide_smem_bytes : 0u;
   c->item_cap = (opts && opts->work_item_capacity) ? (uint32_t)opts->work_item_capacity : (4u << 20);
@@ -894,6 +932,7 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   delete c;
 }
 
@@ -1139,6 +1178,9 @@ TSI_API tsi_status tsi_scene_create(tsi_ctx *c, const tsi_tape *tape, const tsi_
   A(dalloc(&s->d_ctr, 1));
   A(dalloc(&s->d_trace, 1));
   A(cudaMallocHost((void **)&s->h_trace, sizeof(TraceParams)));
+  A(cudaEventCreateWithFlags(&s->traced, cudaEventDisableTiming));
+  A(cudaEventCreateWithFlags(&s->copy_done, cudaEventDisableTiming));
+  A(cudaEventCreateWithFlags(&s->trace_up, cudaEventDisableTiming));
   s->pool.cap_bricks = s->cap_bricks;
   s->bytes = nv * (16 + 8 + 4 * 5 + 16) + bricks * 8 + sizeof(SceneCounters);
   if (e != cudaSuccess) {
@@ -1160,8 +1202,12 @@ TSI_API void tsi_scene_destroy(tsi_scene *s) {
   if (s->ctx) {
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
+    if (s->copy_pending) cudaEventSynchronize(s->copy_done);
     s->ctx->scenes.erase(s);
   }
+  if (s->traced) cudaEventDestroy(s->traced);
+  if (s->copy_done) cudaEventDestroy(s->copy_done);
+  if (s->trace_up) cudaEventDestroy(s->trace_up);
   cudaFree(s->pool.box_xy);
   cudaFree(s->pool.box_z);
   cudaFree(s->pool.t);
@@ -1231,6 +1277,29 @@ TSI_API tsi_status tsi_scene_trace(tsi_scene *s, const tsi_uniforms *u, tsi_imag
     stats->reserved = (float)c->h_rb->visits;
   }
   return TSI_OK;
+}
+
+TSI_API tsi_status tsi_scene_trace_async(tsi_scene *s, const tsi_uniforms *u, tsi_image *out) {
+  if (!s || !u || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  if (out->width != u->resolution[0] || out->height != u->resolution[1])
+    return set_err(TSI_ERR_BUFFER_TOO_SMALL, "tsi_image size does not match the uniforms' resolution");
+  tsi_ctx *c = s->ctx;
+  CK(cudaSetDevice(c->device));
+  tsi_status st = enqueue_trace(s, u);
+  if (st != TSI_OK) return st;
+  CK(cudaEventRecord(s->traced, c->stream));
+  CK(cudaStreamWaitEvent(c->copy_stream, s->traced, 0));
+  st = copy_image_out(s, out, c->copy_stream);
+  if (st != TSI_OK) return st;
+  CK(cudaEventRecord(s->copy_done, c->copy_stream));
+  s->copy_pending = true;
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_scene_trace_wait(tsi_scene *s) {
+  if (!s) return set_err(TSI_ERR_INVALID_ARGUMENT, "null scene");
+  CK(cudaSetDevice(s->ctx->device));
+  return drain_copy(s);
 }
 
 TSI_API tsi_status tsi_scene_image_copy(tsi_scene *s, tsi_image *out) {
@@ -1576,6 +1645,13 @@ TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *c, tsi_request *reqs, uint32_
     }
     g->global = fp.global;  // the captured launches' choice, re-applied at every replay
   }
+  for (uint32_t i = 0; i < n; ++i) {
+    const tsi_status dst = drain_copy(reqs[i].scene);  // no outside event inside the capture
+    if (dst != TSI_OK) {
+      delete g;
+      return dst;
+    }
+  }
   for (uint32_t i = 0; i < n; ++i)
     if (reqs[i].uniforms) {
       tsi_status st = ensure_image(reqs[i].scene, reqs[i].uniforms->resolution[0], reqs[i].uniforms->resolution[1]);
@@ -1629,6 +1705,8 @@ TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g) {
         (r.uniforms && (r.uniforms->resolution[0] != r.scene->img_w || r.uniforms->resolution[1] != r.scene->img_h)))
       return set_err(TSI_ERR_INVALID_ARGUMENT, "requests differ from the captured ones (scene or image size)");
     fill_launch(r.scene, i, r.time, r.t0_or_nan, g->global[i] != 0, c->h_scenes[i], c->h_recs[i]);
+    const tsi_status dst = drain_copy(r.scene);  // the replay's traces rewrite the frame buffers
+    if (dst != TSI_OK) return dst;
     if (r.uniforms) {
       const tsi_status st = fill_trace(r.scene, r.uniforms);
       if (st != TSI_OK) return st;

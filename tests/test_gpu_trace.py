@@ -82,3 +82,29 @@ def test_rendermode_black(device):
     u = api.make_uniforms(scenes.camera_look_at((0, 0, 2.5)), (32, 32), 0.0, rendermode=1.0)
     g = gs.trace(u)
     assert np.all(g["rgba"] == 0) and np.all(g["depth"] == -1)
+
+
+@pytest.mark.gpu
+def test_trace_async_matches_trace(device):
+    """Frames read back asynchronously (pinned buffers, copies overlapping
+    the next inversion) equal the synchronous trace's frames."""
+    import torch
+
+    text = scenes.csg(24, 5, 0.8)
+    params = api.default_params(localsubdiv=6)
+    a = Scene(device, Tape.from_llvm_ir(device, text), params)
+    b = Scene(device, Tape.from_llvm_ir(device, text), params)
+    cam = scenes.camera_look_at((0.5, 0.9, 2.3))
+    res = (160, 96)
+    bufs = [torch.empty((res[1], res[0], 4), dtype=torch.float32, pin_memory=True) for _ in range(4)]
+    want = []
+    for f in range(4):
+        t = f / 60.0
+        u = api.make_uniforms(cam, res, t)
+        a.invert(t)
+        a.trace_async(u, bufs[f].numpy())
+        b.invert(t)
+        want.append(b.trace(u, depth=False, normal=False)["rgba"])
+    a.trace_wait()
+    for f in range(4):
+        assert np.array_equal(bufs[f].numpy(), want[f])
