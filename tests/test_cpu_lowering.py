@@ -44,6 +44,19 @@ def test_library_loads_and_exports_every_header_symbol():
     assert lib.tsi_version() == 1
 
 
+def test_rust_binding_declares_the_public_header():
+    """rust/tsi-sys declares every entry point above the header's
+    diagnostics block, and nothing the header lacks."""
+    header = (ROOT / "include" / "tsi.h").read_text()
+    public = header.split("---------------- diagnostics")[0]
+    names = set(re.findall(r"TSI_API\s+[^;(]*?\b(tsi_\w+)\s*\(", public))
+    rust = (ROOT / "rust" / "tsi-sys" / "src" / "lib.rs").read_text()
+    declared = set(re.findall(r"pub fn (tsi_\w+)\s*\(", rust))
+    all_names = set(re.findall(r"TSI_API\s+[^;(]*?\b(tsi_\w+)\s*\(", header))
+    assert names - declared == set()
+    assert declared - all_names == set()
+
+
 @pytest.mark.parametrize("scene", sorted(FIXTURE_COUNTS))
 def test_golden_tapes(scene):
     tape = load_tape(scene)
