@@ -25,6 +25,45 @@ def test_voxel_pool_exhaustion_is_reported(device):
 
 
 @pytest.mark.gpu
+def test_graph_replay_reports_pool_exhaustion(device):
+    """A graph replay that runs out of voxels reports it at the wait, like
+    the plain call, and a replay after a reset of a large enough scene works."""
+    tape = Tape.from_llvm_ir(device, scenes.spheres16(0))
+    tiny = Scene(device, tape, api.default_params(localsubdiv=7), voxel_capacity=64)
+    ok = Scene(device, tape, api.default_params(localsubdiv=5))
+    g = api.BatchGraph(device, [(tiny, 0.0, float("nan"), None), (ok, 0.0, float("nan"), None)])
+    try:
+        g.launch([0.0, 0.0])
+        with pytest.raises(N.TsiError) as e:
+            g.wait()
+        assert e.value.status == 4  # TSI_ERR_OOM
+    finally:
+        g.close()
+    g = api.BatchGraph(device, [(ok, 0.1, float("nan"), None)])
+    try:
+        ok.reset()
+        g.launch([0.1])
+        st = g.wait()
+        assert st.error_flags == 0 and st.cells_evaluated > 0
+    finally:
+        g.close()
+
+
+@pytest.mark.gpu
+def test_trace_async_rejects_mismatched_frame(device):
+    tape = Tape.from_llvm_ir(device, scenes.spheres16(0))
+    s = Scene(device, tape, api.default_params(localsubdiv=4))
+    s.invert(0.0)
+    u = api.make_uniforms(scenes.camera_look_at((0.4, 0.8, 2.4)), (32, 16), 0.0)
+    img = N.Image(16, 16, None, None, None)
+    assert device.lib.tsi_scene_trace_async(s.handle, C.byref(u), C.byref(img)) == 10  # TSI_ERR_BUFFER_TOO_SMALL
+    rgba = np.zeros((16, 32, 4), np.float32)
+    s.trace_async(u, rgba)
+    s.trace_wait()
+    assert np.array_equal(rgba, s.trace(u, depth=False, normal=False)["rgba"])
+
+
+@pytest.mark.gpu
 def test_work_list_overflow_is_reported():
     with Device(work_item_capacity=16) as dev:
         tape = Tape.from_llvm_ir(dev, scenes.spheres16(0))
