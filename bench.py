@@ -64,6 +64,11 @@ WORKLOAD = dict(name="csg256_L10_1080p_120f", n_prims=256, seed=1, localsubdiv=1
                 eye=(1.6, 1.0, 1.9))
 METRIC = "frames/s @ subdiv 10, 1080p"
 PEAK_FP32_NOMINAL_TOPS = 148 * 128 * 1.965  # G ops/s: 148 SMs x 128 FP32 lanes x 1.965 GHz (non-FMA)
+# DRAM bytes (read + write) per launch from one ncu capture of this workload's
+# frame 4 (profiles/dram_csg256_L10_1080p.md): refine_kernel averaged over the
+# frame's ten level launches, trace_kernel per frame
+TRAFFIC_REFINE_PER_LAUNCH = 0.839e6
+TRAFFIC_TRACE_PER_LAUNCH = 21.11e6
 
 
 def frame_time(i: int, frames: int) -> float:
@@ -540,11 +545,13 @@ def run_gpu(args, rank, world, local, dist) -> None:
                 "synchronous_value": e2e_sync_value},
         "roofline": {"kernel": "refine_kernel (interval tape interpreter)", "bound": "fp32",
                      "achieved": achieved_gops / 1000.0, "peak": PEAK_FP32_NOMINAL_TOPS / 1000.0, "unit": "TOP/s",
-                     "frac": achieved_gops / PEAK_FP32_NOMINAL_TOPS, "traffic": None,
+                     "frac": achieved_gops / PEAK_FP32_NOMINAL_TOPS, "traffic": TRAFFIC_REFINE_PER_LAUNCH,
+                     "traffic_unit": "bytes per launch (ncu, dram read + write)",
                      "peak_source": "nominal FP32 (MEASURED_PEAKS.json has no FP32 figure)",
                      "ops_per_step": ops / args.steps},
         "roofline_trace": {"kernel": "trace_kernel", "bound": "hbm", "achieved": trace_gbs, "peak": hbm_peak,
-                           "unit": "GB/s", "frac": trace_gbs / hbm_peak, "traffic": None,
+                           "unit": "GB/s", "frac": trace_gbs / hbm_peak, "traffic": TRAFFIC_TRACE_PER_LAUNCH,
+                           "traffic_unit": "bytes per launch (ncu, dram read + write)",
                            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "breakdown_ms_per_step": {"invert": sum(inv_ms) / args.steps, "trace": sum(trace_ms) / args.steps},
         "work_per_step": {k: v / args.steps for k, v in totals.items()},
