@@ -443,8 +443,9 @@ TSI_API tsi_status tsi_debug_math(tsi_ctx *ctx, int32_t which, uint32_t n, const
  * pass, the reverse pass and the pruning scan, and the instructions of the
  * first forward pass; then wide items' group finishes (count) and their
  * cycles in the liveness pass, up to the end of compaction, and in
- * enqueueing the children. */
-#define TSI_LEVEL_COUNTERS 34
+ * enqueueing the children; then wide cells that ran the forward pass again
+ * over their children's wider time range, and its cycles. */
+#define TSI_LEVEL_COUNTERS 36
 TSI_API tsi_status tsi_debug_level_profile(tsi_ctx *ctx, uint32_t max_levels, float *ms, uint64_t *counters,
                                            uint32_t *n_levels);
 

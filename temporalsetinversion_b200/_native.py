@@ -48,7 +48,7 @@ LEVEL_COUNTERS = ["parents", "evaluated", "reverse", "skipped", "ambiguous", "em
                   "prune_fallback", "wide_items", "cyc_wide", "cyc_wide_max", "cyc_wide_fwd", "cyc_wide_rev",
                   "cyc_narrow", "cyc_narrow_max", "narrow_long", "narrow_len_max",
                   "cyc_n_fwd", "cyc_n_rev", "cyc_n_prune", "n_fwd_instr",
-                  "wide_fin", "cyc_fin_live", "cyc_fin_compact", "cyc_fin_push"]
+                  "wide_fin", "cyc_fin_live", "cyc_fin_compact", "cyc_fin_push", "wide_refwd", "cyc_wide_refwd"]
 
 
 class Stats(C.Structure):

@@ -146,7 +146,10 @@ enum tsi_stat_index {
   ST_CYC_N_FWD, ST_CYC_N_REV, ST_CYC_N_PRUNE, ST_N_FWD_INSTR,
   // wide items' group finishes: count, SM cycles of the liveness pass, of
   // liveness + compaction + record, and of enqueueing the children
-  ST_WIDE_FIN, ST_CYC_FIN_LIVE, ST_CYC_FIN_COMPACT, ST_CYC_FIN_PUSH, ST_COUNT
+  ST_WIDE_FIN, ST_CYC_FIN_LIVE, ST_CYC_FIN_COMPACT, ST_CYC_FIN_PUSH,
+  // wide cells that ran the forward pass again over their children's wider
+  // time range (count, SM cycles)
+  ST_WIDE_REFWD, ST_CYC_WIDE_REFWD, ST_COUNT
 };
 
 struct LaunchParams {

@@ -1089,14 +1089,44 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   const bool want_prune = (flg & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS;
   const uint32_t words = (root.n_minmax + 15u) >> 4;
 
+  // The time range this cell's children would be evaluated over if it is
+  // re-enqueued and they do not take the point branch: when it is wider
+  // than the cell's own, the decisions for pruning are taken over it in the
+  // same forward pass (values over it in the sensitivity array, unused until
+  // the reverse pass; decision bits in the liveness flags, unused until the
+  // group finishes).  The range is the one computed after classification
+  // below, step for step.
+  float wl = targ.lo, wh = targ.hi;
+  if (evaluate && want_prune) {
+    if (c_child != TSI_NONE && !(child_width <= S.eps)) {
+      for (int q = 0; q < 8; ++q) {
+        const float ct = pool.t[c_child + q];
+        wl = fm_min(wl, fm_min(ct, S.time));
+        wh = fm_max(wh, fm_max(ct, S.time));
+      }
+    }
+    if (swept) {
+      wl = fm_min(wl, fm_min(S.t0, S.time));
+      wh = fm_max(wh, fm_max(S.t0, S.time));
+    }
+  }
+  const bool dual = evaluate && want_prune && (wl < targ.lo || wh > targ.hi);
+  uint32_t *bits2 = reinterpret_cast<uint32_t *>(cell + L.flags);
+
   // ---- forward and reverse over the full tape, bundle by bundle
   Iv field = iv(0.0f);
   Iv sens[4] = {iv(0.0f), iv(0.0f), iv(0.0f), iv(0.0f)};
   if (evaluate) {
     if (want_prune)
-      for (uint32_t w = tid; w < words; w += blockDim.x) bits[w] = 0u;
+      for (uint32_t w = tid; w < words; w += blockDim.x) {
+        bits[w] = 0u;
+        if (dual) bits2[w] = 0u;
+      }
     const long long c0 = clock64();
-    field = cell_forward<D>(W, bt_tab, V, want_prune ? bits : nullptr, cx, cy, cz, targ);
+    if (dual)
+      field = cell_forward2<D>(W, bt_tab, V, G, bits, bits2, cx, cy, cz, targ, Iv{wl, wh});
+    else
+      field = cell_forward<D>(W, bt_tab, V, want_prune ? bits : nullptr, cx, cy, cz, targ);
     const long long c1 = clock64();
     if (take_deriv) {
       cell_reverse<D>(W, bt_tab, V, G, R, sh.sens);
@@ -1202,9 +1232,18 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   if (want_prune && enq && (nl < targ.lo || nh > targ.hi)) {
     // decisions over the children's (wider) time range
     __syncthreads();
-    for (uint32_t w = tid; w < words; w += blockDim.x) bits[w] = 0u;
-    (void)cell_forward<D>(W, bt_tab, V, bits, cx, cy, cz, Iv{nl, nh});
     if (tid == 0) ws[ST_FP32] += (unsigned long long)root.fwd_cost;
+    if (dual && nl == wl && nh == wh) {  // taken in the forward pass
+      for (uint32_t w = tid; w < words; w += blockDim.x) bits[w] = bits2[w];
+    } else {
+      const long long r0 = clock64();
+      for (uint32_t w = tid; w < words; w += blockDim.x) bits[w] = 0u;
+      (void)cell_forward<D>(W, bt_tab, V, bits, cx, cy, cz, Iv{nl, nh});
+      if (tid == 0) {
+        ws[ST_WIDE_REFWD] += 1ull;
+        ws[ST_CYC_WIDE_REFWD] += (unsigned long long)(clock64() - r0);
+      }
+    }
   }
   // ---- hand over to the group: decision bits and time range, then count in
   __syncthreads();

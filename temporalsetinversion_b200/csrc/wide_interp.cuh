@@ -69,6 +69,67 @@ __device__ __forceinline__ Iv cell_forward(const WideDev &W, const uint2 *bt_tab
   return ldv(V, W.nvalues - 1u);
 }
 
+// cell_forward over two time intervals at once: V holds the values over
+// `t` (the field and the reverse pass use them), V2 those over `t2`, whose
+// min/max decisions go to bits2 (those over `t` to bits).  The second
+// evaluation is independent of the first, so a bundle step runs both.
+template <bool D>
+__device__ __forceinline__ Iv cell_forward2(const WideDev &W, const uint2 *bt_tab, float2 *V, float2 *V2,
+                                            uint32_t *bits, uint32_t *bits2, Iv x, Iv y, Iv z, Iv t, Iv t2) {
+  const uint32_t tid = threadIdx.x;
+  const uint4 *__restrict__ slots = W.slots;
+  const uint32_t nb = W.nbundles;
+  const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
+  auto fetch = [&](uint32_t kk) -> uint4 {
+    if (kk >= nb) return zero4;
+    const uint2 b = bt_tab[kk];
+    return tid < (b.y & 0xffffu) ? slots[b.x + tid] : zero4;
+  };
+  if (tid == 0) {
+    stv(V, 0, x);
+    stv(V, 1, y);
+    stv(V, 2, z);
+    stv(V, 3, t);
+    stv(V2, 0, x);
+    stv(V2, 1, y);
+    stv(V2, 2, z);
+    stv(V2, 3, t2);
+  }
+  uint4 q0 = fetch(0), q1 = fetch(1), q2 = fetch(2);
+  __syncthreads();
+  auto decide = [](uint32_t h, Iv A, Iv B) -> uint32_t {
+    const bool amax = (h == H_MAX_II || h == H_MAX_IF);
+    const bool a_below = A.hi < B.lo, b_below = B.hi < A.lo;
+    return ((amax ? b_below : a_below) ? 1u : 0u) | ((amax ? a_below : b_below) ? 2u : 0u);
+  };
+  for (uint32_t k = 0; k < nb; ++k) {
+    const uint4 sl = q0;
+    q0 = q1;
+    q1 = q2;
+    q2 = fetch(k + 3u);
+    const uint2 bt = bt_tab[k];
+    const uint32_t h = bt.y >> 16;
+    if (tid < (bt.y & 0xffffu)) {
+      const float lit = __uint_as_float(sl.w);
+      const bool II = TSI_H_IS_II(h);
+      const Iv A = ldv(V, sl.y), A2 = ldv(V2, sl.y);
+      const Iv B = II ? ldv(V, sl.z) : iv(lit);
+      const Iv B2 = II ? ldv(V2, sl.z) : iv(lit);
+      stv(V, sl.x >> 8, op_forward<D>(h, A, B, lit));
+      stv(V2, sl.x >> 8, op_forward<D>(h, A2, B2, lit));
+      if (TSI_H_IS_MINMAX(h)) {
+        const uint32_t mm = II ? sl.w : sl.z;
+        const uint32_t sh = 2u * (mm & 15u);
+        const uint32_t d = decide(h, A, B), d2 = decide(h, A2, B2);
+        if (d) atomicOr(&bits[mm >> 4], d << sh);
+        if (d2) atomicOr(&bits2[mm >> 4], d2 << sh);
+      }
+    }
+    __syncthreads();
+  }
+  return ldv(V, W.nvalues - 1u);
+}
+
 // Sum of a value's contribution records, last user first, onto +0: the
 // accumulation order of the sequential reverse pass.
 template <bool D>
