@@ -329,6 +329,19 @@ typedef struct tsi_request {
  * distinct. */
 TSI_API tsi_status tsi_batch_run(tsi_ctx *ctx, tsi_request *reqs, uint32_t n);
 
+/* No counterpart in the reference.  Tunes the wide thresholds of the
+ * requests' tapes for running them together: multiplies every tape's
+ * threshold by 1, 2, 4 and 8 in turn, times `frames` fused inversions of the
+ * requests (each request's time advancing by 1/60 per frame, from reset
+ * octrees), and keeps the fastest multiplier on the tapes.  A full GPU
+ * favours the narrow path's throughput over the wide path's latency, so a
+ * batch often runs faster with larger thresholds than each scene alone.
+ * out->wide_threshold is the multiplier kept, out->threshold[k] and
+ * out->ms[k] the multipliers tried and their device times.  The scenes are
+ * left reset. */
+TSI_API tsi_status tsi_batch_autotune(tsi_ctx *ctx, const tsi_request *reqs, uint32_t n, uint32_t frames,
+                                      tsi_autotune_result *out);
+
 /* Captures tsi_batch_run for a fixed request set into a CUDA graph and
  * replays it.  The request array must stay valid while the graph exists:
  * every launch waits for the previous replay, then re-reads each request's

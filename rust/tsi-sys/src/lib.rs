@@ -231,6 +231,8 @@ extern "C" {
     pub fn tsi_scene_get_params(s: *const tsi_scene, out: *mut tsi_params) -> tsi_status;
     pub fn tsi_scene_device_bytes(s: *const tsi_scene) -> u64;
     pub fn tsi_batch_run(ctx: *mut tsi_ctx, reqs: *mut tsi_request, n: u32) -> tsi_status;
+    pub fn tsi_batch_autotune(ctx: *mut tsi_ctx, reqs: *const tsi_request, n: u32, frames: u32,
+                              out: *mut tsi_autotune_result) -> tsi_status;
     pub fn tsi_batch_graph_create(ctx: *mut tsi_ctx, reqs: *mut tsi_request, n: u32, out: *mut *mut tsi_batch_graph)
                                   -> tsi_status;
     pub fn tsi_batch_graph_launch(g: *mut tsi_batch_graph) -> tsi_status;

@@ -147,6 +147,7 @@ SIGNATURES = {
     "tsi_scene_trace_wait": (i32, [C.c_void_p]),
     "tsi_batch_graph_launch": (i32, [C.c_void_p]),
     "tsi_batch_graph_wait": (i32, [C.c_void_p, P(Stats)]),
+    "tsi_batch_autotune": (i32, [C.c_void_p, P(Request), u32, u32, P(AutotuneResult)]),
     "tsi_tape_wide_threshold": (u32, [C.c_void_p]),
     "tsi_tape_set_wide_threshold": (i32, [C.c_void_p, u32]),
     "tsi_scene_autotune": (i32, [C.c_void_p, P(f32), u32, u32, P(AutotuneResult)]),

@@ -447,6 +447,22 @@ class Server:
         self.close()
 
 
+def batch_autotune(device: Device, requests: list, frames: int = 3) -> dict:
+    """tsi_batch_autotune: the wide-threshold multiplier (1, 2, 4 or 8) that
+    runs these scenes fastest together.  requests: list of (scene, time).
+    The scenes are left reset."""
+    n = len(requests)
+    reqs = (N.Request * n)()
+    for i, (scene, time) in enumerate(requests):
+        reqs[i].scene = scene.handle
+        reqs[i].time = float(time)
+        reqs[i].t0_or_nan = math.nan
+    r = N.AutotuneResult()
+    N.check(device.lib.tsi_batch_autotune(device.handle, reqs, n, int(frames), C.byref(r)), "tsi_batch_autotune")
+    return {"scale": int(r.wide_threshold),
+            "trials": [(int(r.threshold[k]), float(r.ms[k])) for k in range(r.candidates)]}
+
+
 class BatchGraph:
     """tsi_batch_run for a fixed set of distinct scenes captured into a CUDA
     graph; each launch re-reads the requests' times and cameras."""

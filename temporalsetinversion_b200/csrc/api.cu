@@ -1623,6 +1623,70 @@ TSI_API tsi_status tsi_batch_run(tsi_ctx *c, tsi_request *reqs, uint32_t n) {
   return status_from_error_bits(c->h_rb->error);
 }
 
+TSI_API tsi_status tsi_batch_autotune(tsi_ctx *c, const tsi_request *reqs, uint32_t n, uint32_t frames,
+                                      tsi_autotune_result *out) {
+  if (!c || !reqs || n == 0 || frames == 0 || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  memset(out, 0, sizeof(*out));
+  CK(cudaSetDevice(c->device));
+  // the distinct tapes with a bundled form, and their thresholds now
+  std::vector<tsi_tape *> tapes;
+  std::vector<uint32_t> base;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!reqs[i].scene || reqs[i].scene->ctx != c) return set_err(TSI_ERR_INVALID_ARGUMENT, "bad request scene");
+    tsi_tape *t = const_cast<tsi_tape *>(reqs[i].scene->tape);
+    if (t->d_wslots && std::find(tapes.begin(), tapes.end(), t) == tapes.end()) {
+      tapes.push_back(t);
+      base.push_back(t->wmin_len);
+    }
+  }
+  auto reset_all = [&]() -> tsi_status {
+    for (uint32_t i = 0; i < n; ++i) {
+      const tsi_status st = tsi_scene_reset(reqs[i].scene);
+      if (st != TSI_OK) return st;
+    }
+    return TSI_OK;
+  };
+  auto apply = [&](uint32_t scale) {
+    for (size_t q = 0; q < tapes.size(); ++q)
+      tapes[q]->wmin_len = base[q] >= 0xffffffffu / scale ? 0xffffffffu : base[q] * scale;
+  };
+  const uint32_t scales[] = {1u, 2u, 4u, 8u};
+  const uint32_t ncand = tapes.empty() ? 1u : 4u;
+  std::vector<tsi_request> rq(n);
+  std::vector<tsi_stats> st(n);
+  float best = INFINITY;
+  uint32_t pick = 1u;
+  for (uint32_t k = 0; k < ncand; ++k) {
+    apply(scales[k]);
+    tsi_status s = reset_all();
+    float ms = 0.0f;
+    for (uint32_t f = 0; f < frames && s == TSI_OK; ++f) {
+      for (uint32_t i = 0; i < n; ++i) {
+        rq[i] = tsi_request{reqs[i].scene, reqs[i].time + (float)f / 60.0f, NAN, nullptr, nullptr, &st[i]};
+      }
+      s = tsi_batch_run(c, rq.data(), n);
+      if (s == TSI_OK) ms += st[0].device_ms;
+    }
+    if (s == TSI_ERR_QUEUE_FULL || s == TSI_ERR_OOM) {
+      ms = INFINITY;  // this scale does not fit the arenas
+    } else if (s != TSI_OK) {
+      apply(1u);
+      reset_all();
+      return s;
+    }
+    out->threshold[k] = scales[k];
+    out->ms[k] = ms;
+    if (ms < best) {
+      best = ms;
+      pick = scales[k];
+    }
+  }
+  out->candidates = ncand;
+  out->wide_threshold = pick;
+  apply(pick);
+  return reset_all();
+}
+
 TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *c, tsi_request *reqs, uint32_t n, tsi_batch_graph **out) {
   if (!c || !reqs || !out || n == 0) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
   if (n > c->max_scenes) return set_err(TSI_ERR_INVALID_ARGUMENT, "graph batch wider than one launch");

@@ -77,3 +77,23 @@ def test_global_working_set_matches_narrow(device):
             assert_cells_equal(gc, wc)
             assert np.array_equal(gd, wd)
             assert np.array_equal(gr, wr)
+
+
+@pytest.mark.gpu
+def test_batch_autotune_scales_thresholds_and_keeps_results(device):
+    texts = [scenes.csg(40, 21 + k, 0.8) for k in range(4)]
+    tapes = [Tape.from_llvm_ir(device, t) for t in texts]
+    base = [t.wide_threshold for t in tapes]
+    sc = [Scene(device, t, api.default_params(localsubdiv=6)) for t in tapes]
+    r = api.batch_autotune(device, [(s, 0.1 * k) for k, s in enumerate(sc)], frames=2)
+    assert [m for m, _ in r["trials"]] == [1, 2, 4, 8]
+    assert r["scale"] in (1, 2, 4, 8)
+    for t, b in zip(tapes, base):
+        assert t.wide_threshold == (NARROW_ONLY if b == NARROW_ONLY else b * r["scale"])
+    # left reset, and the batch gives each scene's plain results
+    res = api.run_batch(device, [(s, 0.1 * k, float("nan"), None) for k, s in enumerate(sc)])
+    assert all(x["stats"].error_flags == 0 for x in res)
+    for k, (text, s) in enumerate(zip(texts, sc)):
+        fresh = Scene(device, Tape.from_llvm_ir(device, text), api.default_params(localsubdiv=6))
+        fresh.invert(0.1 * k)
+        assert_cells_equal(s.cells(), fresh.cells())
