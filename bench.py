@@ -30,6 +30,8 @@ temporally reused frames, like one run of the animation.
           latency beside the plain path's per-frame latency
   batched: 32 scenes (8..2048 primitives, localsubdiv 7..10, 1024x1024)
           per step, as 32 sequential plain calls and as one CUDA-graph replay
+  swept  : swept volume over [0, 1] in 64 sub-steps, localsubdiv 9, 1280x720,
+          delta 0.005 / 0.01 / 0.02: frames/s and cell reuse
 
 --impl reference times the CPU restatement (the reference itself is WGSL
 under wgpu/Vulkan: no Vulkan driver or Rust toolchain exists on these
@@ -431,6 +433,55 @@ def batched_leg(local: int) -> dict:
         dev.close()
 
 
+# ------------------------------------------------------------------ swept leg
+SWEPT = dict(n_prims=64, seed=2, localsubdiv=9, substeps=64, deltas=(0.005, 0.01, 0.02), width=1280, height=720)
+
+
+def swept_leg(local: int) -> dict:
+    """Temporal / swept-volume stress: 64 primitives rotating about random
+    axes with an exp(-t) scale, swept volume on, [0, 1] in 64 sub-steps
+    (frame k inverts over [k/64, (k+1)/64] and traces at 1280x720),
+    localsubdiv 9, for each delta: device frames/s, cells evaluated and the
+    fraction of ambiguous cells carried over (reused) per frame."""
+    import ctypes as C
+
+    from temporalsetinversion_b200 import Device, Scene, Tape, _native as N, api, scenes
+
+    W, H, K = SWEPT["width"], SWEPT["height"], SWEPT["substeps"]
+    view = scenes.camera_look_at(WORKLOAD["eye"])
+    dev = Device(local)
+    try:
+        text = scenes.swept(SWEPT["n_prims"], SWEPT["seed"])
+        out = []
+        for delta in SWEPT["deltas"]:
+            p = api.default_params(localsubdiv=SWEPT["localsubdiv"], delta=delta, swept_volume=1)
+            s = Scene(dev, Tape.from_llvm_ir(dev, text), p, voxel_capacity=16 << 20)
+            thr = s.autotune([(k + 1) / K for k in range(3)], reps=1)["wide_threshold"]
+            ms, cells, reused, enq = 0.0, 0, 0, 0
+            for k in range(K):
+                t0, t1 = k / K, (k + 1) / K
+                st = s.invert(t1, t0)
+                u = api.make_uniforms(view, (W, H), t1)
+                ts = N.Stats()
+                N.check(dev.lib.tsi_scene_trace(s.handle, C.byref(u), None, C.byref(ts)), "tsi_scene_trace")
+                if k > 0:  # frame 0 builds the octree from scratch
+                    ms += st.device_ms + ts.device_ms
+                    cells += st.cells_evaluated
+                    reused += st.cells_reused
+                    enq += st.cells_enqueued
+            out.append({"delta": delta, "frames_per_s": (K - 1) / (ms / 1000.0), "wide_threshold": thr,
+                        "cells_evaluated_per_frame": cells / (K - 1),
+                        "reused_per_frame": reused / (K - 1),
+                        "reuse_fraction": reused / max(1, reused + enq)})
+            s.close()
+        return {"workload": "swept64_L9_720p_64substeps", "runs": out,
+                "note": "reuse_fraction = ambiguous cells kept with their subtree / (kept + re-subdivided); "
+                        "false-empty rate: tests/test_gpu_rigour.py checks swept-volume empties against float64 "
+                        "samples in directed mode"}
+    finally:
+        dev.close()
+
+
 # ------------------------------------------------------------------ GPU leg
 def run_gpu(args, rank, world, local, dist) -> None:
     import ctypes as C
@@ -583,6 +634,11 @@ def run_gpu(args, rank, world, local, dist) -> None:
             line["served"] = served_leg(local)
         except Exception as e:
             line["served"] = {"unavailable": str(e)}
+    if world == 1 and not args.no_swept:
+        try:
+            line["swept"] = swept_leg(local)
+        except Exception as e:
+            line["swept"] = {"unavailable": str(e)}
     if world == 1 and not args.no_batched:
         try:
             line["batched"] = batched_leg(local)
@@ -601,6 +657,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the served-latency leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the 32-scene batched leg")
+    ap.add_argument("--no-swept", action="store_true", help="skip the swept-volume leg")
     ap.add_argument("--small-arenas", action="store_true",
                     help="small work-item, tape and log arenas (use with --voxels 4194304 under a profiler)")
     args = ap.parse_args()

@@ -54,3 +54,31 @@ def test_directed_octree_is_rigorous(device, case):
                 case, t, len(bad), sign, tuple(int(sel[bad[0]][k]) for k in ("level", "ix", "iy", "iz")))
             checked += len(sel)
     assert checked > 100
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("delta", [0.005, 0.02])
+def test_directed_swept_volume_has_no_false_empty(device, delta):
+    """Swept volume (the union of the shape over each frame's [t0, t]):
+    every cell evaluated in the current frame and classified empty is free
+    of the surface at float64 samples of space and of its time interval."""
+    text = scenes.swept(8, 4)
+    tape = api.IR.new(text).gpu_instructions
+    p = api.default_params(localsubdiv=6, pointsample=0, rounding_mode=1, swept_volume=1, delta=delta)
+    s = Scene(device, Tape.upload(device, tape), p)
+    rng = np.random.default_rng(5)
+    checked = 0
+    for k in range(4):
+        t0, t1 = k / 16.0, (k + 1) / 16.0
+        s.invert(t1, t0)
+        cells = s.cells()
+        sel = cells[(cells["t"] == np.float32(t1)) & (cells["f"] == 1.0)]
+        if len(sel) == 0:
+            continue
+        pts = _samples(sel, rng, n_random=12)
+        for tt in np.linspace(t0, t1, 5):
+            f = evaluate(tape, pts[..., 0], pts[..., 1], pts[..., 2], np.float64(np.float32(tt)))
+            bad = np.nonzero(np.any(f <= -1e-9, axis=1))[0]
+            assert len(bad) == 0, "t in [%g, %g]: %d empty cells hold f < 0 at t=%g" % (t0, t1, len(bad), tt)
+        checked += len(sel)
+    assert checked > 50
