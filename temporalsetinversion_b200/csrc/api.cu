@@ -997,7 +997,10 @@ static tsi_status upload_ir(tsi_ctx *c, const std::vector<IrInstr> &ins, tsi_tap
       t->wslots = (uint32_t)nsl;
       t->wbundles = wt.nbundles;
       t->wvalues = wt.nvalues;
-      t->wmin_len = std::max<uint32_t>(256u, 3u * wt.nbundles);
+      // four bundle steps' worth of instructions: near the fastest of the
+      // thresholds tsi_scene_autotune tries on the tapes measured (CSG scenes
+      // of 16 to 1123 primitives, rotating swept scenes)
+      t->wmin_len = std::max<uint32_t>(64u, 4u * wt.nbundles);
       t->wcontrib = wt.ncontrib;
       for (int q = 0; q < 4; ++q) {
         t->warg_gbase[q] = wt.arg_gbase[q];
