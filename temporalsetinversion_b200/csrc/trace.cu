@@ -82,8 +82,11 @@ __device__ __noinline__ F3 tape_normal(const TraceParams &T, uint32_t lane, uint
 template <bool FAST>
 __global__ void __launch_bounds__(256, 4) trace_kernel(const TraceParams *__restrict__ Tp) {
   const TraceParams &T = *Tp;
-  const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t py = blockIdx.y * blockDim.y + threadIdx.y;
+  // a block covers a 32x8 pixel tile and each warp an 8x4 sub-tile, so the
+  // rays of a warp are close together and walk similar nodes
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t px = blockIdx.x * 32u + (warp & 3u) * 8u + (lane & 7u);
+  const uint32_t py = blockIdx.y * 8u + (warp >> 2) * 4u + (lane >> 3);
   const bool valid = px < T.W && py < T.H;
   const uint64_t pix = (uint64_t)py * T.W + px;
   const VoxelPoolDev &pool = T.pool;
@@ -279,8 +282,8 @@ cudaError_t launch_trace(const TraceParams &T, const TraceParams *Tdev, cudaStre
       if (dev >= 0 && dev < 64) set_bytes[dev] = smem;
     }
   }
-  dim3 block(16, 16);
-  dim3 grid((T.W + 15) / 16, (T.H + 15) / 16);
+  dim3 block(256);
+  dim3 grid((T.W + 31) / 32, (T.H + 7) / 8);
   if (T.code) trace_kernel<true><<<grid, block, smem, st>>>(Tdev);
   else trace_kernel<false><<<grid, block, 0, st>>>(Tdev);
   return cudaGetLastError();
