@@ -19,7 +19,8 @@ temporally reused frames, like one run of the animation.
   e2e   : the same frames through the public C API from the host: per step
           the uniforms go up, the frame's RGBA f32 pixels come back to pinned
           host memory (compute.wgsl:4687 `pixels[]`), wall clock; the copy of
-          frame i runs while frame i+1 is inverted (tsi_scene_trace_async);
+          frame i runs while frame i+1 is inverted, the host queues frames
+          without waiting (tsi_scene_invert_async, tsi_scene_trace_async);
           the fully synchronous loop is reported beside it
   roofline: the refinement kernel's algorithmic FP32 operations (opcost.h
           table, per executed interval instruction) against the nominal
@@ -559,15 +560,17 @@ def run_gpu(args, rank, world, local, dist) -> None:
         t0 = time.perf_counter()
         for i in range(e2e_steps):
             t = frame_time(i, F)
-            st = N.Stats()
-            N.check(lib.tsi_scene_invert(scene.handle, t, math.nan, C.byref(st)), "tsi_scene_invert")
             if asynchronous:
+                N.check(lib.tsi_scene_invert_async(scene.handle, t, math.nan), "tsi_scene_invert_async")
                 N.check(lib.tsi_scene_trace_async(scene.handle, C.byref(unis[i]), C.byref(imgs[i & 1])),
                         "tsi_scene_trace_async")
             else:
+                st = N.Stats()
+                N.check(lib.tsi_scene_invert(scene.handle, t, math.nan, C.byref(st)), "tsi_scene_invert")
                 N.check(lib.tsi_scene_trace(scene.handle, C.byref(unis[i]), C.byref(imgs[0]), None),
                         "tsi_scene_trace")
         if asynchronous:
+            N.check(lib.tsi_scene_invert_wait(scene.handle, None), "tsi_scene_invert_wait")
             N.check(lib.tsi_scene_trace_wait(scene.handle), "tsi_scene_trace_wait")
         return reduce_max(dist, time.perf_counter() - t0)
 
@@ -597,7 +600,9 @@ def run_gpu(args, rank, world, local, dist) -> None:
                    "l2": "flushed between steps (256 MB write outside the per-step events)"},
         "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": C.sizeof(N.Uniforms) + 160,
                 "d2h_bytes_per_step": W * H * 16 + C.sizeof(N.Stats),
-                "readback": "frame i's copy to pinned host memory overlaps frame i+1's inversion",
+                "readback": "frames queued without waiting (tsi_scene_invert_async, tsi_scene_trace_async); "
+                            "frame i's copy to pinned host memory overlaps frame i+1's inversion; errors checked "
+                            "at the end (tsi_scene_invert_wait)",
                 "synchronous_value": e2e_sync_value},
         "roofline": {"kernel": "refine_kernel (interval tape interpreter)", "bound": "fp32",
                      "achieved": achieved_gops / 1000.0, "peak": PEAK_FP32_NOMINAL_TOPS / 1000.0, "unit": "TOP/s",

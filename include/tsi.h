@@ -246,6 +246,16 @@ TSI_API tsi_status tsi_scene_reset(tsi_scene *scene);
  * t0_or_nan: start of the swept interval (NaN = time - swept_dt). */
 TSI_API tsi_status tsi_scene_invert(tsi_scene *scene, float time, float t0_or_nan,
                                     tsi_stats *stats);
+/* tsi_scene_invert without waiting: the frame is queued on the context's
+ * stream and the call returns at once, so the host can queue the frame's
+ * trace (tsi_scene_trace_async) and the next frames while the GPU works.
+ * tsi_scene_invert_wait waits for everything queued and returns an error
+ * status if any inversion queued this way since the last wait hit a device
+ * limit (voxel pool, work list, log arena), and, when stats is not NULL,
+ * the counters and device time of the last inversion queued.  Plain
+ * inversions in between report their own errors. */
+TSI_API tsi_status tsi_scene_invert_async(tsi_scene *scene, float time, float t0_or_nan);
+TSI_API tsi_status tsi_scene_invert_wait(tsi_scene *scene, tsi_stats *stats);
 /* One dispatch of `rt_main` (main.rs:649-656).  `out` may be NULL to keep
  * the frame on the device only (see tsi_scene_image_device). */
 TSI_API tsi_status tsi_scene_trace(tsi_scene *scene, const tsi_uniforms *u, tsi_image *out,

@@ -217,6 +217,8 @@ extern "C" {
                                reverse: i32, out: *mut f32) -> tsi_status;
     pub fn tsi_scene_image_device(s: *mut tsi_scene, out: *mut tsi_image_device) -> tsi_status;
     pub fn tsi_scene_image_copy(s: *mut tsi_scene, out: *mut tsi_image) -> tsi_status;
+    pub fn tsi_scene_invert_async(s: *mut tsi_scene, time: f32, t0_or_nan: f32) -> tsi_status;
+    pub fn tsi_scene_invert_wait(s: *mut tsi_scene, stats: *mut tsi_stats) -> tsi_status;
     pub fn tsi_scene_trace_async(s: *mut tsi_scene, u: *const Uniforms, out: *mut tsi_image) -> tsi_status;
     pub fn tsi_scene_trace_wait(s: *mut tsi_scene) -> tsi_status;
     pub fn tsi_tape_wide_threshold(t: *const tsi_tape) -> u32;

@@ -144,6 +144,8 @@ SIGNATURES = {
     "tsi_batch_graph_create": (i32, [C.c_void_p, P(Request), u32, P(C.c_void_p)]),
     "tsi_scene_image_copy": (i32, [C.c_void_p, P(Image)]),
     "tsi_scene_trace_async": (i32, [C.c_void_p, P(Uniforms), P(Image)]),
+    "tsi_scene_invert_async": (i32, [C.c_void_p, f32, f32]),
+    "tsi_scene_invert_wait": (i32, [C.c_void_p, P(Stats)]),
     "tsi_scene_trace_wait": (i32, [C.c_void_p]),
     "tsi_batch_graph_launch": (i32, [C.c_void_p]),
     "tsi_batch_graph_wait": (i32, [C.c_void_p, P(Stats)]),

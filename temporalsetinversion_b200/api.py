@@ -231,6 +231,17 @@ class Scene:
         N.check(self.device.lib.tsi_scene_invert(self.handle, float(time), float(t0), C.byref(st)), "tsi_scene_invert")
         return st
 
+    def invert_async(self, time: float, t0: float = math.nan) -> None:
+        """tsi_scene_invert_async: queue the frame's inversion and return."""
+        N.check(self.device.lib.tsi_scene_invert_async(self.handle, float(time), float(t0)), "tsi_scene_invert_async")
+
+    def invert_wait(self) -> N.Stats:
+        """tsi_scene_invert_wait: wait for the queued inversions; raises on a
+        device error in any of them; counters of the last one."""
+        st = N.Stats()
+        N.check(self.device.lib.tsi_scene_invert_wait(self.handle, C.byref(st)), "tsi_scene_invert_wait")
+        return st
+
     def trace(self, uniforms: N.Uniforms, rgba: bool = True, depth: bool = True, normal: bool = True) -> dict:
         w, h = uniforms.resolution[0], uniforms.resolution[1]
         out = {}

@@ -152,6 +152,11 @@ struct tsi_ctx {
   unsigned long long *d_log_used = nullptr;
   uint64_t log_overflow_cap = 0;
   uint32_t *d_error = nullptr;
+  uint32_t *d_error_sticky = nullptr;  // error words of asynchronous inversions since the last wait
+  // the upload of h_scenes/h_recs of the last launch sequence: the host may
+  // rewrite them only after it ran (inversions queued without waiting)
+  cudaEvent_t launch_up = nullptr;
+  bool launch_up_pending = false;
   unsigned long long *d_stats = nullptr;
   unsigned long long *d_level_stats = nullptr;
   unsigned long long *d_visits = nullptr;
@@ -187,7 +192,7 @@ tsi_status set_err(tsi_status s, const std::string &msg) {
   return s;
 }
 
-LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes, size_t dyn_smem) {
+LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes, size_t dyn_smem, bool sticky) {
   LaunchParams P{};
   P.scenes = c->d_scenes;
   P.n_scenes = n_scenes;
@@ -211,6 +216,7 @@ LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes, size_t dyn_smem) {
   P.wscratch = c->d_wscratch;
   P.wscratch_stride = c->wscratch_stride;
   P.dyn_smem = (uint32_t)dyn_smem;
+  P.error_sticky = sticky ? c->d_error_sticky : nullptr;
   for (int q = 0; q < 2; ++q) {
     P.cell_info[q] = c->d_cell_info[q];
     P.cell_bits[q] = c->d_cell_bits[q];
@@ -400,12 +406,20 @@ tsi_status plan_frame(tsi_ctx *c, tsi_scene *const *scenes, uint32_t n, FramePla
 }
 
 // One frame of set inversion for n scenes, all levels in one launch sequence.
-tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *times, const float *t0s, uint32_t n) {
+bool capturing(tsi_ctx *c);
+
+tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *times, const float *t0s, uint32_t n,
+                          bool sticky = false) {
   if (n == 0) return TSI_OK;
   if (n > c->max_scenes) return set_err(TSI_ERR_INVALID_ARGUMENT, "too many scenes in one launch");
   FramePlan fp;
   tsi_status pst = plan_frame(c, scenes, n, fp);
   if (pst != TSI_OK) return pst;
+  const bool cap = capturing(c);
+  if (c->launch_up_pending && !cap) {
+    CK(cudaEventSynchronize(c->launch_up));
+    c->launch_up_pending = false;
+  }
   for (uint32_t i = 0; i < n; ++i)
     fill_launch(scenes[i], i, times[i], t0s[i], fp.global[i] != 0, c->h_scenes[i], c->h_recs[i]);
   const uint32_t lmax = fp.lmax, rcap = fp.rcap;
@@ -413,11 +427,15 @@ tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *tim
   const int grid = fp.grid;
   CK(cudaMemcpyAsync(c->d_scenes, c->h_scenes, n * sizeof(SceneLaunch), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_recs, c->h_recs, n * sizeof(TapeRec), cudaMemcpyHostToDevice, c->stream));
+  if (!cap) {
+    CK(cudaEventRecord(c->launch_up, c->stream));
+    c->launch_up_pending = true;
+  }
   CK(cudaMemsetAsync(c->d_error, 0, sizeof(uint32_t), c->stream));
   CK(cudaMemsetAsync(c->d_stats, 0, ST_COUNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(c->d_level_stats, 0, (TSI_MAX_LEVELS + 1) * ST_COUNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(c->d_log_used, 0, (TSI_MAX_LEVELS + 1) * sizeof(unsigned long long), c->stream));
-  const LaunchParams P = make_params(c, n, fp.smem);
+  const LaunchParams P = make_params(c, n, fp.smem, sticky);
   CK(launch_frame_begin(P, c->stream));
   const bool prof = c->profile_levels && c->level_events.size() >= lmax + 1;
   for (uint32_t level = 0; level < lmax; ++level) {
@@ -871,6 +889,8 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   CKC(dalloc(&c->d_log_overflow, c->log_overflow_cap));
   CKC(dalloc(&c->d_log_used, TSI_MAX_LEVELS + 1));
   CKC(dalloc(&c->d_error, 1));
+  CKC(dalloc(&c->d_error_sticky, 1));
+  CKC(cudaMemset(c->d_error_sticky, 0, sizeof(uint32_t)));
   CKC(dalloc(&c->d_stats, ST_COUNT));
   CKC(dalloc(&c->d_level_stats, (TSI_MAX_LEVELS + 1) * ST_COUNT));
   if (getenv("TSI_PROFILE_LEVELS")) {
@@ -881,6 +901,7 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   CKC(dalloc(&c->d_visits, 1));
   CKC(cudaMallocHost((void **)&c->h_rb, sizeof(Readback)));
   CKC(cudaEventCreate(&c->ev0));
+  CKC(cudaEventCreateWithFlags(&c->launch_up, cudaEventDisableTiming));
   CKC(cudaEventCreate(&c->ev1));
   CKC(cudaEventCreate(&c->ev2));
   CKC(cudaMemsetAsync(c->d_item_count, 0, (TSI_MAX_LEVELS + 1) * sizeof(uint32_t), c->stream));
@@ -922,6 +943,7 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   cudaFree(c->d_log_overflow);
   cudaFree(c->d_log_used);
   cudaFree(c->d_error);
+  cudaFree(c->d_error_sticky);
   cudaFree(c->d_stats);
   cudaFree(c->d_level_stats);
   for (auto &ev : c->level_events) cudaEventDestroy(ev);
@@ -929,6 +951,7 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   cudaFree(c->d_scratch);
   cudaFreeHost(c->h_rb);
   if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->launch_up) cudaEventDestroy(c->launch_up);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1257,6 +1280,37 @@ TSI_API tsi_status tsi_scene_invert(tsi_scene *s, float time, float t0_or_nan, t
     stats->device_ms = ms;
   }
   return status_from_error_bits(c->h_rb->error);
+}
+
+TSI_API tsi_status tsi_scene_invert_async(tsi_scene *s, float time, float t0_or_nan) {
+  if (!s) return set_err(TSI_ERR_INVALID_ARGUMENT, "null scene");
+  tsi_ctx *c = s->ctx;
+  CK(cudaSetDevice(c->device));
+  CK(cudaEventRecord(c->ev0, c->stream));
+  tsi_status st = enqueue_invert(c, &s, &time, &t0_or_nan, 1, true);
+  if (st != TSI_OK) return st;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  return enqueue_readback(c);
+}
+
+TSI_API tsi_status tsi_scene_invert_wait(tsi_scene *s, tsi_stats *stats) {
+  if (!s) return set_err(TSI_ERR_INVALID_ARGUMENT, "null scene");
+  tsi_ctx *c = s->ctx;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  uint32_t sticky = 0;
+  CK(cudaMemcpy(&sticky, c->d_error_sticky, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  CK(cudaMemset(c->d_error_sticky, 0, sizeof(uint32_t)));
+  if (stats) {
+    SceneCounters ctr;
+    const tsi_status st = read_counters(s, ctr);
+    if (st != TSI_OK) return st;
+    fill_stats(*c->h_rb, stats, (uint64_t)ctr.live_bricks * 8u);
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    stats->device_ms = ms;
+  }
+  return status_from_error_bits(sticky);
 }
 
 TSI_API tsi_status tsi_scene_trace(tsi_scene *s, const tsi_uniforms *u, tsi_image *out, tsi_stats *stats) {

@@ -173,6 +173,8 @@ struct LaunchParams {
   unsigned char *wscratch;               // [grid][wscratch_stride]: wide cell working sets
   unsigned long long wscratch_stride;    // of tapes with WideDev::global set
   uint32_t dyn_smem;                     // dynamic shared memory of the launch, bytes
+  uint32_t *error_sticky;                // or-ed with the frame's error word at frame end
+                                         // (asynchronous inversions), or null
   uint32_t *cell_bits[2];  // [witem_cap * 8][bm_words] per level parity
   uint32_t item_cap;
   uint32_t dealloc_cap;

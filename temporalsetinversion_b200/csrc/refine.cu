@@ -1428,6 +1428,7 @@ __global__ void frame_end_kernel(LaunchParams P) {
   SceneCounters *c = S.ctr;
   __shared__ int32_t fc0;
   __shared__ uint32_t np;
+  if (s == 0 && threadIdx.x == 0 && P.error_sticky) atomicOr(P.error_sticky, *P.error);
   if (threadIdx.x == 0) {
     fc0 = max(c->free_count, 0);
     np = min(c->pending_count, S.pool.cap_bricks);

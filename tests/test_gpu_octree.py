@@ -16,7 +16,7 @@ import pytest
 import oracle
 from conftest import assert_cells_equal
 from golden.make_golden import load_tape
-from temporalsetinversion_b200 import Scene, Tape, api, scenes
+from temporalsetinversion_b200 import Scene, Tape, _native as N, api, scenes
 
 COUNTERS = ["parents_expanded", "cells_evaluated", "cells_reverse", "cells_skipped", "cells_ambiguous",
             "cells_empty", "cells_full", "cells_enqueued", "cells_reused"]
@@ -148,3 +148,43 @@ def test_snapshot_restore_continues_exactly(device):
     other = Scene(device, Tape.upload(device, tape), api.default_params(**dict(params, delta=0.02)))
     with pytest.raises(Exception):
         other.restore(blob)  # other parameters
+
+
+@pytest.mark.gpu
+def test_async_inversions_equal_plain(device):
+    """Frames queued without waiting (inversion and traced frame) give the
+    plain calls' octrees, counters and frames."""
+    src, params, times = CASES["csg64_reuse"]
+    tape = tape_of(src)
+    p = api.default_params(**params)
+    a = Scene(device, Tape.upload(device, tape), p)
+    b = Scene(device, Tape.upload(device, tape), p)
+    cam = scenes.camera_look_at((0.4, 0.8, 2.4))
+    frames = [np.zeros((48, 64, 4), np.float32) for _ in times]
+    want = []
+    for t, buf in zip(times, frames):
+        a.invert_async(t)
+        a.trace_async(api.make_uniforms(cam, (64, 48), t), buf)
+        sb = b.invert(t)
+        want.append(b.trace(api.make_uniforms(cam, (64, 48), t), depth=False, normal=False)["rgba"])
+    sa = a.invert_wait()
+    a.trace_wait()
+    for k in COUNTERS:
+        assert getattr(sa, k) == getattr(sb, k), k
+    assert_cells_equal(a.cells(), b.cells())
+    for got, exp in zip(frames, want):
+        assert np.array_equal(got, exp)
+
+
+@pytest.mark.gpu
+def test_async_inversion_reports_pool_exhaustion(device):
+    tape = Tape.from_llvm_ir(device, scenes.spheres16(0))
+    tiny = Scene(device, tape, api.default_params(localsubdiv=7), voxel_capacity=64)
+    tiny.invert_async(0.0)
+    tiny.invert_async(1 / 60)
+    with pytest.raises(N.TsiError) as e:
+        tiny.invert_wait()
+    assert e.value.status == 4  # TSI_ERR_OOM
+    ok = Scene(device, tape, api.default_params(localsubdiv=5))
+    ok.invert_async(0.0)
+    assert ok.invert_wait().cells_evaluated > 0
