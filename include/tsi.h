@@ -427,6 +427,12 @@ TSI_API tsi_status tsi_tape_eval_boxes_static(const tsi_tape *tape, uint32_t n, 
                                               void *cuda_stream);
 TSI_API uint64_t tsi_static_scratch_bytes(void);
 
+/* Host only.  The frame dump of main.rs:692-715 (save_frames_to_disk):
+ * rt_main's f32 RGBA pixels converted to 8-bit RGBA as its image crate does
+ * (each channel clamped to [0, 1], times 255, rounded to nearest, halves
+ * away from zero; NaN gives 0), ready for a PNG encoder. */
+TSI_API void tsi_rgba8_from_frame(const float *rgba, uint64_t n_pixels, uint8_t *out);
+
 /* ---------------- diagnostics (tests and tools) ---------------- */
 /* Message of the last failing call on this thread. */
 TSI_API const char *tsi_last_error(void);

@@ -248,6 +248,7 @@ extern "C" {
     pub fn tsi_tape_eval_boxes_static(t: *const tsi_tape, n: u32, boxes_dev: *const f32, rounding_mode: i32,
                                       reverse: i32, out_dev: *mut f32, stream: *mut c_void) -> tsi_status;
     pub fn tsi_static_scratch_bytes() -> u64;
+    pub fn tsi_rgba8_from_frame(rgba: *const f32, n_pixels: u64, out: *mut u8);
 }
 
 /// Convenience used by `State::compute`: one frame, returns device ms.

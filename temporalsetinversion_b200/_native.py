@@ -145,6 +145,7 @@ SIGNATURES = {
     "tsi_scene_image_copy": (i32, [C.c_void_p, P(Image)]),
     "tsi_scene_trace_async": (i32, [C.c_void_p, P(Uniforms), P(Image)]),
     "tsi_scene_invert_async": (i32, [C.c_void_p, f32, f32]),
+    "tsi_rgba8_from_frame": (None, [P(f32), u64, P(C.c_uint8)]),
     "tsi_scene_invert_wait": (i32, [C.c_void_p, P(Stats)]),
     "tsi_scene_trace_wait": (i32, [C.c_void_p]),
     "tsi_batch_graph_launch": (i32, [C.c_void_p]),

@@ -458,6 +458,33 @@ class Server:
         self.close()
 
 
+def rgba8(rgba: np.ndarray) -> np.ndarray:
+    """tsi_rgba8_from_frame: an (H, W, 4) float32 frame as 8-bit RGBA."""
+    rgba = np.ascontiguousarray(rgba, dtype=np.float32)
+    out = np.empty(rgba.shape, dtype=np.uint8)
+    N.load().tsi_rgba8_from_frame(_fptr(rgba), rgba.size // 4, out.ctypes.data_as(C.POINTER(C.c_uint8)))
+    return out
+
+
+def save_png(path, rgba: np.ndarray) -> None:
+    """The reference's frame dump (main.rs:692-715): an (H, W, 4) float32
+    frame written as an 8-bit RGBA PNG (no compression filters)."""
+    import struct
+    import zlib
+
+    px = rgba8(rgba)
+    h, w = px.shape[0], px.shape[1]
+    raw = b"".join(b"\x00" + px[y].tobytes() for y in range(h))
+
+    def chunk(kind: bytes, data: bytes) -> bytes:
+        return struct.pack(">I", len(data)) + kind + data + struct.pack(">I", zlib.crc32(kind + data) & 0xFFFFFFFF)
+
+    png = (b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 6, 0, 0, 0)) +
+           chunk(b"IDAT", zlib.compress(raw, 6)) + chunk(b"IEND", b""))
+    with open(path, "wb") as f:
+        f.write(png)
+
+
 def batch_autotune(device: Device, requests: list, frames: int = 3) -> dict:
     """tsi_batch_autotune: the wide-threshold multiplier (1, 2, 4 or 8) that
     runs these scenes fastest together.  requests: list of (scene, time).

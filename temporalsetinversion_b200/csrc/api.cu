@@ -710,6 +710,15 @@ TSI_API const char *tsi_status_string(tsi_status s) {
 
 TSI_API const char *tsi_last_error(void) { return g_last_error.c_str(); }
 
+TSI_API void tsi_rgba8_from_frame(const float *rgba, uint64_t n_pixels, uint8_t *out) {
+  if (!rgba || !out) return;
+  for (uint64_t i = 0; i < n_pixels * 4; ++i) {
+    const float v = rgba[i];
+    const float c = v > 0.0f ? (v < 1.0f ? v : 1.0f) : 0.0f;  // NaN compares false: 0
+    out[i] = (uint8_t)roundf(c * 255.0f);
+  }
+}
+
 TSI_API void tsi_default_params(tsi_params *p) {  // compute.wgsl:3494-3511, ir.rs:343-347
   if (!p) return;
   memset(p, 0, sizeof(*p));

@@ -183,3 +183,21 @@ def test_packed_handlers_and_flags():
     assert h == [33, 9, 20, 1]  # H_BAD_FI, H_MOD_II, H_ATAN2_IF, H_COPY
     assert (words[0] >> 6) & 1 == 1  # x used once
     assert struct.unpack("<f", struct.pack("<I", words[5]))[0] == 2.0
+
+
+def test_frame_dump_png(tmp_path):
+    """rt_main's f32 frame as the reference's 8-bit PNG dump (main.rs:692-715):
+    clamp to [0, 1], scale by 255, round; the file decodes back to it."""
+    import zlib
+
+    rgba = np.array([[[0.0, 1.0, 0.5, 2.0], [-1.0, np.nan, 0.25, 1.0 / 510.0]]], np.float32)
+    px = api.rgba8(rgba)
+    assert px.tolist() == [[[0, 255, 128, 255], [0, 0, 64, 1]]]
+    path = tmp_path / "frame.png"
+    api.save_png(path, rgba)
+    data = path.read_bytes()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    i = data.index(b"IDAT")
+    n = struct.unpack(">I", data[i - 4:i])[0]
+    raw = zlib.decompress(data[i + 4:i + 4 + n])
+    assert raw == b"\x00" + px[0].tobytes()
