@@ -182,6 +182,9 @@ typedef struct tsi_device_opts {
   uint32_t max_scenes_per_launch; /* batch width (0 = default 64) */
   uint32_t wide_smem_bytes;     /* shared memory a wide cell's working set may take; larger ones run
                                  * from global scratch (0 = what keeps the narrow path's occupancy) */
+  uint64_t hbm_budget_bytes;    /* device bytes the context's scenes may hold together (voxel pools
+                                 * and frame buffers); a scene or frame size beyond it is refused
+                                 * with TSI_ERR_OOM (0 = no limit) */
 } tsi_device_opts;
 
 typedef struct tsi_ctx tsi_ctx;
@@ -323,6 +326,12 @@ TSI_API tsi_status tsi_scene_snapshot(tsi_scene *scene, void *host, uint64_t cap
 TSI_API tsi_status tsi_scene_restore(tsi_scene *scene, const void *host, uint64_t bytes);
 TSI_API tsi_status tsi_scene_get_params(const tsi_scene *scene, tsi_params *out);
 TSI_API uint64_t tsi_scene_device_bytes(const tsi_scene *scene);
+/* No counterpart in the reference: the device bytes all scenes of the
+ * context hold, the figure tsi_device_opts.hbm_budget_bytes admits
+ * against.  A server under a memory budget evicts an idle scene with
+ * tsi_scene_snapshot + tsi_scene_destroy and readmits it with
+ * tsi_scene_create + tsi_scene_restore. */
+TSI_API uint64_t tsi_scenes_device_bytes(const tsi_ctx *ctx);
 
 /* ---------------- batched form ---------------- */
 typedef struct tsi_request {

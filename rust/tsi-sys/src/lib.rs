@@ -100,6 +100,7 @@ pub struct tsi_device_opts {
     pub watchdog_iters: u32,
     pub max_scenes_per_launch: u32,
     pub wide_smem_bytes: u32,
+    pub hbm_budget_bytes: u64,
 }
 
 #[repr(C)]
@@ -232,6 +233,7 @@ extern "C" {
     pub fn tsi_scene_restore(s: *mut tsi_scene, host: *const c_void, bytes: u64) -> tsi_status;
     pub fn tsi_scene_get_params(s: *const tsi_scene, out: *mut tsi_params) -> tsi_status;
     pub fn tsi_scene_device_bytes(s: *const tsi_scene) -> u64;
+    pub fn tsi_scenes_device_bytes(ctx: *const tsi_ctx) -> u64;
     pub fn tsi_batch_run(ctx: *mut tsi_ctx, reqs: *mut tsi_request, n: u32) -> tsi_status;
     pub fn tsi_batch_autotune(ctx: *mut tsi_ctx, reqs: *const tsi_request, n: u32, frames: u32,
                               out: *mut tsi_autotune_result) -> tsi_status;

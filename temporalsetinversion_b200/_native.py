@@ -96,7 +96,8 @@ class ImageDevice(C.Structure):
 
 class DeviceOpts(C.Structure):
     _fields_ = [("device", i32), ("work_item_capacity", u64), ("tape_arena_words", u64), ("log_arena_bytes", u64),
-                ("watchdog_iters", u32), ("max_scenes_per_launch", u32), ("wide_smem_bytes", u32)]
+                ("watchdog_iters", u32), ("max_scenes_per_launch", u32), ("wide_smem_bytes", u32),
+                ("hbm_budget_bytes", u64)]
 
 
 class TapeInfo(C.Structure):
@@ -146,6 +147,7 @@ SIGNATURES = {
     "tsi_scene_trace_async": (i32, [C.c_void_p, P(Uniforms), P(Image)]),
     "tsi_scene_invert_async": (i32, [C.c_void_p, f32, f32]),
     "tsi_rgba8_from_frame": (None, [P(f32), u64, P(C.c_uint8)]),
+    "tsi_scenes_device_bytes": (u64, [C.c_void_p]),
     "tsi_scene_invert_wait": (i32, [C.c_void_p, P(Stats)]),
     "tsi_scene_trace_wait": (i32, [C.c_void_p]),
     "tsi_batch_graph_launch": (i32, [C.c_void_p]),

@@ -94,10 +94,11 @@ class Device:
     """A tsi_ctx on one CUDA device (fails with TSI_ERR_NO_DEVICE without one)."""
 
     def __init__(self, device: int = 0, work_item_capacity: int = 0, tape_arena_words: int = 0,
-                 log_arena_bytes: int = 0, max_scenes_per_launch: int = 0, wide_smem_bytes: int = 0):
+                 log_arena_bytes: int = 0, max_scenes_per_launch: int = 0, wide_smem_bytes: int = 0,
+                 hbm_budget_bytes: int = 0):
         self.lib = N.load()
         opts = N.DeviceOpts(device, work_item_capacity, tape_arena_words, log_arena_bytes, 0, max_scenes_per_launch,
-                            wide_smem_bytes)
+                            wide_smem_bytes, hbm_budget_bytes)
         h = C.c_void_p()
         N.check(self.lib.tsi_create(C.byref(opts), C.byref(h)), "tsi_create")
         self.handle = h
@@ -124,6 +125,10 @@ class Device:
             self.close()
         except Exception:
             pass
+
+    def scenes_bytes(self) -> int:
+        """Device bytes the scenes of this device hold (tsi_scenes_device_bytes)."""
+        return int(self.lib.tsi_scenes_device_bytes(self.handle))
 
     def synchronize(self) -> None:
         N.check(self.lib.tsi_synchronize(self.handle), "tsi_synchronize")
@@ -302,6 +307,10 @@ class Scene:
         img = N.Image(width, height, _fptr(out["rgba"]), _fptr(out["depth"]), _fptr(out["normal"]))
         N.check(self.device.lib.tsi_scene_image_copy(self.handle, C.byref(img)), "tsi_scene_image_copy")
         return out
+
+    def device_bytes(self) -> int:
+        """Device bytes of this scene's pool and frame buffers."""
+        return int(self.device.lib.tsi_scene_device_bytes(self.handle))
 
     def snapshot(self) -> bytes:
         """The resident octree as a host blob (tsi_scene_snapshot)."""

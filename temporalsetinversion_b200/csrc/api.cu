@@ -140,6 +140,7 @@ struct tsi_ctx {
   unsigned char *d_wscratch = nullptr;
   size_t wscratch_bytes = 0, wscratch_stride = 0;
   size_t wide_smem_bytes = 0;  // shared-memory budget of a wide cell (0: keep the narrow occupancy)
+  uint64_t hbm_budget = 0;     // bytes the scenes may hold together (0: no limit)
 
   uint2 *d_dealloc[2] = {nullptr, nullptr};
   uint32_t dealloc_cap = 0;
@@ -573,8 +574,18 @@ tsi_status drain_copy(tsi_scene *s) {
   return TSI_OK;
 }
 
+// Device bytes of all scenes of the context (pools and frame buffers).
+uint64_t scenes_bytes(const tsi_ctx *c) {
+  uint64_t b = 0;
+  for (const tsi_scene *s : c->scenes) b += s->bytes;
+  return b;
+}
+
 tsi_status ensure_image(tsi_scene *s, uint32_t w, uint32_t h) {
   if (s->img_w == w && s->img_h == h && s->d_rgba) return TSI_OK;
+  const uint64_t old_img = (uint64_t)s->img_w * s->img_h * 32u, new_img = (uint64_t)w * h * 32u;
+  if (s->ctx->hbm_budget && new_img > old_img && scenes_bytes(s->ctx) + (new_img - old_img) > s->ctx->hbm_budget)
+    return set_err(TSI_ERR_OOM, "frame buffers would exceed the context's HBM budget");
   if (s->copy_pending) {
     const tsi_status st = drain_copy(s);
     if (st != TSI_OK) return st;
@@ -591,6 +602,7 @@ tsi_status ensure_image(tsi_scene *s, uint32_t w, uint32_t h) {
   CK(dalloc(&s->d_normal, np * 3));
   s->img_w = w;
   s->img_h = h;
+  s->bytes = s->bytes - old_img + new_img;
   return TSI_OK;
 }
 
@@ -859,6 +871,7 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   CKC(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
   c->max_scenes = (opts && opts->max_scenes_per_launch) ? opts->max_scenes_per_launch : 64u;
   c->wide_smem_bytes = opts ? opts->wide_smem_bytes : 0u;
+  c->hbm_budget = opts ? opts->hbm_budget_bytes : 0u;
   c->item_cap = (opts && opts->work_item_capacity) ? (uint32_t)opts->work_item_capacity : (4u << 20);
   c->dealloc_cap = c->item_cap * 2u;
   c->rec_cap = c->item_cap * 2u;
@@ -1189,6 +1202,12 @@ TSI_API tsi_status tsi_scene_create(tsi_ctx *c, const tsi_tape *tape, const tsi_
   uint64_t bricks = (voxel_capacity + 7) / 8;
   if (bricks < 2) bricks = 2;
   if (bricks > 0x1fffffffull) return set_err(TSI_ERR_INVALID_ARGUMENT, "voxel capacity too large");
+  {
+    const uint64_t nv = (uint64_t)bricks * 8;
+    const uint64_t need = nv * (16 + 8 + 4 * 5 + 16) + (uint64_t)bricks * 8 + sizeof(SceneCounters);
+    if (c->hbm_budget && scenes_bytes(c) + need > c->hbm_budget)
+      return set_err(TSI_ERR_OOM, "scene would exceed the context's HBM budget");
+  }
   tsi_scene *s = new tsi_scene();
   s->ctx = c;
   c->scenes.insert(s);
@@ -1637,6 +1656,8 @@ TSI_API tsi_status tsi_scene_get_params(const tsi_scene *s, tsi_params *out) {
 }
 
 TSI_API uint64_t tsi_scene_device_bytes(const tsi_scene *s) { return s ? s->bytes : 0; }
+
+TSI_API uint64_t tsi_scenes_device_bytes(const tsi_ctx *c) { return c ? scenes_bytes(c) : 0; }
 
 static tsi_status batch_enqueue(tsi_ctx *c, tsi_request *reqs, uint32_t n) {
   std::vector<tsi_scene *> sc(n);

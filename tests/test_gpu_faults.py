@@ -9,6 +9,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from conftest import assert_cells_equal
 from temporalsetinversion_b200 import Device, Scene, Tape, _native as N, api, scenes
 
 
@@ -120,3 +121,42 @@ def test_log_arena_exhaustion_is_reported():
         assert e.value.status == 4
         s2 = Scene(dev, Tape.from_llvm_ir(dev, scenes.spheres16(0)), api.default_params(localsubdiv=4))
         assert s2.invert(0.0).cells_evaluated > 0
+
+
+@pytest.mark.gpu
+def test_hbm_budget_admits_scenes_and_frames():
+    """Scenes and frame buffers are admitted against the context's HBM
+    budget; an idle scene evicted to host memory (snapshot, destroy) and
+    readmitted (create, restore) continues frame for frame."""
+    text = scenes.spheres16(0)
+    p = api.default_params(localsubdiv=6)
+    with Device() as probe:
+        s = Scene(probe, Tape.from_llvm_ir(probe, text), p, voxel_capacity=1 << 16)
+        per = probe.scenes_bytes()
+        assert per == s.device_bytes() > 0
+        s.close()
+    with Device(hbm_budget_bytes=2 * per + per // 2) as dev:
+        tape = Tape.from_llvm_ir(dev, text)
+        a = Scene(dev, tape, p, voxel_capacity=1 << 16)
+        b = Scene(dev, tape, p, voxel_capacity=1 << 16)
+        assert dev.scenes_bytes() == 2 * per
+        with pytest.raises(N.TsiError) as e:
+            Scene(dev, tape, p, voxel_capacity=1 << 16)
+        assert e.value.status == 4  # TSI_ERR_OOM
+        a.invert(0.0)
+        with pytest.raises(N.TsiError) as e:  # a frame buffer of ~4 scenes' size does not fit
+            a.trace(api.make_uniforms(scenes.camera_look_at((0.3, 0.6, 2.5)), (2048, 2048), 0.0))
+        assert e.value.status == 4
+        # evict a (its octree to the host), admit c, readmit a
+        a.invert(1 / 60)
+        blob = a.snapshot()
+        a.close()
+        c = Scene(dev, tape, p, voxel_capacity=1 << 16)
+        c.close()
+        a2 = Scene(dev, tape, p, voxel_capacity=1 << 16)
+        a2.restore(blob)
+        st = a2.invert(2 / 60)
+        for t in (0.0, 1 / 60, 2 / 60):  # b lived through the same frames resident
+            sb = b.invert(t)
+        assert st.error_flags == 0 and st.cells_evaluated == sb.cells_evaluated
+        assert_cells_equal(a2.cells(), b.cells())
