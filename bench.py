@@ -327,6 +327,120 @@ def served_leg(local: int) -> dict:
         dev.close()
 
 
+# ------------------------------------------------------------------ served mix leg
+SERVED_MIX = dict(pool=64, rates_rps=(200.0, 800.0), seconds=1.5, seed=2000, sweep_fraction=0.2,
+                  continue_fraction=0.7, levels=(8, 9, 10), resolutions=((512, 512), (1280, 720), (1920, 1080)))
+
+
+def served_mix_leg(local: int) -> dict:
+    """Requests drawn as in the served configuration: a pool of 64 seeded
+    256-primitive scenes with localsubdiv uniform in {8, 9, 10}, a fifth of
+    them swept-volume scenes whose requests are [t - 1/60, t] sweeps; each
+    request continues its scene at t + 1/60 with probability 0.7, else
+    jumps to a random t, with a random camera on the radius-2.5 sphere and a
+    resolution drawn from 512x512, 1280x720, 1920x1080.  Poisson arrivals
+    through the serving layer at each rate, against the same request
+    sequence run one synchronous plain call pair at a time."""
+    import threading
+
+    from temporalsetinversion_b200 import Device, Scene, Server, Tape, api, scenes
+
+    cfg = SERVED_MIX
+    rng = np.random.default_rng(cfg["seed"])
+    dev = Device(local)
+    try:
+        pool = []
+        for k in range(cfg["pool"]):
+            swept = rng.uniform() < cfg["sweep_fraction"]
+            L = int(rng.choice(cfg["levels"]))
+            p = api.default_params(localsubdiv=L, delta=WORKLOAD["delta"], swept_volume=int(swept),
+                                   lipschitz_corrected=WORKLOAD["lipschitz_corrected"], pointsample=1)
+            pool.append(Scene(dev, Tape.from_llvm_ir(dev, scenes.csg(256, 100 + k)), p))
+        t_now = [float(rng.uniform(0.0, 1.0)) for _ in pool]
+        # each scene's first frame (its octree from scratch) at the largest
+        # resolution, so the frame buffers hold every later size
+        big = max(cfg["resolutions"], key=lambda r: r[0] * r[1])
+        for s, t in zip(pool, t_now):
+            s.invert(t, t - 1.0 / 60.0 if s.params.swept_volume == 1 else math.nan)
+            s.trace(api.make_uniforms(scenes.camera_on_sphere(rng, 2.5), big, t), rgba=False, depth=False,
+                    normal=False)
+
+        def draw(n):
+            out = []
+            for _ in range(n):
+                j = int(rng.integers(0, len(pool)))
+                if rng.uniform() < cfg["continue_fraction"]:
+                    t_now[j] += 1.0 / 60.0
+                else:
+                    t_now[j] = float(rng.uniform(0.0, 1.0))
+                res = cfg["resolutions"][int(rng.integers(0, 3))]
+                u = api.make_uniforms(scenes.camera_on_sphere(rng, 2.5), res, t_now[j])
+                sweep = pool[j].params.swept_volume == 1
+                out.append((j, t_now[j], t_now[j] - 1.0 / 60.0 if sweep else math.nan, u))
+            return out
+
+        # plain: the requests one synchronous call pair at a time
+        plain_reqs = draw(200)
+        lat = []
+        t0 = time.perf_counter()
+        for j, t, t0r, u in plain_reqs:
+            a = time.perf_counter()
+            pool[j].invert(t, t0r)
+            pool[j].trace(u, rgba=False, depth=False, normal=False)
+            dev.lib.tsi_synchronize(dev.handle)
+            lat.append((time.perf_counter() - a) * 1000.0)
+        plain = {"frames_per_s": len(plain_reqs) / (time.perf_counter() - t0),
+                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+        runs = []
+        with Server(dev) as srv:
+            for rate in cfg["rates_rps"]:
+                n = int(rate * cfg["seconds"])
+                reqs = draw(n)
+                arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+                tickets, lats, errors = [], [], []
+                done = threading.Event()
+
+                def collect():
+                    i = 0
+                    while i < n:
+                        if i >= len(tickets):
+                            time.sleep(0.0002)
+                            continue
+                        try:
+                            r = srv.poll(tickets[i], 1000)
+                        except Exception as e:  # the request failed: count it, go on
+                            errors.append(str(e))
+                            i += 1
+                            continue
+                        if r is not None:
+                            lats.append(r[1])
+                            i += 1
+                    done.set()
+
+                th = threading.Thread(target=collect, daemon=True)
+                th.start()
+                start = time.perf_counter()
+                for k, (j, t, t0r, u) in enumerate(reqs):
+                    delay = start + arrivals[k] - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                    tickets.append(srv.submit(pool[j], t, t0=t0r, uniforms=u))
+                done.wait(300.0)
+                wall = time.perf_counter() - start
+                th.join(5.0)
+                lats = np.sort(np.asarray(lats))
+                runs.append({"rate_rps": rate, "requests": int(len(lats)), "frames_per_s": len(lats) / wall,
+                             "vs_plain_frames_per_s": len(lats) / wall / plain["frames_per_s"],
+                             "p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
+                             "p99_vs_plain_p50": float(np.percentile(lats, 99)) / plain["p50_ms"],
+                             "failed": len(errors), "first_error": errors[0] if errors else None})
+        return {"pool": cfg["pool"], "plain": plain, "runs": runs, "scene_bytes": dev.scenes_bytes(),
+                "note": "cfg4-style mix: 64 scenes (L 8/9/10, 20% swept), 70% continue at t+1/60, "
+                        "resolutions 512^2 / 1280x720 / 1920x1080, random cameras; frames kept on the device"}
+    finally:
+        dev.close()
+
+
 # ------------------------------------------------------------------ batched leg
 BATCHED = dict(scenes=32, prims=(8, 2048), levels=(7, 10), res=1024, seed=3000, warmup=3, steps=6)
 
@@ -639,6 +753,11 @@ def run_gpu(args, rank, world, local, dist) -> None:
             line["served"] = served_leg(local)
         except Exception as e:
             line["served"] = {"unavailable": str(e)}
+    if world == 1 and not args.no_served:
+        try:
+            line["served_mix"] = served_mix_leg(local)
+        except Exception as e:
+            line["served_mix"] = {"unavailable": str(e)}
     if world == 1 and not args.no_swept:
         try:
             line["swept"] = swept_leg(local)

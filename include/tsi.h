@@ -176,8 +176,8 @@ typedef struct tsi_image_device {
 typedef struct tsi_device_opts {
   int32_t device;               /* CUDA ordinal */
   uint64_t work_item_capacity;  /* per-level work list capacity (0 = default) */
-  uint64_t tape_arena_words;    /* pruned tape arena, 8-byte words (0 = default) */
-  uint64_t log_arena_bytes;     /* reverse-AD operand log (0 = default) */
+  uint64_t tape_arena_words;    /* pruned tape arena, 8-byte words (0 = default, 256 Mi words) */
+  uint64_t log_arena_bytes;     /* reverse-AD operand log of long narrow tapes (0 = default, 4 GiB) */
   uint32_t watchdog_iters;      /* bound on every device wait (0 = default) */
   uint32_t max_scenes_per_launch; /* batch width (0 = default 64) */
   uint32_t wide_smem_bytes;     /* shared memory a wide cell's working set may take; larger ones run

@@ -99,6 +99,7 @@ struct tsi_scene {
   VoxelPoolDev pool{};
   SceneCounters *d_ctr = nullptr;
   uint32_t img_w = 0, img_h = 0;
+  uint64_t img_cap = 0;  // pixels the frame buffers hold (frames of any size up to it reuse them)
   float4 *d_rgba = nullptr;
   float *d_depth = nullptr;
   float *d_normal = nullptr;
@@ -582,8 +583,12 @@ uint64_t scenes_bytes(const tsi_ctx *c) {
 }
 
 tsi_status ensure_image(tsi_scene *s, uint32_t w, uint32_t h) {
-  if (s->img_w == w && s->img_h == h && s->d_rgba) return TSI_OK;
-  const uint64_t old_img = (uint64_t)s->img_w * s->img_h * 32u, new_img = (uint64_t)w * h * 32u;
+  if (s->d_rgba && (uint64_t)w * h <= s->img_cap) {  // no reallocation while a request mix varies sizes
+    s->img_w = w;
+    s->img_h = h;
+    return TSI_OK;
+  }
+  const uint64_t old_img = s->img_cap * 32u, new_img = (uint64_t)w * h * 32u;
   if (s->ctx->hbm_budget && new_img > old_img && scenes_bytes(s->ctx) + (new_img - old_img) > s->ctx->hbm_budget)
     return set_err(TSI_ERR_OOM, "frame buffers would exceed the context's HBM budget");
   if (s->copy_pending) {
@@ -602,6 +607,7 @@ tsi_status ensure_image(tsi_scene *s, uint32_t w, uint32_t h) {
   CK(dalloc(&s->d_normal, np * 3));
   s->img_w = w;
   s->img_h = h;
+  s->img_cap = np;
   s->bytes = s->bytes - old_img + new_img;
   return TSI_OK;
 }
@@ -875,8 +881,10 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   c->item_cap = (opts && opts->work_item_capacity) ? (uint32_t)opts->work_item_capacity : (4u << 20);
   c->dealloc_cap = c->item_cap * 2u;
   c->rec_cap = c->item_cap * 2u;
-  c->code_cap = (opts && opts->tape_arena_words) ? opts->tape_arena_words : (96ull << 20);
-  c->log_overflow_cap = (opts && opts->log_arena_bytes) ? opts->log_arena_bytes / 16 : ((2ull << 30) / 16);
+  // defaults sized for fused launches of many scenes (the pruned-tape arena
+  // and the operand log of long narrow tapes fill per level and frame)
+  c->code_cap = (opts && opts->tape_arena_words) ? opts->tape_arena_words : (256ull << 20);
+  c->log_overflow_cap = (opts && opts->log_arena_bytes) ? opts->log_arena_bytes / 16 : ((4ull << 30) / 16);
   c->watchdog = (opts && opts->watchdog_iters) ? opts->watchdog_iters : (1u << 22);
   c->slice_len = 1024;
   // resident warps at the smallest register file

@@ -880,8 +880,10 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
       sh.fcost = 0;
       sh.rcost = 0;
       // a pruned record only for children that go to the narrow path (the
-      // wide path evaluates the full tape)
-      if (total < n_narrow && total < W.min_len) {
+      // wide path evaluates the full tape), or may: children the full wide
+      // list turns away run narrow on this record
+      const bool wide_room = *(const volatile uint32_t *)&P.witem_count[level + 1] + 8u <= P.witem_cap;
+      if (total < n_narrow && (total < W.min_len || !wide_room)) {
         const unsigned long long off = atomicAdd(P.code_count, (unsigned long long)total);
         if (off + total <= P.code_cap) {
           const uint32_t ri = atomicAdd(P.rec_count, 1u);
