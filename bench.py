@@ -28,7 +28,10 @@ temporally reused frames, like one run of the animation.
   cpu_baseline: the CPU oracle (C++ restatement of compute.wgsl, OpenMP)
           on a bounded sample of the same animation
   served : open-loop Poisson requests through the serving layer, p50/p99
-          latency beside the plain path's per-frame latency
+          latency beside the plain path's per-frame latency (eight runs of
+          the workload's animation)
+  served_mix: the same over a 64-scene pool with mixed levels, sweeps,
+          resolutions and cameras
   batched: 32 scenes (8..2048 primitives, localsubdiv 7..10, 1024x1024)
           per step, as 32 sequential plain calls and as one CUDA-graph replay
   swept  : swept volume over [0, 1] in 64 sub-steps, localsubdiv 9, 1280x720,
