@@ -1,0 +1,130 @@
+"""A second, independent restatement of compute.wgsl's per-cell temporal
+logic (cell time range 3603-3613, temporal error bound and Lipschitz
+correction 3971-3996, fast flag 4003-4009, classification and re-enqueue
+4011-4033), in numpy float32, against the oracle's octree: every cell of
+two levels that three frames evaluate, with time_err accumulating, cells
+re-enqueued and parents turning fast.  The cells' field and sensitivities
+come from the oracle's box evaluation, itself checked operation by
+operation in test_cpu_interval_restatement.py.  No device needed."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from temporalsetinversion_b200 import api, scenes
+
+f32 = np.float32
+INF = f32(np.inf)
+
+
+def abs_i(lo, hi):  # ABS_I, 2628-2636
+    if lo <= 0 <= hi:
+        return f32(0), max(-lo, hi)
+    if hi < 0:
+        return -hi, -lo
+    return lo, hi
+
+
+def sqr_i(lo, hi):  # SQR_I, 2689-2697
+    x, y = f32(lo * lo), f32(hi * hi)
+    if lo <= 0 <= hi:
+        return f32(0), max(x, y)
+    return min(x, y), max(x, y)
+
+
+def mul_if(lo, hi, b):  # MUL_IF, 2559-2565
+    return (f32(lo * b), f32(hi * b)) if b >= 0 else (f32(hi * b), f32(lo * b))
+
+
+def cell_update(F, sens, t0, t1, delta, time_err_old, children, lipschitz):
+    """time_err, fast, f, enqueued of a non-new cell evaluated over [t0, t1]."""
+    df_dt = sens[3]
+    dt = f32(f32(t1) - f32(t0))
+    df = mul_if(df_dt[0], df_dt[1], dt)
+    W = mul_if(f32(-1), f32(1), f32(F[1] - F[0]))
+    if df[1] < W[0] or W[1] < df[0]:  # CAP_II, 2664-2670
+        df = (INF, -INF)
+    else:
+        df = (max(df[0], W[0]), min(df[1], W[1]))
+    if lipschitz and abs_i(*df)[1] != 0:
+        s = [sqr_i(*sens[q]) for q in range(3)]
+        acc = (f32(s[1][0] + s[2][0]), f32(s[1][1] + s[2][1]))
+        acc = (f32(s[0][0] + acc[0]), f32(s[0][1] + acc[1]))
+        root = (np.sqrt(max(acc[0], f32(0))), np.sqrt(max(acc[1], f32(0))))
+        lb = abs_i(*root)[0]
+        if not np.isnan(lb):
+            q = [f32(df[0] / lb), f32(df[1] / lb)]  # DIV_IF = DIV_II with [lb, lb]
+            df = (min(q), max(q))
+    if df[0] == -INF or df[1] == INF or np.isnan(df[0]) or np.isnan(df[1]):
+        df = (f32(delta), f32(delta))
+    time_err = f32(time_err_old + np.clip(abs_i(*df)[1], f32(0), f32(delta)))
+    fast = f32(1) if abs_i(*df)[1] >= f32(delta) else f32(0)
+    enq = False
+    if F[0] <= 0 <= F[1]:
+        f = f32(0)
+        bad_dt = np.isnan(df_dt[0]) or np.isnan(df_dt[1]) or abs(df_dt[0]) == INF or abs(df_dt[1]) == INF
+        if bad_dt or time_err >= f32(delta) or not children:
+            time_err, enq = f32(0), True
+    else:
+        f = f32(-1) if F[1] <= 0 else f32(1)
+    return time_err, fast, f, enq
+
+
+def _by_key(cells):
+    return {(int(c["level"]), int(c["ix"]), int(c["iy"]), int(c["iz"])): c for c in cells}
+
+
+@pytest.mark.parametrize("lipschitz", [1, 0])
+@pytest.mark.parametrize("text", [scenes.spheres16(0), scenes.csg(24, 3, 0.9)], ids=["spheres16", "csg24"])
+def test_cells_match_restatement(text, lipschitz):
+    """Every cell of levels 3 and 4 that a frame evaluates, frames at t = 0,
+    1/60 and 2/60 of a localsubdiv-6 octree (time_err accumulating over
+    frames, cells reused or re-enqueued, parents turning fast)."""
+    oracle.build()
+    tape = api.IR.new(text).gpu_instructions
+    delta = 0.01
+    p = api.default_params(localsubdiv=6, pointsample=0, lipschitz_corrected=lipschitz, delta=delta)
+    S = oracle.Scene(tape, p)
+    times = [f32(0.0), f32(1.0 / 60.0), f32(2.0 / 60.0)]
+    S.invert(float(times[0]))
+    prev = _by_key(S.cells())
+    checked = accumulated = 0
+    for t1 in times[1:]:
+        S.invert(float(t1))
+        now = _by_key(S.cells())
+        todo = [k for k, c in now.items() if k[0] in (3, 4) and c["t"] == t1]
+        boxes = np.zeros((len(todo), 8), f32)
+        meta = []
+        for n, k in enumerate(todo):
+            c = now[k]
+            parent = now[(k[0] - 1, k[1] // 2, k[2] // 2, k[3] // 2)]
+            old = prev.get(k)
+            new = old is None
+            point = new or parent["fast"] == 1.0  # width > epsilon at these levels
+            t0 = t1 if point else f32(old["t"])
+            boxes[n, 0:2], boxes[n, 2:4], boxes[n, 4:6] = c["x"], c["y"], c["z"]
+            boxes[n, 6:8] = (min(t0, t1), max(t0, t1))
+            meta.append((k, point, new, old))
+        out = oracle.eval_boxes(tape, boxes, reverse=True)
+        for n, (k, point, new, old) in enumerate(meta):
+            c = now[k]
+            F = (f32(out[n, 0]), f32(out[n, 1]))
+            if point:  # no reverse pass: df stays 0, the cell's fast flag is cleared
+                te = f32(0) if new else f32(old["time_err"])
+                fast = f32(0)
+                if F[0] <= 0 <= F[1]:
+                    f = f32(0)
+                    te = f32(0)  # a point time range always re-enqueues (4018)
+                else:
+                    f = f32(-1) if F[1] <= 0 else f32(1)
+            else:
+                sens = [(f32(out[n, 2 + 2 * q]), f32(out[n, 3 + 2 * q])) for q in range(4)]
+                te, fast, f, _ = cell_update(F, sens, old["t"], t1, delta, f32(old["time_err"]),
+                                             bool(old["has_children"]), lipschitz)
+                accumulated += int(te != 0)
+            assert (c["f"], c["time_err"], c["fast"]) == (f, te, fast), (t1, k, point, (c["f"], c["time_err"],
+                                                                                     c["fast"]), (f, te, fast))
+            checked += 1
+        prev = now
+    assert checked > 100 and accumulated > 10, (checked, accumulated)
