@@ -249,7 +249,8 @@ TSI_API tsi_status tsi_scene_reset(tsi_scene *scene);
  * t0_or_nan: start of the swept interval (NaN = time - swept_dt). */
 TSI_API tsi_status tsi_scene_invert(tsi_scene *scene, float time, float t0_or_nan,
                                     tsi_stats *stats);
-/* tsi_scene_invert without waiting: the frame is queued on the context's
+/* tsi_scene_invert (one `main` dispatch, main.rs:776-783) without waiting
+ * for it, which the reference's event loop never does: the frame is queued on the context's
  * stream and the call returns at once, so the host can queue the frame's
  * trace (tsi_scene_trace_async) and the next frames while the GPU works.
  * tsi_scene_invert_wait waits for everything queued and returns an error
@@ -264,7 +265,8 @@ TSI_API tsi_status tsi_scene_invert_wait(tsi_scene *scene, tsi_stats *stats);
 TSI_API tsi_status tsi_scene_trace(tsi_scene *scene, const tsi_uniforms *u, tsi_image *out,
                                    tsi_stats *stats);
 TSI_API tsi_status tsi_scene_image_device(tsi_scene *scene, tsi_image_device *out);
-/* tsi_scene_trace into host buffers without waiting for the frame: the
+/* tsi_scene_trace (one `rt_main` dispatch, main.rs:649-656) into host
+ * buffers without waiting for the frame: the
  * trace is queued behind the scene's earlier work and the frame's copy to
  * `out` runs on the context's copy stream, overlapping the caller's next
  * device work (the next tsi_scene_invert, say).  `out`'s buffers should be
