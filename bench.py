@@ -36,6 +36,8 @@ temporally reused frames, like one run of the animation.
           per step, as 32 sequential plain calls and as one CUDA-graph replay
   swept  : swept volume over [0, 1] in 64 sub-steps, localsubdiv 9, 1280x720,
           delta 0.005 / 0.01 / 0.02: frames/s and cell reuse
+  split  : the animation cut at the root into eight subtree scenes on this
+          GPU, inverted together, traced and composited by nearest depth
 
 --impl reference times the CPU restatement (the reference itself is WGSL
 under wgpu/Vulkan: no Vulkan driver or Rust toolchain exists on these
@@ -600,6 +602,63 @@ def swept_leg(local: int) -> dict:
         dev.close()
 
 
+SPLIT = dict(level=1, frames=40, part_frames=6)
+
+
+def split_leg(local: int) -> dict:
+    """The headline animation cut at the root into its eight subtrees, all
+    on this GPU (temporalsetinversion_b200.split): per frame the eight
+    subtree scenes are inverted in one fused launch sequence and traced over
+    the 1080p image (tsi_batch_run), then composited by nearest depth
+    (tsi_frames_composite).  Wall-clock frames/s over the animation's first
+    frames, the composite's time, and each part run alone (device time of
+    its inversion + trace): the slowest part bounds one frame of an
+    eight-GPU split, before the exchange."""
+    from temporalsetinversion_b200 import Device, Tape, api, split
+
+    W, H, F = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["frames"]
+    text, params, view = build_workload(WORKLOAD["seed"])
+    dev = Device(local)
+    try:
+        tape = Tape.from_llvm_ir(dev, text)
+        sp = split.SubtreeSplit(dev, tape, params, level=SPLIT["level"], voxel_capacity=16 << 20)
+        n = SPLIT["frames"]
+        warm = 3
+        for i in range(warm):
+            t = frame_time(i, F)
+            sp.frame(t, api.make_uniforms(view, (W, H), t))
+        dev_ms, comp_s = 0.0, 0.0
+        t0 = time.perf_counter()
+        for i in range(warm, n):
+            t = frame_time(i, F)
+            fb, stats = sp.frame(t, api.make_uniforms(view, (W, H), t))
+            dev_ms += stats[0].device_ms
+        wall = time.perf_counter() - t0
+        for _ in range(5):
+            c0 = time.perf_counter()
+            sp.composite(fb)
+            comp_s += time.perf_counter() - c0
+        hits = int((fb["depth"] >= 0).sum().item())
+        # each part alone over the next frames (scenes continue the animation)
+        part_ms = [0.0] * len(sp.scenes)
+        for i in range(n, n + SPLIT["part_frames"]):
+            t = frame_time(i, F)
+            u = api.make_uniforms(view, (W, H), t)
+            for k, s in enumerate(sp.scenes):
+                part_ms[k] += api.run_batch(dev, [(s, t, math.nan, None)])[0]["stats"].device_ms
+                part_ms[k] += s.trace(u, rgba=False, depth=False, normal=False)["device_ms"]
+        part_ms = [m / SPLIT["part_frames"] for m in part_ms]
+        sp.close()
+        return {"parts": len(sp.ids), "level": SPLIT["level"], "frames": n - warm,
+                "frames_per_s": (n - warm) / wall, "device_ms_per_frame": dev_ms / (n - warm),
+                "composite_ms": 1000.0 * comp_s / 5, "hit_pixels": hits,
+                "part_ms": [round(m, 4) for m in part_ms], "part_ms_max": max(part_ms), "part_ms_sum": sum(part_ms),
+                "note": "one GPU holds all eight subtree scenes; wall clock per frame (fused inversion of the parts, "
+                        "eight traces, composite); part_ms = one part's inversion + trace run alone, device time"}
+    finally:
+        dev.close()
+
+
 # ------------------------------------------------------------------ GPU leg
 def run_gpu(args, rank, world, local, dist) -> None:
     import ctypes as C
@@ -766,6 +825,11 @@ def run_gpu(args, rank, world, local, dist) -> None:
             line["swept"] = swept_leg(local)
         except Exception as e:
             line["swept"] = {"unavailable": str(e)}
+    if world == 1 and not args.no_split:
+        try:
+            line["split"] = split_leg(local)
+        except Exception as e:  # report, keep the headline line
+            line["split"] = {"unavailable": str(e)}
     if world == 1 and not args.no_batched:
         try:
             line["batched"] = batched_leg(local)
@@ -785,6 +849,7 @@ def main() -> None:
     ap.add_argument("--no-served", action="store_true", help="skip the served-latency leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the 32-scene batched leg")
     ap.add_argument("--no-swept", action="store_true", help="skip the swept-volume leg")
+    ap.add_argument("--no-split", action="store_true", help="skip the root-split leg")
     ap.add_argument("--small-arenas", action="store_true",
                     help="small work-item, tape and log arenas (use with --voxels 4194304 under a profiler)")
     args = ap.parse_args()

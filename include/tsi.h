@@ -380,6 +380,47 @@ TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g);
 TSI_API tsi_status tsi_batch_graph_wait(tsi_batch_graph *g, tsi_stats *stats);
 TSI_API void tsi_batch_graph_destroy(tsi_batch_graph *g);
 
+/* ---------------- one animation split at the root ----------------
+ * No counterpart in the reference, which keeps one octree per device.  The
+ * root's subtrees are independent for inversion, so one animation can be
+ * cut at `level` into 8^level subtrees, each inverted as a scene of its own
+ * (on this GPU or spread over GPUs), each traced over the whole image, and
+ * the frames composited by nearest depth. */
+
+/* `full` with its root box replaced by the box of cell (level, ix, iy, iz)
+ * of the full octree, index = ix + n (iy + n iz), n = 2^level: the child
+ * bounds of compute.wgsl:3582-3589 applied `level` times, so the subtree's
+ * cells have the full octree's bounds bit for bit, and its leaves the full
+ * octree's epsilon (which depends on localsubdiv only, 3521).  The subtree
+ * root is expanded every frame, like the reference's root (buf_main,
+ * 4690-4708): on a fresh octree its cells equal the full octree's cells of
+ * that subtree; on later frames its top cells are refreshed every frame
+ * where the full octree may carry them over. */
+TSI_API tsi_status tsi_params_subtree(const tsi_params *full, uint32_t level, uint32_t index, tsi_params *out);
+
+/* A composited frame in device memory (caller owned, e.g. tensors of a
+ * framework): rgba 4, depth 1, normal 3 floats and one key per pixel.
+ * key = (bits of depth) << 32 | subtree index for a hit, 0x7fffffff << 32 |
+ * subtree index for a miss, so the nearest hit has the least key (ties and
+ * all-miss pixels go to the lowest subtree index) and keys are positive as
+ * signed 64-bit integers (a collective's MIN over int64 orders them). */
+typedef struct tsi_frame_device {
+  uint32_t width, height;
+  float *rgba, *depth, *normal;
+  uint64_t *key;
+} tsi_frame_device;
+#define TSI_COMPOSITE_MAX 64
+/* Per pixel, the last traced frame of the scene with the least key among
+ * `scenes` (subtree indices `ids`, n <= TSI_COMPOSITE_MAX, all frames of
+ * out's size) into `out`.  Returns when `out` is written. */
+TSI_API tsi_status tsi_frames_composite(tsi_ctx *ctx, tsi_scene *const *scenes, const uint32_t *ids, uint32_t n,
+                                        tsi_frame_device *out);
+/* Zeroes (all bits) every pixel of `frame` whose key differs from
+ * `global_key` (device, the MIN of all parts' keys): after it, the parts'
+ * frames summed as 32-bit integers give the composite of all parts bit for
+ * bit.  Returns when `frame` is written. */
+TSI_API tsi_status tsi_frame_keep_nearest(tsi_ctx *ctx, const uint64_t *global_key, tsi_frame_device *frame);
+
 /* ---------------- serving ---------------- */
 /* No counterpart in the reference (its frames are driven by the window's
  * event loop, main.rs:978-1063).  A server owns a worker thread that drains

@@ -160,6 +160,18 @@ pub struct tsi_autotune_result {
     pub ms: [f32; TSI_AUTOTUNE_MAX],
 }
 
+/// Caller-owned device buffers of a composited frame (one animation split at the root).
+#[repr(C)]
+pub struct tsi_frame_device {
+    pub width: u32,
+    pub height: u32,
+    pub rgba: *mut c_float,
+    pub depth: *mut c_float,
+    pub normal: *mut c_float,
+    pub key: *mut u64,
+}
+pub const TSI_COMPOSITE_MAX: usize = 64;
+
 #[repr(C)]
 pub struct tsi_request {
     pub scene: *mut tsi_scene,
@@ -218,6 +230,11 @@ extern "C" {
                                reverse: i32, out: *mut f32) -> tsi_status;
     pub fn tsi_scene_image_device(s: *mut tsi_scene, out: *mut tsi_image_device) -> tsi_status;
     pub fn tsi_scene_image_copy(s: *mut tsi_scene, out: *mut tsi_image) -> tsi_status;
+    pub fn tsi_params_subtree(full: *const tsi_params, level: u32, index: u32, out: *mut tsi_params) -> tsi_status;
+    pub fn tsi_frames_composite(ctx: *mut tsi_ctx, scenes: *const *mut tsi_scene, ids: *const u32, n: u32,
+                                out: *mut tsi_frame_device) -> tsi_status;
+    pub fn tsi_frame_keep_nearest(ctx: *mut tsi_ctx, global_key: *const u64, frame: *mut tsi_frame_device)
+                                  -> tsi_status;
     pub fn tsi_scene_invert_async(s: *mut tsi_scene, time: f32, t0_or_nan: f32) -> tsi_status;
     pub fn tsi_scene_invert_wait(s: *mut tsi_scene, stats: *mut tsi_stats) -> tsi_status;
     pub fn tsi_scene_trace_async(s: *mut tsi_scene, u: *const Uniforms, out: *mut tsi_image) -> tsi_status;

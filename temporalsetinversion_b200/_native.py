@@ -94,6 +94,11 @@ class ImageDevice(C.Structure):
                 ("normal", C.c_void_p)]
 
 
+class FrameDevice(C.Structure):  # tsi_frame_device: caller-owned device buffers of a composited frame
+    _fields_ = [("width", u32), ("height", u32), ("rgba", C.c_void_p), ("depth", C.c_void_p),
+                ("normal", C.c_void_p), ("key", C.c_void_p)]
+
+
 class DeviceOpts(C.Structure):
     _fields_ = [("device", i32), ("work_item_capacity", u64), ("tape_arena_words", u64), ("log_arena_bytes", u64),
                 ("watchdog_iters", u32), ("max_scenes_per_launch", u32), ("wide_smem_bytes", u32),
@@ -166,6 +171,9 @@ SIGNATURES = {
                                                  P(u32)]),
     "tsi_tape_eval_boxes_static": (i32, [C.c_void_p, u32, C.c_void_p, i32, i32, C.c_void_p, C.c_void_p]),
     "tsi_static_scratch_bytes": (u64, []),
+    "tsi_params_subtree": (i32, [P(Params), u32, u32, P(Params)]),
+    "tsi_frames_composite": (i32, [C.c_void_p, P(C.c_void_p), P(u32), u32, P(FrameDevice)]),
+    "tsi_frame_keep_nearest": (i32, [C.c_void_p, C.c_void_p, P(FrameDevice)]),
 }
 
 _lib = None

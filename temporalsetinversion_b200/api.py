@@ -102,6 +102,7 @@ class Device:
         h = C.c_void_p()
         N.check(self.lib.tsi_create(C.byref(opts), C.byref(h)), "tsi_create")
         self.handle = h
+        self.index = int(device)  # CUDA ordinal
         self._children = weakref.WeakSet()
 
     def close(self) -> None:

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "api_internal.h"
+#include "composite.h"
 #include "device_types.h"
 #include "ir_lower.h"
 #include "tape_compile.h"
@@ -250,6 +251,21 @@ tsi_status status_from_error_bits(uint32_t e) {
   return TSI_OK;
 }
 
+// Levels of parents a frame expands: the root, then every level whose cells
+// are wider than epsilon (localsubdiv for the default root box, fewer for a
+// subtree's root).  Capped at TSI_MAX_LEVELS, which scene creation checks.
+uint32_t tree_levels(const tsi_params &p) {
+  const float eps = 10.0f * ldexpf(1.0f, -p.localsubdiv);
+  float w = 0.0f;
+  for (int a = 0; a < 3; ++a) w = std::max(w, p.root_hi[a] - p.root_lo[a]);
+  uint32_t l = 0;
+  while (w > eps && l < TSI_MAX_LEVELS) {
+    w = w / 2.0f;
+    ++l;
+  }
+  return std::max(1u, l);
+}
+
 void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, bool wide_global, SceneLaunch &L,
                  TapeRec &R) {
   const tsi_params &p = s->p;
@@ -270,7 +286,7 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, bool 
   if (p.rounding_mode == TSI_ROUND_DIRECTED) f |= SF_DIRECTED;
   L.flags = f;
   L.root_rec = slot;
-  L.levels = (uint32_t)p.localsubdiv;
+  L.levels = tree_levels(p);
   L.full_len = s->tape->len;
   L.wide.slots = s->tape->d_wslots;
   L.wide.bundles = s->tape->d_wbundles;
@@ -331,7 +347,7 @@ tsi_status plan_frame(tsi_ctx *c, tsi_scene *const *scenes, uint32_t n, FramePla
   fp.lmax = 0;
   for (uint32_t i = 0; i < n; ++i) {
     const tsi_tape *t = scenes[i]->tape;
-    fp.lmax = std::max(fp.lmax, (uint32_t)scenes[i]->p.localsubdiv);
+    fp.lmax = std::max(fp.lmax, tree_levels(scenes[i]->p));
     rmax = std::max(rmax, t->nregs);
     if (t->d_wslots) mm_max = std::max(mm_max, t->n_minmax);
   }
@@ -1204,6 +1220,11 @@ TSI_API tsi_status tsi_scene_create(tsi_ctx *c, const tsi_tape *tape, const tsi_
   *out = nullptr;
   if (params->localsubdiv < 1 || params->localsubdiv > TSI_MAX_LEVELS - 1)
     return set_err(TSI_ERR_INVALID_ARGUMENT, "localsubdiv out of range");
+  for (int a = 0; a < 3; ++a)
+    if (!(params->root_lo[a] < params->root_hi[a]) || !isfinite(params->root_hi[a] - params->root_lo[a]))
+      return set_err(TSI_ERR_INVALID_ARGUMENT, "root box must have lo < hi, finite");
+  if (tree_levels(*params) > TSI_MAX_LEVELS - 1)
+    return set_err(TSI_ERR_INVALID_ARGUMENT, "root box too wide for localsubdiv (too many levels)");
   if (tape->ctx != c) return set_err(TSI_ERR_INVALID_ARGUMENT, "tape belongs to another context");
   CK(cudaSetDevice(c->device));
   if (voxel_capacity == 0) voxel_capacity = 4ull << 20;
@@ -1476,6 +1497,82 @@ TSI_API tsi_status tsi_scene_image_device(tsi_scene *s, tsi_image_device *out) {
   out->rgba = (const float *)s->d_rgba;
   out->depth = s->d_depth;
   out->normal = s->d_normal;
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_params_subtree(const tsi_params *full, uint32_t level, uint32_t index, tsi_params *out) {
+  if (!full || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  if (level > 10u || (int32_t)level >= full->localsubdiv)
+    return set_err(TSI_ERR_INVALID_ARGUMENT, "subtree level must be below localsubdiv and at most 10");
+  const uint64_t n = 1ull << level;
+  if ((uint64_t)index >= n * n * n) return set_err(TSI_ERR_INVALID_ARGUMENT, "subtree index out of range");
+  const uint32_t ix = (uint32_t)(index % n), iy = (uint32_t)((index / n) % n), iz = (uint32_t)(index / (n * n));
+  tsi_params p = *full;
+  for (uint32_t j = 0; j < level; ++j) {  // one child step per level (compute.wgsl:3582-3589)
+    const uint32_t sh = level - 1u - j;
+    const uint32_t b[3] = {(ix >> sh) & 1u, (iy >> sh) & 1u, (iz >> sh) & 1u};
+    for (int a = 0; a < 3; ++a) {
+      const float lo = p.root_lo[a], d = (p.root_hi[a] - p.root_lo[a]) / 2.0f;
+      p.root_lo[a] = lo + d * (float)b[a];
+      p.root_hi[a] = lo + d * (float)(1u + b[a]);
+    }
+  }
+  *out = p;
+  return TSI_OK;
+}
+
+namespace {
+tsi_status check_frame(const tsi_frame_device *f) {
+  if (!f->rgba || !f->depth || !f->normal || !f->key) return set_err(TSI_ERR_INVALID_ARGUMENT, "null frame buffer");
+  if (((uintptr_t)f->rgba & 15u) || ((uintptr_t)f->key & 7u) || ((uintptr_t)f->depth & 3u) ||
+      ((uintptr_t)f->normal & 3u))
+    return set_err(TSI_ERR_INVALID_ARGUMENT, "frame buffers misaligned (rgba 16, key 8, depth/normal 4 bytes)");
+  return TSI_OK;
+}
+}  // namespace
+
+TSI_API tsi_status tsi_frames_composite(tsi_ctx *c, tsi_scene *const *scenes, const uint32_t *ids, uint32_t n,
+                                        tsi_frame_device *out) {
+  if (!c || !scenes || !ids || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  if (n == 0 || n > TSI_COMPOSITE_MAX) return set_err(TSI_ERR_INVALID_ARGUMENT, "1 to TSI_COMPOSITE_MAX parts");
+  tsi_status st = check_frame(out);
+  if (st != TSI_OK) return st;
+  if (capturing(c)) return set_err(TSI_ERR_BUSY, "composite during graph capture");
+  tsi::CompositeParts P{};
+  for (uint32_t i = 0; i < n; ++i) {
+    const tsi_scene *s = scenes[i];
+    if (!s || s->ctx != c) return set_err(TSI_ERR_INVALID_ARGUMENT, "part is not a scene of this context");
+    if (!s->d_rgba || s->img_w != out->width || s->img_h != out->height)
+      return set_err(TSI_ERR_BUFFER_TOO_SMALL, "a part's last frame differs in size from the composite");
+    for (uint32_t j = 0; j < i; ++j)
+      if (ids[j] == ids[i]) return set_err(TSI_ERR_INVALID_ARGUMENT, "subtree indices must differ");
+    P.rgba[i] = s->d_rgba;
+    P.depth[i] = s->d_depth;
+    P.normal[i] = s->d_normal;
+    P.id[i] = ids[i];
+  }
+  P.n = n;
+  CK(cudaSetDevice(c->device));
+  const uint64_t npix = (uint64_t)out->width * out->height;
+  CK(tsi::launch_composite(P, npix, reinterpret_cast<float4 *>(out->rgba), out->depth, out->normal,
+                           reinterpret_cast<unsigned long long *>(out->key), c->sm_count * 8, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_frame_keep_nearest(tsi_ctx *c, const uint64_t *global_key, tsi_frame_device *frame) {
+  if (!c || !global_key || !frame) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  tsi_status st = check_frame(frame);
+  if (st != TSI_OK) return st;
+  if ((uintptr_t)global_key & 7u) return set_err(TSI_ERR_INVALID_ARGUMENT, "global key misaligned");
+  if (capturing(c)) return set_err(TSI_ERR_BUSY, "keep-nearest during graph capture");
+  CK(cudaSetDevice(c->device));
+  const uint64_t npix = (uint64_t)frame->width * frame->height;
+  CK(tsi::launch_keep_nearest(reinterpret_cast<const unsigned long long *>(frame->key),
+                              reinterpret_cast<const unsigned long long *>(global_key), npix,
+                              reinterpret_cast<float4 *>(frame->rgba), frame->depth, frame->normal,
+                              c->sm_count * 8, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return TSI_OK;
 }
 
