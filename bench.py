@@ -49,6 +49,9 @@ animation depend on each other through the resident octree, so each rank
 renders its own animation (scene seed = rank); per-GPU work is fixed
 ("scaling": "weak") and value is the total frames/s of all ranks with the
 time taken as the maximum over ranks.  No collective is on the data path.
+(One animation split at the root over GPUs, with its nearest-depth
+exchange, is temporalsetinversion_b200.split; the `split` leg measures its
+parts on one GPU.)
 """
 from __future__ import annotations
 
