@@ -2,14 +2,16 @@
 GPU classifies as empty (f = +1) or full (f = -1) may contain a sign change
 of f, checked by dense float64 point sampling (tests/point_eval.py) of the
 same tape.  Point sampling is off, so every classification rests on an
-interval enclosure.  Only cells evaluated in the current frame are checked:
-a cell carried over from an earlier frame is only guaranteed up to the
-temporal tolerance delta (compute.wgsl:3996), not exactly."""
+interval enclosure.  Cells evaluated in the current frame are checked
+exactly; a cell carried over from an earlier frame is only guaranteed up to
+its ancestors' accumulated time_err (compute.wgsl:3996), checked with that
+tolerance (tests/carried_ref.py)."""
 from __future__ import annotations
 
 import numpy as np
 import pytest
 
+from carried_ref import carried_excursions
 from point_eval import evaluate
 from temporalsetinversion_b200 import Scene, Tape, api, scenes
 
@@ -82,3 +84,29 @@ def test_directed_swept_volume_has_no_false_empty(device, delta):
             assert len(bad) == 0, "t in [%g, %g]: %d empty cells hold f < 0 at t=%g" % (t0, t1, len(bad), tt)
         checked += len(sel)
     assert checked > 50
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("lipschitz", [0, 1])
+def test_directed_carried_cells_stay_within_ancestors_time_err(device, lipschitz):
+    """Directed mode, 40 frames: every empty or full cell carried over from
+    an earlier frame keeps its sign at float64 samples up to its ancestors'
+    time_err (times |grad f| <= 1 with the Lipschitz correction; the directed
+    mode's MIN/MAX hull keeps the correction's gradient bound a lower bound,
+    where the reference's (1, 1) rule does not, see
+    tests/test_cpu_carried_cells.py)."""
+    text = scenes.csg(64, 5, 0.85)
+    tape = api.IR.new(text).gpu_instructions
+    p = api.default_params(localsubdiv=6, pointsample=0, rounding_mode=1, lipschitz_corrected=lipschitz, delta=0.03)
+    s = Scene(device, Tape.upload(device, tape), p)
+    rng = np.random.default_rng(3)
+    checked = 0
+    for k in range(40):
+        t = k / 60.0
+        s.invert(t)
+        exc, bound = carried_excursions(tape, s.cells(), t, rng)
+        over = exc > bound + 1e-6
+        assert not over.any(), "t=%g: %d carried cells cross by more than their ancestors' time_err (%g > %g)" % (
+            t, over.sum(), exc[over][0], bound[over][0])
+        checked += len(exc)
+    assert checked > 50, checked
