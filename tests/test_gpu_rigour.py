@@ -94,7 +94,10 @@ def test_directed_carried_cells_stay_within_ancestors_time_err(device, lipschitz
     time_err (times |grad f| <= 1 with the Lipschitz correction; the directed
     mode's MIN/MAX hull keeps the correction's gradient bound a lower bound,
     where the reference's (1, 1) rule does not, see
-    tests/test_cpu_carried_cells.py)."""
+    tests/test_cpu_carried_cells.py).  With the hull every sensitivity
+    component of a cell with an undecided min/max contains 0, so lb = 0, df
+    becomes delta and the cell is re-enqueued: with the correction few cells
+    carry over (4 in these 40 frames), all within the bound."""
     text = scenes.csg(64, 5, 0.85)
     tape = api.IR.new(text).gpu_instructions
     p = api.default_params(localsubdiv=6, pointsample=0, rounding_mode=1, lipschitz_corrected=lipschitz, delta=0.03)
@@ -109,4 +112,4 @@ def test_directed_carried_cells_stay_within_ancestors_time_err(device, lipschitz
         assert not over.any(), "t=%g: %d carried cells cross by more than their ancestors' time_err (%g > %g)" % (
             t, over.sum(), exc[over][0], bound[over][0])
         checked += len(exc)
-    assert checked > 50, checked
+    assert checked > (50 if lipschitz == 0 else 0), checked
