@@ -1,6 +1,7 @@
 """A second, independent restatement of the reference's ray tracer, in
 numpy float32 scalars, against the oracle's trace of the same octree: the
-camera ray (compute.wgsl:4590-4594, rt_main 4651-4685), slab test
+camera ray (compute.wgsl:4590-4594, rt_main 4651-4685, with the per-scene
+eye offsets and rotationMatrix 4524-4587 of scenes 0, 3, 4, 5), slab test
 (4059-4070), the traversal state machine with its per-node 2x2x2 march
 (4189-4403: descend, leave through the far side, a leaf ends the ray),
 darkening, the movement colour of stale leaves, normals (stored, or by
@@ -174,13 +175,58 @@ def trace(tree, tape, prm, ro, rd, time):
     return c, dist, normal
 
 
-def camera_rays(view, w, h):  # ray_direction 4590-4594 and view * vec4(d, 0), fov 90, scene 1
+PI = f32(math.pi)  # compute.wgsl:2476
+
+
+def rotation(axis, angle):  # rotationMatrix, 4524-4587: columns, each 4 floats
+    n = length(axis)
+    ax = [f32(axis[a] / n) for a in range(3)]
+    s_, c_ = f32(math.sin(float(angle))), f32(math.cos(float(angle)))
+    oc = f32(ONE - c_)
+    x, y, z = ax
+
+    def t(a, b):
+        return f32(f32(oc * a) * b)
+    return [[f32(t(x, x) + c_), f32(t(x, y) - f32(z * s_)), f32(t(z, x) + f32(y * s_)), ZERO],
+            [f32(t(x, y) + f32(z * s_)), f32(t(y, y) + c_), f32(t(y, z) - f32(x * s_)), ZERO],
+            [f32(t(z, x) - f32(y * s_)), f32(t(y, z) + f32(x * s_)), f32(t(z, z) + c_), ZERO],
+            [ZERO, ZERO, ZERO, ONE]]
+
+
+def matmul(a, b):  # a * b, both as lists of columns; each sum in index order
+    out = []
+    for col in range(4):
+        out.append([f32(f32(f32(f32(a[0][r] * b[col][0]) + f32(a[1][r] * b[col][1])) + f32(a[2][r] * b[col][2]))
+                        + f32(a[3][r] * b[col][3])) for r in range(4)])
+    return out
+
+
+def scene_camera(view, scene_id, h):
+    """rt_main 4660-4683: the eye (view column 3) and view after the scene's
+    offset and rotation, and the pixel row shift of scene 0."""
+    cols = [[f32(view[4 * c + r]) for r in range(4)] for c in range(4)]
+    eye = cols[3][:3]
+    if scene_id == 3:
+        eye = [f32(eye[a] + f32(v)) for a, v in enumerate((7.7, -2.21, 7.7))]
+        cols = matmul(rotation((ZERO, ONE, ZERO), f32(f32(PI / f32(4)) * f32(3))), cols)
+    elif scene_id == 4:
+        eye = [f32(eye[a] + f32(v)) for a, v in enumerate((0.0, -0.78, -7.0))]
+    elif scene_id == 5:
+        eye = [f32(eye[a] + f32(v)) for a, v in enumerate((7.13, 2.14, -5.6))]
+        cols = matmul(rotation((ZERO, ONE, ZERO), f32(PI / f32(4))), cols)
+        cols = matmul(rotation((f32(-1), ZERO, f32(-1)), f32(f32(PI / f32(4)) * f32(0.45))), cols)
+    shift = f32(f32(h) * f32(0.32)) if scene_id == 0 else ZERO
+    return eye, [v for c in cols for v in c], shift
+
+
+def camera_rays(view, w, h, shift=ZERO):  # ray_direction 4590-4594 and view * vec4(d, 0), fov 90
     m = [f32(v) for v in view]
     rad = f32(f32(90) * f32(math.pi / 180))
     z = f32(f32(h) / f32(math.tan(float(f32(rad / f32(2))))))
     for py in range(h):
         for px in range(w):
-            d = [f32(f32(f32(px) - f32(f32(w) / f32(2))) + HALF), f32(-f32(f32(f32(py) - f32(f32(h) / f32(2))) + HALF)),
+            pyf = f32(f32(py) - shift)
+            d = [f32(f32(f32(px) - f32(f32(w) / f32(2))) + HALF), f32(-f32(f32(pyf - f32(f32(h) / f32(2))) + HALF)),
                  f32(-z)]
             n = length(d)
             d = [f32(d[a] / n) for a in range(3)]
@@ -235,3 +281,53 @@ def test_trace_matches_restatement(scene, shading):
             aged += int(d >= 0 and not prm.normal_viz and ZERO < c[1] < c[0])  # red, partly faded to white
     assert hits > 100, hits
     assert prm.normal_viz or aged > 50, aged
+
+
+# per scene id: the eye the shader should end up with
+SCENE_EYES = {0: (0.5, 0.9, 1.3), 3: (0.6, 0.5, 1.2), 4: (0.4, 0.6, 1.4), 5: (0.7, 0.4, 1.1)}
+OFFSETS = {0: (0, 0, 0), 3: (7.7, -2.21, 7.7), 4: (0.0, -0.78, -7.0), 5: (7.13, 2.14, -5.6)}
+
+
+def _base_view(scene_id):
+    """A uniforms.view whose scene-adjusted camera looks at the origin from
+    SCENE_EYES: rotation undone in float64, eye minus the scene's offset."""
+    want = np.asarray(scenes.camera_look_at(SCENE_EYES[scene_id]), np.float64).reshape(4, 4)  # rows = columns
+    rot = np.eye(4)
+    if scene_id == 3:
+        rot = np.asarray(rotation((ZERO, ONE, ZERO), f32(f32(PI / f32(4)) * f32(3))), np.float64)
+    elif scene_id == 5:
+        r1 = np.asarray(rotation((ZERO, ONE, ZERO), f32(PI / f32(4))), np.float64)
+        r2 = np.asarray(rotation((f32(-1), ZERO, f32(-1)), f32(f32(PI / f32(4)) * f32(0.45))), np.float64)
+        rot = (r2.T @ r1.T).T  # column lists: the product r2 * r1 as columns
+    base = want.copy()
+    base[:3] = (np.linalg.inv(rot.T) @ want[:3].T).T  # undo view' = R * view on the direction columns
+    base[3, :3] = np.asarray(SCENE_EYES[scene_id]) - np.asarray(OFFSETS[scene_id])
+    return [float(v) for v in base.reshape(-1)]
+
+
+@pytest.mark.parametrize("scene_id", sorted(SCENE_EYES))
+def test_scene_cameras_match_restatement(scene_id):
+    """The per-scene cameras of rt_main (eye offsets, view rotations, scene
+    0's row shift) on a 40x24 image of a localsubdiv-7 octree, per pixel."""
+    oracle.build()
+    tape = api.IR.new(scenes.spheres16(0)).gpu_instructions
+    prm = api.default_params(localsubdiv=7, delta=0.01, scene_id=scene_id)
+    S = oracle.Scene(tape, prm)
+    S.invert(0.0)
+    tree = Octree(S.cells())
+    w, h = 40, 24
+    view = _base_view(scene_id)
+    got = S.trace(api.make_uniforms(view, (w, h), 0.0))
+    eye, m, shift = scene_camera(view, scene_id, h)
+    hits = 0
+    with np.errstate(all="ignore"):
+        for px, py, rd in camera_rays(m, w, h, shift):
+            c, d, n = trace(tree, tape, prm, eye, rd, f32(0))
+            where = "scene %d pixel (%d, %d)" % (scene_id, px, py)
+            assert got["depth"][py, px].view(np.uint32) == d.view(np.uint32), (where, got["depth"][py, px], d)
+            assert np.array_equal(got["normal"][py, px], np.array(n, f32)), where
+            want = np.array([f32(float(v) ** 0.45) for v in c], f32)
+            ulps = np.abs(got["rgba"][py, px, :3].view(np.int32).astype(np.int64) - want.view(np.int32).astype(np.int64))
+            assert np.all(ulps <= 2), (where, got["rgba"][py, px], c)
+            hits += int(d >= 0)
+    assert hits > 30, hits
