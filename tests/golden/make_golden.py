@@ -5,8 +5,11 @@
                         pure-Python restatement of src/ir.rs, in the 32-byte
                         GPUInstruction layout (literals as f32 bit patterns).
   oracle_cases.json   — summaries (counters and a SHA-256 of the sorted cell
-                        records) of CPU-oracle runs on small cases, so that a
-                        change to the oracle is caught.
+                        records) of CPU-oracle runs on small cases, and
+                        SHA-256s of a 64x36 trace of each final octree
+                        (depth, normal, rgba), so that a change to the
+                        oracle is caught and the device path can be checked
+                        against them without running the oracle.
 
 Run from the repository root with the reference checkout available:
     python tests/golden/make_golden.py [/path/to/reference]
@@ -80,16 +83,39 @@ def oracle_cases():
     return cases
 
 
+IMAGE_EYE = (0.3, 0.6, 2.5)
+IMAGE_RES = (64, 36)
+
+
+def image_digests(img: dict) -> dict:
+    out = {k: hashlib.sha256(np.ascontiguousarray(img[k], dtype=np.float32).tobytes()).hexdigest()
+           for k in ("depth", "normal", "rgba")}
+    out["hits"] = int((img["depth"] >= 0).sum())
+    return out
+
+
+def case_tape(case):
+    from temporalsetinversion_b200 import api
+    _, (kind, src), _, _ = case
+    return api.IR.new(src).gpu_instructions if kind == "gen" else load_tape(src)
+
+
+def image_uniforms(case):
+    from temporalsetinversion_b200 import api, scenes
+    return api.make_uniforms(scenes.camera_look_at(IMAGE_EYE), IMAGE_RES, case[3][-1])
+
+
 def run_case(case):
     import oracle
     from temporalsetinversion_b200 import api
-    name, (kind, src), params, times = case
-    tape = api.IR.new(src).gpu_instructions if kind == "gen" else load_tape(src)
+    name, _, params, times = case
+    tape = case_tape(case)
     p = api.default_params(**params)
     S = oracle.Scene(tape, p)
     frames = [S.invert(t) for t in times]
     cells = S.cells()
-    return {"frames": frames, "cells": int(len(cells)), "digest": cells_digest(cells)}
+    return {"frames": frames, "cells": int(len(cells)), "digest": cells_digest(cells),
+            "image": image_digests(S.trace(image_uniforms(case)))}
 
 
 def main() -> None:
