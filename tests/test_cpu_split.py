@@ -1,7 +1,7 @@
 """One animation split at the root (temporalsetinversion_b200.split), on the
 CPU: the subtree root boxes, the subtree scenes' semantics against the full
 octree (oracle), the nearest-depth composite against the full trace, and the
-cross-rank exchange of split.combine_ranks with two gloo ranks."""
+cross-rank exchange of split.combine_ranks with two and three gloo ranks."""
 from __future__ import annotations
 
 import os
@@ -118,7 +118,7 @@ def _free_port() -> int:
     return port
 
 
-def _rank_worker(rank: int, world: int, port: int, q):
+def _rank_worker(rank: int, world: int, dst: int, port: int, q):
     sys.path.insert(0, str(ROOT))
     sys.path.insert(0, str(ROOT / "tests"))
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
@@ -141,8 +141,8 @@ def _rank_worker(rank: int, world: int, port: int, q):
         arrs = {k: v.numpy() for k, v in frame.items()}
         ref.keep_nearest(arrs, gkey.numpy())
 
-    out = SP.combine_ranks(fb, keep, dst=0)
-    if rank == 0:
+    out = SP.combine_ranks(fb, keep, dst=dst)
+    if rank == dst:
         q.put({k: v.numpy().copy() for k, v in out.items()})
     else:
         q.put(out)
@@ -150,16 +150,18 @@ def _rank_worker(rank: int, world: int, port: int, q):
     dist.destroy_process_group()
 
 
-def test_two_ranks_combine_to_the_single_rank_composite():
-    """Two gloo ranks holding subtrees {0, 2, 4, 6} and {1, 3, 5, 7}: the
-    MIN all-reduce of keys, keep-nearest and SUM reduce of bits give rank 0
-    the one-rank composite of all eight subtrees bit for bit."""
+@pytest.mark.parametrize("world,dst", [(2, 0), (3, 2)])
+def test_ranks_combine_to_the_single_rank_composite(world, dst):
+    """gloo ranks holding every world-th subtree ({0, 2, 4, 6} and
+    {1, 3, 5, 7}; or {0, 3, 6}, {1, 4, 7}, {2, 5}): the MIN all-reduce of
+    keys, keep-nearest and SUM reduce of bits give rank `dst` the one-rank
+    composite of all eight subtrees bit for bit."""
     import torch.multiprocessing as mp
     oracle.build()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_worker, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank_worker, args=(r, world, dst, port, q)) for r in range(world)]
     for pr in procs:
         pr.start()
     got = [q.get(timeout=180) for _ in procs]
