@@ -337,7 +337,8 @@ def served_leg(local: int) -> dict:
 
 # ------------------------------------------------------------------ served mix leg
 SERVED_MIX = dict(pool=64, rates_rps=(200.0, 800.0), seconds=1.5, seed=2000, sweep_fraction=0.2,
-                  continue_fraction=0.7, levels=(8, 9, 10), resolutions=((512, 512), (1280, 720), (1920, 1080)))
+                  continue_fraction=0.7, levels=(8, 9, 10), resolutions=((512, 512), (1280, 720), (1920, 1080)),
+                  hbm_budget_bytes=150 * 10**9)
 
 
 def served_mix_leg(local: int) -> dict:
@@ -355,7 +356,7 @@ def served_mix_leg(local: int) -> dict:
 
     cfg = SERVED_MIX
     rng = np.random.default_rng(cfg["seed"])
-    dev = Device(local)
+    dev = Device(local, hbm_budget_bytes=SERVED_MIX["hbm_budget_bytes"])  # scenes and frames admitted against it
     try:
         pool = []
         for k in range(cfg["pool"]):
@@ -443,6 +444,7 @@ def served_mix_leg(local: int) -> dict:
                              "p99_vs_plain_p50": float(np.percentile(lats, 99)) / plain["p50_ms"],
                              "failed": len(errors), "first_error": errors[0] if errors else None})
         return {"pool": cfg["pool"], "plain": plain, "runs": runs, "scene_bytes": dev.scenes_bytes(),
+                "hbm_budget_bytes": cfg["hbm_budget_bytes"],
                 "note": "cfg4-style mix: 64 scenes (L 8/9/10, 20% swept), 70% continue at t+1/60, "
                         "resolutions 512^2 / 1280x720 / 1920x1080, random cameras; frames kept on the device"}
     finally:
