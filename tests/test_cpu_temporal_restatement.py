@@ -3,7 +3,8 @@ logic (cell time range 3603-3613, temporal error bound and Lipschitz
 correction 3971-3996, fast flag 4003-4009, classification and re-enqueue
 4011-4033), in numpy float32, against the oracle's octree: every cell of
 two levels that three frames evaluate, with time_err accumulating, cells
-re-enqueued and parents turning fast.  The cells' field and sensitivities
+re-enqueued and parents turning fast; and the point-sampled leaves
+(3603-3621).  The cells' field and sensitivities
 come from the oracle's box evaluation, itself checked operation by
 operation in test_cpu_interval_restatement.py.  No device needed."""
 from __future__ import annotations
@@ -128,3 +129,42 @@ def test_cells_match_restatement(text, lipschitz):
             checked += 1
         prev = now
     assert checked > 100 and accumulated > 10, (checked, accumulated)
+
+
+@pytest.mark.parametrize("text", [scenes.spheres16(0), scenes.csg(24, 3, 0.9)], ids=["spheres16", "csg24"])
+def test_point_sampled_leaves_match_restatement(text):
+    """Leaves (width <= epsilon) with point sampling (compute.wgsl:3603-3621,
+    4011-4045): evaluated at the current time at the midpoint (lo + hi) / 2
+    of their box, f from the sign of that value (0 only where it is 0), never
+    re-enqueued, fast cleared, time_err and the normal kept from the cell's
+    previous life (0 for a new cell: no derivative is taken at a point
+    time).  Every leaf of two frames of a localsubdiv-6 octree."""
+    oracle.build()
+    tape = api.IR.new(text).gpu_instructions
+    L = 6
+    p = api.default_params(localsubdiv=L, pointsample=1, lipschitz_corrected=1, delta=0.01)
+    S = oracle.Scene(tape, p)
+    prev = {}
+    checked = 0
+    for t in (f32(0.0), f32(1.0 / 60.0)):
+        S.invert(float(t))
+        now = _by_key(S.cells())
+        leaves = [k for k, c in now.items() if k[0] == L and c["t"] == t]
+        boxes = np.zeros((len(leaves), 8), f32)
+        for n, k in enumerate(leaves):
+            c = now[k]
+            for a, ax in enumerate("xyz"):
+                boxes[n, 2 * a: 2 * a + 2] = f32(f32(c[ax][0] + c[ax][1]) / f32(2))  # MID, 2510-2512
+            boxes[n, 6:8] = t
+        out = oracle.eval_boxes(tape, boxes, reverse=False)
+        for n, k in enumerate(leaves):
+            c, old = now[k], prev.get(k)
+            F = (f32(out[n, 0]), f32(out[n, 1]))
+            f = f32(0) if F[0] <= 0 <= F[1] else (f32(-1) if F[1] <= 0 else f32(1))
+            te = f32(0) if old is None else f32(old["time_err"])
+            nrm = (f32(0), f32(0), f32(0)) if old is None else (old["dx"], old["dy"], old["dz"])
+            assert (c["f"], c["fast"], c["time_err"], c["has_children"]) == (f, f32(0), te, 0), (t, k)
+            assert (c["dx"], c["dy"], c["dz"]) == nrm, (t, k)
+            checked += 1
+        prev = now
+    assert checked > 200, checked
