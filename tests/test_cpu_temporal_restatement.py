@@ -3,8 +3,8 @@ logic (cell time range 3603-3613, temporal error bound and Lipschitz
 correction 3971-3996, fast flag 4003-4009, classification and re-enqueue
 4011-4033), in numpy float32, against the oracle's octree: every cell of
 two levels that three frames evaluate, with time_err accumulating, cells
-re-enqueued and parents turning fast; and the point-sampled leaves
-(3603-3621).  The cells' field and sensitivities
+re-enqueued and parents turning fast; the point-sampled leaves
+(3603-3621); and the swept-volume branch (3603-3605, 3629, 4028-4044).  The cells' field and sensitivities
 come from the oracle's box evaluation, itself checked operation by
 operation in test_cpu_interval_restatement.py.  No device needed."""
 from __future__ import annotations
@@ -168,3 +168,86 @@ def test_point_sampled_leaves_match_restatement(text):
             checked += 1
         prev = now
     assert checked > 200, checked
+
+
+def _temporal_bound(F, sens, t0, t1, delta, lipschitz):
+    """|df| clamped to [0, delta] as time_err's increment (3971-3996) and df_dt."""
+    df_dt = sens[3]
+    dt = f32(f32(t1) - f32(t0))
+    df = mul_if(df_dt[0], df_dt[1], dt)
+    W = mul_if(f32(-1), f32(1), f32(F[1] - F[0]))
+    df = (INF, -INF) if (df[1] < W[0] or W[1] < df[0]) else (max(df[0], W[0]), min(df[1], W[1]))
+    if lipschitz and abs_i(*df)[1] != 0:
+        s = [sqr_i(*sens[q]) for q in range(3)]
+        acc = (f32(s[1][0] + s[2][0]), f32(s[1][1] + s[2][1]))
+        acc = (f32(s[0][0] + acc[0]), f32(s[0][1] + acc[1]))
+        lb = abs_i(np.sqrt(max(acc[0], f32(0))), np.sqrt(max(acc[1], f32(0))))[0]
+        if not np.isnan(lb):
+            q = [f32(df[0] / lb), f32(df[1] / lb)]
+            df = (min(q), max(q))
+    if df[0] == -INF or df[1] == INF or np.isnan(df[0]) or np.isnan(df[1]):
+        df = (f32(delta), f32(delta))
+    return np.clip(abs_i(*df)[1], f32(0), f32(delta)), df_dt
+
+
+@pytest.mark.parametrize("lipschitz", [0, 1])
+def test_swept_volume_cells_match_restatement(lipschitz):
+    """Swept volume (compute.wgsl:3603-3605, 3629, 4028-4044): a cell's time
+    range is [t0, t] when new or at most epsilon wide, else [its last time,
+    t]; interior cells with children are skipped; an empty cell keeps its f
+    (1 when new, mallocV 3444), full cells turn -1, ambiguous 0 with the
+    re-enqueue rule; no fast flag; nothing is ever deallocated.  Every cell
+    of four frames [k/16, (k+1)/16] of a localsubdiv-5 octree of rotating
+    primitives."""
+    with np.errstate(all="ignore"):
+        oracle.build()
+        tape = api.IR.new(scenes.swept(8, 4)).gpu_instructions
+        delta, L = 0.01, 5
+        p = api.default_params(localsubdiv=L, pointsample=0, swept_volume=1, lipschitz_corrected=lipschitz,
+                               delta=delta)
+        eps = f32(10.0 * 2.0 ** -L)
+        S = oracle.Scene(tape, p)
+        prev = {}
+        checked = skipped = 0
+        for k in range(4):
+            t0, t1 = f32(k / 16.0), f32((k + 1) / 16.0)
+            S.invert(float(t1), float(t0))
+            now = _by_key(S.cells())
+            assert set(prev) <= set(now), "a swept-volume cell was deallocated"
+            todo = [key for key, c in now.items() if key[0] >= 1 and c["t"] == t1]
+            boxes = np.zeros((len(todo), 8), f32)
+            meta = []
+            for n, key in enumerate(todo):
+                c, old = now[key], prev.get(key)
+                width = f32(c["x"][1] - c["x"][0])
+                lo = t0 if (old is None or width <= eps) else f32(old["t"])
+                boxes[n, 0:2], boxes[n, 2:4], boxes[n, 4:6] = c["x"], c["y"], c["z"]
+                boxes[n, 6:8] = (min(lo, t1), max(lo, t1))
+                meta.append((key, old, width, lo))
+            out = oracle.eval_boxes(tape, boxes, reverse=True)
+            for n, (key, old, width, lo) in enumerate(meta):
+                c = now[key]
+                if old is not None and old["f"] < 0 and old["has_children"]:  # interior: skipped (3629)
+                    assert (c["f"], c["time_err"]) == (old["f"], old["time_err"]), key
+                    skipped += 1
+                    continue
+                F = (f32(out[n, 0]), f32(out[n, 1]))
+                sens = [(f32(out[n, 2 + 2 * q]), f32(out[n, 3 + 2 * q])) for q in range(4)]
+                inc, df_dt = _temporal_bound(F, sens, lo, t1, delta, lipschitz)
+                te = f32((f32(0) if old is None else f32(old["time_err"])) + inc)
+                f_old = f32(1) if old is None else f32(old["f"])
+                if F[0] <= 0 <= F[1]:
+                    f = f32(0)
+                    bad = any(np.isnan(v) or abs(v) == INF for v in df_dt)
+                    if width > eps and (old is None or bad or lo == t1 or te >= f32(delta)
+                                        or not old["has_children"]):
+                        te = f32(0)
+                else:
+                    f = f32(-1) if F[1] <= 0 else f_old
+                mids = tuple(f32(f32(sens[q][0] + sens[q][1]) / f32(2)) for q in range(3))
+                assert (c["f"], c["time_err"], c["fast"]) == (f, te, f32(0)), (k, key, (c["f"], c["time_err"]),
+                                                                                (f, te))
+                assert (c["dx"], c["dy"], c["dz"]) == mids, key
+                checked += 1
+            prev = now
+        assert checked > 500, (checked, skipped)
