@@ -8,7 +8,12 @@
  * this machine or the GPU machine) and ships no tests or golden vectors;
  * the only reference fixtures are the scene tapes scenes/{cables,cradle,piano,sponza}.ll, which fix
  * inputs, not outputs.  This file is therefore a line-by-line restatement
- * of the reference's algorithm, each function citing the lines it follows:
+ * of the reference's algorithm, each function citing the lines it follows.
+ * A second restatement written separately in numpy (tests/test_cpu_*_restatement.py:
+ * interval ops and reverse rules, the whole-tape passes, the per-cell
+ * temporal logic, point-sampled leaves, swept volume, the tracer and
+ * cameras) agrees with it bit for bit; that checks the restatement, not the
+ * reference's own outputs.  The parts restated:
  *
  *   interval ops           src/compute.wgsl:2474-2975, fix 3462-3472
  *   refinement `main`      src/compute.wgsl:3513-4056 (run level by level)
