@@ -8,7 +8,10 @@ instruction's sensitivity plus the operand's, the larg == rarg case keeping
 the second write).  The scene moves its primitives linearly in t, so every
 operation of its tape is restated here (the per-op rules are those of
 test_cpu_interval_restatement.py, checked there one instruction at a time).
-Field and all four argument sensitivities, bit for bit.  No device needed."""
+The reference's own four scene tapes run through the same restated passes,
+with their elementary functions (sin, cos, exp, pow, floor, mod, atan2)
+taken from the oracle one instruction at a time.  Field and all four
+argument sensitivities, bit for bit.  No device needed."""
 from __future__ import annotations
 
 import numpy as np
@@ -144,9 +147,11 @@ def _rules(op, top, a, b, lit):
     return None, _div_rr_b(np.full_like(b0, L[0]), np.full_like(b0, L[1]), b0, b1)
 
 
-def restate(tape: np.ndarray, boxes: np.ndarray) -> np.ndarray:
+def restate(tape: np.ndarray, boxes: np.ndarray, forward=None, rules=None) -> np.ndarray:
     """Field interval and the four arguments' sensitivities per box, as the
     oracle's eval_boxes(reverse=True) lays them out."""
+    forward = forward or _forward
+    rules = rules or _rules
     n = len(tape)
     val = [None] * n
     for q in range(4):
@@ -161,7 +166,7 @@ def restate(tape: np.ndarray, boxes: np.ndarray) -> np.ndarray:
             lit = tape[j]["literal"]
             a = val[la] if top in (0, 1) else zero
             b = val[ra] if top in (0, 2) else zero
-            lo_, hi_ = _forward(op, top, a, b, lit)
+            lo_, hi_ = forward(op, top, a, b, lit)
             val[j] = fix(np.asarray(lo_, f32), np.asarray(hi_, f32))
             ops.append((j, op, top, la, ra, lit))
         uses = [_unpack(tape[j]["opcode_uses"])[1] for j in range(n)]
@@ -176,7 +181,7 @@ def restate(tape: np.ndarray, boxes: np.ndarray) -> np.ndarray:
                 skip = zero_j & (uses[la] == 1) & (uses[ra] == 1)
             else:
                 skip = zero_j & (uses[ra] == 1)
-            r_l, r_r = _rules(op, top, val[la], val[ra], lit)
+            r_l, r_r = rules(op, top, val[la], val[ra], lit)
             new = {}
             for slot, rule in ((la, r_l), (ra, r_r)):
                 if rule is None:
@@ -222,3 +227,74 @@ def test_whole_tape_matches_restatement(seed):
         len(bad), len(boxes), boxes[bad[0]], got[bad[0]], want[bad[0]])
     # the boxes reach both sides of the surface and zero sensitivities (the skip rule)
     assert (got[:, 0] > 0).any() and (got[:, 1] < 0).any()
+
+
+# Elementary functions (SIN 14, COS 15, EXP 9, LOG 10, POW 13, FLOOR 25,
+# MOD 29, ATAN2 30) are the driver's in the reference and the library's own
+# fixed sequences here; for the reference's scene tapes their value and rule
+# are taken from the oracle one instruction at a time, everything else (the
+# sequencing and every other operation) is restated above.
+ELEMENTARY = {9, 10, 13, 14, 15, 25, 29, 30}
+
+
+def _one_op_tape(op, top, lit):
+    from temporalsetinversion_b200.api import GPU_INSTR_DTYPE
+    t = np.zeros(5, GPU_INSTR_DTYPE)
+    for q in range(4):
+        t[q]["index_"] = q
+        t[q]["opcode_uses"] = (((q + 1) | (3 << 14)) << 16) | (1 if q < 2 else 0)
+    t[4]["index_"] = 4
+    t[4]["opcode_uses"] = ((op | (top << 14)) << 16) | 1
+    t[4]["larg_rarg"] = (0 << 16) | (1 if top == 0 else 0)
+    t[4]["literal"] = lit
+    return t
+
+
+def _oracle_op(op, top, a, b, lit):
+    """(value, rule for larg, rule for rarg) of one elementary instruction."""
+    boxes = np.zeros((len(a[0]), 8), f32)
+    boxes[:, 0], boxes[:, 1] = a
+    if top == 0:
+        boxes[:, 2], boxes[:, 3] = b
+    boxes[:, 6:8] = (0.0, 1.0)  # a time interval: the reverse pass runs
+    out = oracle.eval_boxes(_one_op_tape(op, top, lit), boxes, reverse=True).astype(f32)
+    return (out[:, 0], out[:, 1]), (out[:, 2], out[:, 3]), ((out[:, 4], out[:, 5]) if top == 0 else None)
+
+
+def restate_with_elementary(tape: np.ndarray, boxes: np.ndarray) -> np.ndarray:
+    """restate() for tapes that also hold elementary functions."""
+    cache = {}
+
+    def fwd(op, top, a, b, lit):
+        if op in ELEMENTARY and top in (0, 1):
+            key = (op, top, id(a), id(b), float(lit))
+            cache[key] = _oracle_op(op, top, a, b, lit)
+            return cache[key][0]
+        return _forward(op, top, a, b, lit)
+
+    def rules(op, top, a, b, lit):
+        if op in ELEMENTARY and top in (0, 1):
+            _, r_l, r_r = cache.get((op, top, id(a), id(b), float(lit))) or _oracle_op(op, top, a, b, lit)
+            return r_l, r_r
+        return _rules(op, top, a, b, lit)
+
+    return restate(tape, boxes, fwd, rules)
+
+
+@pytest.mark.parametrize("scene", ["cables", "cradle", "piano", "sponza"])
+def test_reference_scene_tapes_match_restatement(scene):
+    """The reference's own scene tapes (scenes/*.ll, lowered as committed
+    under tests/golden/tapes): field and argument sensitivities bit for bit
+    on random space-time boxes."""
+    from golden.make_golden import load_tape
+    oracle.build()
+    tape = load_tape(scene)
+    rng = np.random.default_rng(sum(map(ord, scene)))
+    boxes = _boxes(rng, 2000)
+    boxes[:, 0:6] = (boxes[:, 0:6] * f32(4)).astype(f32)  # the scenes span the [-5, 5] root box
+    got = oracle.eval_boxes(tape, boxes, reverse=True).astype(f32)
+    want = restate_with_elementary(tape, boxes)
+    bad = np.nonzero(np.any(got.view(np.uint32) != want.view(np.uint32), axis=1))[0]
+    assert len(bad) == 0, "%d of %d boxes differ, e.g. box %s: oracle %s restated %s" % (
+        len(bad), len(boxes), boxes[bad[0]], got[bad[0]], want[bad[0]])
+    assert ((got[:, 0] <= 0) & (got[:, 1] >= 0)).sum() > 20
