@@ -1,6 +1,7 @@
 """Octree ray tracing on the GPU against the oracle's restatement of
-compute.wgsl `trace` / `rt_main`: depth within 1e-4 of the scene extent
-(the 10-unit root box), normals within 1e-3 in cosine, colours within 1e-5."""
+compute.wgsl `trace` / `rt_main`: depth, normal and colour images bit for
+bit, with stored and finite-difference normals, normal visualisation, the
+per-scene cameras, render mode and asynchronous read-back."""
 from __future__ import annotations
 
 import numpy as np
@@ -10,23 +11,9 @@ import oracle
 from golden.make_golden import load_tape
 from temporalsetinversion_b200 import Scene, Tape, api, scenes
 
-EXTENT = 10.0
-
-
 def _compare(g, o):
-    dg, do = g["depth"], o["depth"]
-    hit_g, hit_o = dg >= 0, do >= 0
-    mism = int((hit_g != hit_o).sum())
-    assert mism <= max(2, hit_o.size // 2000), "hit masks differ in %d pixels" % mism
-    both = hit_g & hit_o
-    assert np.all(np.abs(dg[both] - do[both]) <= 1e-4 * EXTENT)
-    ng, no = g["normal"][both], o["normal"][both]
-    lg, lo = np.linalg.norm(ng, axis=1), np.linalg.norm(no, axis=1)
-    nz = (lg > 0) & (lo > 0)
-    cos = (ng[nz] * no[nz]).sum(1) / (lg[nz] * lo[nz])
-    assert np.all(cos >= 1 - 1e-3)
-    same = (hit_g == hit_o)
-    assert np.allclose(g["rgba"][same], o["rgba"][same], atol=1e-5)
+    bad = [k for k in ("depth", "normal", "rgba") if g[k].tobytes() != o[k].tobytes()]
+    assert not bad, "images differ: %s" % {k: int((g[k] != o[k]).sum()) for k in bad}
 
 
 @pytest.mark.gpu
