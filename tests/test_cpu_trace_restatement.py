@@ -331,3 +331,30 @@ def test_scene_cameras_match_restatement(scene_id):
             assert np.all(ulps <= 2), (where, got["rgba"][py, px], c)
             hits += int(d >= 0)
     assert hits > 30, hits
+
+
+def test_swept_volume_field_normals_match_restatement():
+    """Swept volume with finite-difference normals: the normal is taken at
+    the time of the hit leaf's parent (compute.wgsl:4337-4342), not at the
+    frame's time (traced here at t = 0.6 after sweeps up to 0.5), per pixel."""
+    oracle.build()
+    tape = api.IR.new(scenes.swept(8, 4)).gpu_instructions
+    prm = api.default_params(localsubdiv=6, pointsample=0, swept_volume=1, fast_normals=1)
+    S = oracle.Scene(tape, prm)
+    S.invert(0.25, 0.0)
+    S.invert(0.5, 0.25)
+    tree = Octree(S.cells())
+    w, h = 40, 24
+    view = scenes.camera_look_at((0.4, 0.6, 1.6))
+    time = f32(0.6)
+    got = S.trace(api.make_uniforms(view, (w, h), float(time)))
+    ro = [f32(view[12]), f32(view[13]), f32(view[14])]
+    hits = 0
+    with np.errstate(all="ignore"):
+        for px, py, rd in camera_rays(view, w, h):
+            c, d, n = trace(tree, tape, prm, ro, rd, time)
+            where = "pixel (%d, %d)" % (px, py)
+            assert got["depth"][py, px].view(np.uint32) == d.view(np.uint32), where
+            assert np.array_equal(got["normal"][py, px], np.array(n, f32), equal_nan=True), where
+            hits += int(d >= 0)
+    assert hits > 50, hits
