@@ -469,10 +469,12 @@ TSI_API void tsi_server_destroy(tsi_server *s);
  * else TSI_ERR_BUFFER_TOO_SMALL (split the call).  Nothing in the array needs
  * to start at zero: each launch writes every register and log entry before
  * reading it.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress), so make it before any stream capture.  All
- * calls share the one array per device: calls that can overlap on the GPU
- * (different streams, or different contexts on the same device) race on it
- * and must be ordered by the caller. */
+ * address (cudaGetSymbolAddress) and loads the evaluation kernel, so make it
+ * before any stream capture.  The call makes the tape's device current and
+ * puts the caller's current device back before it returns.  All calls share
+ * the one array per device: calls that can overlap on the GPU (different
+ * streams, or different contexts on the same device) race on it and must be
+ * ordered by the caller. */
 #define TSI_STATIC_SCRATCH_BYTES (16u << 20)
 TSI_API tsi_status tsi_tape_eval_boxes_static(const tsi_tape *tape, uint32_t n, const float *boxes_dev,
                                               int32_t rounding_mode, int32_t reverse, float *out_dev,

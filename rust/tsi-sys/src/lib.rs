@@ -3,7 +3,7 @@
 //! `GPUInstruction` here is layout-identical to `ir::GPUInstruction`
 //! (src/ir.rs:88-97) and `Uniforms` to `uniforms::Uniforms`
 //! (src/uniforms.rs:6-17), so the host passes its existing values through
-//! unchanged (see INTEGRATION.md).  Not compiled in this repository's CI
+//! unchanged.  Not compiled in this repository's CI
 //! (no Rust toolchain on the build machines).
 #![allow(non_camel_case_types)]
 use std::os::raw::{c_char, c_float, c_int, c_void};

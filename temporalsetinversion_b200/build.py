@@ -1,7 +1,10 @@
 """Build recipe for the native library (nvcc, sm_100a, in-tree output).
 
 Compiles temporalsetinversion_b200/csrc/*.cu|*.cpp into
-temporalsetinversion_b200/_lib/libtsi.so.  Device code is built with
+temporalsetinversion_b200/_lib/libtsi.so (loaded by the Python package) and
+the same objects into the static library temporalsetinversion_b200/_lib/libtsi.a
+(nvcc -lib), which a host program links with the CUDA runtime
+(-lcudart_static -lrt -lpthread -ldl, and the C++ runtime).  Device code is built with
 --fmad=false so that f32 arithmetic is never contracted into FMA (the
 interval formulas and the ray tracer follow the reference's plain f32
 operation sequence), host code with -ffp-contract=off for the same reason.
@@ -21,6 +24,7 @@ CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_lib"
 OBJ_DIR = ROOT / "_build" / "obj"
 LIB = OUT_DIR / "libtsi.so"
+STATIC_LIB = OUT_DIR / "libtsi.a"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + [
@@ -80,6 +84,14 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         if r.returncode:
             sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
             raise RuntimeError("link failed")
+    if force or jobs or not STATIC_LIB.exists():
+        if STATIC_LIB.exists():
+            STATIC_LIB.unlink()
+        cmd = [nvcc] + _host_cc_flags() + ARCH + ["-lib", "-o", str(STATIC_LIB)] + objs
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode:
+            sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+            raise RuntimeError("static library failed")
     return LIB
 
 

@@ -122,6 +122,15 @@ cudaError_t launch_evalbox(bool directed, const uint2 *code, uint32_t len, uint3
   return cudaGetLastError();
 }
 
+// Loads both instances of the box kernel on the current device (module
+// loading is lazy, so without this the first launch of each would load it).
+cudaError_t evalbox_preload() {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, evalbox_kernel<true>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, evalbox_kernel<false>);
+  return e;
+}
+
 cudaError_t launch_math(int which, uint32_t n, const float *a, const float *b, float *out, cudaStream_t st) {
   math_kernel<<<(n + 255) / 256, 256, 0, st>>>(which, n, a, b, out);
   return cudaGetLastError();

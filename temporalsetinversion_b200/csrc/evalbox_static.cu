@@ -24,6 +24,7 @@ namespace tsi {
 cudaError_t launch_evalbox(bool directed, const uint2 *code, uint32_t len, uint32_t nregs, uint32_t out_reg,
                            uint32_t n, const float *boxes, int reverse, float *out, float2 *regs, float4 *log,
                            cudaStream_t st);
+cudaError_t evalbox_preload();
 }
 
 
@@ -37,15 +38,19 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void *g_scratch_addr[kMaxDevices];  // device address of g_static_scratch, per device
 
-// Set-up, once per device, with that device current.
+// Set-up, once per device, with that device current: the array's device
+// address, and both instances of the box kernel loaded (module loading is
+// lazy), so that later calls load nothing.
 tsi_status scratch_address(int device, void **out) {
   if (device < 0 || device >= kMaxDevices) return TSI_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(g_mu);
   if (!g_scratch_addr[device]) {
     void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e == cudaSuccess && p) e = tsi::evalbox_preload();
     if (e != cudaSuccess || !p) {
       tsi_internal_set_error(cudaGetErrorString(e));
+      cudaGetLastError();
       return TSI_ERR_CUDA;
     }
     g_scratch_addr[device] = p;
@@ -76,21 +81,28 @@ extern "C" TSI_API tsi_status tsi_tape_eval_boxes_static(const tsi_tape *tape, u
                            "static scratch of TSI_STATIC_SCRATCH_BYTES; split the call");
     return TSI_ERR_BUFFER_TOO_SMALL;
   }
+  // the tape's device is made current for the call; the caller's current
+  // device is put back before returning
+  int caller_dev = -1;
+  if (cudaGetDevice(&caller_dev) != cudaSuccess) caller_dev = -1;
   if (cudaSetDevice(v.device) != cudaSuccess) {
     tsi_internal_set_error("cudaSetDevice failed");
+    cudaGetLastError();
     return TSI_ERR_CUDA;
   }
   void *base = nullptr;
   st = scratch_address(v.device, &base);
-  if (st != TSI_OK) return st;
-  float2 *regs = (float2 *)base;
-  float4 *log = (float4 *)((unsigned char *)base + regs_bytes);
-  cudaStream_t s = cuda_stream ? (cudaStream_t)cuda_stream : v.stream;
-  const cudaError_t e = tsi::launch_evalbox(rounding_mode == TSI_ROUND_DIRECTED, v.code, v.len, v.nregs, v.out_reg, n,
-                                            boxes_dev, reverse, out_dev, regs, log, s);
-  if (e != cudaSuccess) {
-    tsi_internal_set_error(cudaGetErrorString(e));
-    return TSI_ERR_CUDA;
+  if (st == TSI_OK) {
+    float2 *regs = (float2 *)base;
+    float4 *log = (float4 *)((unsigned char *)base + regs_bytes);
+    cudaStream_t s = cuda_stream ? (cudaStream_t)cuda_stream : v.stream;
+    const cudaError_t e = tsi::launch_evalbox(rounding_mode == TSI_ROUND_DIRECTED, v.code, v.len, v.nregs, v.out_reg,
+                                              n, boxes_dev, reverse, out_dev, regs, log, s);
+    if (e != cudaSuccess) {
+      tsi_internal_set_error(cudaGetErrorString(e));
+      st = TSI_ERR_CUDA;
+    }
   }
-  return TSI_OK;
+  if (caller_dev >= 0 && caller_dev != v.device) cudaSetDevice(caller_dev);
+  return st;
 }

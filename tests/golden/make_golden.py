@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import os
 import math
 import struct
 import sys
@@ -119,7 +120,10 @@ def run_case(case):
 
 
 def main() -> None:
-    ref = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    # the reference checkout: the first argument, else TSI_REFERENCE_DIR, else
+    # a `reference` folder beside this repository
+    default = os.environ.get("TSI_REFERENCE_DIR", str(ROOT.parent / "reference"))
+    ref = Path(sys.argv[1]) if len(sys.argv) > 1 else Path(default)
     if (ref / "scenes").exists():
         write_tapes(ref)
     results = {case[0]: run_case(case) for case in oracle_cases()}

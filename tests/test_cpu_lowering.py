@@ -4,6 +4,7 @@ reference's four scene files.  No device needed."""
 from __future__ import annotations
 
 import ctypes as C
+import os
 import re
 import struct
 from pathlib import Path
@@ -16,7 +17,9 @@ from golden.make_golden import load_tape
 from temporalsetinversion_b200 import _native as N, api, scenes
 
 ROOT = Path(__file__).resolve().parents[1]
-REF = Path("/root/reference")
+# the reference checkout: TSI_REFERENCE_DIR, else a `reference` folder beside
+# this repository; the tests that read its scene files skip without it
+REF = Path(os.environ.get("TSI_REFERENCE_DIR", str(ROOT.parent / "reference")))
 FIXTURE_COUNTS = {"cables": 297, "cradle": 329, "piano": 325, "sponza": 307}
 
 
