@@ -23,13 +23,23 @@ temporally reused frames, like one run of the animation.
           without waiting (tsi_scene_invert_async, tsi_scene_trace_async);
           the fully synchronous loop is reported beside it
   roofline: the refinement kernel's algorithmic FP32 operations (opcost.h
-          table, per executed interval instruction) against the nominal
-          FP32 rate, plus the tracer's node traffic against measured HBM
-  cpu_baseline: the CPU oracle (C++ restatement of compute.wgsl, OpenMP)
-          on a bounded sample of the same animation
-  served : open-loop Poisson requests through the serving layer, p50/p99
-          latency beside the plain path's per-frame latency (eight runs of
-          the workload's animation)
+          table: the FULL tape's forward ops per evaluated cell, pruning not
+          subtracted) over the inversion's device time, against the nominal
+          FP32 rate; the executed (pruned) ops beside it; cells/s,
+          interval-instruction evaluations/s and rays/s on the line
+  roofline_trace: the tracer's node traffic (40 B per node visited + 16 B
+          per pixel) against measured HBM, visits per ray beside it
+  invert_levels: device ms and cells of each level's launch (CUDA events
+          between launches, a separate context after the timed region)
+  cpu_baseline: the CPU oracle (C++ restatement of compute.wgsl, OpenMP;
+          tape lowered by the oracle's own ir.rs restatement) on a bounded
+          sample of the same frames
+  temporal: the reference's published comparison, temporal set inversion
+          against full per-frame re-evaluation (tsi_scene_reset each frame)
+  served : open-loop Poisson requests through the continuous server at
+          rates relative to the plain path's capacity (and the static-batch
+          server at one rate), p50/p99 latency beside the plain path's
+          per-frame latency (eight runs of the workload's animation)
   served_mix: the same over a 64-scene pool with mixed levels, sweeps,
           resolutions and cameras
   batched: 32 scenes (8..2048 primitives, localsubdiv 7..10, 1024x1024)
@@ -41,8 +51,8 @@ temporally reused frames, like one run of the animation.
 
 --impl reference times the CPU restatement (the reference itself is WGSL
 under wgpu/Vulkan: no Vulkan driver or Rust toolchain exists on these
-machines) on the same workload and prints the same line with
-"impl": "reference".
+machines) on the GPU arm's frames (warm-up frames untimed, then the timed
+steps) and prints the same line with "impl": "reference".
 
 Multi-GPU (--gpus N, launched under torchrun): replicas.  The frames of one
 animation depend on each other through the resident octree, so each rank
@@ -56,6 +66,7 @@ parts on one GPU.)
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import math
 import os
@@ -76,10 +87,12 @@ WORKLOAD = dict(name="csg256_L10_1080p_120f", n_prims=256, seed=1, localsubdiv=1
 METRIC = "frames/s @ subdiv 10, 1080p"
 PEAK_FP32_NOMINAL_TOPS = 148 * 128 * 1.965  # G ops/s: 148 SMs x 128 FP32 lanes x 1.965 GHz (non-FMA)
 # DRAM bytes (read + write) per launch from one ncu capture of this workload's
-# frame 4 (profiles/dram_csg256_L10_1080p.md): refine_kernel averaged over the
-# frame's ten level launches, trace_kernel per frame
+# frame 4 (dram__bytes_read.sum + dram__bytes_write.sum): refine_kernel
+# averaged over the frame's ten level launches, trace_kernel per frame.
+# Constants of that capture, not measured by this run.
 TRAFFIC_REFINE_PER_LAUNCH = 0.839e6
 TRAFFIC_TRACE_PER_LAUNCH = 21.11e6
+TRAFFIC_SOURCE = "one ncu capture of frame 4 of this workload (constant, not measured by this run)"
 
 
 def frame_time(i: int, frames: int) -> float:
@@ -204,68 +217,268 @@ def build_workload(seed: int):
 
 
 # ------------------------------------------------------------------ CPU legs
-def cpu_sample(text: str, params, view, frames: int = 3, threads: int = 0) -> dict:
-    """Oracle on the first `frames` frames of the animation (invert + trace)."""
+def reference_params(**kw):
+    """tsi_params for the CPU oracle without loading the library: the
+    PARAMETERS block defaults (compute.wgsl:3494-3511) and the root box of
+    ir.rs:343-347, overridden by name (tests check them against
+    tsi_default_params)."""
+    from temporalsetinversion_b200 import _native as N
+    p = N.Params()
+    p.localsubdiv, p.delta, p.pointsample, p.fastenabled = 8, 0.01, 1, 1
+    p.lipschitz_corrected = p.swept_volume = p.fast_normals = p.normal_viz = p.rounding_mode = 0
+    p.fast_multiplier, p.scene_id, p.octree_darken_factor = 1.0, 1, 0.98
+    for i in range(3):
+        p.root_lo[i], p.root_hi[i] = -5.0, 5.0
+    p.pruning, p.swept_dt = 1, 1.0 / 60.0
+    p.cinematic, p.samples, p.see_background = 0, 8, 0
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def workload_params_ref():
+    return reference_params(localsubdiv=WORKLOAD["localsubdiv"], delta=WORKLOAD["delta"],
+                            lipschitz_corrected=WORKLOAD["lipschitz_corrected"], pointsample=WORKLOAD["pointsample"],
+                            fast_normals=WORKLOAD["fast_normals"])
+
+
+def oracle_scene(text: str, params):
+    """The CPU oracle on the scene's tape, lowered by the oracle's own
+    restatement of ir.rs (oracle/ir_ref.py), so nothing of the product's
+    library runs in the CPU legs."""
+    import oracle
+    from oracle import ir_ref
+    from temporalsetinversion_b200.api import GPU_INSTR_DTYPE
+    rows = ir_ref.lower(text, 0.0)
+    tape = np.zeros(len(rows), GPU_INSTR_DTYPE)
+    for k, r in enumerate(rows):
+        tape[k] = (r[0], r[1], r[2], r[3], (r[4], r[5]), (r[6], r[7]))
+    return oracle.Scene(tape, params)
+
+
+def cpu_frames(S, view, frames, threads: int) -> float:
+    """Invert + trace the animation's frames `frames` on the oracle with
+    `threads` OpenMP threads (the octree re-seeded at frame 0 of each run of
+    the animation, as in the GPU arm); seconds."""
     import oracle
     from temporalsetinversion_b200 import api
-    if threads:
-        oracle.set_threads(threads)
-    tape = api.IR.new(text).gpu_instructions
-    S = oracle.Scene(tape, params)
+    oracle.set_threads(threads)
+    F = WORKLOAD["frames"]
     t0 = time.perf_counter()
-    for i in range(frames):
-        t = frame_time(i, WORKLOAD["frames"])
+    for i in frames:
+        t = frame_time(i, F)
+        if i % F == 0:
+            S.reset()
         S.invert(t)
-        u = api.make_uniforms(view, (WORKLOAD["width"], WORKLOAD["height"]), t)
-        S.trace(u)
-    dt = time.perf_counter() - t0
-    return {"value": frames / dt, "unit": "frames/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": "CPU oracle (C++ restatement of compute.wgsl main + rt_main, OpenMP) on frames 0..%d of the "
-                      "workload (first_eval frame included), full 1920x1080 trace, %.1f s" % (frames - 1, dt)}
+        S.trace(api.make_uniforms(view, (WORKLOAD["width"], WORKLOAD["height"]), t))
+    return time.perf_counter() - t0
+
+
+def all_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline_sample(text: str, view, warmup: int) -> dict:
+    """The oracle on a bounded sample of the GPU arm's frames: frames
+    0 .. warmup-1 untimed (the first_eval frame builds the octree), then two
+    frames on one thread and ten frames on all host threads, timed."""
+    S = oracle_scene(text, workload_params_ref())
+    cores = all_cores()
+    cpu_frames(S, view, range(warmup), cores)
+    one = cpu_frames(S, view, range(warmup, warmup + 2), 1)
+    many = cpu_frames(S, view, range(warmup + 2, warmup + 12), cores)
+    return {"value": 10 / many, "unit": "frames/s", "cores": cores, "kind": "port",
+            "sample": "CPU oracle (C++ restatement of compute.wgsl main + rt_main, OpenMP; tape lowered by "
+                      "oracle/ir_ref.py) on frames %d..%d of the workload after untimed frames 0..%d, full "
+                      "1920x1080 trace, %.1f s" % (warmup + 2, warmup + 11, warmup - 1, many),
+            "single_thread": {"value": 2 / one, "unit": "frames/s", "cores": 1,
+                              "sample": "frames %d..%d on one thread, %.1f s" % (warmup, warmup + 1, one)}}
+
+
+def line_config(tape_slots: int, registers=None, world: int = 1) -> dict:
+    cfg = {"workload": WORKLOAD["name"], "localsubdiv": 10, "resolution": "1920x1080", "frames": WORKLOAD["frames"],
+           "tape_slots": tape_slots, "parallelism": "replicas" if world > 1 else "single",
+           "l2": "flushed between steps (256 MB write outside the per-step events)"}
+    if registers is not None:
+        cfg["registers"] = registers
+    return cfg
 
 
 def run_reference(args, rank, world, dist) -> None:
+    """The CPU restatement of the reference's path (the reference's own WGSL
+    under wgpu/Vulkan cannot run on these machines) on the GPU arm's frames:
+    frames 0 .. warmup-1 untimed, then `steps` frames timed (at most one run
+    of the 120-frame animation), all host threads.  Rank 0 only."""
     if rank != 0:
         return
-    text, params, view = build_workload(WORKLOAD["seed"])
-    frames = max(1, min(args.steps, 3))
-    res = cpu_sample(text, params, view, frames=frames)
+    from temporalsetinversion_b200 import scenes
+    text = scenes.csg(WORKLOAD["n_prims"], WORKLOAD["seed"])
+    view = scenes.camera_look_at(WORKLOAD["eye"])
+    S = oracle_scene(text, workload_params_ref())
+    cores = all_cores()
+    W, K = args.warmup, max(1, min(args.steps, WORKLOAD["frames"]))
+    cpu_frames(S, view, range(W), cores)
+    dt = cpu_frames(S, view, range(W, W + K), cores)
+    value = K / dt
+    tape_slots = 4697
     line = {
-        "metric": METRIC, "value": res["value"], "unit": "frames/s", "n_gpus": world, "steps": frames,
-        "warmup": 0, "ms_per_step": 1000.0 / res["value"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded CSG scene, LLVM IR tape)",
-        "config": {"workload": WORKLOAD["name"], "localsubdiv": 10, "resolution": "1920x1080", "frames": 120,
-                   "tape_slots": 4697, "l2": "n/a (CPU)"},
+        "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": 1000.0 * dt / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded CSG scene emitted as LLVM IR, lowered like scenes/*.ll)",
+        "config": line_config(tape_slots, world=world),
         "impl": "reference",
-        "cpu_baseline": {"value": res["value"], "unit": "frames/s", "cores": res["cores"], "kind": "port",
-                         "sample": res["sample"] + "; the reference's WGSL path (wgpu/Vulkan) cannot run here"},
-        "e2e": {"value": res["value"], "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": "frames/s", "cores": cores, "kind": "port",
+                         "sample": "CPU oracle (C++ restatement of compute.wgsl main + rt_main, OpenMP; tape lowered "
+                                   "by oracle/ir_ref.py) on frames %d..%d after untimed frames 0..%d, the GPU arm's "
+                                   "frames; the reference's WGSL path (wgpu/Vulkan) cannot run here" % (W, W + K - 1, W - 1)},
+        "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ temporal leg
+TEMPORAL = dict(frames=40, skip=4)
+
+
+def temporal_leg(local: int) -> dict:
+    """The reference's published comparison (docs/index.html:41): temporal
+    set inversion against full per-frame re-evaluation at delta 0.01.  The
+    headline animation's frames inverted twice, on the carried-over octree
+    and with tsi_scene_reset before every frame (the first_eval path); the
+    same frames' inversion (and inversion + 1080p trace) device times."""
+    from temporalsetinversion_b200 import Device, Scene, Tape, _native as N, api
+    text, params, view = build_workload(WORKLOAD["seed"])
+    W, H, F = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["frames"]
+    dev = Device(local)
+    try:
+        scene = Scene(dev, Tape.from_llvm_ir(dev, text), params, voxel_capacity=64 << 20)
+        out = {}
+        for mode in ("carried", "reset"):
+            scene.reset()
+            inv, tr, cells = 0.0, 0.0, 0
+            for i in range(TEMPORAL["frames"]):
+                t = frame_time(i, F)
+                if mode == "reset":
+                    scene.reset()
+                st = scene.invert(t)
+                ts = N.Stats()
+                u = api.make_uniforms(view, (W, H), t)
+                N.check(dev.lib.tsi_scene_trace(scene.handle, C.byref(u), None, C.byref(ts)), "tsi_scene_trace")
+                if i >= TEMPORAL["skip"]:
+                    inv += st.device_ms
+                    tr += ts.device_ms
+                    cells += st.cells_evaluated
+            n = TEMPORAL["frames"] - TEMPORAL["skip"]
+            out[mode] = {"invert_ms": inv / n, "frame_ms": (inv + tr) / n, "cells_evaluated": cells // n}
+        return {"frames": "%d..%d" % (TEMPORAL["skip"], TEMPORAL["frames"] - 1), **out,
+                "invert_speedup": out["reset"]["invert_ms"] / out["carried"]["invert_ms"],
+                "frame_speedup": out["reset"]["frame_ms"] / out["carried"]["frame_ms"],
+                "cells_ratio": out["reset"]["cells_evaluated"] / max(1, out["carried"]["cells_evaluated"]),
+                "note": "headline animation (256 primitives, localsubdiv 10, delta 0.01); reset = the octree "
+                        "rebuilt from the root every frame; device ms per frame"}
+    finally:
+        dev.close()
+
+
+# ------------------------------------------------------------------ serving helpers
+def open_loop(srv, items, arrivals, submit) -> dict:
+    """Submits items[k] at start + arrivals[k] (Poisson open loop), collects
+    every ticket; latencies of the completed requests, wall time from the
+    first submission to the last completion, refused submissions."""
+    import threading
+
+    from temporalsetinversion_b200 import _native as N
+    tickets, lats, errors = [], [], []
+    refused = [0]
+    submitted_all = threading.Event()
+    done = threading.Event()
+
+    def collect():
+        i = 0
+        while True:
+            if i >= len(tickets):
+                if submitted_all.is_set() and i >= len(tickets):
+                    break
+                time.sleep(0.0002)
+                continue
+            try:
+                r = srv.poll(tickets[i], 1000)
+            except Exception as e:  # the request failed: count it, go on
+                errors.append(str(e))
+                i += 1
+                continue
+            if r is not None:
+                lats.append(r[1])
+                i += 1
+        done.set()
+
+    th = threading.Thread(target=collect, daemon=True)
+    th.start()
+    start = time.perf_counter()
+    for k, it in enumerate(items):
+        delay = start + arrivals[k] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        try:
+            tickets.append(submit(srv, it))
+        except N.TsiError as e:  # queue full or over the memory budget
+            refused[0] += 1
+    submitted_all.set()
+    done.wait(300.0)
+    wall = time.perf_counter() - start
+    th.join(5.0)
+    lats = np.sort(np.asarray(lats)) if lats else np.zeros(1)
+    return {"requests": int(len(lats)), "frames_per_s": len(lats) / wall, "p50_ms": float(np.percentile(lats, 50)),
+            "p99_ms": float(np.percentile(lats, 99)), "max_ms": float(lats[-1]), "failed": len(errors),
+            "refused": refused[0], "first_error": errors[0] if errors else None}
+
+
+def served_runs(dev, plain: dict, rates, seconds: float, rng, draw, submit, static_at=None) -> list:
+    """Open-loop runs through the continuous server at each rate (and the
+    static-batch server at `static_at` for comparison)."""
+    from temporalsetinversion_b200 import Server
+    runs = []
+    plan = [(r, False) for r in rates] + ([(static_at, True)] if static_at else [])
+    for rate, static in plan:
+        n = int(rate * seconds)
+        items = draw(n)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+        with Server(dev, static_batches=static) as srv:
+            r = open_loop(srv, items, arrivals, submit)
+            ss = srv.stats()
+        r.update({"rate_rps": rate, "rate_vs_plain": rate / plain["frames_per_s"],
+                  "form": "static batches" if static else "continuous",
+                  "vs_plain_frames_per_s": r["frames_per_s"] / plain["frames_per_s"],
+                  "p99_vs_plain_p50": r["p99_ms"] / plain["p50_ms"], "p99_vs_plain_p99": r["p99_ms"] / plain["p99_ms"],
+                  "mean_running": ss["mean_batch"]})
+        runs.append(r)
+    return runs
+
+
 # ------------------------------------------------------------------ served leg
-SERVED = dict(scenes=8, rates_rps=(400.0, 1600.0), seconds=1.5, seed=1000)
+SERVED = dict(scenes=8, rates_vs_plain=(0.8, 2.0, 4.0), static_vs_plain=2.0, seconds=1.5, seed=1000)
 
 
 def served_leg(local: int) -> dict:
     """Open-loop Poisson arrivals over SERVED["scenes"] concurrent runs of the
     workload's animation (scene k starts at frame 15 k; each request: the
     next frame of one scene, inverted and traced at 1920x1080 with the frame
-    left on the device) through the serving layer at each rate of
-    SERVED["rates_rps"], against the plain path's per-frame latency and
-    frames/s on one scene (one synchronous tsi_scene_invert +
-    tsi_scene_trace per frame)."""
-    import threading
-
-    from temporalsetinversion_b200 import Device, Scene, Server, Tape, api
+    left on the device), at rates relative to the plain path's capacity,
+    through the continuous server (and the static-batch server at one rate),
+    against the plain path's per-frame latency and frames/s on one scene (one
+    synchronous tsi_scene_invert + tsi_scene_trace per frame)."""
+    from temporalsetinversion_b200 import Device, Scene, Tape, api
 
     W, H, F = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["frames"]
     dev = Device(local)
     try:
         work = [build_workload(WORKLOAD["seed"]) for k in range(SERVED["scenes"])]
         sc = [Scene(dev, Tape.from_llvm_ir(dev, t), p) for t, p, _ in work]
-        # plain path: one scene, one synchronous call pair per frame
         lat_plain = []
         for i in range(40):
             t = frame_time(i, F)
@@ -278,67 +491,38 @@ def served_leg(local: int) -> dict:
                 lat_plain.append((time.perf_counter() - t0) * 1000.0)
         plain = {"p50_ms": float(np.percentile(lat_plain, 50)), "p99_ms": float(np.percentile(lat_plain, 99)),
                  "frames_per_s": 1000.0 * len(lat_plain) / float(np.sum(lat_plain))}
-        # wide thresholds for running the eight together (the plain path above
-        # keeps the single-scene ones)
-        tune = api.batch_autotune(dev, [(s, frame_time(15 * k, F)) for k, s in enumerate(sc)], frames=3)
         rng = np.random.default_rng(SERVED["seed"])
         frame = [15 * k for k in range(SERVED["scenes"])]
-        runs = []
-        with Server(dev) as srv:
-            for rate in SERVED["rates_rps"]:
-                n = int(rate * SERVED["seconds"])
-                arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
-                which = rng.integers(0, SERVED["scenes"], n)
-                tickets = []
-                done = threading.Event()
-                lats = []
-                b0 = srv.stats()
 
-                def collect():
-                    i = 0
-                    while i < n:
-                        if i >= len(tickets):
-                            time.sleep(0.0002)
-                            continue
-                        r = srv.poll(tickets[i], 1000)
-                        if r is not None:
-                            lats.append(r[1])
-                            i += 1
-                    done.set()
+        def draw(n):
+            which = rng.integers(0, SERVED["scenes"], n)
+            out = []
+            for j in which:
+                j = int(j)
+                t = frame_time(frame[j], F)
+                frame[j] += 1
+                out.append((j, t, api.make_uniforms(work[j][2], (W, H), t)))
+            return out
 
-                th = threading.Thread(target=collect, daemon=True)
-                th.start()
-                start = time.perf_counter()
-                for k in range(n):
-                    delay = start + arrivals[k] - time.perf_counter()
-                    if delay > 0:
-                        time.sleep(delay)
-                    j = int(which[k])
-                    t = frame_time(frame[j], F)
-                    frame[j] += 1
-                    tickets.append(srv.submit(sc[j], t, uniforms=api.make_uniforms(work[j][2], (W, H), t)))
-                done.wait(120.0)
-                wall = time.perf_counter() - start
-                th.join(5.0)
-                b1 = srv.stats()
-                lats = np.sort(np.asarray(lats))
-                nb = max(1, b1["batches"] - b0["batches"])
-                runs.append({"rate_rps": rate, "requests": int(len(lats)), "frames_per_s": len(lats) / wall,
-                             "vs_plain_frames_per_s": len(lats) / wall / plain["frames_per_s"],
-                             "p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
-                             "max_ms": float(lats[-1]), "p99_vs_plain_p50": float(np.percentile(lats, 99)) / plain["p50_ms"],
-                             "mean_batch": (b1["completed"] - b0["completed"]) / nb})
-        return {"scenes": SERVED["scenes"], "plain": plain, "runs": runs, "batch_threshold_scale": tune["scale"],
+        def submit(srv, it):
+            j, t, u = it
+            return srv.submit(sc[j], t, uniforms=u)
+
+        rates = [r * plain["frames_per_s"] for r in SERVED["rates_vs_plain"]]
+        runs = served_runs(dev, plain, rates, SERVED["seconds"], rng, draw, submit,
+                           static_at=SERVED["static_vs_plain"] * plain["frames_per_s"])
+        return {"scenes": SERVED["scenes"], "plain": plain, "runs": runs,
                 "note": "Poisson arrivals, next frame of a random scene (8 runs of the workload's animation), "
-                        "invert + 1080p trace, frame kept on device; latency from submit to completion"}
+                        "invert + 1080p trace, frame kept on device; latency from submit to completion; "
+                        "rates relative to the plain path's frames/s"}
     finally:
         dev.close()
 
 
 # ------------------------------------------------------------------ served mix leg
-SERVED_MIX = dict(pool=64, rates_rps=(200.0, 800.0), seconds=1.5, seed=2000, sweep_fraction=0.2,
-                  continue_fraction=0.7, levels=(8, 9, 10), resolutions=((512, 512), (1280, 720), (1920, 1080)),
-                  hbm_budget_bytes=150 * 10**9)
+SERVED_MIX = dict(pool=64, rates_vs_plain=(0.8, 2.0, 4.0), static_vs_plain=2.0, seconds=1.5, seed=2000,
+                  sweep_fraction=0.2, continue_fraction=0.7, levels=(8, 9, 10),
+                  resolutions=((512, 512), (1280, 720), (1920, 1080)), hbm_budget_bytes=150 * 10**9)
 
 
 def served_mix_leg(local: int) -> dict:
@@ -348,15 +532,15 @@ def served_mix_leg(local: int) -> dict:
     request continues its scene at t + 1/60 with probability 0.7, else
     jumps to a random t, with a random camera on the radius-2.5 sphere and a
     resolution drawn from 512x512, 1280x720, 1920x1080.  Poisson arrivals
-    through the serving layer at each rate, against the same request
-    sequence run one synchronous plain call pair at a time."""
-    import threading
-
-    from temporalsetinversion_b200 import Device, Scene, Server, Tape, api, scenes
+    at rates relative to the plain path's capacity through the continuous
+    server (and the static-batch server at one rate), against the same kind
+    of request sequence run one synchronous plain call pair at a time;
+    scenes and frames are admitted against a 150 GB HBM budget."""
+    from temporalsetinversion_b200 import Device, Scene, Tape, api, scenes
 
     cfg = SERVED_MIX
     rng = np.random.default_rng(cfg["seed"])
-    dev = Device(local, hbm_budget_bytes=SERVED_MIX["hbm_budget_bytes"])  # scenes and frames admitted against it
+    dev = Device(local, hbm_budget_bytes=cfg["hbm_budget_bytes"])
     try:
         pool = []
         for k in range(cfg["pool"]):
@@ -388,7 +572,6 @@ def served_mix_leg(local: int) -> dict:
                 out.append((j, t_now[j], t_now[j] - 1.0 / 60.0 if sweep else math.nan, u))
             return out
 
-        # plain: the requests one synchronous call pair at a time
         plain_reqs = draw(200)
         lat = []
         t0 = time.perf_counter()
@@ -400,53 +583,19 @@ def served_mix_leg(local: int) -> dict:
             lat.append((time.perf_counter() - a) * 1000.0)
         plain = {"frames_per_s": len(plain_reqs) / (time.perf_counter() - t0),
                  "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
-        runs = []
-        with Server(dev) as srv:
-            for rate in cfg["rates_rps"]:
-                n = int(rate * cfg["seconds"])
-                reqs = draw(n)
-                arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
-                tickets, lats, errors = [], [], []
-                done = threading.Event()
 
-                def collect():
-                    i = 0
-                    while i < n:
-                        if i >= len(tickets):
-                            time.sleep(0.0002)
-                            continue
-                        try:
-                            r = srv.poll(tickets[i], 1000)
-                        except Exception as e:  # the request failed: count it, go on
-                            errors.append(str(e))
-                            i += 1
-                            continue
-                        if r is not None:
-                            lats.append(r[1])
-                            i += 1
-                    done.set()
+        def submit(srv, it):
+            j, t, t0r, u = it
+            return srv.submit(pool[j], t, t0=t0r, uniforms=u)
 
-                th = threading.Thread(target=collect, daemon=True)
-                th.start()
-                start = time.perf_counter()
-                for k, (j, t, t0r, u) in enumerate(reqs):
-                    delay = start + arrivals[k] - time.perf_counter()
-                    if delay > 0:
-                        time.sleep(delay)
-                    tickets.append(srv.submit(pool[j], t, t0=t0r, uniforms=u))
-                done.wait(300.0)
-                wall = time.perf_counter() - start
-                th.join(5.0)
-                lats = np.sort(np.asarray(lats))
-                runs.append({"rate_rps": rate, "requests": int(len(lats)), "frames_per_s": len(lats) / wall,
-                             "vs_plain_frames_per_s": len(lats) / wall / plain["frames_per_s"],
-                             "p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
-                             "p99_vs_plain_p50": float(np.percentile(lats, 99)) / plain["p50_ms"],
-                             "failed": len(errors), "first_error": errors[0] if errors else None})
+        rates = [r * plain["frames_per_s"] for r in cfg["rates_vs_plain"]]
+        runs = served_runs(dev, plain, rates, cfg["seconds"], rng, draw, submit,
+                           static_at=cfg["static_vs_plain"] * plain["frames_per_s"])
         return {"pool": cfg["pool"], "plain": plain, "runs": runs, "scene_bytes": dev.scenes_bytes(),
                 "hbm_budget_bytes": cfg["hbm_budget_bytes"],
                 "note": "cfg4-style mix: 64 scenes (L 8/9/10, 20% swept), 70% continue at t+1/60, "
-                        "resolutions 512^2 / 1280x720 / 1920x1080, random cameras; frames kept on the device"}
+                        "resolutions 512^2 / 1280x720 / 1920x1080, random cameras; frames kept on the device; "
+                        "rates relative to the plain path's frames/s"}
     finally:
         dev.close()
 
@@ -664,6 +813,50 @@ def split_leg(local: int) -> dict:
         dev.close()
 
 
+# ------------------------------------------------------------------ level profile
+def level_profile(local: int, text: str, params, frames=(4, 5, 6, 7, 8)) -> dict:
+    """Device ms of each level's refinement launch (CUDA events between the
+    launches, TSI_PROFILE_LEVELS) and cells evaluated per level, averaged
+    over the animation's frames `frames` (carried-over frames), on a separate
+    context after the timed region."""
+    from temporalsetinversion_b200 import Device, Scene, Tape, _native as N
+    os.environ["TSI_PROFILE_LEVELS"] = "1"
+    try:
+        dev = Device(local)
+    finally:
+        del os.environ["TSI_PROFILE_LEVELS"]
+    try:
+        scene = Scene(dev, Tape.from_llvm_ir(dev, text), params, voxel_capacity=64 << 20)
+        F = WORKLOAD["frames"]
+        acc_ms, acc_cells, n = None, None, 0
+        for i in range(max(frames) + 1):
+            scene.invert(frame_time(i, F))
+            if i not in frames:
+                continue
+            L = 32
+            ms = (C.c_float * L)()
+            ctr = (C.c_uint64 * (L * len(N.LEVEL_COUNTERS)))()
+            nl = C.c_uint32(0)
+            N.check(dev.lib.tsi_debug_level_profile(dev.handle, L, ms, ctr, C.byref(nl)), "tsi_debug_level_profile")
+            k = min(nl.value, L)
+            NC = len(N.LEVEL_COUNTERS)
+            lm = [ms[j] for j in range(k)]
+            rows = [[ctr[j * NC + q] for q in range(NC)] for j in range(k)]
+            acc_ms = lm if acc_ms is None else [a + b for a, b in zip(acc_ms, lm)]
+            acc_cells = rows if acc_cells is None else [[a + b for a, b in zip(r0, r1)] for r0, r1 in zip(acc_cells, rows)]
+            n += 1
+        names = N.LEVEL_COUNTERS
+        keep = ("evaluated", "wide_items", "cyc_wide_max", "cyc_narrow", "cyc_narrow_max", "instr_fwd", "instr_full")
+        per = {name: [r[names.index(name)] // n for r in acc_cells] for name in keep}
+        # narrow items per level: every narrow item counted its parents; wide
+        # cells count one parent per group finish
+        return {"ms": [round(v / n, 4) for v in acc_ms], "counters": per, "frames": list(frames),
+                "note": "CUDA events between the level launches of one frame; counters per level (SM cycles "
+                        "are clock64 of the item on its SM)"}
+    finally:
+        dev.close()
+
+
 # ------------------------------------------------------------------ GPU leg
 def run_gpu(args, rank, world, local, dist) -> None:
     import ctypes as C
@@ -686,7 +879,7 @@ def run_gpu(args, rank, world, local, dist) -> None:
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
 
     totals = {k: 0 for k in ("cells_evaluated", "instr_forward", "instr_reverse", "instr_full_equiv", "fp32_ops",
-                             "cells_reused", "cells_reverse")}
+                             "fp32_ops_full_fwd", "fp32_ops_full_rev", "cells_reused", "cells_reverse")}
     inv_ms, trace_ms = [], []
     visits = 0.0
 
@@ -763,9 +956,13 @@ def run_gpu(args, rank, world, local, dist) -> None:
         return
     peaks = measured_peaks()
     inv_total_s = sum(inv_ms) / 1000.0
-    ops = totals["fp32_ops"]
-    achieved_gops = ops / inv_total_s / 1e9 if inv_total_s > 0 else 0.0
     trace_s = sum(trace_ms) / 1000.0
+    # algorithmic work (opcost.h table) on the FULL tape, whatever pruning
+    # saved: forward ops of every evaluated cell; reverse ops beside it
+    alg_fwd, alg_rev = totals["fp32_ops_full_fwd"], totals["fp32_ops_full_rev"]
+    executed = totals["fp32_ops"]
+    peak_gops = PEAK_FP32_NOMINAL_TOPS
+    achieved_gops = alg_fwd / inv_total_s / 1e9 if inv_total_s > 0 else 0.0
     trace_bytes = visits * 40.0 + W * H * 16.0 * len(trace_ms)
     trace_gbs = trace_bytes / trace_s / 1e9 if trace_s > 0 else 0.0
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
@@ -775,25 +972,35 @@ def run_gpu(args, rank, world, local, dist) -> None:
         "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded CSG scene emitted as LLVM IR, lowered like scenes/*.ll)",
-        "config": {"workload": WORKLOAD["name"], "localsubdiv": 10, "resolution": "1920x1080", "frames": F,
-                   "tape_slots": tape.instruction_count, "registers": tape.registers,
-                   "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "flushed between steps (256 MB write outside the per-step events)"},
+        "config": line_config(tape.instruction_count, tape.registers, world),
         "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": C.sizeof(N.Uniforms) + 160,
                 "d2h_bytes_per_step": W * H * 16 + C.sizeof(N.Stats),
                 "readback": "frames queued without waiting (tsi_scene_invert_async, tsi_scene_trace_async); "
                             "frame i's copy to pinned host memory overlaps frame i+1's inversion; errors checked "
                             "at the end (tsi_scene_invert_wait)",
                 "synchronous_value": e2e_sync_value},
+        "cells_per_s": totals["cells_evaluated"] / inv_total_s if inv_total_s > 0 else 0.0,
+        "instr_evals_per_s": totals["instr_full_equiv"] / inv_total_s if inv_total_s > 0 else 0.0,
+        "rays_per_s": W * H * len(trace_ms) / trace_s if trace_s > 0 else 0.0,
         "roofline": {"kernel": "refine_kernel (interval tape interpreter)", "bound": "fp32",
-                     "achieved": achieved_gops / 1000.0, "peak": PEAK_FP32_NOMINAL_TOPS / 1000.0, "unit": "TOP/s",
-                     "frac": achieved_gops / PEAK_FP32_NOMINAL_TOPS, "traffic": TRAFFIC_REFINE_PER_LAUNCH,
-                     "traffic_unit": "bytes per launch (ncu, dram read + write)",
-                     "peak_source": "nominal FP32 (MEASURED_PEAKS.json has no FP32 figure)",
-                     "ops_per_step": ops / args.steps},
+                     "achieved": achieved_gops / 1000.0, "peak": peak_gops / 1000.0, "unit": "TOP/s",
+                     "frac": achieved_gops / peak_gops,
+                     "work": "opcost.h forward FP32 ops of the full tape (fix included) per evaluated cell, "
+                             "pruning not subtracted; achieved = that / inversion device time",
+                     "alg_fwd_ops_per_step": alg_fwd / args.steps, "alg_rev_ops_per_step": alg_rev / args.steps,
+                     "frac_with_reverse": (alg_fwd + alg_rev) / inv_total_s / 1e9 / peak_gops if inv_total_s > 0 else 0.0,
+                     "executed_ops_per_step": executed / args.steps,
+                     "executed_frac": executed / inv_total_s / 1e9 / peak_gops if inv_total_s > 0 else 0.0,
+                     "cells_evaluated_per_step": totals["cells_evaluated"] / args.steps,
+                     "invert_ms_per_step": sum(inv_ms) / args.steps,
+                     "traffic": TRAFFIC_REFINE_PER_LAUNCH, "traffic_unit": "bytes per launch (ncu, dram read + write)",
+                     "traffic_source": TRAFFIC_SOURCE,
+                     "peak_source": "nominal FP32 rate, 148 SMs x 128 lanes x 1.965 GHz (MEASURED_PEAKS.json has no "
+                                    "FP32 figure)"},
         "roofline_trace": {"kernel": "trace_kernel", "bound": "hbm", "achieved": trace_gbs, "peak": hbm_peak,
                            "unit": "GB/s", "frac": trace_gbs / hbm_peak, "traffic": TRAFFIC_TRACE_PER_LAUNCH,
-                           "traffic_unit": "bytes per launch (ncu, dram read + write)",
+                           "traffic_unit": "bytes per launch (ncu, dram read + write)", "traffic_source": TRAFFIC_SOURCE,
+                           "visits_per_ray": visits / (W * H * len(trace_ms)) if trace_ms else 0.0,
                            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "breakdown_ms_per_step": {"invert": sum(inv_ms) / args.steps, "trace": sum(trace_ms) / args.steps},
         "work_per_step": {k: v / args.steps for k, v in totals.items()},
@@ -801,20 +1008,23 @@ def run_gpu(args, rank, world, local, dist) -> None:
         "gpu_launches": gpu_launches,
         "wall_s": wall,
     }
+    if world == 1:
+        try:
+            line["invert_levels"] = level_profile(local, text, params)
+        except Exception as e:
+            line["invert_levels"] = {"unavailable": str(e)}
     if not args.no_cpu_baseline and world == 1:
         try:
-            cb = cpu_sample(text, params, view, frames=2)
-            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
-            cores = cb["cores"]
-            one = cpu_sample(text, params, view, frames=2, threads=1)  # the same frames on one core
-            line["cpu_baseline"]["single_thread"] = {"value": one["value"], "unit": "frames/s", "cores": 1,
-                                                     "sample": one["sample"]}
-            import oracle
-            oracle.set_threads(cores)
+            line["cpu_baseline"] = cpu_baseline_sample(text, view, args.warmup)
         except Exception as e:  # the oracle needs g++ on the host
             line["cpu_baseline"] = {"value": None, "unit": "frames/s", "cores": 0, "kind": "port",
                                     "sample": "unavailable: %s" % e}
     dev.close()
+    if world == 1 and not args.no_temporal:
+        try:
+            line["temporal"] = temporal_leg(local)
+        except Exception as e:
+            line["temporal"] = {"unavailable": str(e)}
     if world == 1 and not args.no_served:
         try:
             line["served"] = served_leg(local)
@@ -855,6 +1065,7 @@ def main() -> None:
     ap.add_argument("--no-batched", action="store_true", help="skip the 32-scene batched leg")
     ap.add_argument("--no-swept", action="store_true", help="skip the swept-volume leg")
     ap.add_argument("--no-split", action="store_true", help="skip the root-split leg")
+    ap.add_argument("--no-temporal", action="store_true", help="skip the temporal-reuse comparison leg")
     ap.add_argument("--small-arenas", action="store_true",
                     help="small work-item, tape and log arenas (use with --voxels 4194304 under a profiler)")
     args = ap.parse_args()

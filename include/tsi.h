@@ -105,6 +105,10 @@ typedef struct tsi_params {
   float root_hi[3];
   int32_t pruning;              /* per-cell tape pruning (1 = on); never changes results */
   float swept_dt;               /* swept interval length when t0 is NaN (1/60, compute.wgsl:3605) */
+  int32_t cinematic;            /* path tracing with sun light, shadow rays and sky (`cinematic`,
+                                 * compute.wgsl:3499, get_color_single 4444-4523) */
+  int32_t samples;              /* cinematic samples per pixel (`totalsamples`, 3507) */
+  int32_t see_background;       /* cinematic: primary misses see the sky (3506) */
 } tsi_params;
 
 /* Uniforms, uniforms.rs:8-17 / compute.wgsl:3419-3428 (96 bytes).
@@ -140,6 +144,16 @@ typedef struct tsi_stats {
   uint64_t items_high_water;    /* largest per-level work list */
   uint64_t tape_words;          /* pruned tape instructions written */
   uint64_t prune_fallbacks;     /* warps that re-ran on the full tape */
+  /* Algorithmic FP32 work (opcost.h table) of the frame on the FULL tape,
+   * whatever pruning saved: cells_evaluated x the full tape's forward cost
+   * (fix included), and cells_reverse x its reverse cost (every instruction,
+   * the zero-sensitivity skip of compute.wgsl:3802-3805 not subtracted). */
+  uint64_t fp32_ops_full_fwd;
+  uint64_t fp32_ops_full_rev;
+  /* Cells evaluated without tape pruning although pruning was requested:
+   * pruning tracks liveness in a 64-bit mask, so tapes of more than 64
+   * interval registers run unpruned (same results, more work). */
+  uint64_t cells_unpruned_regs;
   uint32_t levels;
   uint32_t error_flags;
   float device_ms;              /* device time of the call (CUDA events) */
@@ -346,8 +360,13 @@ typedef struct tsi_request {
 } tsi_request;
 
 /* Inverts all requests' scenes in one fused launch sequence (every level
- * of every scene shares each launch), then traces them.  Scenes must be
- * distinct. */
+ * of every scene shares each launch); each scene's trace starts on a
+ * low-priority stream as soon as its own last level is done.  Scenes must be
+ * distinct.  More requests than one launch takes (max_scenes_per_launch) run
+ * as consecutive launch sequences.  Each request's stats are its own
+ * scene's counters and error bits (voxels_live included); device_ms is the
+ * whole call's device time.  The return status reports the error bits of
+ * every request. */
 TSI_API tsi_status tsi_batch_run(tsi_ctx *ctx, tsi_request *reqs, uint32_t n);
 
 /* No counterpart in the reference.  Tunes the wide thresholds of the
@@ -372,10 +391,10 @@ typedef struct tsi_batch_graph tsi_batch_graph;
 TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *ctx, tsi_request *reqs, uint32_t n,
                                           tsi_batch_graph **out);
 TSI_API tsi_status tsi_batch_graph_launch(tsi_batch_graph *g);
-/* Waits for the last replay and reports it: the status from its device
- * error word (voxel pool, work list, log arena, watchdog) and, when stats is
- * not NULL, its counters summed over the batch with device_ms = the replay's
- * device time.  Plain calls on the same context between the launch and the
+/* Waits for the last replay and reports it: the status from its scenes'
+ * error words (voxel pool, work list, log arena, watchdog) and, when stats
+ * is not NULL, its counters summed over the batch with device_ms = the
+ * replay's device time.  Plain calls on the same context between the launch and the
  * wait overwrite what it reads. */
 TSI_API tsi_status tsi_batch_graph_wait(tsi_batch_graph *g, tsi_stats *stats);
 TSI_API void tsi_batch_graph_destroy(tsi_batch_graph *g);
@@ -423,26 +442,42 @@ TSI_API tsi_status tsi_frame_keep_nearest(tsi_ctx *ctx, const uint64_t *global_k
 
 /* ---------------- serving ---------------- */
 /* No counterpart in the reference (its frames are driven by the window's
- * event loop, main.rs:978-1063).  A server owns a worker thread that drains
- * a queue of requests on one context, fusing the pending requests of
- * distinct scenes into one tsi_batch_run (requests for one scene run in
- * submission order, one per batch).  While a server exists only the server
- * uses its context.  A request's uniforms, image and stats pointers must
- * stay valid until its ticket completes. */
+ * event loop, main.rs:978-1063, and each `main` dispatch's persistent
+ * workgroups dequeue until the queue drains, compute.wgsl:3525-3556).
+ * A server owns a worker thread that runs requests on one context with
+ * continuous batching: a request joins the running inversion at the next
+ * launch step as soon as a slot is free and its scene has no other request
+ * running (a scene's requests run in submission order), runs one octree
+ * level per step alongside the other slots, and is traced on a
+ * low-priority stream while the others go on.  A request's frame buffers
+ * are admitted against the context's memory budget at submission (and
+ * again when it starts); one that would exceed it completes with
+ * TSI_ERR_OOM.  With TSI_SERVER_STATIC_BATCHES the worker instead fuses the
+ * queued requests of distinct scenes into one tsi_batch_run at a time (the
+ * earlier form, kept for comparison).  While a server exists only the
+ * server uses its context.  A request's uniforms, image and stats pointers
+ * must stay valid until its ticket completes; its stats are its own scene's
+ * counters, with device_ms from its start to its frame being ready. */
 typedef struct tsi_server tsi_server;
+#define TSI_SERVER_STATIC_BATCHES 1u
 typedef struct tsi_server_opts {
-  uint32_t max_batch;       /* scenes fused per launch (0: the context's maximum) */
+  uint32_t max_batch;       /* requests running at once (0: the context's maximum) */
+  uint32_t flags;           /* TSI_SERVER_STATIC_BATCHES */
+  uint32_t max_queue;       /* queued requests beyond which submit returns TSI_ERR_BUSY (0: 4096) */
   uint32_t reserved;
 } tsi_server_opts;
 typedef struct tsi_server_stats {
   uint64_t completed;       /* requests finished */
-  uint64_t batches;         /* fused launches run */
-  float mean_batch;         /* requests per launch */
+  uint64_t batches;         /* launch steps (fused launches with TSI_SERVER_STATIC_BATCHES) */
+  float mean_batch;         /* requests finished per step or launch */
   float p50_ms, p99_ms;     /* submit-to-completion latency of finished requests */
   float max_ms;
+  uint32_t queued;          /* requests waiting to start */
 } tsi_server_stats;
 TSI_API tsi_status tsi_server_create(tsi_ctx *ctx, const tsi_server_opts *opts, tsi_server **out);
-/* Queues one request; *ticket identifies it for tsi_server_poll. */
+/* Queues one request; *ticket identifies it for tsi_server_poll.
+ * TSI_ERR_BUSY when the queue is full, TSI_ERR_OOM when the request's frame
+ * cannot fit the context's memory budget. */
 TSI_API tsi_status tsi_server_submit(tsi_server *s, const tsi_request *req, uint64_t *ticket);
 /* The request's status once it has completed (its stats are filled in and
  * the ticket is released); TSI_ERR_BUSY if it is still pending after
@@ -450,8 +485,8 @@ TSI_API tsi_status tsi_server_submit(tsi_server *s, const tsi_request *req, uint
  * ticket.  latency_ms (may be NULL) receives its submit-to-completion time. */
 TSI_API tsi_status tsi_server_poll(tsi_server *s, uint64_t ticket, uint32_t wait_ms, float *latency_ms);
 TSI_API tsi_status tsi_server_stats_get(tsi_server *s, tsi_server_stats *out);
-/* Stops the worker after the running batch; requests still queued complete
- * with TSI_ERR_SHUTDOWN. */
+/* Stops the worker after the running requests; requests still queued
+ * complete with TSI_ERR_SHUTDOWN. */
 TSI_API void tsi_server_destroy(tsi_server *s);
 
 /* ---------------- allocation-free evaluation ---------------- */

@@ -17,6 +17,9 @@
  *   atan2   : octant reduction, atan(a) = pi/4 + atan((a-1)/(a+1)) above
  *             tan(pi/8), Taylor series of atan below
  *   powi    : binary exponentiation (integer exponents, POW_II's contract)
+ *   acos    : atan2(sqrt((1 - x)(1 + x)), x) (cinematic sky model)
+ *   pow     : exp(y log x) for x > 0, 0 or 1 at x = 0, NaN for x < 0 (the
+ *             exp2(y log2 x) convention of GPU drivers for negative x)
  * The oracle is compiled with -ffp-contract=off so that no FMA contracts.
  */
 #ifndef ORACLE_FMATH_H
@@ -61,6 +64,39 @@ static inline float of_sin(float x) {
     case 1: return c;
     case 2: return -s;
     default: return -c;
+  }
+}
+
+/* cos: the same reduction and polynomials as of_sin, quadrant shifted by one */
+static inline float of_cos(float x) {
+  if (!(fabsf(x) <= 3.0e38f)) return x - x;
+  const float two_over_pi = 0.6366197466850281f;
+  const float p1 = 1.5703125f, p2 = 0.0004838705062866211f, p3 = -4.371138828673793e-08f;
+  float k = rintf(x * two_over_pi);
+  float r = x - k * p1;
+  r = r - k * p2;
+  r = r - k * p3;
+  float qf = k - 4.0f * floorf(k * 0.25f);
+  int q = (int)qf;
+  float r2 = r * r;
+  float ps = -2.5052107943679403e-08f;
+  ps = 2.7557318844628753e-06f + r2 * ps;
+  ps = -0.00019841270113829523f + r2 * ps;
+  ps = 0.008333333767950535f + r2 * ps;
+  ps = -0.1666666716337204f + r2 * ps;
+  float s = r + r * (r2 * ps);
+  float pc = 2.0876755879584152e-09f;
+  pc = -2.755731998149713e-07f + r2 * pc;
+  pc = 2.4801587642286904e-05f + r2 * pc;
+  pc = -0.0013888889225199819f + r2 * pc;
+  pc = 0.0416666679084301f + r2 * pc;
+  pc = -0.5f + r2 * pc;
+  float c = 1.0f + r2 * pc;
+  switch (q) {
+    case 0: return c;
+    case 1: return -s;
+    case 2: return -c;
+    default: return s;
   }
 }
 
@@ -181,6 +217,8 @@ static inline float of_powf(float x, float y) {
   if (x < 0.0f) return OF_NAN;
   return of_exp(y * of_log(x));
 }
+
+static inline float of_acos(float x) { return of_atan2(sqrtf((1.0f - x) * (1.0f + x)), x); }
 
 /* IEEE 754-2019 minimumNumber / maximumNumber: NaN loses, -0 < +0 */
 static inline float of_min(float a, float b) {

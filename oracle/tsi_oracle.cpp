@@ -473,6 +473,7 @@ struct Params { /* mirrors tsi_params (include/tsi.h) field by field */
   float root_lo[3], root_hi[3];
   int32_t pruning;
   float swept_dt;
+  int32_t cinematic, samples, see_background;
 };
 
 struct Stats { /* subset of tsi_stats, same field order for the counters */

@@ -41,6 +41,9 @@ pub struct tsi_params {
     pub root_hi: [f32; 3],
     pub pruning: i32,
     pub swept_dt: f32,
+    pub cinematic: i32,
+    pub samples: i32,
+    pub see_background: i32,
 }
 
 #[repr(C)]
@@ -76,6 +79,9 @@ pub struct tsi_stats {
     pub items_high_water: u64,
     pub tape_words: u64,
     pub prune_fallbacks: u64,
+    pub fp32_ops_full_fwd: u64,
+    pub fp32_ops_full_rev: u64,
+    pub cells_unpruned_regs: u64,
     pub levels: u32,
     pub error_flags: u32,
     pub device_ms: f32,
@@ -186,6 +192,8 @@ pub struct tsi_request {
 #[derive(Debug, Copy, Clone, Default)]
 pub struct tsi_server_opts {
     pub max_batch: u32,
+    pub flags: u32,
+    pub max_queue: u32,
     pub reserved: u32,
 }
 
@@ -198,7 +206,10 @@ pub struct tsi_server_stats {
     pub p50_ms: f32,
     pub p99_ms: f32,
     pub max_ms: f32,
+    pub queued: u32,
 }
+
+pub const TSI_SERVER_STATIC_BATCHES: u32 = 1;
 
 pub enum tsi_ctx {}
 pub enum tsi_tape {}

@@ -35,7 +35,7 @@ class Params(C.Structure):
                 ("lipschitz_corrected", i32), ("swept_volume", i32), ("fast_normals", i32), ("normal_viz", i32),
                 ("rounding_mode", i32), ("fast_multiplier", f32), ("scene_id", i32),
                 ("octree_darken_factor", f32), ("root_lo", f32 * 3), ("root_hi", f32 * 3), ("pruning", i32),
-                ("swept_dt", f32)]
+                ("swept_dt", f32), ("cinematic", i32), ("samples", i32), ("see_background", i32)]
 
 
 class Uniforms(C.Structure):  # uniforms.rs:8-17
@@ -56,7 +56,7 @@ class Stats(C.Structure):
         "parents_expanded", "cells_evaluated", "cells_reverse", "cells_skipped", "cells_ambiguous", "cells_empty",
         "cells_full", "cells_enqueued", "cells_reused", "instr_forward", "instr_reverse", "instr_full_equiv",
         "fp32_ops", "bricks_allocated", "bricks_freed", "voxels_live", "items_high_water", "tape_words",
-        "prune_fallbacks")] + [("levels", u32), ("error_flags", u32), ("device_ms", f32), ("reserved", f32)]
+        "prune_fallbacks", "fp32_ops_full_fwd", "fp32_ops_full_rev", "cells_unpruned_regs")] + [("levels", u32), ("error_flags", u32), ("device_ms", f32), ("reserved", f32)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -76,13 +76,16 @@ class AutotuneResult(C.Structure):
                 ("ms", f32 * AUTOTUNE_MAX)]
 
 
+SERVER_STATIC_BATCHES = 1
+
+
 class ServerOpts(C.Structure):
-    _fields_ = [("max_batch", u32), ("reserved", u32)]
+    _fields_ = [("max_batch", u32), ("flags", u32), ("max_queue", u32), ("reserved", u32)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("completed", u64), ("batches", u64), ("mean_batch", f32), ("p50_ms", f32), ("p99_ms", f32),
-                ("max_ms", f32)]
+                ("max_ms", f32), ("queued", u32)]
 
 
 class Image(C.Structure):

@@ -406,20 +406,26 @@ def run_batch(device: Device, requests: list, graph: bool = False) -> list:
 
 
 class Server:
-    """A worker thread on one device that fuses the pending requests of
-    distinct scenes into one launch sequence (tsi_server_*).  While it
-    exists, only the server uses the device."""
+    """A worker thread on one device that runs requests with continuous
+    batching (tsi_server_*): a request joins the running inversion at the
+    next launch step when a slot is free and its scene is idle, and is traced
+    on a low-priority stream while the others go on.  With
+    static_batches=True it instead fuses the queued requests of distinct
+    scenes into one launch sequence at a time.  While it exists, only the
+    server uses the device."""
 
-    def __init__(self, device: Device, max_batch: int = 0):
+    def __init__(self, device: Device, max_batch: int = 0, static_batches: bool = False, max_queue: int = 0):
         self.device = device
         h = C.c_void_p()
-        N.check(device.lib.tsi_server_create(device.handle, C.byref(N.ServerOpts(max_batch, 0)), C.byref(h)),
-                "tsi_server_create")
+        opts = N.ServerOpts(max_batch, N.SERVER_STATIC_BATCHES if static_batches else 0, max_queue, 0)
+        N.check(device.lib.tsi_server_create(device.handle, C.byref(opts), C.byref(h)), "tsi_server_create")
         self.handle = h
         self._keep = {}  # request structs and buffers alive until the ticket completes
 
     def submit(self, scene: "Scene", time: float, t0: float = float("nan"), uniforms=None,
                image: bool = False) -> int:
+        """Queues one request; image=True copies its frame's rgba and depth
+        to host arrays that poll() returns."""
         req = N.Request()
         req.scene = scene.handle
         req.time = float(time)
@@ -433,7 +439,8 @@ class Server:
             if image:
                 w, hgt = uniforms.resolution[0], uniforms.resolution[1]
                 keep["rgba"] = np.empty((hgt, w, 4), np.float32)
-                img = N.Image(w, hgt, _fptr(keep["rgba"]), None, None)
+                keep["depth"] = np.empty((hgt, w), np.float32)
+                img = N.Image(w, hgt, _fptr(keep["rgba"]), _fptr(keep["depth"]), None)
                 keep["img"] = img
                 req.out = C.pointer(img)
         ticket = C.c_uint64(0)
@@ -441,14 +448,17 @@ class Server:
         self._keep[ticket.value] = keep
         return ticket.value
 
-    def poll(self, ticket: int, wait_ms: int = 60000):
-        """(stats, latency ms, rgba or None) once done; None while pending."""
+    def poll(self, ticket: int, wait_ms: int = 60000, with_depth: bool = False):
+        """(stats, latency ms, rgba or None) once done -- with_depth adds the
+        depth image -- or None while pending."""
         lat = C.c_float(0.0)
         status = self.device.lib.tsi_server_poll(self.handle, ticket, wait_ms, C.byref(lat))
         if status == 11:  # TSI_ERR_BUSY
             return None
         keep = self._keep.pop(ticket, {})
         N.check(status, "tsi_server_poll")
+        if with_depth:
+            return keep.get("stats"), lat.value, keep.get("rgba"), keep.get("depth")
         return keep.get("stats"), lat.value, keep.get("rgba")
 
     def stats(self) -> dict:

@@ -9,6 +9,7 @@
 // back.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stddef.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -20,6 +21,7 @@
 #include <vector>
 
 #include "api_internal.h"
+#include "api_state.h"
 #include "composite.h"
 #include "device_types.h"
 #include "ir_lower.h"
@@ -28,21 +30,14 @@
 #include "tsi.h"
 
 namespace tsi {
-cudaError_t launch_refine(const LaunchParams &P, uint32_t level, uint32_t rcap, int grid, int block, size_t smem,
-                          cudaStream_t st);
-cudaError_t launch_frame_begin(const LaunchParams &P, cudaStream_t st);
-cudaError_t launch_frame_end(const LaunchParams &P, cudaStream_t st);
-cudaError_t refine_set_smem(size_t bytes);
-cudaError_t refine_occupancy(int block, size_t smem, int *blocks_per_sm);
-cudaError_t refine_static_smem(size_t *bytes);
 cudaError_t launch_evalbox(bool directed, const uint2 *code, uint32_t len, uint32_t nregs, uint32_t out_reg,
                            uint32_t n, const float *boxes, int reverse, float *out, float2 *regs, float4 *log,
                            cudaStream_t st);
 cudaError_t launch_math(int which, uint32_t n, const float *a, const float *b, float *out, cudaStream_t st);
-
 }  // namespace tsi
 
 using namespace tsi;
+using namespace tsi_host;
 
 namespace {
 
@@ -58,9 +53,6 @@ thread_local std::string g_last_error;
     }                                                                                \
   } while (0)
 
-constexpr int kBlock = 256;
-constexpr int kWarpsPerBlock = kBlock / 32;
-
 template <typename T>
 cudaError_t dalloc(T **p, size_t count) {
   *p = nullptr;
@@ -68,115 +60,7 @@ cudaError_t dalloc(T **p, size_t count) {
   return cudaMalloc((void **)p, count * sizeof(T));
 }
 
-struct Readback {
-  uint32_t error;
-  uint32_t pad;
-  unsigned long long stats[ST_COUNT];
-  unsigned long long visits;
-  uint32_t item_count[TSI_MAX_LEVELS + 1];
-};
-
 }  // namespace
-
-struct tsi_tape {
-  tsi_ctx *ctx = nullptr;
-  uint2 *d_code = nullptr;
-  uint32_t len = 0;  // instructions after the 4 ARG slots
-  uint32_t count = 0, nregs = 0, out_reg = 0, n_minmax = 0;
-  uint64_t fwd_cost = 0, rev_cost = 0;
-  // bundled form for the wide path (absent when the tape is short)
-  uint4 *d_wslots = nullptr;
-  uint2 *d_wbundles = nullptr;
-  uint32_t *d_wmm = nullptr;
-  uint32_t wslots = 0, wbundles = 0, wvalues = 0, wmin_len = 0xffffffffu, wcontrib = 0;
-  uint32_t warg_gbase[4] = {TSI_NONE, TSI_NONE, TSI_NONE, TSI_NONE}, warg_gcount[4] = {0, 0, 0, 0};
-};
-
-struct tsi_scene {
-  tsi_ctx *ctx = nullptr;
-  const tsi_tape *tape = nullptr;
-  tsi_params p{};
-  uint32_t cap_bricks = 0;
-  VoxelPoolDev pool{};
-  SceneCounters *d_ctr = nullptr;
-  uint32_t img_w = 0, img_h = 0;
-  uint64_t img_cap = 0;  // pixels the frame buffers hold (frames of any size up to it reuse them)
-  float4 *d_rgba = nullptr;
-  float *d_depth = nullptr;
-  float *d_normal = nullptr;
-  // the tracer's arguments: written on the host, uploaded before each trace
-  // (a captured upload reads the pinned copy when the graph replays)
-  TraceParams *h_trace = nullptr, *d_trace = nullptr;
-  // asynchronous frame read-back (tsi_scene_trace_async): the trace's end,
-  // the copy's end on the context's copy stream, and the upload of h_trace
-  cudaEvent_t traced = nullptr, copy_done = nullptr, trace_up = nullptr;
-  bool copy_pending = false, trace_up_pending = false;
-  uint64_t bytes = 0;
-};
-
-struct tsi_ctx {
-  int device = 0;
-  int sm_count = 0;
-  size_t smem_per_sm = 0, smem_reserved = 0;  // shared memory of an SM, reserved per block
-  cudaStream_t stream = nullptr;
-  cudaStream_t copy_stream = nullptr;  // frame read-back of tsi_scene_trace_async
-  uint32_t max_scenes = 64;
-  SceneLaunch *d_scenes = nullptr, *h_scenes = nullptr;
-  TapeRec *d_recs = nullptr, *h_recs = nullptr;
-  uint32_t rec_cap = 0;
-  uint32_t *d_rec_count = nullptr;
-  uint2 *d_code = nullptr;
-  unsigned long long *d_code_count = nullptr;
-  uint64_t code_cap = 0;
-  WorkItem *d_items[2] = {nullptr, nullptr};
-  uint32_t item_cap = 0;
-  uint32_t *d_item_count = nullptr, *d_item_cursor = nullptr;
-  WorkItem *d_witems[2] = {nullptr, nullptr};
-  uint32_t *d_witem_count = nullptr, *d_witem_cursor = nullptr;
-  // wide path: per-cell hand-over to the group (per level parity) and, for
-  // tapes whose working set exceeds shared memory, per-block scratch
-  CellInfo *d_cell_info[2] = {nullptr, nullptr};
-  uint32_t *d_cell_bits[2] = {nullptr, nullptr};
-  size_t cell_arena_bytes = 0;  // of each parity's info + bits
-  uint32_t witem_cap = 0, bm_words = 0;
-  unsigned char *d_wscratch = nullptr;
-  size_t wscratch_bytes = 0, wscratch_stride = 0;
-  size_t wide_smem_bytes = 0;  // shared-memory budget of a wide cell (0: keep the narrow occupancy)
-  uint64_t hbm_budget = 0;     // bytes the scenes may hold together (0: no limit)
-
-  uint2 *d_dealloc[2] = {nullptr, nullptr};
-  uint32_t dealloc_cap = 0;
-  uint32_t *d_dealloc_count = nullptr, *d_dealloc_cursor = nullptr;
-  float4 *d_log = nullptr;
-  uint2 *d_dec = nullptr;
-  uint32_t slice_len = 0;
-  uint32_t max_warps = 0;
-  float4 *d_log_overflow = nullptr;
-  unsigned long long *d_log_used = nullptr;
-  uint64_t log_overflow_cap = 0;
-  uint32_t *d_error = nullptr;
-  uint32_t *d_error_sticky = nullptr;  // error words of asynchronous inversions since the last wait
-  // the upload of h_scenes/h_recs of the last launch sequence: the host may
-  // rewrite them only after it ran (inversions queued without waiting)
-  cudaEvent_t launch_up = nullptr;
-  bool launch_up_pending = false;
-  unsigned long long *d_stats = nullptr;
-  unsigned long long *d_level_stats = nullptr;
-  unsigned long long *d_visits = nullptr;
-  Readback *h_rb = nullptr;
-  // per-level profile of the last inversion (events when profiling is on)
-  bool profile_levels = false;
-  std::vector<cudaEvent_t> level_events;
-  uint32_t last_levels = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
-  // scratch for tsi_tape_eval_boxes
-  void *d_scratch = nullptr;
-  size_t scratch_bytes = 0;
-  uint32_t watchdog = 0;
-  // objects created on this context, released by tsi_destroy if still alive
-  std::set<tsi_tape *> tapes;
-  std::set<tsi_scene *> scenes;
-};
 
 struct tsi_batch_graph {
   tsi_ctx *ctx = nullptr;
@@ -188,11 +72,18 @@ struct tsi_batch_graph {
   std::vector<uint8_t> global;  // per request: wide cells in the global scratch
 };
 
-namespace {
+namespace tsi_host {
 
 tsi_status set_err(tsi_status s, const std::string &msg) {
   g_last_error = msg;
   return s;
+}
+
+tsi_status cuda_err(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return TSI_OK;
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();
+  return TSI_ERR_CUDA;
 }
 
 LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes, size_t dyn_smem, bool sticky) {
@@ -202,9 +93,14 @@ LaunchParams make_params(tsi_ctx *c, uint32_t n_scenes, size_t dyn_smem, bool st
   P.rec_cap = c->rec_cap;
   P.recs = c->d_recs;
   P.rec_count = c->d_rec_count;
+  P.rec_low = c->d_rec_low;
+  P.rec_base = c->max_scenes;
   P.code_arena = c->d_code;
   P.code_count = c->d_code_count;
+  P.code_low = c->d_code_low;
   P.code_cap = c->code_cap;
+  P.step_code_start = c->d_step_code_start;
+  P.step_rec_start = c->d_step_rec_start;
   P.items[0] = c->d_items[0];
   P.items[1] = c->d_items[1];
   P.item_count = c->d_item_count;
@@ -330,13 +226,6 @@ constexpr size_t kWideCellMaxBytes = 192u << 10;
 // Beyond this a tape has no wide form (global scratch per block of the grid).
 constexpr size_t kWideCellMaxGlobalBytes = 8u << 20;
 
-// Launch geometry of one frame for n scenes.
-struct FramePlan {
-  uint32_t lmax = 0, rcap = 4;
-  size_t smem = 0;
-  int grid = 0;
-  std::vector<uint8_t> global;  // per scene: wide cells in the global scratch
-};
 
 // Sizes the launch for these scenes and grows the wide path's arenas (no
 // allocation when they are large enough, so a plan made once before stream
@@ -426,8 +315,10 @@ tsi_status plan_frame(tsi_ctx *c, tsi_scene *const *scenes, uint32_t n, FramePla
 // One frame of set inversion for n scenes, all levels in one launch sequence.
 bool capturing(tsi_ctx *c);
 
+// With fork = true the end of every level's launch is recorded in
+// c->fork_events[level] (the batched form starts each scene's trace there).
 tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *times, const float *t0s, uint32_t n,
-                          bool sticky = false) {
+                          bool sticky = false, bool fork = false) {
   if (n == 0) return TSI_OK;
   if (n > c->max_scenes) return set_err(TSI_ERR_INVALID_ARGUMENT, "too many scenes in one launch");
   FramePlan fp;
@@ -449,62 +340,120 @@ tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *tim
     CK(cudaEventRecord(c->launch_up, c->stream));
     c->launch_up_pending = true;
   }
-  CK(cudaMemsetAsync(c->d_error, 0, sizeof(uint32_t), c->stream));
-  CK(cudaMemsetAsync(c->d_stats, 0, ST_COUNT * sizeof(unsigned long long), c->stream));
-  CK(cudaMemsetAsync(c->d_level_stats, 0, (TSI_MAX_LEVELS + 1) * ST_COUNT * sizeof(unsigned long long), c->stream));
-  CK(cudaMemsetAsync(c->d_log_used, 0, (TSI_MAX_LEVELS + 1) * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(c->d_error, 0, n * sizeof(uint32_t), c->stream));
+  CK(cudaMemsetAsync(c->d_stats, 0, (size_t)n * ST_COUNT * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(c->d_level_stats, 0, TSI_STEP_RING * ST_COUNT * sizeof(unsigned long long), c->stream));
   const LaunchParams P = make_params(c, n, fp.smem, sticky);
   CK(launch_frame_begin(P, c->stream));
   const bool prof = c->profile_levels && c->level_events.size() >= lmax + 1;
   for (uint32_t level = 0; level < lmax; ++level) {
     if (prof) CK(cudaEventRecord(c->level_events[level], c->stream));
     CK(launch_refine(P, level, rcap, grid, kBlock, smem, c->stream));
+    if (fork) CK(cudaEventRecord(c->fork_events[level], c->stream));
   }
   if (prof) CK(cudaEventRecord(c->level_events[lmax], c->stream));
   c->last_levels = lmax;
-  CK(launch_frame_end(P, c->stream));
+  CK(launch_frame_end(P, 0, n, c->stream));
   return TSI_OK;
 }
 
-tsi_status enqueue_readback(tsi_ctx *c) {
-  CK(cudaMemcpyAsync(&c->h_rb->error, c->d_error, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(c->h_rb->stats, c->d_stats, ST_COUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                     c->stream));
+tsi_status ensure_readback_rows(tsi_ctx *c, uint32_t n) {
+  if (n <= c->rb_rows) return TSI_OK;
+  if (capturing(c)) return set_err(TSI_ERR_BUSY, "readback rows grown during graph capture");
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFreeHost(c->h_err);
+  cudaFreeHost(c->h_stats);
+  c->h_err = nullptr;
+  c->h_stats = nullptr;
+  c->rb_rows = 0;
+  const uint32_t rows = std::max(n, 64u);
+  CK(cudaMallocHost((void **)&c->h_err, rows * sizeof(uint32_t)));
+  CK(cudaMallocHost((void **)&c->h_stats, (size_t)rows * ST_COUNT * sizeof(unsigned long long)));
+  memset(c->h_err, 0, rows * sizeof(uint32_t));
+  memset(c->h_stats, 0, (size_t)rows * ST_COUNT * sizeof(unsigned long long));
+  c->rb_rows = rows;
+  return TSI_OK;
+}
+
+// Error words and stats rows of the launch's n scenes into readback rows
+// row0 .. row0 + n - 1, and the list sizes of its steps.
+tsi_status enqueue_readback(tsi_ctx *c, uint32_t n, uint32_t row0 = 0) {
+  if (row0 + n > c->rb_rows) return set_err(TSI_ERR_INVALID_ARGUMENT, "readback rows not reserved");
+  CK(cudaMemcpyAsync(c->h_err + row0, c->d_error, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_stats + (size_t)row0 * ST_COUNT, c->d_stats, (size_t)n * ST_COUNT * sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(c->h_rb->item_count, c->d_item_count, sizeof(c->h_rb->item_count), cudaMemcpyDeviceToHost,
                      c->stream));
   return TSI_OK;
 }
 
-void fill_stats(const Readback &rb, tsi_stats *st, uint64_t voxels_live) {
+void fill_stats(const tsi_ctx *c, uint32_t row, const tsi_scene *s, tsi_stats *st, uint64_t voxels_live) {
   if (!st) return;
-  memset(st, 0, sizeof(*st));
-  st->parents_expanded = rb.stats[ST_PARENTS];
-  st->cells_evaluated = rb.stats[ST_EVAL];
-  st->cells_reverse = rb.stats[ST_REVERSE];
-  st->cells_skipped = rb.stats[ST_SKIPPED];
-  st->cells_ambiguous = rb.stats[ST_AMBIG];
-  st->cells_empty = rb.stats[ST_EMPTY];
-  st->cells_full = rb.stats[ST_FULL];
-  st->cells_enqueued = rb.stats[ST_ENQUEUED];
-  st->cells_reused = rb.stats[ST_REUSED];
-  st->instr_forward = rb.stats[ST_INSTR_FWD];
-  st->instr_reverse = rb.stats[ST_INSTR_REV];
-  st->instr_full_equiv = rb.stats[ST_INSTR_FULL];
-  st->fp32_ops = rb.stats[ST_FP32];
-  st->bricks_allocated = rb.stats[ST_BRICK_ALLOC];
-  st->bricks_freed = rb.stats[ST_BRICK_FREE];
-  st->tape_words = rb.stats[ST_TAPE_WORDS];
-  st->prune_fallbacks = rb.stats[ST_PRUNE_FALLBACK];
-  st->voxels_live = voxels_live;
+  fill_stats_row(c->h_stats + (size_t)row * ST_COUNT, c->h_err[row], s, st, voxels_live);
   uint64_t hw = 0;
   uint32_t levels = 0;
-  for (int l = 0; l <= TSI_MAX_LEVELS; ++l) {
-    hw = std::max<uint64_t>(hw, rb.item_count[l]);
-    if (rb.item_count[l]) levels = (uint32_t)l + 1;
+  for (uint32_t l = 0; l < TSI_STEP_RING; ++l) {
+    hw = std::max<uint64_t>(hw, c->h_rb->item_count[l]);
+    if (c->h_rb->item_count[l]) levels = l + 1;
   }
   st->items_high_water = hw;
   st->levels = levels;
-  st->error_flags = rb.error;
+}
+
+void fill_stats_row(const unsigned long long *r, uint32_t err, const tsi_scene *s, tsi_stats *st,
+                    uint64_t voxels_live) {
+  if (!st) return;
+  memset(st, 0, sizeof(*st));
+  st->parents_expanded = r[ST_PARENTS];
+  st->cells_evaluated = r[ST_EVAL];
+  st->cells_reverse = r[ST_REVERSE];
+  st->cells_skipped = r[ST_SKIPPED];
+  st->cells_ambiguous = r[ST_AMBIG];
+  st->cells_empty = r[ST_EMPTY];
+  st->cells_full = r[ST_FULL];
+  st->cells_enqueued = r[ST_ENQUEUED];
+  st->cells_reused = r[ST_REUSED];
+  st->instr_forward = r[ST_INSTR_FWD];
+  st->instr_reverse = r[ST_INSTR_REV];
+  st->instr_full_equiv = r[ST_INSTR_FULL];
+  st->fp32_ops = r[ST_FP32];
+  st->bricks_allocated = r[ST_BRICK_ALLOC];
+  st->bricks_freed = r[ST_BRICK_FREE];
+  st->tape_words = r[ST_TAPE_WORDS];
+  st->prune_fallbacks = r[ST_PRUNE_FALLBACK];
+  if (s) {
+    st->fp32_ops_full_fwd = r[ST_EVAL] * s->tape->fwd_cost;
+    st->fp32_ops_full_rev = r[ST_REVERSE] * s->tape->rev_cost;
+    if (s->p.pruning && s->tape->nregs > TSI_PRUNE_MAX_REGS) st->cells_unpruned_regs = r[ST_EVAL];
+  }
+  st->voxels_live = voxels_live;
+  st->error_flags = err;
+}
+
+// tsi_stats summed over readback rows 0 .. n-1 (a batch or graph replay as
+// a whole); the error word is the or of the rows'.
+void fill_stats_sum(const tsi_ctx *c, tsi_scene *const *scenes, uint32_t n, tsi_stats *st) {
+  if (!st) return;
+  tsi_stats acc;
+  memset(&acc, 0, sizeof(acc));
+  for (uint32_t i = 0; i < n; ++i) {
+    tsi_stats one;
+    fill_stats(c, i, scenes ? scenes[i] : nullptr, &one, 0);
+    uint64_t *a = &acc.parents_expanded;
+    const uint64_t *b = &one.parents_expanded;
+    for (size_t k = 0; k < (offsetof(tsi_stats, levels) - offsetof(tsi_stats, parents_expanded)) / sizeof(uint64_t); ++k)
+      a[k] += b[k];
+    acc.items_high_water = one.items_high_water;
+    acc.levels = one.levels;
+    acc.error_flags |= one.error_flags;
+  }
+  *st = acc;
+}
+
+uint32_t readback_error_or(const tsi_ctx *c, uint32_t n) {
+  uint32_t e = 0;
+  for (uint32_t i = 0; i < n; ++i) e |= c->h_err[i];
+  return e;
 }
 
 // camera of rt_main (compute.wgsl:4651-4685), computed once per frame
@@ -659,23 +608,24 @@ tsi_status fill_trace(tsi_scene *s, const tsi_uniforms *u) {
   return TSI_OK;
 }
 
-tsi_status enqueue_trace(tsi_scene *s, const tsi_uniforms *u) {
+tsi_status enqueue_trace(tsi_scene *s, const tsi_uniforms *u, cudaStream_t st_) {
   tsi_ctx *c = s->ctx;
   tsi_status st = fill_trace(s, u);
   if (st != TSI_OK) return st;
   const TraceParams &T = *s->h_trace;
   if (T.W == 0 || T.H == 0) return TSI_OK;
   const bool cap = capturing(c);
-  CK(cudaMemcpyAsync(s->d_trace, s->h_trace, sizeof(TraceParams), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s->d_trace, s->h_trace, sizeof(TraceParams), cudaMemcpyHostToDevice, st_));
   if (!cap) {
-    CK(cudaEventRecord(s->trace_up, c->stream));
+    CK(cudaEventRecord(s->trace_up, st_));
     s->trace_up_pending = true;
     // the frame buffers are free once the last asynchronous copy read them
-    if (s->copy_pending) CK(cudaStreamWaitEvent(c->stream, s->copy_done, 0));
+    if (s->copy_pending) CK(cudaStreamWaitEvent(st_, s->copy_done, 0));
   }
-  CK(launch_trace(T, s->d_trace, c->stream));
+  CK(launch_trace(T, s->d_trace, st_));
   return TSI_OK;
 }
+tsi_status enqueue_trace(tsi_scene *s, const tsi_uniforms *u) { return enqueue_trace(s, u, s->ctx->stream); }
 
 tsi_status copy_image_out(tsi_scene *s, tsi_image *out, cudaStream_t st) {
   if (!out) return TSI_OK;
@@ -716,7 +666,7 @@ tsi_status read_counters(tsi_scene *s, SceneCounters &ctr) {
   return TSI_OK;
 }
 
-}  // namespace
+}  // namespace tsi_host
 
 extern "C" {
 
@@ -774,6 +724,9 @@ TSI_API void tsi_default_params(tsi_params *p) {  // compute.wgsl:3494-3511, ir.
   }
   p->pruning = 1;
   p->swept_dt = 1.0f / 60.0f;
+  p->cinematic = 0;
+  p->samples = 8;
+  p->see_background = 0;
 }
 
 TSI_API tsi_status tsi_ir_lower(const char *text, size_t len, float time, tsi_gpu_instruction *out, uint32_t cap,
@@ -889,7 +842,13 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
       return fail(TSI_ERR_CUDA);                                           \
     }                                                                      \
   } while (0)
-  CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  // inversions run on the highest-priority stream, so that their
+  // latency-bound launches get SMs ahead of queued trace blocks; traces of
+  // the batched form run on the lowest-priority one
+  int prio_low = 0, prio_high = 0;
+  CKC(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+  CKC(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_high));
+  CKC(cudaStreamCreateWithPriority(&c->trace_stream, cudaStreamNonBlocking, prio_low));
   CKC(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
   c->max_scenes = (opts && opts->max_scenes_per_launch) ? opts->max_scenes_per_launch : 64u;
   c->wide_smem_bytes = opts ? opts->wide_smem_bytes : 0u;
@@ -916,41 +875,50 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   CKC(dalloc(&c->d_recs, c->rec_cap));
   CKC(cudaMallocHost((void **)&c->h_recs, c->max_scenes * sizeof(TapeRec)));
   CKC(dalloc(&c->d_rec_count, 1));
+  CKC(dalloc(&c->d_rec_low, 1));
   CKC(dalloc(&c->d_code, c->code_cap));
   CKC(dalloc(&c->d_code_count, 1));
+  CKC(dalloc(&c->d_code_low, 1));
+  CKC(dalloc(&c->d_step_code_start, TSI_STEP_RING));
+  CKC(dalloc(&c->d_step_rec_start, TSI_STEP_RING));
   CKC(dalloc(&c->d_items[0], c->item_cap));
   CKC(dalloc(&c->d_items[1], c->item_cap));
-  CKC(dalloc(&c->d_item_count, TSI_MAX_LEVELS + 1));
-  CKC(dalloc(&c->d_item_cursor, TSI_MAX_LEVELS + 1));
+  CKC(dalloc(&c->d_item_count, TSI_STEP_RING));
+  CKC(dalloc(&c->d_item_cursor, TSI_STEP_RING));
   CKC(dalloc(&c->d_witems[0], c->item_cap));
   CKC(dalloc(&c->d_witems[1], c->item_cap));
-  CKC(dalloc(&c->d_witem_count, TSI_MAX_LEVELS + 1));
-  CKC(dalloc(&c->d_witem_cursor, TSI_MAX_LEVELS + 1));
+  CKC(dalloc(&c->d_witem_count, TSI_STEP_RING));
+  CKC(dalloc(&c->d_witem_cursor, TSI_STEP_RING));
   CKC(dalloc(&c->d_dealloc[0], c->dealloc_cap));
   CKC(dalloc(&c->d_dealloc[1], c->dealloc_cap));
-  CKC(dalloc(&c->d_dealloc_count, TSI_MAX_LEVELS + 1));
-  CKC(dalloc(&c->d_dealloc_cursor, TSI_MAX_LEVELS + 1));
+  CKC(dalloc(&c->d_dealloc_count, TSI_STEP_RING));
+  CKC(dalloc(&c->d_dealloc_cursor, TSI_STEP_RING));
   CKC(dalloc(&c->d_log, (size_t)c->max_warps * c->slice_len * 32u));
   CKC(dalloc(&c->d_dec, (size_t)c->max_warps * c->slice_len));
   CKC(dalloc(&c->d_log_overflow, c->log_overflow_cap));
-  CKC(dalloc(&c->d_log_used, TSI_MAX_LEVELS + 1));
-  CKC(dalloc(&c->d_error, 1));
+  CKC(dalloc(&c->d_log_used, TSI_STEP_RING));
+  CKC(dalloc(&c->d_error, c->max_scenes));
   CKC(dalloc(&c->d_error_sticky, 1));
   CKC(cudaMemset(c->d_error_sticky, 0, sizeof(uint32_t)));
-  CKC(dalloc(&c->d_stats, ST_COUNT));
-  CKC(dalloc(&c->d_level_stats, (TSI_MAX_LEVELS + 1) * ST_COUNT));
+  CKC(dalloc(&c->d_stats, (size_t)c->max_scenes * ST_COUNT));
+  CKC(dalloc(&c->d_level_stats, (size_t)TSI_STEP_RING * ST_COUNT));
+  c->fork_events.resize(TSI_STEP_RING);
+  for (auto &ev : c->fork_events) CKC(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CKC(cudaEventCreateWithFlags(&c->join_event, cudaEventDisableTiming));
   if (getenv("TSI_PROFILE_LEVELS")) {
     c->profile_levels = true;
     c->level_events.resize(TSI_MAX_LEVELS + 1);
     for (auto &ev : c->level_events) CKC(cudaEventCreate(&ev));
   }
   CKC(dalloc(&c->d_visits, 1));
-  CKC(cudaMallocHost((void **)&c->h_rb, sizeof(Readback)));
+  CKC(cudaMallocHost((void **)&c->h_rb, sizeof(TsiReadback)));
+  memset(c->h_rb, 0, sizeof(TsiReadback));
+  if (ensure_readback_rows(c, c->max_scenes) != TSI_OK) return fail(TSI_ERR_CUDA);
   CKC(cudaEventCreate(&c->ev0));
   CKC(cudaEventCreateWithFlags(&c->launch_up, cudaEventDisableTiming));
   CKC(cudaEventCreate(&c->ev1));
   CKC(cudaEventCreate(&c->ev2));
-  CKC(cudaMemsetAsync(c->d_item_count, 0, (TSI_MAX_LEVELS + 1) * sizeof(uint32_t), c->stream));
+  CKC(cudaMemsetAsync(c->d_item_count, 0, TSI_STEP_RING * sizeof(uint32_t), c->stream));
   CKC(cudaStreamSynchronize(c->stream));
 #undef CKC
   *out = c;
@@ -961,6 +929,7 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->trace_stream) cudaStreamSynchronize(c->trace_stream);
   while (!c->scenes.empty()) tsi_scene_destroy(*c->scenes.begin());
   while (!c->tapes.empty()) tsi_tape_destroy(*c->tapes.begin());
   cudaFree(c->d_scenes);
@@ -968,8 +937,12 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   cudaFree(c->d_recs);
   cudaFreeHost(c->h_recs);
   cudaFree(c->d_rec_count);
+  cudaFree(c->d_rec_low);
   cudaFree(c->d_code);
   cudaFree(c->d_code_count);
+  cudaFree(c->d_code_low);
+  cudaFree(c->d_step_code_start);
+  cudaFree(c->d_step_rec_start);
   cudaFree(c->d_items[0]);
   cudaFree(c->d_items[1]);
   cudaFree(c->d_item_count);
@@ -993,14 +966,19 @@ TSI_API void tsi_destroy(tsi_ctx *c) {
   cudaFree(c->d_stats);
   cudaFree(c->d_level_stats);
   for (auto &ev : c->level_events) cudaEventDestroy(ev);
+  for (auto &ev : c->fork_events) cudaEventDestroy(ev);
+  if (c->join_event) cudaEventDestroy(c->join_event);
   cudaFree(c->d_visits);
   cudaFree(c->d_scratch);
   cudaFreeHost(c->h_rb);
+  cudaFreeHost(c->h_err);
+  cudaFreeHost(c->h_stats);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->launch_up) cudaEventDestroy(c->launch_up);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->trace_stream) cudaStreamDestroy(c->trace_stream);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   delete c;
 }
@@ -1324,7 +1302,7 @@ TSI_API tsi_status tsi_scene_invert(tsi_scene *s, float time, float t0_or_nan, t
   tsi_status st = enqueue_invert(c, &s, &time, &t0_or_nan, 1);
   if (st != TSI_OK) return st;
   CK(cudaEventRecord(c->ev1, c->stream));
-  st = enqueue_readback(c);
+  st = enqueue_readback(c, 1);
   if (st != TSI_OK) return st;
   CK(cudaStreamSynchronize(c->stream));
   float ms = 0.0f;
@@ -1333,10 +1311,10 @@ TSI_API tsi_status tsi_scene_invert(tsi_scene *s, float time, float t0_or_nan, t
     SceneCounters ctr;
     st = read_counters(s, ctr);
     if (st != TSI_OK) return st;
-    fill_stats(*c->h_rb, stats, (uint64_t)ctr.live_bricks * 8u);
+    fill_stats(c, 0, s, stats, (uint64_t)ctr.live_bricks * 8u);
     stats->device_ms = ms;
   }
-  return status_from_error_bits(c->h_rb->error);
+  return status_from_error_bits(c->h_err[0]);
 }
 
 TSI_API tsi_status tsi_scene_invert_async(tsi_scene *s, float time, float t0_or_nan) {
@@ -1347,7 +1325,7 @@ TSI_API tsi_status tsi_scene_invert_async(tsi_scene *s, float time, float t0_or_
   tsi_status st = enqueue_invert(c, &s, &time, &t0_or_nan, 1, true);
   if (st != TSI_OK) return st;
   CK(cudaEventRecord(c->ev1, c->stream));
-  return enqueue_readback(c);
+  return enqueue_readback(c, 1);
 }
 
 TSI_API tsi_status tsi_scene_invert_wait(tsi_scene *s, tsi_stats *stats) {
@@ -1362,7 +1340,7 @@ TSI_API tsi_status tsi_scene_invert_wait(tsi_scene *s, tsi_stats *stats) {
     SceneCounters ctr;
     const tsi_status st = read_counters(s, ctr);
     if (st != TSI_OK) return st;
-    fill_stats(*c->h_rb, stats, (uint64_t)ctr.live_bricks * 8u);
+    fill_stats(c, 0, s, stats, (uint64_t)ctr.live_bricks * 8u);
     float ms = 0.0f;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     stats->device_ms = ms;
@@ -1775,15 +1753,32 @@ static tsi_status batch_enqueue(tsi_ctx *c, tsi_request *reqs, uint32_t n) {
     times[i] = reqs[i].time;
     t0s[i] = reqs[i].t0_or_nan;
   }
+  tsi_status st = ensure_readback_rows(c, n);
+  if (st != TSI_OK) return st;
+  // Batches wider than one launch run as consecutive launch sequences; each
+  // one's error words and counters go to its own readback rows, so nothing
+  // of an earlier chunk is lost.  Every scene's trace starts on the trace
+  // stream as soon as its own last level is done, overlapping the deeper
+  // levels of the other scenes (and the next chunk's inversion).
+  bool forked = false;  // traces queued on the trace stream (joined back below)
   for (uint32_t i0 = 0; i0 < n; i0 += c->max_scenes) {
     const uint32_t m = std::min(c->max_scenes, n - i0);
-    tsi_status st = enqueue_invert(c, sc.data() + i0, times.data() + i0, t0s.data() + i0, m);
+    st = enqueue_invert(c, sc.data() + i0, times.data() + i0, t0s.data() + i0, m, false, true);
+    if (st != TSI_OK) return st;
+    for (uint32_t i = i0; i < i0 + m; ++i) {
+      if (!reqs[i].uniforms) continue;
+      const uint32_t last = tree_levels(sc[i]->p) - 1u;
+      CK(cudaStreamWaitEvent(c->trace_stream, c->fork_events[last], 0));
+      forked = true;
+      st = enqueue_trace(reqs[i].scene, reqs[i].uniforms, c->trace_stream);
+      if (st != TSI_OK) return st;
+    }
+    st = enqueue_readback(c, m, i0);
     if (st != TSI_OK) return st;
   }
-  for (uint32_t i = 0; i < n; ++i) {
-    if (!reqs[i].uniforms) continue;
-    tsi_status st = enqueue_trace(reqs[i].scene, reqs[i].uniforms);
-    if (st != TSI_OK) return st;
+  if (forked) {
+    CK(cudaEventRecord(c->join_event, c->trace_stream));
+    CK(cudaStreamWaitEvent(c->stream, c->join_event, 0));
   }
   return TSI_OK;
 }
@@ -1801,18 +1796,21 @@ TSI_API tsi_status tsi_batch_run(tsi_ctx *c, tsi_request *reqs, uint32_t n) {
       if (st != TSI_OK) return st;
     }
   }
-  st = enqueue_readback(c);
-  if (st != TSI_OK) return st;
   CK(cudaStreamSynchronize(c->stream));
   float ms = 0.0f;
   CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  uint32_t err = 0;
   for (uint32_t i = 0; i < n; ++i) {
+    err |= c->h_err[i];
     if (reqs[i].stats) {
-      fill_stats(*c->h_rb, reqs[i].stats, 0);
+      SceneCounters ctr;
+      st = read_counters(reqs[i].scene, ctr);
+      if (st != TSI_OK) return st;
+      fill_stats(c, i, reqs[i].scene, reqs[i].stats, (uint64_t)ctr.live_bricks * 8u);
       reqs[i].stats->device_ms = ms;
     }
   }
-  return status_from_error_bits(c->h_rb->error);
+  return status_from_error_bits(err);
 }
 
 TSI_API tsi_status tsi_batch_autotune(tsi_ctx *c, const tsi_request *reqs, uint32_t n, uint32_t frames,
@@ -1925,7 +1923,6 @@ TSI_API tsi_status tsi_batch_graph_create(tsi_ctx *c, tsi_request *reqs, uint32_
   if (st == TSI_OK) st = batch_enqueue(c, g->reqs.data(), n);
   if (st == TSI_OK && cudaEventRecordWithFlags(c->ev1, c->stream, cudaEventRecordExternal) != cudaSuccess)
     st = set_err(TSI_ERR_CUDA, "event record in capture");
-  if (st == TSI_OK) st = enqueue_readback(c);
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
   if (st != TSI_OK || e != cudaSuccess) {
@@ -1979,13 +1976,16 @@ TSI_API tsi_status tsi_batch_graph_wait(tsi_batch_graph *g, tsi_stats *stats) {
   CK(cudaSetDevice(c->device));
   CK(cudaStreamSynchronize(c->stream));
   if (!g->launched) return set_err(TSI_ERR_INVALID_ARGUMENT, "graph not launched");
+  const uint32_t n = (uint32_t)g->reqs.size();
   if (stats) {
-    fill_stats(*c->h_rb, stats, 0);
+    std::vector<tsi_scene *> sc(n);
+    for (uint32_t i = 0; i < n; ++i) sc[i] = g->reqs[i].scene;
+    fill_stats_sum(c, sc.data(), n, stats);
     float ms = 0.0f;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     stats->device_ms = ms;
   }
-  return status_from_error_bits(c->h_rb->error);
+  return status_from_error_bits(readback_error_or(c, n));
 }
 
 TSI_API void tsi_batch_graph_destroy(tsi_batch_graph *g) {

@@ -16,6 +16,13 @@
 #include "tape_format.h"
 
 #define TSI_MAX_LEVELS 24
+// Work lists are indexed by launch step, not by octree level: in the plain
+// and batched forms step = level, in the continuous (served) form scenes
+// join at any step and run one level per step.  Per-step counters live in a
+// ring of TSI_STEP_RING entries; the item lists are double-buffered by the
+// step's parity.
+#define TSI_STEP_RING 32u
+#define TSI_STEP_MASK (TSI_STEP_RING - 1u)
 #define TSI_PRUNE_MAX_REGS 64u  // pruning tracks liveness in one 64-bit mask
 #define TSI_PRUNE_MIN_LEN 8u    // shorter tapes are not worth pruning
 
@@ -152,21 +159,41 @@ enum tsi_stat_index {
   ST_WIDE_REFWD, ST_CYC_WIDE_REFWD, ST_COUNT
 };
 
+// Ring and buffer indices of one launch step.
+struct StepIdx {
+  uint32_t cur, next;  // counters of this step's lists and of the next step's
+  uint32_t buf, nbuf;  // item buffers (step parity)
+};
+
 struct LaunchParams {
   SceneLaunch *scenes;
   uint32_t n_scenes;
   uint32_t rec_cap;
+  // Tape records: [0, rec_base) are the scenes' root records (one per scene
+  // slot); pruned records are taken from a ring over [rec_base, rec_cap) by a
+  // 64-bit counter, and the code arena is a ring over code_cap words.  An
+  // allocation may not pass the low-water marks (counter values below which
+  // records and code may still be read) by a whole ring: the plain form
+  // resets counters and marks to 0 per frame; the continuous form moves the
+  // marks to the oldest running scene's first step.
   TapeRec *recs;
-  uint32_t *rec_count;
+  unsigned long long *rec_count;
+  unsigned long long *rec_low;
+  uint32_t rec_base;
+  uint32_t pad1;
   uint2 *code_arena;
   unsigned long long *code_count;
+  unsigned long long *code_low;
   unsigned long long code_cap;
+  // counters at the start of each step (continuous form's low-water marks)
+  unsigned long long *step_code_start;  // [TSI_STEP_RING]
+  unsigned long long *step_rec_start;   // [TSI_STEP_RING]
   WorkItem *items[2];
-  uint32_t *item_count;    // [TSI_MAX_LEVELS + 1]
-  uint32_t *item_cursor;   // [TSI_MAX_LEVELS + 1]
+  uint32_t *item_count;    // [TSI_STEP_RING]
+  uint32_t *item_cursor;   // [TSI_STEP_RING]
   WorkItem *witems[2];     // wide items: one parent each, one block per child cell
-  uint32_t *witem_count;   // [TSI_MAX_LEVELS + 1]
-  uint32_t *witem_cursor;  // [TSI_MAX_LEVELS + 1], in child cells
+  uint32_t *witem_count;   // [TSI_STEP_RING]
+  uint32_t *witem_cursor;  // [TSI_STEP_RING], in child cells
   uint32_t witem_cap;      // wide items per level; more go to the narrow list
   uint32_t bm_words;       // branch-decision words per wide cell (2 bits per min/max)
   CellInfo *cell_info[2];  // [witem_cap * 8] per level parity
@@ -179,7 +206,7 @@ struct LaunchParams {
   uint32_t item_cap;
   uint32_t dealloc_cap;
   uint2 *dealloc[2];       // (scene, brick)
-  uint32_t *dealloc_count; // [TSI_MAX_LEVELS + 1]
+  uint32_t *dealloc_count; // [TSI_STEP_RING]
   uint32_t *dealloc_cursor;
   // per-warp scratch: operand log [slice_len][32] float4, then decisions [slice_len] uint2
   float4 *log_slices;
@@ -187,11 +214,22 @@ struct LaunchParams {
   uint32_t slice_len;
   uint32_t pad0;
   float4 *log_overflow;
-  // [TSI_MAX_LEVELS + 1], in float4 units: a level's logs are dead once the
-  // next level starts, so every level fills the arena from its start
+  // [TSI_STEP_RING], in float4 units: a step's logs are dead once the
+  // next step starts, so every step fills the arena from its start
   unsigned long long *log_overflow_used;
   unsigned long long log_overflow_cap;
-  uint32_t *error;
-  unsigned long long *stats;        // [ST_COUNT]
-  unsigned long long *level_stats;  // [TSI_MAX_LEVELS + 1][ST_COUNT], per refine launch
+  uint32_t *error;                  // [n_scenes]: error bits of each scene
+  unsigned long long *stats;        // [n_scenes][ST_COUNT]: counters of each scene
+  unsigned long long *level_stats;  // [TSI_STEP_RING][ST_COUNT], per refine launch, or null
 };
+
+// Slots that join the continuous form at one step (step_begin_kernel's
+// parameter).
+#define TSI_SEEDS_MAX 256u
+struct StepSeeds {
+  uint32_t n;       // slots joining at this step
+  uint32_t oldest;  // first step of the oldest running slot (low-water marks)
+  uint32_t slot[TSI_SEEDS_MAX];
+};
+
+static_assert(TSI_MAX_LEVELS + 1 <= TSI_STEP_RING, "a frame's levels fit the step ring");

@@ -140,6 +140,25 @@ __device__ uint32_t alloc_brick(const SceneLaunch &S, uint32_t *error) {
   return b * 8u;
 }
 
+// Reserves n words of the code arena (a ring of code_cap words); returns the
+// word offset, or ~0 when the ring has no room left above the low-water mark
+// (the tape then stays unpruned).  A tape never wraps around the ring's end.
+__device__ __forceinline__ unsigned long long code_alloc(const LaunchParams &P, uint32_t n) {
+  const unsigned long long c = atomicAdd(P.code_count, (unsigned long long)n);
+  if (c + n > *P.code_low + P.code_cap) return ~0ull;
+  const unsigned long long off = c % P.code_cap;
+  return off + n <= P.code_cap ? off : ~0ull;
+}
+
+// Takes a tape record from the ring [rec_base, rec_cap); TSI_NONE when the
+// ring has no room left above the low-water mark.
+__device__ __forceinline__ uint32_t rec_alloc(const LaunchParams &P) {
+  const unsigned long long r = atomicAdd(P.rec_count, 1ull);
+  const unsigned long long ring = (unsigned long long)(P.rec_cap - P.rec_base);
+  if (r >= *P.rec_low + ring) return TSI_NONE;
+  return P.rec_base + (uint32_t)(r % ring);
+}
+
 __device__ __forceinline__ void find_valid(const LaunchParams &P, uint32_t &rec, TapeRec &TR, float tl, float th) {
   TR = P.recs[rec];
   while (TR.parent != TSI_NONE && !(TR.t_lo <= tl && th <= TR.t_hi)) {
@@ -156,12 +175,13 @@ __device__ __forceinline__ void find_valid(const LaunchParams &P, uint32_t &rec,
 // (readers take min(count, capacity) entries); narrow-list overflow is
 // dropped and reported.
 __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint32_t scene, uint32_t rec,
-                              uint32_t level, uint32_t E, const uint32_t *cells, bool wide,
+                              const StepIdx &si, uint32_t plevel, uint32_t E, const uint32_t *cells, bool wide,
                               unsigned long long *ws) {
   uint32_t rest = E;
+  uint32_t *err = P.error + scene;
   if (wide) {
     const uint32_t n = __popc(E);
-    const uint32_t pos = atomicAdd(&P.witem_count[level + 1], n);
+    const uint32_t pos = atomicAdd(&P.witem_count[si.next], n);
     uint32_t j = 0;
     while (rest && pos + j < P.witem_cap) {
       const uint32_t bit = __ffs(rest) - 1u;
@@ -169,7 +189,7 @@ __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint3
       const uint32_t c = cells[bit];
       uint32_t b = S.pool.child[c], fresh = 0;
       if (b == TSI_NONE) {
-        b = alloc_brick(S, P.error);
+        b = alloc_brick(S, err);
         if (b != TSI_NONE) {
           S.pool.child[c] = b;
           fresh = 1;
@@ -180,24 +200,24 @@ __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint3
       wi.scene = scene;
       wi.rec = rec;
       wi.n = 1;
-      wi.level = level + 1;
+      wi.level = plevel + 1;
       wi.parent[0] = c;
       wi.parent[1] = b;
       wi.parent[2] = fresh;
       wi.parent[3] = 0;
-      P.witems[(level + 1) & 1][pos + j++] = wi;
+      P.witems[si.nbuf][pos + j++] = wi;
     }
   }
   if (rest == 0) return;
   const uint32_t nitems = (__popc(rest) + 3u) >> 2;
-  const uint32_t pos = atomicAdd(&P.item_count[level + 1], nitems);
-  if (pos + nitems > P.item_cap) atomicOr(P.error, EB_QUEUE_FULL);
-  WorkItem *dst = P.items[(level + 1) & 1];
+  const uint32_t pos = atomicAdd(&P.item_count[si.next], nitems);
+  if (pos + nitems > P.item_cap) atomicOr(err, EB_QUEUE_FULL);
+  WorkItem *dst = P.items[si.nbuf];
   for (uint32_t j = 0; j < nitems && pos + j < P.item_cap; ++j) {
     WorkItem wi;
     wi.scene = scene;
     wi.rec = rec;
-    wi.level = level + 1;
+    wi.level = plevel + 1;
     uint32_t c = 0;
     while (rest && c < 4u) {
       const uint32_t bit = __ffs(rest) - 1u;
@@ -215,12 +235,12 @@ __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint3
 // the brick allocations proceed in parallel; the first wide-list slots go
 // to the lowest enqueued octants, as in push_children.
 __device__ __forceinline__ void push_children_warp(const LaunchParams &P, const SceneLaunch &S, uint32_t scene,
-                                                   uint32_t rec, uint32_t level, uint32_t E, uint32_t base,
-                                                   bool wide, unsigned long long *ws, uint32_t lane) {
+                                                   uint32_t rec, const StepIdx &si, uint32_t plevel, uint32_t E,
+                                                   uint32_t base, bool wide, unsigned long long *ws, uint32_t lane) {
   uint32_t rest = E;
   if (wide && E) {
     uint32_t pos = 0;
-    if (lane == 0) pos = atomicAdd(&P.witem_count[level + 1], (uint32_t)__popc(E));
+    if (lane == 0) pos = atomicAdd(&P.witem_count[si.next], (uint32_t)__popc(E));
     pos = __shfl_sync(FULL_MASK, pos, 0);
     const uint32_t avail = pos < P.witem_cap ? P.witem_cap - pos : 0u;
     const uint32_t j = __popc(E & ((1u << lane) - 1u));
@@ -229,7 +249,7 @@ __device__ __forceinline__ void push_children_warp(const LaunchParams &P, const 
       const uint32_t c = base + lane;
       uint32_t b = S.pool.child[c], fresh = 0;
       if (b == TSI_NONE) {
-        b = alloc_brick(S, P.error);
+        b = alloc_brick(S, P.error + scene);
         if (b != TSI_NONE) {
           S.pool.child[c] = b;
           fresh = 1;
@@ -240,19 +260,19 @@ __device__ __forceinline__ void push_children_warp(const LaunchParams &P, const 
       wi.scene = scene;
       wi.rec = rec;
       wi.n = 1;
-      wi.level = level + 1;
+      wi.level = plevel + 1;
       wi.parent[0] = c;
       wi.parent[1] = b;
       wi.parent[2] = fresh;
       wi.parent[3] = 0;
-      P.witems[(level + 1) & 1][pos + j] = wi;
+      P.witems[si.nbuf][pos + j] = wi;
     }
     rest = E & ~__ballot_sync(FULL_MASK, take);
   }
   if (lane == 0 && rest) {
     uint32_t cells[8];
     for (int q = 0; q < 8; ++q) cells[q] = base + q;
-    push_children(P, S, scene, rec, level, rest, cells, false, ws);
+    push_children(P, S, scene, rec, si, plevel, rest, cells, false, ws);
   }
 }
 
@@ -267,8 +287,9 @@ __device__ __forceinline__ float warp_max(float v) {
 
 // scratch for one item: operand log + decisions, in the warp's slice or the
 // shared overflow arena (long tapes)
-__device__ __forceinline__ bool item_scratch(const LaunchParams &P, uint32_t level, uint32_t len, uint32_t lane,
-                                             float4 *slice_log, uint2 *slice_dec, float4 *&lg, uint2 *&dg) {
+__device__ __forceinline__ bool item_scratch(const LaunchParams &P, const StepIdx &si, uint32_t scene, uint32_t len,
+                                             uint32_t lane, float4 *slice_log, uint2 *slice_dec, float4 *&lg,
+                                             uint2 *&dg) {
   if (len <= P.slice_len) {
     lg = slice_log;
     dg = slice_dec;
@@ -276,10 +297,10 @@ __device__ __forceinline__ bool item_scratch(const LaunchParams &P, uint32_t lev
   }
   const unsigned long long need = (unsigned long long)len * 32ull + ((unsigned long long)len + 1ull) / 2ull;
   unsigned long long off = 0;
-  if (lane == 0) off = atomicAdd(P.log_overflow_used + level, need);
+  if (lane == 0) off = atomicAdd(P.log_overflow_used + si.cur, need);
   off = __shfl_sync(FULL_MASK, off, 0);
   if (off + need > P.log_overflow_cap) {
-    if (lane == 0) atomicOr(P.error, EB_LOG_OOM);
+    if (lane == 0) atomicOr(P.error + scene, EB_LOG_OOM);
     return false;
   }
   lg = P.log_overflow + off;
@@ -288,8 +309,9 @@ __device__ __forceinline__ bool item_scratch(const LaunchParams &P, uint32_t lev
 }
 
 template <bool D>
-__device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t level, uint32_t rf_off,
-                                          float4 *slice_log, uint2 *slice_dec, unsigned long long *ws) {
+__device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem &it, const StepIdx &si,
+                                          uint32_t rf_off, float4 *slice_log, uint2 *slice_dec,
+                                          unsigned long long *ws) {
   float2 *rf = reinterpret_cast<float2 *>(tsi_dyn_smem) + rf_off;  // this warp's register file
   using A = IA<D>;
   const uint32_t lane = threadIdx.x & 31u;
@@ -310,7 +332,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
   // ---- allocate or reuse the 8 children (3564-3580)
   uint32_t base = pchild;
   if (active && new_voxel && k == 0) {
-    base = alloc_brick(S, P.error);
+    base = alloc_brick(S, P.error + it.scene);
     if (base != TSI_NONE) atomicAdd(&ws[ST_BRICK_ALLOC], 1ull);
   }
   base = __shfl_sync(FULL_MASK, base, lane & ~7u);
@@ -384,7 +406,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     const float tl = warp_min(evaluate ? targ.lo : fm_inf());
     const float th = warp_max(evaluate ? targ.hi : -fm_inf());
     TR = P.recs[rec];
-    if (!(TR.c_level == level && TR.c_lo <= tl && th <= TR.c_hi)) find_valid(P, rec, TR, tl, th);
+    if (!(TR.c_level == it.level && TR.c_lo <= tl && th <= TR.c_hi)) find_valid(P, rec, TR, tl, th);
     for (int attempt = 0; attempt < 2; ++attempt) {
       want_prune = (flags & SF_PRUNING) && TR.len >= TSI_PRUNE_MIN_LEN && TR.nregs <= TSI_PRUNE_MAX_REGS;
       if (lane == 0 && attempt == 0) {
@@ -396,7 +418,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
       if (any_deriv || want_prune) {
         float4 *lgs = nullptr;
         uint2 *dgs = nullptr;
-        if (!item_scratch(P, level, TR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
+        if (!item_scratch(P, si, it.scene, TR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
         lg = lgs;
         dg = want_prune ? dgs : nullptr;
       }
@@ -496,12 +518,12 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     const uint32_t m = __ballot_sync(FULL_MASK, dealloc);
     if (m) {
       uint32_t basei = 0;
-      if (lane == 0) basei = atomicAdd(&P.dealloc_count[level + 1], (uint32_t)__popc(m));
+      if (lane == 0) basei = atomicAdd(&P.dealloc_count[si.next], (uint32_t)__popc(m));
       basei = __shfl_sync(FULL_MASK, basei, 0);
       if (dealloc) {
         const uint32_t pos = basei + __popc(m & ((1u << lane) - 1u));
-        if (pos < P.dealloc_cap) P.dealloc[(level + 1) & 1][pos] = make_uint2(it.scene, dealloc_brick);
-        else atomicOr(P.error, EB_QUEUE_FULL);
+        if (pos < P.dealloc_cap) P.dealloc[si.nbuf][pos] = make_uint2(it.scene, dealloc_brick);
+        else atomicOr(P.error + it.scene, EB_QUEUE_FULL);
       }
     }
   }
@@ -560,7 +582,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
       if (want_prune && WR.len < S.wide.min_len) {
         float4 *lgs;
         uint2 *dgs;
-        if (!item_scratch(P, level, PR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
+        if (!item_scratch(P, si, it.scene, PR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
         lg = lgs;
         dg = dgs;
         const Iv tw = enq ? Iv{nl, nh} : targ;
@@ -607,11 +629,8 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     unsigned long long off = 0;
     uint32_t ri = TSI_NONE;
     if (k == 0 && pruned) {
-      off = atomicAdd(P.code_count, (unsigned long long)cnt);
-      if (off + cnt <= P.code_cap) {
-        ri = atomicAdd(P.rec_count, 1u);
-        if (ri >= P.rec_cap) ri = TSI_NONE;
-      }
+      off = code_alloc(P, cnt);
+      if (off != ~0ull) ri = rec_alloc(P);
     }
     const uint32_t gl0 = lane & ~7u;
     cnt = __shfl_sync(FULL_MASK, cnt, gl0);
@@ -633,7 +652,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
         nr.rev_cost = rcost;
         nr.c_lo = hl;
         nr.c_hi = hh;
-        nr.c_level = level + 1u;
+        nr.c_level = it.level + 1u;
         P.recs[ri] = nr;
         atomicAdd(&ws[ST_TAPE_WORDS], (unsigned long long)cnt);
       }
@@ -646,7 +665,8 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
 #pragma unroll
     for (int b2 = 0; b2 < 8; ++b2) cb[b2] = __shfl_sync(FULL_MASK, C, gl0 + b2);
     const uint32_t next_len = (new_rec == prec) ? PR.len : ((new_rec == rec) ? TR.len : cnt);
-    if (k == 0 && E != 0) push_children(P, S, it.scene, new_rec, level, E, cb, next_len >= S.wide.min_len, ws);
+    if (k == 0 && E != 0)
+      push_children(P, S, it.scene, new_rec, si, it.level, E, cb, next_len >= S.wide.min_len, ws);
   }
 
   // ---- counters
@@ -670,8 +690,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
 
 // Recursive free of a dropped subtree (compute.wgsl:3533-3543, freeV
 // 3452-3460): 8 lanes per brick; children bricks go to the next level's list.
-__device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level, bool valid,
-                              unsigned long long *ws) {
+__device__ void dealloc_brick(const LaunchParams &P, uint2 item, const StepIdx &si, bool valid) {
   const uint32_t lane = threadIdx.x & 31u, k = lane & 7u;
   const SceneLaunch &S = P.scenes[valid ? item.x : 0];
   const VoxelPoolDev &pool = S.pool;
@@ -689,20 +708,20 @@ __device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t level,
   const uint32_t m = __ballot_sync(FULL_MASK, push);
   if (m) {
     uint32_t basei = 0;
-    if (lane == 0) basei = atomicAdd(&P.dealloc_count[level + 1], (uint32_t)__popc(m));
+    if (lane == 0) basei = atomicAdd(&P.dealloc_count[si.next], (uint32_t)__popc(m));
     basei = __shfl_sync(FULL_MASK, basei, 0);
     if (push) {
       const uint32_t pos = basei + __popc(m & ((1u << lane) - 1u));
-      if (pos < P.dealloc_cap) P.dealloc[(level + 1) & 1][pos] = make_uint2(item.x, ch >> 3);
-      else atomicOr(P.error, EB_QUEUE_FULL);
+      if (pos < P.dealloc_cap) P.dealloc[si.nbuf][pos] = make_uint2(item.x, ch >> 3);
+      else atomicOr(P.error + item.x, EB_QUEUE_FULL);
     }
   }
-  const uint32_t fm = __ballot_sync(FULL_MASK, valid && k == 0);
   if (valid && k == 0) {
     const uint32_t pos = atomicAdd(&S.ctr->pending_count, 1u);
     if (pos < pool.cap_bricks) pool.pending[pos] = item.y;
+    atomicAdd(&P.stats[(size_t)item.x * ST_COUNT + ST_BRICK_FREE], 1ull);  // the brick's own scene
+    if (P.level_stats) atomicAdd(&P.level_stats[(size_t)si.cur * ST_COUNT + ST_BRICK_FREE], 1ull);
   }
-  if (lane == 0) ws[ST_BRICK_FREE] += __popc(fm);
 }
 
 // ======================================================================
@@ -780,7 +799,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s
 // The last cell of a wide item to finish: prunes the full tape with the
 // branch decisions shared by all enqueued siblings and enqueues them.
 template <bool GM>
-__device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkItem &it, uint32_t level,
+__device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkItem &it, const StepIdx &si,
                                              uint32_t unit0, WideShared &sh, unsigned long long *ws) {
   unsigned char *cell = cell_base<GM>(P);
   const uint32_t tid = threadIdx.x;
@@ -788,7 +807,7 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
   const WideDev &W = S.wide;
   const TapeRec root = P.recs[S.root_rec];
   const uint32_t n_narrow = root.len;
-  const CellInfo *info = P.cell_info[level & 1] + unit0;
+  const CellInfo *info = P.cell_info[si.buf] + unit0;
   const long long f0 = clock64();
   if (tid == 0) {
     ws[ST_PARENTS] += 1;
@@ -821,7 +840,7 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
     uint32_t *cb = reinterpret_cast<uint32_t *>(cell + L.bits);  // decisions shared by the enqueued cells
     uint8_t *flags = cell + L.flags;
     const uint32_t words = (root.n_minmax + 15u) >> 4;
-    const uint32_t *gbits = P.cell_bits[level & 1] + (size_t)unit0 * P.bm_words;
+    const uint32_t *gbits = P.cell_bits[si.buf] + (size_t)unit0 * P.bm_words;
     for (uint32_t w = tid; w < words; w += blockDim.x) {
       uint32_t acc = 0xffffffffu;
       for (int q = 0; q < 8; ++q)
@@ -882,12 +901,12 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
       // a pruned record only for children that go to the narrow path (the
       // wide path evaluates the full tape), or may: children the full wide
       // list turns away run narrow on this record
-      const bool wide_room = *(const volatile uint32_t *)&P.witem_count[level + 1] + 8u <= P.witem_cap;
+      const bool wide_room = *(const volatile uint32_t *)&P.witem_count[si.next] + 8u <= P.witem_cap;
       if (total < n_narrow && (total < W.min_len || !wide_room)) {
-        const unsigned long long off = atomicAdd(P.code_count, (unsigned long long)total);
-        if (off + total <= P.code_cap) {
-          const uint32_t ri = atomicAdd(P.rec_count, 1u);
-          if (ri < P.rec_cap) {
+        const unsigned long long off = code_alloc(P, total);
+        if (off != ~0ull) {
+          const uint32_t ri = rec_alloc(P);
+          if (ri != TSI_NONE) {
             sh.ri = ri;
             sh.off = off;
           }
@@ -976,7 +995,7 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
         nr.rev_cost = sh.rcost;
         nr.c_lo = sh.hl;
         nr.c_hi = sh.hh;
-        nr.c_level = level + 1u;
+        nr.c_level = it.level + 1u;
         P.recs[sh.ri] = nr;
         ws[ST_TAPE_WORDS] += sh.cnt;
       }
@@ -986,7 +1005,7 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
   const long long f2 = clock64();
   if (tid < 32u) {
     const uint32_t len = (new_rec == S.root_rec) ? root.len : sh.cnt;
-    push_children_warp(P, S, it.scene, new_rec, level, E, it.parent[1], len >= W.min_len, ws, tid);
+    push_children_warp(P, S, it.scene, new_rec, si, it.level, E, it.parent[1], len >= W.min_len, ws, tid);
   }
   if (tid == 0) {
     const long long f3 = clock64();
@@ -998,7 +1017,7 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
 // One child cell (octant k) of a wide item.  unit = item * 8 + k.
 template <bool D, bool GM>
 __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, uint32_t k, uint32_t unit,
-                                          uint32_t level, WideShared &sh, unsigned long long *ws) {
+                                          const StepIdx &si, WideShared &sh, unsigned long long *ws) {
   unsigned char *cell = cell_base<GM>(P);  // the cell's working set
   using A = IA<D>;
   const uint32_t tid = threadIdx.x;
@@ -1018,7 +1037,7 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   const CellLayout L = cell_layout(W, P.bm_words);
   if constexpr (!GM) {  // the host sized the launch for this cell; never write past it
     if (L.flags + ((W.nvalues + 15u) & ~15u) > P.dyn_smem) {
-      if (tid == 0) atomicOr(P.error, EB_SMEM);
+      if (tid == 0) atomicOr(P.error + it.scene, EB_SMEM);
       return;
     }
   }
@@ -1197,9 +1216,9 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
     pool.fast[C] = c_fast;
     if (dealloc || new_voxel) pool.child[C] = c_child;
     if (dealloc) {
-      const uint32_t pos = atomicAdd(&P.dealloc_count[level + 1], 1u);
-      if (pos < P.dealloc_cap) P.dealloc[(level + 1) & 1][pos] = make_uint2(it.scene, old_child >> 3);
-      else atomicOr(P.error, EB_QUEUE_FULL);
+      const uint32_t pos = atomicAdd(&P.dealloc_count[si.next], 1u);
+      if (pos < P.dealloc_cap) P.dealloc[si.nbuf][pos] = make_uint2(it.scene, old_child >> 3);
+      else atomicOr(P.error + it.scene, EB_QUEUE_FULL);
     }
     ws[ST_EVAL] += evaluate ? 1ull : 0ull;
     ws[ST_REVERSE] += take_deriv ? 1ull : 0ull;
@@ -1250,7 +1269,7 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   // ---- hand over to the group: decision bits and time range, then count in
   __syncthreads();
   if (want_prune && enq) {
-    uint32_t *dst = P.cell_bits[level & 1] + (size_t)unit * P.bm_words;
+    uint32_t *dst = P.cell_bits[si.buf] + (size_t)unit * P.bm_words;
     for (uint32_t w = tid; w < words; w += blockDim.x) dst[w] = bits[w];
   }
   if (tid == 0) {
@@ -1259,7 +1278,7 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
     ci.nh = enq ? nh : fm_inf();
     ci.enq = enq ? 1u : 0u;
     ci.pad = 0;
-    P.cell_info[level & 1][unit] = ci;
+    P.cell_info[si.buf][unit] = ci;
   }
   __threadfence();
   __syncthreads();
@@ -1267,11 +1286,41 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   __syncthreads();
   if (!sh.last) return;
   __threadfence();
-  finish_group<GM>(P, it, level, unit & ~7u, sh, ws);
+  finish_group<GM>(P, it, si, unit & ~7u, sh, ws);
 }
 
-__global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ LaunchParams P, uint32_t level,
+// A warp's counters belong to the scene whose items it counted: they are
+// added to that scene's stats row (and the launch's level row) when the warp
+// moves on to another scene's item and at the end of the launch.
+__device__ __forceinline__ void flush_stats(const LaunchParams &P, unsigned long long *ws, uint32_t scene,
+                                            uint32_t cur, uint32_t lane) {
+  __syncwarp();
+  unsigned long long *row = P.stats + (size_t)scene * ST_COUNT;
+  unsigned long long *lv = P.level_stats ? P.level_stats + (size_t)cur * ST_COUNT : nullptr;
+  for (uint32_t i = lane; i < ST_COUNT; i += 32u) {
+    const unsigned long long v = ws[i];
+    if (!v) continue;
+    ws[i] = 0;
+    if (i == ST_CYC_WIDE_MAX || i == ST_CYC_NARROW_MAX || i == ST_NARROW_LEN_MAX) {
+      atomicMax(row + i, v);
+      if (lv) atomicMax(lv + i, v);
+    } else {
+      atomicAdd(row + i, v);
+      if (lv) atomicAdd(lv + i, v);
+    }
+  }
+  __syncwarp();
+}
+
+// One launch step over every scene of the launch: the wide items, the narrow
+// items and the deallocation items of the step's lists.
+__global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ LaunchParams P, uint32_t step,
                                                      uint32_t rcap) {
+  StepIdx si;
+  si.cur = step & TSI_STEP_MASK;
+  si.next = (step + 1u) & TSI_STEP_MASK;
+  si.buf = step & 1u;
+  si.nbuf = (step + 1u) & 1u;
   __shared__ unsigned long long s_stats[kWarps][ST_COUNT];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -1281,28 +1330,38 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
   unsigned long long *ws = s_stats[wib];
   for (uint32_t i = lane; i < ST_COUNT; i += 32u) ws[i] = 0;
   __syncwarp();
+  uint32_t wscene = TSI_NONE;  // the scene whose counters ws holds (warp uniform)
+  auto take = [&](uint32_t sc) {
+    if (sc != wscene) {
+      if (wscene != TSI_NONE) flush_stats(P, ws, wscene, si.cur, lane);
+      wscene = sc;
+    }
+  };
 
   __shared__ WideShared sh;
   __shared__ uint32_t s_idx;
-  // wide items: one block per child cell
+  // wide items: one block per child cell (thread 0 and warp 0 count into
+  // s_stats[0], warp 0's counters)
   auto wide_phase = [&]() {
-    const uint32_t n_units = min(P.witem_count[level], P.witem_cap) * 8u;
+    const uint32_t n_units = min(P.witem_count[si.cur], P.witem_cap) * 8u;
     while (true) {
-      if (threadIdx.x == 0) s_idx = atomicAdd(&P.witem_cursor[level], 1u);
+      if (threadIdx.x == 0) s_idx = atomicAdd(&P.witem_cursor[si.cur], 1u);
       __syncthreads();
       const uint32_t u = s_idx;
       __syncthreads();
       if (u >= n_units) break;
-      WorkItem *itp = P.witems[level & 1] + (u >> 3);
+      WorkItem *itp = P.witems[si.buf] + (u >> 3);
+      const uint32_t sc = itp->scene;
+      if (wib == 0) take(sc);
       const long long c0 = clock64();
-      const SceneLaunch &S = P.scenes[itp->scene];
+      const SceneLaunch &S = P.scenes[sc];
       const bool directed = (S.flags & SF_DIRECTED) != 0;
       if (S.wide.global) {
-        if (directed) process_cell<true, true>(P, itp, u & 7u, u, level, sh, s_stats[0]);
-        else process_cell<false, true>(P, itp, u & 7u, u, level, sh, s_stats[0]);
+        if (directed) process_cell<true, true>(P, itp, u & 7u, u, si, sh, s_stats[0]);
+        else process_cell<false, true>(P, itp, u & 7u, u, si, sh, s_stats[0]);
       } else {
-        if (directed) process_cell<true, false>(P, itp, u & 7u, u, level, sh, s_stats[0]);
-        else process_cell<false, false>(P, itp, u & 7u, u, level, sh, s_stats[0]);
+        if (directed) process_cell<true, false>(P, itp, u & 7u, u, si, sh, s_stats[0]);
+        else process_cell<false, false>(P, itp, u & 7u, u, si, sh, s_stats[0]);
       }
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -1315,17 +1374,18 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
   };
   // narrow items: one warp per item
   auto narrow_phase = [&]() {
-    const uint32_t n_items = min(P.item_count[level], P.item_cap);
-    const WorkItem *items = P.items[level & 1];
+    const uint32_t n_items = min(P.item_count[si.cur], P.item_cap);
+    const WorkItem *items = P.items[si.buf];
     while (true) {
       uint32_t idx = 0;
-      if (lane == 0) idx = atomicAdd(&P.item_cursor[level], 1u);
+      if (lane == 0) idx = atomicAdd(&P.item_cursor[si.cur], 1u);
       idx = __shfl_sync(FULL_MASK, idx, 0);
       if (idx >= n_items) break;
       const WorkItem &it = items[idx];
+      take(it.scene);
       const long long c0 = clock64();
-      if (P.scenes[it.scene].flags & SF_DIRECTED) process_item<true>(P, it, level, rf_off, slice_log, slice_dec, ws);
-      else process_item<false>(P, it, level, rf_off, slice_log, slice_dec, ws);
+      if (P.scenes[it.scene].flags & SF_DIRECTED) process_item<true>(P, it, si, rf_off, slice_log, slice_dec, ws);
+      else process_item<false>(P, it, si, rf_off, slice_log, slice_dec, ws);
       __syncwarp();
       if (lane == 0) {
         const unsigned long long c = (unsigned long long)(clock64() - c0);
@@ -1344,93 +1404,126 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
     narrow_phase();
   }
   // deallocation items: 4 bricks per warp
-  const uint32_t n_dealloc = min(P.dealloc_count[level], P.dealloc_cap);
-  const uint2 *dl = P.dealloc[level & 1];
+  const uint32_t n_dealloc = min(P.dealloc_count[si.cur], P.dealloc_cap);
+  const uint2 *dl = P.dealloc[si.buf];
   while (true) {
     uint32_t idx = 0;
-    if (lane == 0) idx = atomicAdd(&P.dealloc_cursor[level], 4u);
+    if (lane == 0) idx = atomicAdd(&P.dealloc_cursor[si.cur], 4u);
     idx = __shfl_sync(FULL_MASK, idx, 0);
     if (idx >= n_dealloc) break;
     const uint32_t j = idx + (lane >> 3);
     const bool valid = j < n_dealloc;
     const uint2 item = valid ? dl[j] : make_uint2(0u, 0u);
-    dealloc_brick(P, item, level, valid, ws);
+    dealloc_brick(P, item, si, valid);
   }
-  __syncwarp();
-  for (uint32_t i = lane; i < ST_COUNT; i += 32u) {
-    if (!ws[i]) continue;
-    if (i == ST_CYC_WIDE_MAX || i == ST_CYC_NARROW_MAX || i == ST_NARROW_LEN_MAX) {
-      atomicMax(&P.stats[i], ws[i]);
-      atomicMax(&P.level_stats[level * ST_COUNT + i], ws[i]);
-    } else {
-      atomicAdd(&P.stats[i], ws[i]);
-      atomicAdd(&P.level_stats[level * ST_COUNT + i], ws[i]);
-    }
-  }
-
+  if (wscene != TSI_NONE) flush_stats(P, ws, wscene, si.cur, lane);
 }
 
-// Per frame: reset level lists and the tape arena, seed the root of every
-// scene (buf_main's enqueue(0), compute.wgsl:4706).
-__global__ void frame_begin_kernel(LaunchParams P) {
-  const uint32_t t = threadIdx.x;
-  for (uint32_t l = t; l <= TSI_MAX_LEVELS; l += blockDim.x) {
-    P.item_count[l] = 0;
-    P.item_cursor[l] = 0;
-    P.witem_count[l] = 0;
-    P.witem_cursor[l] = 0;
-    P.dealloc_count[l] = 0;
-    P.dealloc_cursor[l] = 0;
+// buf_main's enqueue(0) (compute.wgsl:4706) for scene s: its root as a work
+// item of the step (a wide item, with the root's children brick, when the
+// root tape is long enough).
+__device__ void seed_root(const LaunchParams &P, uint32_t s, const StepIdx &si) {
+  WorkItem w;
+  w.scene = s;
+  w.rec = P.scenes[s].root_rec;
+  w.n = 1;
+  w.level = 0;
+  w.parent[0] = w.parent[1] = w.parent[2] = w.parent[3] = 0u;
+  const SceneLaunch &S = P.scenes[s];
+  const uint32_t len = P.recs[S.root_rec].len;
+  if (len >= S.wide.min_len) {
+    const uint32_t pos = atomicAdd(&P.witem_count[si.cur], 1u);
+    if (pos < P.witem_cap) {
+      uint32_t b = S.pool.child[0], fresh = 0;
+      if (b == TSI_NONE) {
+        b = alloc_brick(S, P.error + s);
+        if (b != TSI_NONE) {
+          S.pool.child[0] = b;
+          fresh = 1;
+          atomicAdd(&P.stats[(size_t)s * ST_COUNT + ST_BRICK_ALLOC], 1ull);
+          if (P.level_stats) atomicAdd(&P.level_stats[(size_t)si.cur * ST_COUNT + ST_BRICK_ALLOC], 1ull);
+        }
+      }
+      w.parent[1] = b;
+      w.parent[2] = fresh;
+      w.parent[3] = 0;
+      P.witems[si.buf][pos] = w;
+      return;
+    }
   }
+  const uint32_t pos = atomicAdd(&P.item_count[si.cur], 1u);
+  if (pos < P.item_cap) P.items[si.buf][pos] = w;
+  else atomicOr(P.error + s, EB_QUEUE_FULL);
+}
+
+__device__ __forceinline__ void clear_step(const LaunchParams &P, uint32_t c) {
+  P.item_count[c] = 0;
+  P.item_cursor[c] = 0;
+  P.witem_count[c] = 0;
+  P.witem_cursor[c] = 0;
+  P.dealloc_count[c] = 0;
+  P.dealloc_cursor[c] = 0;
+  P.log_overflow_used[c] = 0;
+}
+
+// Per frame of the plain and batched forms (steps 0, 1, ... are the levels):
+// clear every step's lists and the tape arenas, seed the root of every scene
+// at step 0.  With n_scenes = 0 it only clears (the continuous form's start).
+__global__ void frame_begin_kernel(const __grid_constant__ LaunchParams P) {
+  const uint32_t t = threadIdx.x;
+  for (uint32_t l = t; l < TSI_STEP_RING; l += blockDim.x) clear_step(P, l);
   if (t == 0) {
-    *P.rec_count = P.n_scenes;
+    *P.rec_count = 0;
     *P.code_count = 0;
+    *P.rec_low = 0;
+    *P.code_low = 0;
   }
   __syncthreads();
-  for (uint32_t s = t; s < P.n_scenes; s += blockDim.x) {
-    WorkItem w;
-    w.scene = s;
-    w.rec = P.scenes[s].root_rec;
-    w.n = 1;
-    w.level = 0;
-    w.parent[0] = w.parent[1] = w.parent[2] = w.parent[3] = 0u;
-    const SceneLaunch &S = P.scenes[s];
-    const uint32_t len = P.recs[S.root_rec].len;
-    if (len >= S.wide.min_len) {  // wide item: the root's children brick now
-      const uint32_t pos = atomicAdd(P.witem_count, 1u);
-      if (pos < P.witem_cap) {
-        uint32_t b = S.pool.child[0], fresh = 0;
-        if (b == TSI_NONE) {
-          b = alloc_brick(S, P.error);
-          if (b != TSI_NONE) {
-            S.pool.child[0] = b;
-            fresh = 1;
-            atomicAdd(&P.stats[ST_BRICK_ALLOC], 1ull);
-            atomicAdd(&P.level_stats[ST_BRICK_ALLOC], 1ull);
-          }
-        }
-        w.parent[1] = b;
-        w.parent[2] = fresh;
-        w.parent[3] = 0;
-        P.witems[0][pos] = w;
-        continue;
-      }
-    }
-    const uint32_t pos = atomicAdd(P.item_count, 1u);
-    if (pos < P.item_cap) P.items[0][pos] = w;
-    else atomicOr(P.error, EB_QUEUE_FULL);
-  }
+  StepIdx si0;
+  si0.cur = 0;
+  si0.next = 1;
+  si0.buf = 0;
+  si0.nbuf = 1;
+  for (uint32_t s = t; s < P.n_scenes; s += blockDim.x) seed_root(P, s, si0);
 }
 
-// Per frame end: bricks freed this frame become allocatable.
-__global__ void frame_end_kernel(LaunchParams P) {
-  const uint32_t s = blockIdx.x;
+// Start of one step of the continuous form: record the arena counters at the
+// step's start, move the low-water marks to the oldest running slot's first
+// step, clear the next step's lists, clear the stats rows and error words of
+// the slots that join at this step and seed their roots.
+__global__ void step_begin_kernel(const __grid_constant__ LaunchParams P, uint32_t step,
+                                  const __grid_constant__ StepSeeds sd) {
+  StepIdx si;
+  si.cur = step & TSI_STEP_MASK;
+  si.next = (step + 1u) & TSI_STEP_MASK;
+  si.buf = step & 1u;
+  si.nbuf = (step + 1u) & 1u;
+  const uint32_t t = threadIdx.x;
+  if (t == 0) {
+    P.step_code_start[si.cur] = *P.code_count;
+    P.step_rec_start[si.cur] = *P.rec_count;
+    *P.code_low = P.step_code_start[sd.oldest & TSI_STEP_MASK];
+    *P.rec_low = P.step_rec_start[sd.oldest & TSI_STEP_MASK];
+    clear_step(P, si.next);
+  }
+  const uint32_t n = min(sd.n, (uint32_t)TSI_SEEDS_MAX);
+  for (uint32_t i = t; i < n * ST_COUNT; i += blockDim.x) P.stats[(size_t)sd.slot[i / ST_COUNT] * ST_COUNT + i % ST_COUNT] = 0;
+  for (uint32_t i = t; i < n; i += blockDim.x) P.error[sd.slot[i]] = 0;
+  __syncthreads();
+  for (uint32_t i = t; i < n; i += blockDim.x) seed_root(P, sd.slot[i], si);
+}
+
+// Per frame end of scenes first .. first + gridDim.x - 1: bricks freed during
+// the frame become allocatable; the scene's error word is or-ed into the
+// sticky word (asynchronous inversions).
+__global__ void frame_end_kernel(const __grid_constant__ LaunchParams P, uint32_t first) {
+  const uint32_t s = first + blockIdx.x;
   if (s >= P.n_scenes) return;
   const SceneLaunch &S = P.scenes[s];
   SceneCounters *c = S.ctr;
   __shared__ int32_t fc0;
   __shared__ uint32_t np;
-  if (s == 0 && threadIdx.x == 0 && P.error_sticky) atomicOr(P.error_sticky, *P.error);
+  if (threadIdx.x == 0 && P.error_sticky) atomicOr(P.error_sticky, P.error[s]);
   if (threadIdx.x == 0) {
     fc0 = max(c->free_count, 0);
     np = min(c->pending_count, S.pool.cap_bricks);
@@ -1447,17 +1540,22 @@ __global__ void frame_end_kernel(LaunchParams P) {
 }
 
 // host-side launch helpers
-cudaError_t launch_refine(const LaunchParams &P, uint32_t level, uint32_t rcap, int grid, int block, size_t smem,
+cudaError_t launch_refine(const LaunchParams &P, uint32_t step, uint32_t rcap, int grid, int block, size_t smem,
                           cudaStream_t st) {
-  refine_kernel<<<grid, block, smem, st>>>(P, level, rcap);
+  refine_kernel<<<grid, block, smem, st>>>(P, step, rcap);
   return cudaGetLastError();
 }
 cudaError_t launch_frame_begin(const LaunchParams &P, cudaStream_t st) {
   frame_begin_kernel<<<1, 64, 0, st>>>(P);
   return cudaGetLastError();
 }
-cudaError_t launch_frame_end(const LaunchParams &P, cudaStream_t st) {
-  frame_end_kernel<<<P.n_scenes, 256, 0, st>>>(P);
+cudaError_t launch_step_begin(const LaunchParams &P, uint32_t step, const StepSeeds &sd, cudaStream_t st) {
+  step_begin_kernel<<<1, 256, 0, st>>>(P, step, sd);
+  return cudaGetLastError();
+}
+cudaError_t launch_frame_end(const LaunchParams &P, uint32_t first, uint32_t count, cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  frame_end_kernel<<<count, 256, 0, st>>>(P, first);
   return cudaGetLastError();
 }
 // The attribute belongs to the kernel on the current device, shared by every

@@ -28,3 +28,23 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["value"] == line["value"] and cb["cores"] >= 1 and cb["kind"] == "port" and cb["sample"]
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_runs_without_the_product_library():
+    """The reference arm lowers its tape with the oracle's ir.rs restatement
+    and builds its parameters itself: libtsi.so is never loaded."""
+    code = ("import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '3'];"
+            "runpy.run_path('bench.py', run_name='__main__');"
+            "maps = open('/proc/self/maps').read();"
+            "print('LIBTSI_LOADED' if 'libtsi.so' in maps else 'LIBTSI_ABSENT')")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "LIBTSI_ABSENT" in r.stdout and "LIBTSI_LOADED" not in r.stdout
+
+
+def test_reference_params_equal_library_defaults():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from temporalsetinversion_b200 import api
+    a, b = bench.reference_params(localsubdiv=10, delta=0.01), api.default_params(localsubdiv=10, delta=0.01)
+    assert bytes(a) == bytes(b)

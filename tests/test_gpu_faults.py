@@ -51,6 +51,36 @@ def test_graph_replay_reports_pool_exhaustion(device):
 
 
 @pytest.mark.gpu
+def test_batch_wider_than_one_launch_reports_every_chunk():
+    """A batch of more scenes than one launch takes runs as consecutive
+    launch sequences; an exhausted pool in the FIRST chunk is still reported
+    (status and that request's error bits), and every other request's
+    counters are its own."""
+    with Device(max_scenes_per_launch=4) as dev:
+        tape = Tape.from_llvm_ir(dev, scenes.spheres16(0))
+        tiny = Scene(dev, tape, api.default_params(localsubdiv=7), voxel_capacity=64)
+        rest = [Scene(dev, tape, api.default_params(localsubdiv=5)) for _ in range(6)]
+        alone = Scene(dev, tape, api.default_params(localsubdiv=5))
+        want = alone.invert(0.0)
+        reqs = [(tiny, 0.0, float("nan"), None)] + [(s, 0.0, float("nan"), None) for s in rest]
+        with pytest.raises(N.TsiError) as e:
+            api.run_batch(dev, reqs)
+        assert e.value.status == 4  # TSI_ERR_OOM, from the first of two chunks
+        out = [N.Stats() for _ in reqs]
+        arr = (N.Request * len(reqs))()
+        for i, (sc, t, t0, _) in enumerate(reqs):
+            sc.reset()
+            arr[i].scene, arr[i].time, arr[i].t0_or_nan = sc.handle, t, t0
+            arr[i].stats = C.pointer(out[i])
+        assert dev.lib.tsi_batch_run(dev.handle, arr, len(reqs)) == 4
+        assert out[0].error_flags != 0
+        for st in out[1:]:
+            assert st.error_flags == 0
+            assert (st.cells_evaluated, st.cells_enqueued, st.voxels_live) == (
+                want.cells_evaluated, want.cells_enqueued, want.voxels_live)
+
+
+@pytest.mark.gpu
 def test_trace_async_rejects_mismatched_frame(device):
     tape = Tape.from_llvm_ir(device, scenes.spheres16(0))
     s = Scene(device, tape, api.default_params(localsubdiv=4))
