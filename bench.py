@@ -34,6 +34,8 @@ temporally reused frames, like one run of the animation.
   cpu_baseline: the CPU oracle (C++ restatement of compute.wgsl, OpenMP;
           tape lowered by the oracle's own ir.rs restatement) on a bounded
           sample of the same frames
+  cinematic: path-traced frames (two bounces, shadow rays, sky, 8 samples)
+          of the small configuration's scene at 640x360
   temporal: the reference's published comparison, temporal set inversion
           against full per-frame re-evaluation (tsi_scene_reset each frame)
   served : open-loop Poisson requests through the continuous server at
@@ -381,6 +383,43 @@ def temporal_leg(local: int) -> dict:
                 "cells_ratio": out["reset"]["cells_evaluated"] / max(1, out["carried"]["cells_evaluated"]),
                 "note": "headline animation (256 primitives, localsubdiv 10, delta 0.01); reset = the octree "
                         "rebuilt from the root every frame; device ms per frame"}
+    finally:
+        dev.close()
+
+
+# ------------------------------------------------------------------ cinematic leg
+CINEMATIC = dict(localsubdiv=8, width=640, height=360, samples=8, frames=10)
+
+
+def cinematic_leg(local: int) -> dict:
+    """Path-traced frames (tsi_params.cinematic: two bounces, sun and shadow
+    rays, sky, 8 samples per pixel, finite-difference normals) of the small
+    plain configuration's scene (16 moving spheres, localsubdiv 8,
+    640x360): device ms of the trace per frame and rays per second (primary,
+    bounce and shadow rays counted as traced: at most 4 per sample)."""
+    from temporalsetinversion_b200 import Device, Scene, Tape, _native as N, api, scenes
+    cfg = CINEMATIC
+    dev = Device(local)
+    try:
+        p = api.default_params(localsubdiv=cfg["localsubdiv"], pointsample=0, fast_normals=1, cinematic=1,
+                               samples=cfg["samples"], see_background=1)
+        s = Scene(dev, Tape.from_llvm_ir(dev, scenes.spheres16(0)), p)
+        view = scenes.camera_look_at((0.3, 0.6, 2.5))
+        ms = []
+        for i in range(cfg["frames"] + 2):
+            t = i / 60.0
+            s.invert(t)
+            ts = N.Stats()
+            u = api.make_uniforms(view, (cfg["width"], cfg["height"]), t)
+            N.check(dev.lib.tsi_scene_trace(s.handle, C.byref(u), None, C.byref(ts)), "tsi_scene_trace")
+            if i >= 2:
+                ms.append(ts.device_ms)
+        mean = sum(ms) / len(ms)
+        px = cfg["width"] * cfg["height"]
+        return {"trace_ms_per_frame": mean, "frames_per_s": 1000.0 / mean,
+                "primary_rays_per_s": px * cfg["samples"] / (mean / 1000.0),
+                "config": "16 spheres, localsubdiv 8, %dx%d, %d samples, fast normals" % (
+                    cfg["width"], cfg["height"], cfg["samples"])}
     finally:
         dev.close()
 
@@ -1020,6 +1059,11 @@ def run_gpu(args, rank, world, local, dist) -> None:
             line["cpu_baseline"] = {"value": None, "unit": "frames/s", "cores": 0, "kind": "port",
                                     "sample": "unavailable: %s" % e}
     dev.close()
+    if world == 1 and not args.no_cinematic:
+        try:
+            line["cinematic"] = cinematic_leg(local)
+        except Exception as e:
+            line["cinematic"] = {"unavailable": str(e)}
     if world == 1 and not args.no_temporal:
         try:
             line["temporal"] = temporal_leg(local)
@@ -1066,6 +1110,7 @@ def main() -> None:
     ap.add_argument("--no-swept", action="store_true", help="skip the swept-volume leg")
     ap.add_argument("--no-split", action="store_true", help="skip the root-split leg")
     ap.add_argument("--no-temporal", action="store_true", help="skip the temporal-reuse comparison leg")
+    ap.add_argument("--no-cinematic", action="store_true", help="skip the path-tracing leg")
     ap.add_argument("--small-arenas", action="store_true",
                     help="small work-item, tape and log arenas (use with --voxels 4194304 under a profiler)")
     args = ap.parse_args()

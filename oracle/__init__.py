@@ -67,12 +67,14 @@ def load() -> C.CDLL:
         lib.oracle_scene_voxels_live.restype = u64
         lib.oracle_scene_voxels_live.argtypes = [vp]
         lib.oracle_scene_trace.argtypes = [vp, vp, fp, fp, fp, u32, u32, C.POINTER(u64)]
-        for name in ("oracle_sin", "oracle_exp", "oracle_log"):
+        for name in ("oracle_sin", "oracle_exp", "oracle_log", "oracle_cos", "oracle_acos", "oracle_linear_to_srgb"):
             getattr(lib, name).restype = f32
             getattr(lib, name).argtypes = [f32]
         for name in ("oracle_atan2", "oracle_fmin", "oracle_fmax"):
             getattr(lib, name).restype = f32
             getattr(lib, name).argtypes = [f32, f32]
+        lib.oracle_frand_seq.argtypes = [u32, u32, fp]
+        lib.oracle_sunsky.argtypes = [fp, f32, f32, fp]
         lib.oracle_powi.restype = f32
         lib.oracle_powi.argtypes = [f32, C.c_int]
         lib.oracle_num_threads.restype = C.c_int
@@ -139,6 +141,22 @@ class Scene:
             self.lib.oracle_scene_destroy(self.h)
         except Exception:
             pass
+
+
+def frand_seq(seed: int, n: int) -> np.ndarray:
+    """frand, frand0to1, frand, ... (compute.wgsl:2451-2472) from one seed."""
+    lib = load()
+    out = np.zeros(n, np.float32)
+    lib.oracle_frand_seq(C.c_uint32(seed), C.c_uint32(n), _fp(out))
+    return out
+
+
+def sunsky(view, sun) -> np.ndarray:
+    lib = load()
+    v = np.asarray(view, np.float32)
+    out = np.zeros(3, np.float32)
+    lib.oracle_sunsky(_fp(v), C.c_float(sun[0]), C.c_float(sun[1]), _fp(out))
+    return out
 
 
 def set_threads(n: int) -> None:

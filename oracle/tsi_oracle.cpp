@@ -20,6 +20,8 @@
  *   root seeding           src/main.rs:749-766, compute.wgsl:4690-4708
  *   ray tracer             src/compute.wgsl:4059-4107, 4189-4403
  *   camera + shading       src/compute.wgsl:4590-4594, 4620-4688
+ *   cinematic path tracing src/compute.wgsl:4429-4523 (bounces, shadow rays),
+ *                          2451-2472 (frand), 497-677 (sky), 4600-4607 (sRGB)
  *
  * It consumes the tape in the reference's own 32-byte GPUInstruction layout
  * (src/ir.rs:88-97) and decodes it per instruction exactly as the shader
@@ -982,6 +984,191 @@ V3 primary_ray(const Camera &cam, const Uniforms &u, uint32_t px, uint32_t py) {
   return g;
 }
 
+/* ---------------- cinematic path tracing ----------------
+   rt_main with `cinematic` on (compute.wgsl:3499): per pixel, `samples`
+   jittered rays (get_color_supersample 4620-4648), each a two-bounce path
+   (get_color_single 4444-4523): at a hit the path continues in a
+   cosine-power lobe around the normal (getSampleBiased 4429-4438), and a
+   shadow ray towards a jittered sun direction adds sun light and a specular
+   highlight when it escapes; a path that escapes sees the sky (sunsky
+   520-677).  Random numbers: the PCG hash of frand / frand0to1
+   (2451-2472) on the per-pixel seed of rt_main (4664). */
+inline uint32_t pcg_word(uint32_t s) {
+  uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+  return (w >> 22u) ^ w;
+}
+inline float frand(uint32_t &seed) { /* -1 to 1 */
+  seed = seed * 747796405u + 1u;
+  return ((float)pcg_word(seed) / 4294967295.0f) * 2.0f - 1.0f;
+}
+inline float frand0to1(uint32_t &seed) {
+  seed = seed * 747796405u + 1u;
+  return (float)pcg_word(seed) / 4294967295.0f;
+}
+inline float dot3(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline V3 normalize3(V3 a) {
+  const float l = len3(a);
+  return v3(a.x / l, a.y / l, a.z / l);
+}
+inline V3 cross3(V3 a, V3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+inline float clampf(float x, float lo, float hi) { return of_min(of_max(x, lo), hi); }
+inline V3 exp3(V3 a) { return v3(of_exp(a.x), of_exp(a.y), of_exp(a.z)); }
+inline V3 pow3(V3 a, V3 b) { return v3(of_powf(a.x, b.x), of_powf(a.y, b.y), of_powf(a.z, b.z)); }
+
+V3 from_spherical(float px, float py) { /* 497-518 */
+  return v3(of_cos(px) * of_sin(py), of_sin(px) * of_sin(py), of_cos(py));
+}
+
+V3 ortho(V3 v) { /* 4405-4427 */
+  if (fabsf(v.x) > fabsf(v.z)) return v3(-v.y, v.x, 0.0f);
+  return v3(0.0f, -v.z, v.y);
+}
+
+V3 sample_biased(V3 d, float power, uint32_t &seed) { /* getSampleBiased 4429-4438 */
+  const V3 dir = normalize3(d);
+  const V3 o1 = normalize3(ortho(dir));
+  const V3 o2 = normalize3(cross3(dir, o1));
+  float rx = frand0to1(seed);
+  float ry = frand0to1(seed);
+  rx = (rx * 2.0f) * PI_F;
+  ry = of_powf(ry, 1.0f / (power + 1.0f));
+  const float oneminus = sqrtf(1.0f - ry * ry);
+  return add(add(muls(o1, of_cos(rx) * oneminus), muls(o2, of_sin(rx) * oneminus)), muls(dir, ry));
+}
+
+/* sunsky (520-677) with turbidity 1, sunSize 1, sky sun intensity 1000 (the
+   private globals of 421-427); it returns 0.01 * sky (the sun disk term is
+   computed there but not added).  pow with the constant exponent 2.0 is
+   x * x, the rewrite shader compilers apply (Mesa's NIR among them); it is
+   defined for the negative cosines between view and sun, where the
+   exp(2 log x) form has no value. */
+V3 sunsky(V3 view, float spx, float spy) {
+  const float pi = 3.1415927410125732f;
+  const float sun_cos = of_cos((1.0f * pi) / 180.0f);
+  const V3 sun_dir = normalize3(from_spherical((spx - 0.0f) * 6.28000020980835f, (spy - 0.5f) * 3.140000104904175f));
+  const float cos_view_sun = dot3(view, sun_dir);
+  const float cos_sun_up = dot3(sun_dir, v3(0.0f, 0.0f, 1.0f));
+  const float cos_up_view = dot3(v3(0.0f, 0.0f, 1.0f), view);
+  if (sun_cos == 1.0f) return v3(1.0f, 0.0f, 0.0f);
+  /* SunIntensity 482-495 */
+  const float sunE = 1000.0f * of_max(0.0f, 1.0f - of_exp(-((1.6110731611233942f - of_acos(cos_sun_up)) / 1.5f)));
+  const V3 rayleigh = v3(5.176821105123963e-6f, 1.2785348189936485e-5f, 2.8530756026157178e-5f);
+  /* totalMie 438-456, T = 1 */
+  const float c = (0.20000000298023224f * 1.0f) * 9.99999983775159e-18f;
+  const V3 lambda = v3(6.800000278417428e-7f, 5.499999815583578e-7f, 4.4999998749517545e-7f);
+  const V3 K = v3(0.6859999895095825f, 0.6779999732971191f, 0.6660000085830688f);
+  const float two_pi = 2.0f * 3.1415927410125732f;
+  const V3 q = divv(v3(two_pi, two_pi, two_pi), lambda); /* pow(q, vec3(4.0 - 2.0)) = q * q */
+  const V3 tm = mul(muls(mul(q, q), (0.4339999854564667f * c) * 3.1415927410125732f), K);
+  const V3 mie = muls(tm, 0.004999999888241291f);
+  const float zenith = of_max(0.0f, cos_up_view);
+  const float r_len = 8400.0f / zenith, m_len = 1250.0f / zenith;
+  const V3 fex = exp3(v3(-(rayleigh.x * r_len + mie.x * m_len), -(rayleigh.y * r_len + mie.y * m_len),
+                         -(rayleigh.z * r_len + mie.z * m_len)));
+  /* RayleighPhase 429-436, hgPhase 458-480 */
+  const float rphase = (3.0f / (16.0f * 3.1415927410125732f)) * (1.0f + (cos_view_sun * cos_view_sun));
+  const float g = 0.800000011920929f;
+  const float hg = (1.0f / (4.0f * 3.1415927410125732f)) *
+                   ((1.0f - (g * g)) / of_powf((1.0f - (2.0f * g) * cos_view_sun) + (g * g), 1.5f));
+  const V3 r_eye = muls(rayleigh, rphase), m_eye = muls(mie, hg);
+  const V3 total = add(rayleigh, mie), light = add(r_eye, m_eye);
+  const V3 se = muls(divv(light, total), sunE);
+  V3 sky = mul(se, sub(v3(1.0f, 1.0f, 1.0f), fex));
+  const float t = clampf(of_powf(1.0f - dot3(v3(0.0f, 0.0f, 1.0f), sun_dir), 5.0f), 0.0f, 1.0f);
+  const V3 pw = pow3(mul(se, fex), v3(0.5f, 0.5f, 0.5f));
+  /* mix(1, pw, t) = 1 (1 - t) + pw t */
+  const V3 mx = v3(1.0f * (1.0f - t) + pw.x * t, 1.0f * (1.0f - t) + pw.y * t, 1.0f * (1.0f - t) + pw.z * t);
+  sky = mul(sky, mx);
+  return muls(sky, 0.009999999776482582f);
+}
+
+struct CineOut {
+  float r, g, b, a;
+};
+
+/* get_color_single, cinematic (4444-4523) */
+CineOut color_single(const Scene &S, V3 ro, V3 rd, float time, uint32_t &seed, float *d0, V3 *n0) {
+  V3 frm = ro, dir = rd;
+  V3 lum = v3(1.0f, 1.0f, 1.0f), direct = v3(0.0f, 0.0f, 0.0f);
+  float spx = -0.1f, spy = 0.7f, sun_int = 3.0f, spec_int = 1.0f, albedo = 1.0f, sunsize = 0.01f, bg = 1.0f;
+  if (S.p.scene_id == 3) {
+    spx = 0.36f;
+    spy = 0.72f;
+    spec_int = 1.0f;
+    sunsize = 0.1f;
+    albedo = 1.5f;
+    bg = 2.0f;
+    sun_int = 2.0f;
+  } else if (S.p.scene_id == 4) {
+    spx = -0.1f;
+    spy = 0.57f;
+    sunsize = 0.01f;
+  } else if (S.p.scene_id == 5) {
+    spx = 0.63f;
+    spy = 0.65f;
+    sunsize = 0.02f;
+  }
+  for (int i = 0; i < 2; ++i) {
+    TraceOut tr;
+    trace(S, frm, dir, time, tr);
+    if (i == 0) {
+      *d0 = tr.d;
+      *n0 = tr.n;
+    }
+    const V3 n = tr.n;
+    const V3 hitpoint = add(frm, muls(dir, tr.d));
+    if (tr.d >= 0.0f) {
+      const V3 old = dir;
+      dir = sample_biased(n, 3.0f, seed);
+      lum = muls(mul(lum, tr.c), albedo);
+      frm = add(hitpoint, muls(n, 0.05f));
+      const V3 sd = normalize3(from_spherical((spx - 0.0f) * 6.28f, (spy - 0.5f) * 3.14f));
+      const V3 sundir = v3(sd.x, sd.z, sd.y);
+      const float jx = frand(seed), jy = frand(seed), jz = frand(seed);
+      const V3 sample_dir = normalize3(add(sundir, muls(v3(jx, jy, jz), sunsize)));
+      const float sunlight = dot3(n, sample_dir);
+      TraceOut sh;
+      trace(S, frm, sample_dir, time, sh);
+      if (sunlight > 0.0f && sh.d < 0.0f) {
+        direct = add(direct, muls(muls(lum, sunlight), sun_int));
+        const V3 half = normalize3(add(v3(-old.x, -old.y, -old.z), sundir));
+        const float spec = (100.0f * of_powf(of_max(dot3(n, half), 0.0f), 30.0f)) * spec_int;
+        direct = add(direct, muls(lum, spec));
+      }
+    } else {
+      if (i == 0 && !S.p.see_background) return CineOut{10.0f, 10.0f, 10.0f, 0.0f};
+      const V3 sky = sunsky(v3(dir.x, dir.z, dir.y), spx, spy); /* getBackground 4440-4442 */
+      const V3 c = add(direct, mul(lum, sky));
+      return CineOut{c.x * bg, c.y * bg, c.z * bg, 1.0f * bg};
+    }
+  }
+  return CineOut{direct.x, direct.y, direct.z, 1.0f};
+}
+
+/* primary ray through the (possibly jittered) pixel position (px, py),
+   py already shifted for scene 0 (4590-4594, 4629-4631) */
+V3 primary_ray_at(const Camera &cam, const Uniforms &u, float pxf, float pyf) {
+  float xy0 = (pxf - (float)u.res[0] / 2.0f) + 0.5f;
+  float xy1 = (pyf - (float)u.res[1] / 2.0f) + 0.5f;
+  V3 d = v3(xy0, -xy1, -cam.zdist);
+  float l = len3(d);
+  d = v3(d.x / l, d.y / l, d.z / l);
+  V3 g;
+  g.x = ((cam.m[0] * d.x + cam.m[4] * d.y) + cam.m[8] * d.z) + cam.m[12] * 0.0f;
+  g.y = ((cam.m[1] * d.x + cam.m[5] * d.y) + cam.m[9] * d.z) + cam.m[13] * 0.0f;
+  g.z = ((cam.m[2] * d.x + cam.m[6] * d.y) + cam.m[10] * d.z) + cam.m[14] * 0.0f;
+  return g;
+}
+
+/* LinearToSRGB (4600-4607) of one channel */
+inline float linear_to_srgb(float x) {
+  const float rgb = clampf(x, 0.0f, 1.0f);
+  const float m = (rgb < 0.0031308f) ? 1.0f : 0.0f;
+  const float a = of_powf(rgb, 1.0f / 2.4f) * 1.055f - 0.055f;
+  const float b = rgb * 12.92f;
+  return a * (1.0f - m) + b * m;
+}
+
 }  // namespace
 
 /* ---------------- extern "C" API used by tests and bench ---------------- */
@@ -1097,6 +1284,60 @@ int oracle_scene_trace(void *s, const void *uniforms, float *rgba, float *depth,
   const uint32_t W = u.res[0], H = u.res[1];
   if (y1 > H) y1 = H;
   uint64_t vis = 0;
+  if (S->p.cinematic) { /* get_color_supersample 4620-4648 with cinematic on */
+    const int samples = S->p.samples > 0 ? S->p.samples : 1;
+    const uint32_t seed0 = (uint32_t)(12345.0f * (of_sin(u.time * 12345.0f) * 0.5f + 0.5f)); /* 4664 */
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long long yy = y0; yy < (long long)y1; ++yy) {
+      for (uint32_t x = 0; x < W; ++x) {
+        const uint64_t i = (uint64_t)yy * W + x;
+        uint32_t seed = (uint32_t)i + seed0;
+        float cr = 0.0f, cg = 0.0f, cb = 0.0f, ca = 0.0f, d0 = -1.0f;
+        V3 n0 = v3(0, 0, 0);
+        for (int smp = 0; smp < samples; ++smp) {
+          const float ox = frand(seed), oy = frand(seed);
+          const float pxf = (float)x + (ox * 1.0f) * 0.5f;
+          const float pyf = ((float)yy - cam.yshift) + (oy * 1.0f) * 0.5f;
+          const V3 rd = primary_ray_at(cam, u, pxf, pyf);
+          if (u.rendermode == 0.0f) {
+            float dd = -1.0f;
+            V3 nn = v3(0, 0, 0);
+            const CineOut o = color_single(*S, cam.eye, rd, u.time, seed, &dd, &nn);
+            cr = cr + o.r;
+            cg = cg + o.g;
+            cb = cb + o.b;
+            ca = ca + o.a;
+            if (smp == 0) {
+              d0 = dd;
+              n0 = nn;
+            }
+          }
+        }
+        const float fs = (float)samples;
+        cr = cr / fs;
+        cg = cg / fs;
+        cb = cb / fs;
+        ca = ca / fs;
+        cr = linear_to_srgb(cr);
+        cg = linear_to_srgb(cg);
+        cb = linear_to_srgb(cb);
+        if (rgba) {
+          rgba[i * 4 + 0] = of_powf(cr, 0.45f);
+          rgba[i * 4 + 1] = of_powf(cg, 0.45f);
+          rgba[i * 4 + 2] = of_powf(cb, 0.45f);
+          rgba[i * 4 + 3] = ca;
+        }
+        if (depth) depth[i] = d0;
+        if (normal) {
+          normal[i * 3 + 0] = n0.x;
+          normal[i * 3 + 1] = n0.y;
+          normal[i * 3 + 2] = n0.z;
+        }
+      }
+    }
+    if (visits) *visits = 0;
+    return 0;
+  }
 #pragma omp parallel for schedule(dynamic, 4) reduction(+ : vis)
   for (long long yy = y0; yy < (long long)y1; ++yy) {
     for (uint32_t x = 0; x < W; ++x) {
@@ -1138,6 +1379,20 @@ int oracle_scene_trace(void *s, const void *uniforms, float *rgba, float *depth,
   if (visits) *visits = vis;
   return 0;
 }
+
+/* cinematic pieces under test: the frand sequence, the sky, sRGB */
+void oracle_frand_seq(uint32_t seed, uint32_t n, float *out) {
+  for (uint32_t i = 0; i < n; ++i) out[i] = (i & 1u) ? frand0to1(seed) : frand(seed);
+}
+void oracle_sunsky(const float *view, float spx, float spy, float *out) {
+  const V3 s = sunsky(v3(view[0], view[1], view[2]), spx, spy);
+  out[0] = s.x;
+  out[1] = s.y;
+  out[2] = s.z;
+}
+float oracle_linear_to_srgb(float x) { return linear_to_srgb(x); }
+float oracle_cos(float x) { return of_cos(x); }
+float oracle_acos(float x) { return of_acos(x); }
 
 /* f32 math under test */
 float oracle_sin(float x) { return of_sin(x); }

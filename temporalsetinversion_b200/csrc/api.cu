@@ -596,6 +596,10 @@ tsi_status fill_trace(tsi_scene *s, const tsi_uniforms *u) {
   T.normal = s->d_normal;
   T.visits = c->d_visits;
   T.swept = s->p.swept_volume ? 1u : 0u;
+  T.cinematic = s->p.cinematic ? 1u : 0u;
+  T.samples = s->p.samples > 0 ? (uint32_t)s->p.samples : 1u;
+  T.see_background = s->p.see_background ? 1u : 0u;
+  T.scene_id = s->p.scene_id;
   if (s->p.fast_normals) {  // normals by finite differences of the full tape
     if (s->tape->nregs > 96u)
       return set_err(TSI_ERR_TAPE_TOO_WIDE, "fast normals need a tape of at most 96 interval registers");

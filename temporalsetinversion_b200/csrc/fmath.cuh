@@ -14,6 +14,10 @@
 //   atan2: octant reduction; atan(a) = pi/4 + atan((a-1)/(a+1)) above
 //          tan(pi/8); Taylor series of atan to degree 17
 //   powi : binary exponentiation (POW_II only uses integer exponents)
+//   cos  : fm_sin's reduction and polynomials, quadrant shifted by one
+//   acos : atan2(sqrt((1 - x)(1 + x)), x) (the cinematic sky model)
+//   pow  : exp(y log x) for x > 0; 0 or 1 at x = 0; NaN for x < 0 (the
+//          exp2(y log2 x) convention of GPU drivers for negative x)
 // Error bounds used by the directed-rounding mode are in interval.cuh.
 #pragma once
 #include <stdint.h>
@@ -66,6 +70,38 @@ TSI_DEV float fm_sin(float x) {
     case 1: return c;
     case 2: return -s;
     default: return -c;
+  }
+}
+
+TSI_DEV float fm_cos(float x) {
+  if (!(fabsf(x) <= 3.0e38f)) return fm_sub(x, x);
+  const float two_over_pi = 0.6366197466850281f;
+  const float p1 = 1.5703125f, p2 = 0.0004838705062866211f, p3 = -4.371138828673793e-08f;
+  float k = rintf(fm_mul(x, two_over_pi));
+  float r = fm_sub(x, fm_mul(k, p1));
+  r = fm_sub(r, fm_mul(k, p2));
+  r = fm_sub(r, fm_mul(k, p3));
+  float qf = fm_sub(k, fm_mul(4.0f, floorf(fm_mul(k, 0.25f))));
+  int q = (int)qf;
+  float r2 = fm_mul(r, r);
+  float ps = -2.5052107943679403e-08f;
+  ps = fm_add(2.7557318844628753e-06f, fm_mul(r2, ps));
+  ps = fm_add(-0.00019841270113829523f, fm_mul(r2, ps));
+  ps = fm_add(0.008333333767950535f, fm_mul(r2, ps));
+  ps = fm_add(-0.1666666716337204f, fm_mul(r2, ps));
+  float s = fm_add(r, fm_mul(r, fm_mul(r2, ps)));
+  float pc = 2.0876755879584152e-09f;
+  pc = fm_add(-2.755731998149713e-07f, fm_mul(r2, pc));
+  pc = fm_add(2.4801587642286904e-05f, fm_mul(r2, pc));
+  pc = fm_add(-0.0013888889225199819f, fm_mul(r2, pc));
+  pc = fm_add(0.0416666679084301f, fm_mul(r2, pc));
+  pc = fm_add(-0.5f, fm_mul(r2, pc));
+  float c = fm_add(1.0f, fm_mul(r2, pc));
+  switch (q) {
+    case 0: return c;
+    case 1: return -s;
+    case 2: return -c;
+    default: return s;
   }
 }
 
@@ -184,5 +220,7 @@ TSI_DEV float fm_powf(float x, float y) {
   if (x < 0.0f) return fm_nan();
   return fm_exp(fm_mul(y, fm_log(x)));
 }
+
+TSI_DEV float fm_acos(float x) { return fm_atan2(__fsqrt_rn(fm_mul(fm_sub(1.0f, x), fm_add(1.0f, x))), x); }
 
 }  // namespace tsi

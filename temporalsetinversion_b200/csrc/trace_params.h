@@ -23,6 +23,10 @@ struct TraceParams {
   const uint2 *code;
   uint32_t len, nregs, out_reg;
   uint32_t swept;
+  // cinematic path tracing (compute.wgsl:3499, 3506-3507): samples per
+  // pixel, primary misses see the sky, the scene's sun and material
+  uint32_t cinematic, samples, see_background;
+  int32_t scene_id;
   float4 *rgba;
   float *depth;
   float *normal;      // 3 floats per pixel

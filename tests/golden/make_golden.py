@@ -78,6 +78,9 @@ def oracle_cases():
         ("csg24_L6_lip", ("gen", scenes.csg(24, 3)), dict(localsubdiv=6, lipschitz_corrected=1, pointsample=1),
          [0.0, 0.05, 0.1, 0.15]),
         ("swept8_L5", ("gen", scenes.swept(8, 4)), dict(localsubdiv=5, swept_volume=1), [0.25, 0.5, 0.75]),
+        # cinematic path tracing (two bounces, shadow rays, sky) with tape normals
+        ("spheres16_L6_cinematic", ("gen", scenes.spheres16(0)),
+         dict(localsubdiv=6, pointsample=0, cinematic=1, fast_normals=1, samples=2, see_background=1), [0.0, 1 / 60]),
     ]
     for name in SCENES:
         cases.append(("%s_L5" % name, ("tape", name), dict(localsubdiv=5), [0.0, 1 / 60]))
