@@ -344,7 +344,7 @@ def run_reference(args, rank, world, dist) -> None:
 
 
 # ------------------------------------------------------------------ temporal leg
-TEMPORAL = dict(frames=40, skip=4)
+TEMPORAL = dict(frames=40, skip=4, slow=10)
 
 
 def temporal_leg(local: int) -> dict:
@@ -352,37 +352,43 @@ def temporal_leg(local: int) -> dict:
     set inversion against full per-frame re-evaluation at delta 0.01.  The
     headline animation's frames inverted twice, on the carried-over octree
     and with tsi_scene_reset before every frame (the first_eval path); the
-    same frames' inversion (and inversion + 1080p trace) device times."""
+    same frames' inversion (and inversion + 1080p trace) device times.  Run
+    at the animation's own speed and at a tenth of it (frame times i/1190
+    instead of i/119), where less of the surface moves between frames."""
     from temporalsetinversion_b200 import Device, Scene, Tape, _native as N, api
     text, params, view = build_workload(WORKLOAD["seed"])
     W, H, F = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["frames"]
     dev = Device(local)
     try:
         scene = Scene(dev, Tape.from_llvm_ir(dev, text), params, voxel_capacity=64 << 20)
-        out = {}
-        for mode in ("carried", "reset"):
-            scene.reset()
-            inv, tr, cells = 0.0, 0.0, 0
-            for i in range(TEMPORAL["frames"]):
-                t = frame_time(i, F)
-                if mode == "reset":
-                    scene.reset()
-                st = scene.invert(t)
-                ts = N.Stats()
-                u = api.make_uniforms(view, (W, H), t)
-                N.check(dev.lib.tsi_scene_trace(scene.handle, C.byref(u), None, C.byref(ts)), "tsi_scene_trace")
-                if i >= TEMPORAL["skip"]:
-                    inv += st.device_ms
-                    tr += ts.device_ms
-                    cells += st.cells_evaluated
-            n = TEMPORAL["frames"] - TEMPORAL["skip"]
-            out[mode] = {"invert_ms": inv / n, "frame_ms": (inv + tr) / n, "cells_evaluated": cells // n}
-        return {"frames": "%d..%d" % (TEMPORAL["skip"], TEMPORAL["frames"] - 1), **out,
-                "invert_speedup": out["reset"]["invert_ms"] / out["carried"]["invert_ms"],
-                "frame_speedup": out["reset"]["frame_ms"] / out["carried"]["frame_ms"],
-                "cells_ratio": out["reset"]["cells_evaluated"] / max(1, out["carried"]["cells_evaluated"]),
+        res = {}
+        for speed, div in (("animation", 1), ("slow", TEMPORAL["slow"])):
+            out = {}
+            for mode in ("carried", "reset"):
+                scene.reset()
+                inv, tr, cells = 0.0, 0.0, 0
+                for i in range(TEMPORAL["frames"]):
+                    t = frame_time(i, F) / div
+                    if mode == "reset":
+                        scene.reset()
+                    st = scene.invert(t)
+                    ts = N.Stats()
+                    u = api.make_uniforms(view, (W, H), t)
+                    N.check(dev.lib.tsi_scene_trace(scene.handle, C.byref(u), None, C.byref(ts)), "tsi_scene_trace")
+                    if i >= TEMPORAL["skip"]:
+                        inv += st.device_ms
+                        tr += ts.device_ms
+                        cells += st.cells_evaluated
+                n = TEMPORAL["frames"] - TEMPORAL["skip"]
+                out[mode] = {"invert_ms": inv / n, "frame_ms": (inv + tr) / n, "cells_evaluated": cells // n}
+            out["invert_speedup"] = out["reset"]["invert_ms"] / out["carried"]["invert_ms"]
+            out["frame_speedup"] = out["reset"]["frame_ms"] / out["carried"]["frame_ms"]
+            out["cells_ratio"] = out["reset"]["cells_evaluated"] / max(1, out["carried"]["cells_evaluated"])
+            res[speed] = out
+        return {"frames": "%d..%d" % (TEMPORAL["skip"], TEMPORAL["frames"] - 1), **res,
                 "note": "headline animation (256 primitives, localsubdiv 10, delta 0.01); reset = the octree "
-                        "rebuilt from the root every frame; device ms per frame"}
+                        "rebuilt from the root every frame; device ms per frame; slow = the same animation at a "
+                        "tenth of its speed"}
     finally:
         dev.close()
 
@@ -750,14 +756,38 @@ def batched_leg(local: int) -> dict:
 SWEPT = dict(n_prims=64, seed=2, localsubdiv=9, substeps=64, deltas=(0.005, 0.01, 0.02), width=1280, height=720)
 
 
+def swept_false_empty(tape, cells, t0: float, t1: float, eps: float, rng, max_cells: int = 1500) -> dict:
+    """Cells evaluated in this frame and classified empty (f = +1), wider than
+    a leaf (leaves are point-sampled, not bounded), checked at float64
+    samples of their box (corners, centre, 8 random points) at 5 times of
+    [t0, t1]: a cell with f <= 0 at a sample is a false empty."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from point_eval import evaluate
+    w = np.maximum(cells["x"][:, 1] - cells["x"][:, 0], 0.0)
+    sel = cells[(cells["t"] == np.float32(t1)) & (cells["f"] == 1.0) & (w > eps)]
+    if len(sel) == 0:
+        return {"checked": 0, "false_empty": 0}
+    sel = sel[rng.choice(len(sel), min(len(sel), max_cells), replace=False)]
+    lo = np.stack([sel["x"][:, 0], sel["y"][:, 0], sel["z"][:, 0]], axis=1).astype(np.float64)
+    hi = np.stack([sel["x"][:, 1], sel["y"][:, 1], sel["z"][:, 1]], axis=1).astype(np.float64)
+    corners = np.array([[(k >> 0) & 1, (k >> 1) & 1, (k >> 2) & 1] for k in range(8)], np.float64)
+    u = np.concatenate([corners, [[0.5, 0.5, 0.5]], rng.uniform(size=(8, 3))], axis=0)
+    pts = lo[:, None, :] + u[None, :, :] * (hi - lo)[:, None, :]
+    bad = np.zeros(len(sel), bool)
+    for tt in np.linspace(t0, t1, 5):
+        f = evaluate(tape, pts[..., 0], pts[..., 1], pts[..., 2], np.float64(np.float32(tt)))
+        bad |= np.any(f <= 0.0, axis=1)
+    return {"checked": int(len(sel)), "false_empty": int(bad.sum())}
+
+
 def swept_leg(local: int) -> dict:
     """Temporal / swept-volume stress: 64 primitives rotating about random
     axes with an exp(-t) scale, swept volume on, [0, 1] in 64 sub-steps
     (frame k inverts over [k/64, (k+1)/64] and traces at 1280x720),
     localsubdiv 9, for each delta: device frames/s, cells evaluated and the
-    fraction of ambiguous cells carried over (reused) per frame."""
-    import ctypes as C
-
+    fraction of ambiguous cells carried over (reused) per frame; and the
+    false-empty rate against float64 samples, in round-to-nearest (the
+    reference's arithmetic) and in directed rounding."""
     from temporalsetinversion_b200 import Device, Scene, Tape, _native as N, api, scenes
 
     W, H, K = SWEPT["width"], SWEPT["height"], SWEPT["substeps"]
@@ -765,32 +795,47 @@ def swept_leg(local: int) -> dict:
     dev = Device(local)
     try:
         text = scenes.swept(SWEPT["n_prims"], SWEPT["seed"])
+        tape_np = api.IR.new(text).gpu_instructions
+        eps = 10.0 * 2.0 ** -SWEPT["localsubdiv"]
         out = []
         for delta in SWEPT["deltas"]:
-            p = api.default_params(localsubdiv=SWEPT["localsubdiv"], delta=delta, swept_volume=1)
-            s = Scene(dev, Tape.from_llvm_ir(dev, text), p, voxel_capacity=16 << 20)
-            thr = s.autotune([(k + 1) / K for k in range(3)], reps=1)["wide_threshold"]
-            ms, cells, reused, enq = 0.0, 0, 0, 0
-            for k in range(K):
-                t0, t1 = k / K, (k + 1) / K
-                st = s.invert(t1, t0)
-                u = api.make_uniforms(view, (W, H), t1)
-                ts = N.Stats()
-                N.check(dev.lib.tsi_scene_trace(s.handle, C.byref(u), None, C.byref(ts)), "tsi_scene_trace")
-                if k > 0:  # frame 0 builds the octree from scratch
-                    ms += st.device_ms + ts.device_ms
-                    cells += st.cells_evaluated
-                    reused += st.cells_reused
-                    enq += st.cells_enqueued
-            out.append({"delta": delta, "frames_per_s": (K - 1) / (ms / 1000.0), "wide_threshold": thr,
-                        "cells_evaluated_per_frame": cells / (K - 1),
-                        "reused_per_frame": reused / (K - 1),
-                        "reuse_fraction": reused / max(1, reused + enq)})
-            s.close()
+            row = {"delta": delta}
+            for mode, rounding in (("nearest", 0), ("directed", 1)):
+                p = api.default_params(localsubdiv=SWEPT["localsubdiv"], delta=delta, swept_volume=1,
+                                       rounding_mode=rounding)
+                s = Scene(dev, Tape.from_llvm_ir(dev, text), p, voxel_capacity=16 << 20)
+                thr = s.autotune([(k + 1) / K for k in range(3)], reps=1)["wide_threshold"] if rounding == 0 else None
+                rng = np.random.default_rng(int(delta * 1e4) + rounding)
+                ms, cells, reused, enq, checked, false_empty = 0.0, 0, 0, 0, 0, 0
+                for k in range(K):
+                    t0, t1 = k / K, (k + 1) / K
+                    st = s.invert(t1, t0)
+                    u = api.make_uniforms(view, (W, H), t1)
+                    ts = N.Stats()
+                    N.check(dev.lib.tsi_scene_trace(s.handle, C.byref(u), None, C.byref(ts)), "tsi_scene_trace")
+                    if k > 0:  # frame 0 builds the octree from scratch
+                        ms += st.device_ms + ts.device_ms
+                        cells += st.cells_evaluated
+                        reused += st.cells_reused
+                        enq += st.cells_enqueued
+                    if k % 8 == 7:  # every eighth sub-step: float64 samples of its empty cells
+                        fe = swept_false_empty(tape_np, s.cells(), t0, t1, eps, rng)
+                        checked += fe["checked"]
+                        false_empty += fe["false_empty"]
+                res = {"frames_per_s": (K - 1) / (ms / 1000.0), "cells_evaluated_per_frame": cells / (K - 1),
+                       "reused_per_frame": reused / (K - 1), "reuse_fraction": reused / max(1, reused + enq),
+                       "empty_cells_checked": checked, "false_empty": false_empty,
+                       "false_empty_rate": false_empty / max(1, checked)}
+                if thr is not None:
+                    res["wide_threshold"] = thr
+                row[mode] = res
+                s.close()
+            out.append(row)
         return {"workload": "swept64_L9_720p_64substeps", "runs": out,
                 "note": "reuse_fraction = ambiguous cells kept with their subtree / (kept + re-subdivided); "
-                        "false-empty rate: tests/test_gpu_rigour.py checks swept-volume empties against float64 "
-                        "samples in directed mode"}
+                        "false_empty: of the sampled empty cells (evaluated in the frame, wider than a leaf, at "
+                        "most 1500 per checked sub-step, every eighth sub-step) those with f <= 0 at a float64 "
+                        "sample of their box over the sub-step's time interval"}
     finally:
         dev.close()
 

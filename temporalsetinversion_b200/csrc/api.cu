@@ -859,10 +859,21 @@ TSI_API tsi_status tsi_create(const tsi_device_opts *opts, tsi_ctx **out) {
   c->hbm_budget = opts ? opts->hbm_budget_bytes : 0u;
   c->item_cap = (opts && opts->work_item_capacity) ? (uint32_t)opts->work_item_capacity : (4u << 20);
   c->dealloc_cap = c->item_cap * 2u;
-  c->rec_cap = c->item_cap * 2u;
+  // pruned records form a ring of a power-of-two size above the scene
+  // slots' root records (ring indices are masked, not divided)
+  {
+    uint32_t ring = 1u;
+    while (ring < c->item_cap * 2u && ring < (1u << 30)) ring <<= 1;
+    c->rec_cap = c->max_scenes + ring;
+  }
   // defaults sized for fused launches of many scenes (the pruned-tape arena
   // and the operand log of long narrow tapes fill per level and frame)
   c->code_cap = (opts && opts->tape_arena_words) ? opts->tape_arena_words : (256ull << 20);
+  {  // the code arena is a ring of a power-of-two size (rounded down)
+    uint64_t pw = 1;
+    while (pw * 2 <= c->code_cap) pw *= 2;
+    c->code_cap = pw;
+  }
   c->log_overflow_cap = (opts && opts->log_arena_bytes) ? opts->log_arena_bytes / 16 : ((4ull << 30) / 16);
   c->watchdog = (opts && opts->watchdog_iters) ? opts->watchdog_iters : (1u << 22);
   c->slice_len = 1024;

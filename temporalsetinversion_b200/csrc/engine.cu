@@ -131,6 +131,14 @@ tsi_status Engine::admit(const tsi_request &r, uint64_t ticket) {
   const auto it = std::find(planned_.begin(), planned_.end(), sc);
   const bool g = planned_global_[it - planned_.begin()] != 0;
   fill_launch(sc, i, r.time, r.t0_or_nan, g, h_desc_[i], h_rec_[i]);
+  // Under load the narrow path's throughput beats the wide path's latency:
+  // a request admitted while others run gets its tape's wide threshold
+  // scaled by the number of requests then running (x1 alone, x2 from 2,
+  // x4 from 4, x8 from 8).  Results never depend on the threshold.
+  const uint32_t running = (uint32_t)slots_.size() - nfree_;
+  const uint32_t scale = running >= 8 ? 8u : running >= 4 ? 4u : running >= 2 ? 2u : 1u;
+  uint32_t &ml = h_desc_[i].wide.min_len;
+  ml = (ml >= 0xffffffffu / scale) ? 0xffffffffu : ml * scale;
   Slot &s = slots_[i];
   s.busy = true;
   s.inverting = true;

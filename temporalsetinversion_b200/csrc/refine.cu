@@ -140,23 +140,33 @@ __device__ uint32_t alloc_brick(const SceneLaunch &S, uint32_t *error) {
   return b * 8u;
 }
 
-// Reserves n words of the code arena (a ring of code_cap words); returns the
-// word offset, or ~0 when the ring has no room left above the low-water mark
-// (the tape then stays unpruned).  A tape never wraps around the ring's end.
+__device__ __forceinline__ StepIdx step_idx(uint32_t step) {
+  StepIdx si;
+  si.cur = step & TSI_STEP_MASK;
+  si.next = (step + 1u) & TSI_STEP_MASK;
+  si.buf = step & 1u;
+  si.nbuf = (step + 1u) & 1u;
+  return si;
+}
+
+// Reserves n words of the code arena (a ring of code_cap words, a power of
+// two); returns the word offset, or ~0 when the ring has no room left above
+// the low-water mark (the tape then stays unpruned).  A tape never wraps
+// around the ring's end.
 __device__ __forceinline__ unsigned long long code_alloc(const LaunchParams &P, uint32_t n) {
   const unsigned long long c = atomicAdd(P.code_count, (unsigned long long)n);
   if (c + n > *P.code_low + P.code_cap) return ~0ull;
-  const unsigned long long off = c % P.code_cap;
+  const unsigned long long off = c & (P.code_cap - 1ull);
   return off + n <= P.code_cap ? off : ~0ull;
 }
 
-// Takes a tape record from the ring [rec_base, rec_cap); TSI_NONE when the
-// ring has no room left above the low-water mark.
+// Takes a tape record from the ring [rec_base, rec_cap) (a power-of-two
+// size); TSI_NONE when the ring has no room left above the low-water mark.
 __device__ __forceinline__ uint32_t rec_alloc(const LaunchParams &P) {
   const unsigned long long r = atomicAdd(P.rec_count, 1ull);
-  const unsigned long long ring = (unsigned long long)(P.rec_cap - P.rec_base);
+  const uint32_t ring = P.rec_cap - P.rec_base;
   if (r >= *P.rec_low + ring) return TSI_NONE;
-  return P.rec_base + (uint32_t)(r % ring);
+  return P.rec_base + ((uint32_t)r & (ring - 1u));
 }
 
 __device__ __forceinline__ void find_valid(const LaunchParams &P, uint32_t &rec, TapeRec &TR, float tl, float th) {
@@ -175,8 +185,9 @@ __device__ __forceinline__ void find_valid(const LaunchParams &P, uint32_t &rec,
 // (readers take min(count, capacity) entries); narrow-list overflow is
 // dropped and reported.
 __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint32_t scene, uint32_t rec,
-                              const StepIdx &si, uint32_t plevel, uint32_t E, const uint32_t *cells, bool wide,
+                              uint32_t step, uint32_t plevel, uint32_t E, const uint32_t *cells, bool wide,
                               unsigned long long *ws) {
+  const StepIdx si = step_idx(step);
   uint32_t rest = E;
   uint32_t *err = P.error + scene;
   if (wide) {
@@ -235,8 +246,9 @@ __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint3
 // the brick allocations proceed in parallel; the first wide-list slots go
 // to the lowest enqueued octants, as in push_children.
 __device__ __forceinline__ void push_children_warp(const LaunchParams &P, const SceneLaunch &S, uint32_t scene,
-                                                   uint32_t rec, const StepIdx &si, uint32_t plevel, uint32_t E,
+                                                   uint32_t rec, uint32_t step, uint32_t plevel, uint32_t E,
                                                    uint32_t base, bool wide, unsigned long long *ws, uint32_t lane) {
+  const StepIdx si = step_idx(step);
   uint32_t rest = E;
   if (wide && E) {
     uint32_t pos = 0;
@@ -272,7 +284,7 @@ __device__ __forceinline__ void push_children_warp(const LaunchParams &P, const 
   if (lane == 0 && rest) {
     uint32_t cells[8];
     for (int q = 0; q < 8; ++q) cells[q] = base + q;
-    push_children(P, S, scene, rec, si, plevel, rest, cells, false, ws);
+    push_children(P, S, scene, rec, step, plevel, rest, cells, false, ws);
   }
 }
 
@@ -287,9 +299,10 @@ __device__ __forceinline__ float warp_max(float v) {
 
 // scratch for one item: operand log + decisions, in the warp's slice or the
 // shared overflow arena (long tapes)
-__device__ __forceinline__ bool item_scratch(const LaunchParams &P, const StepIdx &si, uint32_t scene, uint32_t len,
+__device__ __forceinline__ bool item_scratch(const LaunchParams &P, uint32_t step, uint32_t scene, uint32_t len,
                                              uint32_t lane, float4 *slice_log, uint2 *slice_dec, float4 *&lg,
                                              uint2 *&dg) {
+  const StepIdx si = step_idx(step);
   if (len <= P.slice_len) {
     lg = slice_log;
     dg = slice_dec;
@@ -309,9 +322,10 @@ __device__ __forceinline__ bool item_scratch(const LaunchParams &P, const StepId
 }
 
 template <bool D>
-__device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem &it, const StepIdx &si,
+__device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem &it, uint32_t step,
                                           uint32_t rf_off, float4 *slice_log, uint2 *slice_dec,
                                           unsigned long long *ws) {
+  const StepIdx si = step_idx(step);
   float2 *rf = reinterpret_cast<float2 *>(tsi_dyn_smem) + rf_off;  // this warp's register file
   using A = IA<D>;
   const uint32_t lane = threadIdx.x & 31u;
@@ -418,7 +432,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
       if (any_deriv || want_prune) {
         float4 *lgs = nullptr;
         uint2 *dgs = nullptr;
-        if (!item_scratch(P, si, it.scene, TR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
+        if (!item_scratch(P, step, it.scene, TR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
         lg = lgs;
         dg = want_prune ? dgs : nullptr;
       }
@@ -582,7 +596,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
       if (want_prune && WR.len < S.wide.min_len) {
         float4 *lgs;
         uint2 *dgs;
-        if (!item_scratch(P, si, it.scene, PR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
+        if (!item_scratch(P, step, it.scene, PR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
         lg = lgs;
         dg = dgs;
         const Iv tw = enq ? Iv{nl, nh} : targ;
@@ -666,7 +680,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     for (int b2 = 0; b2 < 8; ++b2) cb[b2] = __shfl_sync(FULL_MASK, C, gl0 + b2);
     const uint32_t next_len = (new_rec == prec) ? PR.len : ((new_rec == rec) ? TR.len : cnt);
     if (k == 0 && E != 0)
-      push_children(P, S, it.scene, new_rec, si, it.level, E, cb, next_len >= S.wide.min_len, ws);
+      push_children(P, S, it.scene, new_rec, step, it.level, E, cb, next_len >= S.wide.min_len, ws);
   }
 
   // ---- counters
@@ -690,7 +704,8 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
 
 // Recursive free of a dropped subtree (compute.wgsl:3533-3543, freeV
 // 3452-3460): 8 lanes per brick; children bricks go to the next level's list.
-__device__ void dealloc_brick(const LaunchParams &P, uint2 item, const StepIdx &si, bool valid) {
+__device__ void dealloc_brick(const LaunchParams &P, uint2 item, uint32_t step, bool valid) {
+  const StepIdx si = step_idx(step);
   const uint32_t lane = threadIdx.x & 31u, k = lane & 7u;
   const SceneLaunch &S = P.scenes[valid ? item.x : 0];
   const VoxelPoolDev &pool = S.pool;
@@ -799,8 +814,9 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s
 // The last cell of a wide item to finish: prunes the full tape with the
 // branch decisions shared by all enqueued siblings and enqueues them.
 template <bool GM>
-__device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkItem &it, const StepIdx &si,
+__device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkItem &it, uint32_t step,
                                              uint32_t unit0, WideShared &sh, unsigned long long *ws) {
+  const StepIdx si = step_idx(step);
   unsigned char *cell = cell_base<GM>(P);
   const uint32_t tid = threadIdx.x;
   const SceneLaunch &S = P.scenes[it.scene];
@@ -1005,7 +1021,7 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
   const long long f2 = clock64();
   if (tid < 32u) {
     const uint32_t len = (new_rec == S.root_rec) ? root.len : sh.cnt;
-    push_children_warp(P, S, it.scene, new_rec, si, it.level, E, it.parent[1], len >= W.min_len, ws, tid);
+    push_children_warp(P, S, it.scene, new_rec, step, it.level, E, it.parent[1], len >= W.min_len, ws, tid);
   }
   if (tid == 0) {
     const long long f3 = clock64();
@@ -1017,7 +1033,8 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
 // One child cell (octant k) of a wide item.  unit = item * 8 + k.
 template <bool D, bool GM>
 __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, uint32_t k, uint32_t unit,
-                                          const StepIdx &si, WideShared &sh, unsigned long long *ws) {
+                                          uint32_t step, WideShared &sh, unsigned long long *ws) {
+  const StepIdx si = step_idx(step);
   unsigned char *cell = cell_base<GM>(P);  // the cell's working set
   using A = IA<D>;
   const uint32_t tid = threadIdx.x;
@@ -1286,7 +1303,7 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   __syncthreads();
   if (!sh.last) return;
   __threadfence();
-  finish_group<GM>(P, it, si, unit & ~7u, sh, ws);
+  finish_group<GM>(P, it, step, unit & ~7u, sh, ws);
 }
 
 // A warp's counters belong to the scene whose items it counted: they are
@@ -1357,11 +1374,11 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
       const SceneLaunch &S = P.scenes[sc];
       const bool directed = (S.flags & SF_DIRECTED) != 0;
       if (S.wide.global) {
-        if (directed) process_cell<true, true>(P, itp, u & 7u, u, si, sh, s_stats[0]);
-        else process_cell<false, true>(P, itp, u & 7u, u, si, sh, s_stats[0]);
+        if (directed) process_cell<true, true>(P, itp, u & 7u, u, step, sh, s_stats[0]);
+        else process_cell<false, true>(P, itp, u & 7u, u, step, sh, s_stats[0]);
       } else {
-        if (directed) process_cell<true, false>(P, itp, u & 7u, u, si, sh, s_stats[0]);
-        else process_cell<false, false>(P, itp, u & 7u, u, si, sh, s_stats[0]);
+        if (directed) process_cell<true, false>(P, itp, u & 7u, u, step, sh, s_stats[0]);
+        else process_cell<false, false>(P, itp, u & 7u, u, step, sh, s_stats[0]);
       }
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -1384,8 +1401,8 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
       const WorkItem &it = items[idx];
       take(it.scene);
       const long long c0 = clock64();
-      if (P.scenes[it.scene].flags & SF_DIRECTED) process_item<true>(P, it, si, rf_off, slice_log, slice_dec, ws);
-      else process_item<false>(P, it, si, rf_off, slice_log, slice_dec, ws);
+      if (P.scenes[it.scene].flags & SF_DIRECTED) process_item<true>(P, it, step, rf_off, slice_log, slice_dec, ws);
+      else process_item<false>(P, it, step, rf_off, slice_log, slice_dec, ws);
       __syncwarp();
       if (lane == 0) {
         const unsigned long long c = (unsigned long long)(clock64() - c0);
@@ -1414,7 +1431,7 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
     const uint32_t j = idx + (lane >> 3);
     const bool valid = j < n_dealloc;
     const uint2 item = valid ? dl[j] : make_uint2(0u, 0u);
-    dealloc_brick(P, item, si, valid);
+    dealloc_brick(P, item, step, valid);
   }
   if (wscene != TSI_NONE) flush_stats(P, ws, wscene, si.cur, lane);
 }
@@ -1422,7 +1439,8 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
 // buf_main's enqueue(0) (compute.wgsl:4706) for scene s: its root as a work
 // item of the step (a wide item, with the root's children brick, when the
 // root tape is long enough).
-__device__ void seed_root(const LaunchParams &P, uint32_t s, const StepIdx &si) {
+__device__ void seed_root(const LaunchParams &P, uint32_t s, uint32_t step) {
+  const StepIdx si = step_idx(step);
   WorkItem w;
   w.scene = s;
   w.rec = P.scenes[s].root_rec;
@@ -1479,12 +1497,7 @@ __global__ void frame_begin_kernel(const __grid_constant__ LaunchParams P) {
     *P.code_low = 0;
   }
   __syncthreads();
-  StepIdx si0;
-  si0.cur = 0;
-  si0.next = 1;
-  si0.buf = 0;
-  si0.nbuf = 1;
-  for (uint32_t s = t; s < P.n_scenes; s += blockDim.x) seed_root(P, s, si0);
+  for (uint32_t s = t; s < P.n_scenes; s += blockDim.x) seed_root(P, s, 0u);
 }
 
 // Start of one step of the continuous form: record the arena counters at the
@@ -1510,7 +1523,7 @@ __global__ void step_begin_kernel(const __grid_constant__ LaunchParams P, uint32
   for (uint32_t i = t; i < n * ST_COUNT; i += blockDim.x) P.stats[(size_t)sd.slot[i / ST_COUNT] * ST_COUNT + i % ST_COUNT] = 0;
   for (uint32_t i = t; i < n; i += blockDim.x) P.error[sd.slot[i]] = 0;
   __syncthreads();
-  for (uint32_t i = t; i < n; i += blockDim.x) seed_root(P, sd.slot[i], si);
+  for (uint32_t i = t; i < n; i += blockDim.x) seed_root(P, sd.slot[i], step);
 }
 
 // Per frame end of scenes first .. first + gridDim.x - 1: bricks freed during

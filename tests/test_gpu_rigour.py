@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 from carried_ref import carried_excursions
+from golden.make_golden import load_tape
 from point_eval import evaluate
 from temporalsetinversion_b200 import Scene, Tape, api, scenes
 
@@ -56,6 +57,42 @@ def test_directed_octree_is_rigorous(device, case):
                 case, t, len(bad), sign, tuple(int(sel[bad[0]][k]) for k in ("level", "ix", "iy", "iz")))
             checked += len(sel)
     assert checked > 100
+
+
+# the benchmark's 256-primitive tape (4697 slots) and the reference's `cables`
+# scene (sin, cos, exp, atan2): a bounded random subset of each frame's
+# classified cells is sampled
+BIG_CASES = {
+    "csg256_L8": (lambda: api.IR.new(scenes.csg(256, 1)).gpu_instructions, 8),
+    "cables_L7": (lambda: load_tape("cables"), 7),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", sorted(BIG_CASES))
+def test_directed_octree_is_rigorous_at_scale(device, case):
+    make, levels = BIG_CASES[case]
+    tape = make()
+    p = api.default_params(localsubdiv=levels, pointsample=0, rounding_mode=1)
+    s = Scene(device, Tape.upload(device, tape), p)
+    rng = np.random.default_rng(17)
+    checked = 0
+    for t in (0.0, 0.05, 0.1):
+        s.invert(t)
+        cells = s.cells()
+        now = cells[(cells["t"] == np.float32(t)) & (cells["f"] != 0)]
+        for sign in (1.0, -1.0):
+            sel = now[now["f"] == sign]
+            if len(sel) == 0:
+                continue
+            sel = sel[rng.choice(len(sel), min(len(sel), 1500), replace=False)]
+            pts = _samples(sel, rng, n_random=8)
+            f = evaluate(tape, pts[..., 0], pts[..., 1], pts[..., 2], np.float64(np.float32(t)))
+            bad = np.nonzero(np.any(sign * f <= -1e-9, axis=1))[0]
+            assert len(bad) == 0, "%s t=%g: %d cells classified %+d contain f of the other sign, e.g. key %s" % (
+                case, t, len(bad), sign, tuple(int(sel[bad[0]][k]) for k in ("level", "ix", "iy", "iz")))
+            checked += len(sel)
+    assert checked > 500, checked
 
 
 @pytest.mark.gpu
