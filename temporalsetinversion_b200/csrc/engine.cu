@@ -184,7 +184,7 @@ tsi_status Engine::step() {
   sd.oldest = (uint32_t)oldest;
   LaunchParams P = make_params(c_, (uint32_t)slots_.size(), plan_.smem, false);
   P.level_stats = nullptr;
-  ECK(tsi::launch_step_begin(P, (uint32_t)s, sd, c_->stream));
+  if (sd.n) ECK(tsi::launch_step_begin(P, (uint32_t)s, sd, c_->stream));
   ECK(tsi::launch_refine(P, (uint32_t)s, plan_.rcap, plan_.grid, kBlock, plan_.smem, c_->stream));
   const cudaEvent_t done = step_ev_[s % kStepRing];
   ECK(cudaEventRecord(done, c_->stream));

@@ -1306,6 +1306,17 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   finish_group<GM>(P, it, step, unit & ~7u, sh, ws);
 }
 
+// Clears the lists and counters of ring entry c.
+__device__ __forceinline__ void clear_step(const LaunchParams &P, uint32_t c) {
+  P.item_count[c] = 0;
+  P.item_cursor[c] = 0;
+  P.witem_count[c] = 0;
+  P.witem_cursor[c] = 0;
+  P.dealloc_count[c] = 0;
+  P.dealloc_cursor[c] = 0;
+  P.log_overflow_used[c] = 0;
+}
+
 // A warp's counters belong to the scene whose items it counted: they are
 // added to that scene's stats row (and the launch's level row) when the warp
 // moves on to another scene's item and at the end of the launch.
@@ -1340,6 +1351,9 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
   si.nbuf = (step + 1u) & 1u;
   __shared__ unsigned long long s_stats[kWarps][ST_COUNT];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  // the lists of the step after next start empty (no launch of this step
+  // touches them; the next step fills them)
+  if (blockIdx.x == 0 && threadIdx.x == 0) clear_step(P, (step + 2u) & TSI_STEP_MASK);
   const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
   const uint32_t rf_off = wib * rcap * 32u;  // this warp's register file in tsi_dyn_smem (float2 units)
   float4 *slice_log = P.log_slices + (size_t)gw * P.slice_len * 32u;
@@ -1474,15 +1488,6 @@ __device__ void seed_root(const LaunchParams &P, uint32_t s, uint32_t step) {
   else atomicOr(P.error + s, EB_QUEUE_FULL);
 }
 
-__device__ __forceinline__ void clear_step(const LaunchParams &P, uint32_t c) {
-  P.item_count[c] = 0;
-  P.item_cursor[c] = 0;
-  P.witem_count[c] = 0;
-  P.witem_cursor[c] = 0;
-  P.dealloc_count[c] = 0;
-  P.dealloc_cursor[c] = 0;
-  P.log_overflow_used[c] = 0;
-}
 
 // Per frame of the plain and batched forms (steps 0, 1, ... are the levels):
 // clear every step's lists and the tape arenas, seed the root of every scene
@@ -1500,10 +1505,11 @@ __global__ void frame_begin_kernel(const __grid_constant__ LaunchParams P) {
   for (uint32_t s = t; s < P.n_scenes; s += blockDim.x) seed_root(P, s, 0u);
 }
 
-// Start of one step of the continuous form: record the arena counters at the
-// step's start, move the low-water marks to the oldest running slot's first
-// step, clear the next step's lists, clear the stats rows and error words of
-// the slots that join at this step and seed their roots.
+// Start of a step of the continuous form at which slots join: record the
+// arena counters at the step's start, move the low-water marks to the oldest
+// running slot's first step (always a step at which slots joined), clear
+// the stats rows and error words of the joining slots and seed their roots.
+// (Each refinement launch clears the lists of the step after its next.)
 __global__ void step_begin_kernel(const __grid_constant__ LaunchParams P, uint32_t step,
                                   const __grid_constant__ StepSeeds sd) {
   StepIdx si;

@@ -2,7 +2,8 @@
 rigour tests of the directed-rounding mode: the value of f(x, y, z, t) that
 the tape's instructions define, evaluated at many points at once with
 numpy.  Operand order and op_top follow ir.rs:141-171; ATAN2 takes its
-operands swapped (compute.wgsl:2724), MOD is floor-mod (2819)."""
+operands swapped (compute.wgsl:2724: ATAN2_II(x = larg, y = rarg), so the
+value is atan2(rarg, larg)), MOD is floor-mod (2819)."""
 from __future__ import annotations
 
 import numpy as np
@@ -43,7 +44,7 @@ def evaluate(tape: np.ndarray, x, y, z, t) -> np.ndarray:
             elif op == FLOOR: v = np.floor(a)
             elif op == RET: v = a
             elif op == MOD: v = a - b * np.floor(a / b)
-            elif op == ATAN2: v = np.arctan2(a, b)
+            elif op == ATAN2: v = np.arctan2(b, a)  # ATAN2_II(x = larg, y = rarg): atan2(rarg, larg)
             else:
                 raise ValueError("opcode %d not handled by the point evaluator" % op)
             vals.append(np.broadcast_to(v, x.shape).astype(np.float64))

@@ -8,14 +8,18 @@ import pytest
 
 import oracle
 from point_eval import evaluate
+from golden.make_golden import load_tape
 from temporalsetinversion_b200 import api, scenes
 
 
-@pytest.mark.parametrize("text", [scenes.spheres16(0), scenes.csg(24, 3, 0.9), scenes.swept(8, 4)],
-                         ids=["spheres16", "csg24", "swept8"])
-def test_point_eval_matches_oracle(text):
+@pytest.mark.parametrize("src", ["spheres16", "csg24", "swept8", "cables", "cradle", "piano", "sponza"])
+def test_point_eval_matches_oracle(src):
+    """Generated scenes and the reference's four scene tapes (cables has sin,
+    cos, exp and the operand-swapped atan2)."""
     oracle.build()
-    tape = api.IR.new(text).gpu_instructions
+    gen = {"spheres16": lambda: scenes.spheres16(0), "csg24": lambda: scenes.csg(24, 3, 0.9),
+           "swept8": lambda: scenes.swept(8, 4)}
+    tape = api.IR.new(gen[src]()).gpu_instructions if src in gen else load_tape(src)
     rng = np.random.default_rng(5)
     pts = rng.uniform(-1.2, 1.2, (256, 4)).astype(np.float32)
     pts[:, 3] = rng.uniform(0, 1, 256).astype(np.float32)
