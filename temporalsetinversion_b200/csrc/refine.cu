@@ -874,7 +874,7 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
       auto fetch = [&](int kk) -> uint4 {
         if (kk < 0) return zero4;
         const uint2 b = bt_tab[kk];
-        return tid < (b.y & 0xffffu) ? slots[ns + b.x + tid] : zero4;
+        return tid < b.y ? slots[ns + b.x + tid] : zero4;
       };
       if (tid == 0) flags[W.nvalues - 1u] = 1;
       int kb = (int)W.nbundles - 1;
@@ -885,9 +885,9 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
         const uint4 s1 = q0;
         q0 = q1;
         q1 = fetch(kb - 2);
-        if (tid < (bt.y & 0xffffu) && flags[s1.x]) {
+        if (tid < bt.y && flags[s1.x]) {
           bool la = s1.z != TSI_NONE, lb = s1.w != TSI_NONE;
-          if (TSI_H_IS_MINMAX(bt.y >> 16)) {
+          if (s1.y != TSI_NONE) {  // a min/max: its ordinal
             const uint32_t d = (cb[s1.y >> 4] >> (2u * (s1.y & 15u))) & 3u;
             if (d & 1u) lb = false;
             else if (d & 2u) la = false;

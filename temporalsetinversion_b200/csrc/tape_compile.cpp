@@ -2,6 +2,8 @@
 #include "tape_compile.h"
 
 #include <algorithm>
+#include <set>
+#include <utility>
 #include <cstring>
 
 #include "opcost.h"
@@ -210,58 +212,71 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
       ++ncontrib;
     }
   }
-  // List scheduling, one handler per bundle: the block executes a bundle
-  // with one thread per slot, so a bundle of one handler runs without
-  // divergence.  Each bundle takes the handler with the most instructions
-  // ready (the oldest ready instruction's on a tie), oldest first.
-  const uint32_t width = WideTape::kWidth;
-  std::vector<int32_t> bundle_of(n, -1);
-  for (uint32_t a = 0; a < 4; ++a) bundle_of[a] = -2;  // arguments: before everything
-  std::vector<std::vector<uint32_t>> bundles;
-  std::vector<uint32_t> pending;
-  pending.reserve(n - 4);
-  for (uint32_t j = 4; j < n; ++j) pending.push_back(j);
-  std::vector<uint32_t> ready_count(64, 0);
-  while (!pending.empty()) {
-    const int32_t k = int32_t(bundles.size());
-    auto ready = [&](uint32_t j) {
-      return (opa[j] == TSI_NONE || (bundle_of[opa[j]] != -1 && bundle_of[opa[j]] < k)) &&
-             (opb[j] == TSI_NONE || (bundle_of[opb[j]] != -1 && bundle_of[opb[j]] < k));
-    };
-    std::fill(ready_count.begin(), ready_count.end(), 0u);
-    uint32_t hsel = 64, best = 0;
-    for (uint32_t j : pending) {
-      if (!ready(j)) continue;
-      const uint32_t c = ++ready_count[handler(j)];
-      if (c > best) {
-        best = c;
-        hsel = handler(j);
+  // List scheduling into bundles of warp groups: a bundle is one block step,
+  // at most 8 groups of at most 32 mutually independent instructions, each
+  // group of one handler (so a warp runs its group without divergence and
+  // groups of different handlers share a step).  Priority is the longest
+  // chain from the instruction to the field; a step repeatedly takes the 32
+  // highest-priority ready instructions of the handler whose best ready
+  // instruction has the highest priority (the oldest instruction on a tie).
+  // Users of a step's instructions become ready at the next step.
+  const uint32_t groups_per_bundle = WideTape::kWidth / 32u;
+  std::vector<uint32_t> prio(n, 0);
+  for (uint32_t j = n; j-- > 4;) {
+    uint32_t p = 0;
+    for (uint32_t u : users[j]) p = std::max(p, prio[u]);
+    prio[j] = p + 1u;
+  }
+  std::vector<uint32_t> indeg(n, 0);
+  for (uint32_t j = 4; j < n; ++j) {
+    if (opa[j] != TSI_NONE && opa[j] >= 4) ++indeg[j];
+    if (opb[j] != TSI_NONE && opb[j] >= 4 && opb[j] != opa[j]) ++indeg[j];
+  }
+  using Key = std::pair<uint32_t, uint32_t>;  // (~priority, instruction): highest priority, then oldest, first
+  std::vector<std::set<Key>> ready(64);
+  for (uint32_t j = 4; j < n; ++j)
+    if (indeg[j] == 0) ready[handler(j)].insert(Key(~prio[j], j));
+  std::vector<std::vector<std::vector<uint32_t>>> bundles;  // bundle -> groups -> instructions
+  uint32_t scheduled = 0;
+  std::vector<uint32_t> next;
+  while (scheduled < n - 4) {
+    std::vector<std::vector<uint32_t>> groups;
+    while (groups.size() < groups_per_bundle) {
+      uint32_t hb = 64;
+      for (uint32_t h = 0; h < 64; ++h)
+        if (!ready[h].empty() && (hb == 64 || *ready[h].begin() < *ready[hb].begin())) hb = h;
+      if (hb == 64) break;
+      std::vector<uint32_t> g;
+      while (g.size() < 32u && !ready[hb].empty()) {
+        g.push_back(ready[hb].begin()->second);
+        ready[hb].erase(ready[hb].begin());
       }
-      if (c == width) break;
+      groups.push_back(std::move(g));
     }
-    std::vector<uint32_t> b, rest;
-    rest.reserve(pending.size());
-    for (uint32_t j : pending) {
-      if (b.size() < width && handler(j) == hsel && ready(j)) {
-        b.push_back(j);
-        bundle_of[j] = k;
-      } else {
-        rest.push_back(j);
-      }
-    }
-    if (b.empty()) {
+    if (groups.empty()) {
       status = TSI_ERR_INVALID_ARGUMENT;
       why = "bundle scheduling made no progress";
       return false;
     }
-    bundles.push_back(b);
-    pending.swap(rest);
+    next.clear();
+    for (const auto &g : groups)
+      for (uint32_t j : g) {
+        ++scheduled;
+        for (uint32_t u : users[j])
+          if (--indeg[u] == 0) next.push_back(u);
+      }
+    for (uint32_t u : next) ready[handler(u)].insert(Key(~prio[u], u));
+    bundles.push_back(std::move(groups));
   }
   const uint32_t nb = uint32_t(bundles.size());
-  const uint32_t nslots = n - 4;
+  // slots: a bundle's groups at 32-slot strides (lane = slot - first - 32 x
+  // group); the lanes a group leaves free are padding slots (handler
+  // TSI_H_PAD, no operands, no records)
+  uint32_t nslots = 0;
+  for (const auto &bg : bundles) nslots += 32u * uint32_t(bg.size() - 1) + uint32_t(bg.back().size());
   out.slots.assign(size_t(nslots) * 12, 0);
   out.bundles.assign(size_t(nb) * 2, 0);
-  out.narrow_mm.assign(nslots, TSI_NONE);
+  out.narrow_mm.assign(n - 4, TSI_NONE);
   {
     uint32_t mm = 0;
     for (uint32_t j = 4; j < n; ++j) {
@@ -271,12 +286,19 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
   }
   uint32_t off = 0;
   for (uint32_t k = 0; k < nb; ++k) {
-    const std::vector<uint32_t> &b = bundles[k];
-    for (size_t s = 0; s < b.size(); ++s) {
-      const uint32_t j = b[s];
+    const auto &bg = bundles[k];
+    const uint32_t count = 32u * uint32_t(bg.size() - 1) + uint32_t(bg.back().size());
+    for (uint32_t s = 0; s < count; ++s) {
+      uint32_t *S = &out.slots[size_t(off + s) * 12];
+      const auto &g = bg[s / 32u];
+      if (s % 32u >= g.size()) {  // padding
+        S[0] = TSI_H_PAD;
+        S[5] = S[6] = S[7] = S[8] = S[9] = S[10] = TSI_NONE;
+        continue;
+      }
+      const uint32_t j = g[s % 32u];
       const uint32_t w0 = narrow.code[2 * (j - 4)], w1 = narrow.code[2 * (j - 4) + 1];
       const uint32_t h = TSI_W0_H(w0);
-      uint32_t *S = &out.slots[size_t(off + s) * 12];
       S[0] = h | (TSI_W0_FA(w0) << 6) | (TSI_W0_FB(w0) << 7) | (j << 8);
       // the min/max ordinal sits in the word the handler does not use: the
       // literal's for two registers, B's for a register and a literal
@@ -294,8 +316,8 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
       S[11] = gbase[j] == TSI_NONE ? 0u : uint32_t(users[j].size());
     }
     out.bundles[2 * k] = off;
-    out.bundles[2 * k + 1] = uint32_t(b.size()) | (TSI_W0_H(narrow.code[2 * (b[0] - 4)]) << 16);
-    off += uint32_t(b.size());
+    out.bundles[2 * k + 1] = count;
+    off += count;
   }
   for (uint32_t a = 0; a < 4; ++a) {
     out.arg_gbase[a] = gbase[a];

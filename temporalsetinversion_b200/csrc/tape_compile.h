@@ -21,15 +21,20 @@ struct PackedTape {
 };
 
 // Bundled ("wide") form of a full tape, for evaluating one cell with a whole
-// block: instructions are list-scheduled into bundles of at most kWidth
-// mutually independent instructions of one handler (one per thread).  Every
-// SSA value keeps its own slot (no register reuse), so the reverse pass
-// reads operands where the forward pass left them.  Per slot (3 x uint4):
+// block: instructions are list-scheduled into bundles (block steps) of at
+// most kWidth / 32 groups of at most 32 mutually independent instructions,
+// one handler per group, so every warp runs its group without divergence
+// while groups of different handlers share a step.  A group fills the 32
+// slots of its warp; lanes it leaves free hold padding slots (handler
+// TSI_H_PAD).  Every SSA value keeps its own slot (no register reuse), so
+// the reverse pass reads operands where the forward pass left them.  Per
+// slot (3 x uint4):
 //   s0.x  handler | single-use A << 6 | single-use B << 7 | dst SSA << 8
 //   s0.y  A SSA (0 if absent)
 //   s0.z  B SSA; for a register-literal min/max its min/max ordinal
 //   s0.w  f32 literal; for a two-register min/max its min/max ordinal
-//   s1    dst SSA, min/max ordinal, A SSA, B SSA (TSI_NONE if absent)
+//   s1    dst SSA, min/max ordinal (TSI_NONE unless a min/max), A SSA, B SSA
+//         (TSI_NONE if absent; a padding slot: 0, TSI_NONE, TSI_NONE, TSI_NONE)
 //   s2    contribution record of A, of B (TSI_NONE: the operand has one
 //         user, which writes its sensitivity directly); first record and
 //         record count of dst (count 0: dst has at most one user)
@@ -40,7 +45,7 @@ struct PackedTape {
 struct WideTape {
   static constexpr uint32_t kWidth = 256;  // threads of the evaluating block
   std::vector<uint32_t> slots;    // 12 words per slot
-  std::vector<uint32_t> bundles;  // 2 words per bundle: first slot, count | handler << 16
+  std::vector<uint32_t> bundles;  // 2 words per bundle: first slot, slot count (padding included)
   std::vector<uint32_t> narrow_mm;  // per narrow instruction: min/max ordinal or TSI_NONE
   uint32_t arg_gbase[4] = {TSI_NONE, TSI_NONE, TSI_NONE, TSI_NONE};  // records of x, y, z, t
   uint32_t arg_gcount[4] = {0, 0, 0, 0};

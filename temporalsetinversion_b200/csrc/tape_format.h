@@ -47,4 +47,6 @@ enum tsi_handler {
 #define TSI_H_IS_II(h) ((h) >= H_ADD_II && (h) <= H_BAD_II)
 #define TSI_H_IS_FI(h) ((h) >= H_SUB_FI && (h) <= H_BAD_FI)
 #define TSI_H_HAS_A(h) ((h) != H_CONST)
+// Handler field of a padding slot of the bundled (wide) tape: no operation.
+#define TSI_H_PAD 63u
 #define TSI_H_IS_MINMAX(h) ((h) == H_MIN_II || (h) == H_MAX_II || (h) == H_MIN_IF || (h) == H_MAX_IF)

@@ -1,10 +1,11 @@
-"""The bundled (wide) tape form, checked on the host: every slot scheduled
-once, after its operands, at most 256 slots and one handler per bundle
-(one block executes a bundle, one thread per slot), every value in its own
-SSA slot, and contribution records that let a value with several users sum
-its sensitivity in reverse program order (the order of the sequential
-reverse pass, which fixes the rounding) wherever its users were scheduled.
-No device needed."""
+"""The bundled (wide) tape form, checked on the host: every instruction
+scheduled once, after its operands; at most 256 slots per bundle (one block
+executes a bundle, one thread per slot) in groups of 32 slots (one warp
+each) of one handler, the lanes a group leaves free holding padding slots;
+every value in its own SSA slot; and contribution records that let a value
+with several users sum its sensitivity in reverse program order (the order
+of the sequential reverse pass, which fixes the rounding) wherever its users
+were scheduled.  No device needed."""
 from __future__ import annotations
 
 import ctypes as C
@@ -24,13 +25,18 @@ def wide(tape: np.ndarray):
     ptr = arr.ctypes.data_as(C.POINTER(N.GPUInstruction))
     info, nb = N.TapeInfo(), C.c_uint32(0)
     N.check(lib.tsi_compile_wide_gpu_instructions(ptr, len(arr), None, 0, None, 0, C.byref(info), C.byref(nb)), "wide")
-    n_slots = len(arr) - 4
-    slots = np.zeros(n_slots * 12, np.uint32)
     bundles = np.zeros(nb.value * 2, np.uint32)
+    N.check(lib.tsi_compile_wide_gpu_instructions(ptr, len(arr), None, 0, bundles.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                  len(bundles), C.byref(info), C.byref(nb)), "wide")
+    n_slots = int(bundles[-2]) + int(bundles[-1])  # padding slots included
+    slots = np.zeros(n_slots * 12, np.uint32)
     N.check(lib.tsi_compile_wide_gpu_instructions(
         ptr, len(arr), slots.ctypes.data_as(C.POINTER(C.c_uint32)), len(slots),
         bundles.ctypes.data_as(C.POINTER(C.c_uint32)), len(bundles), C.byref(info), C.byref(nb)), "wide")
     return slots.reshape(n_slots, 12), bundles.reshape(-1, 2), info
+
+
+PAD = 63
 
 
 CASES = {
@@ -51,19 +57,31 @@ def test_wide_schedule_invariants(case):
     assert info.registers == n  # one value slot per SSA value
     bundle_of = {a: -1 for a in range(4)}
     seen = np.zeros(n, bool)
-    for k, (first, word) in enumerate(bundles):
-        count, h = int(word) & 0xFFFF, int(word) >> 16
-        assert 1 <= count <= 256
+    next_first = 0
+    for k, (first, count) in enumerate(bundles):
+        first, count = int(first), int(count)
+        assert first == next_first and 1 <= count <= 256
+        next_first = first + count
         group = slots[first:first + count]
-        assert {int(s[0]) & 63 for s in group} == {h}, "bundle %d mixes handlers" % k
+        for w in range(0, count, 32):
+            warp = group[w:w + 32]
+            hs = {int(s[0]) & 63 for s in warp} - {PAD}
+            assert len(hs) == 1, "bundle %d warp %d mixes handlers %s" % (k, w // 32, hs)
+            live = [int(s[0]) & 63 != PAD for s in warp]
+            assert live[0] and live == sorted(live, reverse=True), "padding only after a group's slots"
         for s in group:
+            if int(s[0]) & 63 == PAD:
+                assert list(map(int, s[4:12])) == [0, NONE, NONE, NONE, NONE, NONE, NONE, 0]
+                continue
             j = int(s[4])
             assert int(s[0]) >> 8 == j
             assert not seen[j]
             seen[j] = True
             bundle_of[j] = k
+    assert next_first == len(slots)
     assert seen[4:].all()
     users, rec = {}, {}
+    slots = slots[(slots[:, 0] & 63) != PAD]
     for s in slots:
         j, a, b = int(s[4]), int(s[6]), int(s[7])
         h = int(s[0]) & 63
@@ -97,8 +115,10 @@ def test_wide_schedule_invariants(case):
     assert len(taken) == info.reserved  # contribution records per cell
 
 
-def test_wide_schedule_length_csg256():
-    """The csg256 tape (4693 instructions, dependency depth 31) packs into
-    a few dozen single-handler bundles of up to 256 slots."""
-    _, bundles, _ = wide(CASES["csg256"]())
-    assert len(bundles) <= 80
+@pytest.mark.parametrize("case,steps", [("csg256", 32), ("csg64", 29), ("cables", 44), ("spheres16", 27)])
+def test_wide_schedule_length(case, steps):
+    """Warp groups of different handlers share a step, so a tape takes about
+    as many bundle steps as its dependency depth (csg256: 4693 instructions
+    of depth 31 in 32 steps; cables: depth 44)."""
+    _, bundles, _ = wide(CASES[case]())
+    assert len(bundles) <= steps
