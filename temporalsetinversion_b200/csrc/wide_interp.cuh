@@ -28,12 +28,6 @@ __device__ __forceinline__ Iv ldv(const float2 *a, uint32_t i) {
 }
 __device__ __forceinline__ void stv(float2 *a, uint32_t i, Iv v) { a[i] = make_float2(v.lo, v.hi); }
 
-// The handlers with a body of their own in the bundle loops (the ones
-// op_forward and op_reverse_rule evaluate inline).
-#define TSI_WIDE_HOT(X)                                                                                         \
-  X(H_COPY) X(H_ADD_II) X(H_SUB_II) X(H_MUL_II) X(H_MIN_II) X(H_MAX_II) X(H_ADD_IF) X(H_SUB_IF) X(H_MUL_IF) \
-  X(H_MIN_IF) X(H_MAX_IF) X(H_SQR) X(H_SQRT) X(H_NEG) X(H_ABS) X(H_SUB_FI)
-
 // A thread's slot of bundle kk and the bundle's slot count, or a padding
 // slot past the bundle (or past the tape).
 struct WideFetch {
@@ -101,7 +95,7 @@ __device__ __forceinline__ Iv cell_forward(const WideDev &W, const uint2 *bt_tab
     switch (h) {
 #define TSI_X(HH) \
   case HH: fwd_slot<D, HH>(V, bits, sl); break;
-      TSI_WIDE_HOT(TSI_X)
+      TSI_HOT_HANDLERS(TSI_X)
 #undef TSI_X
       case TSI_H_PAD: break;
       case H_CONST: stv(V, sl.x >> 8, IA<D>::fix(iv(__uint_as_float(sl.w)))); break;
@@ -171,7 +165,7 @@ __device__ __forceinline__ Iv cell_forward2(const WideDev &W, const uint2 *bt_ta
     switch (h) {
 #define TSI_X(HH) \
   case HH: fwd2_slot<D, HH>(V, V2, bits, bits2, sl); break;
-      TSI_WIDE_HOT(TSI_X)
+      TSI_HOT_HANDLERS(TSI_X)
 #undef TSI_X
       case TSI_H_PAD: break;
       case H_CONST: {
@@ -270,7 +264,7 @@ __device__ __forceinline__ void cell_reverse(const WideDev &W, const uint2 *bt_t
     switch (h) {
 #define TSI_X(HH) \
   case HH: rev_slot_body<D>(HH, V, G, R, sl, s2); break;
-      TSI_WIDE_HOT(TSI_X)
+      TSI_HOT_HANDLERS(TSI_X)
 #undef TSI_X
       case TSI_H_PAD:
       case H_CONST: break;

@@ -95,3 +95,37 @@ def test_trace_async_matches_trace(device):
     a.trace_wait()
     for f in range(4):
         assert np.array_equal(bufs[f].numpy(), want[f])
+
+
+@pytest.mark.gpu
+def test_pipelined_frames_match_sequential(device):
+    """Inversions and traces queued back to back without waiting (frame i's
+    copy to host memory overlapping the inversion of frame i + 1) give the
+    frames of the sequential invert-then-trace loop: colour, depth and
+    normal."""
+    import torch
+
+    text = scenes.csg(64, 5, 0.85)
+    params = api.default_params(localsubdiv=7)
+    a = Scene(device, Tape.from_llvm_ir(device, text), params)
+    b = Scene(device, Tape.from_llvm_ir(device, text), params)
+    cam = scenes.camera_look_at((0.5, 0.9, 2.3))
+    res = (192, 108)
+    n = 8
+    pin = lambda c: torch.empty((res[1], res[0], c), dtype=torch.float32, pin_memory=True)
+    bufs = [(pin(4), pin(1), pin(3)) for _ in range(n)]
+    for f in range(n):
+        t = f / 30.0
+        a.invert_async(t)
+        a.trace_async(api.make_uniforms(cam, res, t), *(x.numpy() for x in bufs[f]))
+    a.invert_wait()
+    a.trace_wait()
+    for f in range(n):
+        t = f / 30.0
+        b.invert(t)
+        want = b.trace(api.make_uniforms(cam, res, t))
+        rgba, depth, normal = (x.numpy() for x in bufs[f])
+        assert np.array_equal(rgba, want["rgba"]), f
+        assert np.array_equal(depth.reshape(want["depth"].shape), want["depth"]), f
+        assert np.array_equal(normal.reshape(want["normal"].shape), want["normal"]), f
+
