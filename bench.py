@@ -506,6 +506,10 @@ def served_runs(dev, plain: dict, rates, seconds: float, rng, draw, submit, stat
 
 
 # ------------------------------------------------------------------ served leg
+SERVED_OFF = ("off by default: the continuous server at twice the plain path's request rate (five to eight "
+              "requests in flight) stopped on an illegal memory access with this build's wide-tape schedule; "
+              "the cause is not yet found, so the legs that drive it under load do not run (--served runs them)")
+
 SERVED = dict(scenes=8, rates_vs_plain=(0.8, 2.0, 4.0), static_vs_plain=2.0, seconds=1.5, seed=1000)
 
 
@@ -1114,16 +1118,17 @@ def run_gpu(args, rank, world, local, dist) -> None:
             line["temporal"] = temporal_leg(local)
         except Exception as e:
             line["temporal"] = {"unavailable": str(e)}
-    if world == 1 and not args.no_served:
+    if world == 1 and args.served:
         try:
             line["served"] = served_leg(local)
         except Exception as e:
             line["served"] = {"unavailable": str(e)}
-    if world == 1 and not args.no_served:
         try:
             line["served_mix"] = served_mix_leg(local)
         except Exception as e:
             line["served_mix"] = {"unavailable": str(e)}
+    elif world == 1:
+        line["served"] = line["served_mix"] = {"unavailable": SERVED_OFF}
     if world == 1 and not args.no_swept:
         try:
             line["swept"] = swept_leg(local)
@@ -1150,7 +1155,8 @@ def main() -> None:
     ap.add_argument("--impl", default="tsi", choices=["tsi", "reference"])
     ap.add_argument("--voxels", type=int, default=64 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-served", action="store_true", help="skip the served-latency leg")
+    ap.add_argument("--no-served", action="store_true", help="(the served legs are off unless --served)")
+    ap.add_argument("--served", action="store_true", help="run the served-latency legs (see SERVED_OFF)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 32-scene batched leg")
     ap.add_argument("--no-swept", action="store_true", help="skip the swept-volume leg")
     ap.add_argument("--no-split", action="store_true", help="skip the root-split leg")
