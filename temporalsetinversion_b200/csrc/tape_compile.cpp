@@ -221,6 +221,18 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
   // instruction has the highest priority (the oldest instruction on a tie).
   // Users of a step's instructions become ready at the next step.
   const uint32_t groups_per_bundle = WideTape::kWidth / 32u;
+  // the handlers the device evaluates inline (interp.cuh TSI_HOT_HANDLERS
+  // and constants); the others run out of line
+  auto inline_handler = [](uint32_t h) {
+    switch (h) {
+      case H_CONST: case H_COPY: case H_ADD_II: case H_SUB_II: case H_MUL_II: case H_MIN_II: case H_MAX_II:
+      case H_ADD_IF: case H_SUB_IF: case H_MUL_IF: case H_MIN_IF: case H_MAX_IF: case H_SQR: case H_SQRT:
+      case H_NEG: case H_ABS: case H_SUB_FI:
+        return true;
+      default:
+        return false;
+    }
+  };
   std::vector<uint32_t> prio(n, 0);
   for (uint32_t j = n; j-- > 4;) {
     uint32_t p = 0;
@@ -241,17 +253,36 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
   std::vector<uint32_t> next;
   while (scheduled < n - 4) {
     std::vector<std::vector<uint32_t>> groups;
+    // an out-of-line handler waits while it has slack (its best ready
+    // instruction is off the step's critical path) and inline work is ready,
+    // so that its instructions gather into few steps
+    uint32_t cp = 0;
+    bool inline_ready = false;
+    for (uint32_t h = 0; h < 64; ++h)
+      if (!ready[h].empty()) {
+        cp = std::max(cp, ~ready[h].begin()->first);
+        inline_ready = inline_ready || inline_handler(h);
+      }
+    auto eligible = [&](uint32_t h) {
+      return inline_handler(h) || !inline_ready || ~ready[h].begin()->first >= cp;
+    };
     while (groups.size() < groups_per_bundle) {
       uint32_t hb = 64;
       for (uint32_t h = 0; h < 64; ++h)
-        if (!ready[h].empty() && (hb == 64 || *ready[h].begin() < *ready[hb].begin())) hb = h;
+        if (!ready[h].empty() && eligible(h) && (hb == 64 || *ready[h].begin() < *ready[hb].begin())) hb = h;
       if (hb == 64) break;
-      std::vector<uint32_t> g;
-      while (g.size() < 32u && !ready[hb].empty()) {
-        g.push_back(ready[hb].begin()->second);
-        ready[hb].erase(ready[hb].begin());
-      }
-      groups.push_back(std::move(g));
+      // a group of an out-of-line handler (elementary functions, divisions:
+      // a step of them costs several steps of the others) takes every ready
+      // instruction of its handler into this step, so that such handlers
+      // occupy as few steps as possible
+      do {
+        std::vector<uint32_t> g;
+        while (g.size() < 32u && !ready[hb].empty()) {
+          g.push_back(ready[hb].begin()->second);
+          ready[hb].erase(ready[hb].begin());
+        }
+        groups.push_back(std::move(g));
+      } while (!inline_handler(hb) && !ready[hb].empty() && groups.size() < groups_per_bundle);
     }
     if (groups.empty()) {
       status = TSI_ERR_INVALID_ARGUMENT;
