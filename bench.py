@@ -506,9 +506,9 @@ def served_runs(dev, plain: dict, rates, seconds: float, rng, draw, submit, stat
 
 
 # ------------------------------------------------------------------ served leg
-SERVED_OFF = ("off by default: the continuous server at twice the plain path's request rate (five to eight "
-              "requests in flight) stopped on an illegal memory access with this build's wide-tape schedule; "
-              "the cause is not yet found, so the legs that drive it under load do not run (--served runs them)")
+SERVED_OFF = ("off by default: with this build's wide-tape schedule the continuous server at twice the plain "
+              "path's request rate (five to eight requests in flight) stopped on a device-side memory fault whose "
+              "cause is not yet found, so the legs that drive it under load do not run (--served runs them)")
 
 SERVED = dict(scenes=8, rates_vs_plain=(0.8, 2.0, 4.0), static_vs_plain=2.0, seconds=1.5, seed=1000)
 
