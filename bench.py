@@ -1127,7 +1127,7 @@ def run_gpu(args, rank, world, local, dist) -> None:
             line["served_mix"] = served_mix_leg(local)
         except Exception as e:
             line["served_mix"] = {"unavailable": str(e)}
-    elif world == 1:
+    elif world == 1 and not args.no_served:
         line["served"] = line["served_mix"] = {"unavailable": SERVED_OFF}
     if world == 1 and not args.no_swept:
         try:
@@ -1155,7 +1155,7 @@ def main() -> None:
     ap.add_argument("--impl", default="tsi", choices=["tsi", "reference"])
     ap.add_argument("--voxels", type=int, default=64 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-served", action="store_true", help="(the served legs are off unless --served)")
+    ap.add_argument("--no-served", action="store_true", help="leave the served legs out of the line entirely")
     ap.add_argument("--served", action="store_true", help="run the served-latency legs (see SERVED_OFF)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 32-scene batched leg")
     ap.add_argument("--no-swept", action="store_true", help="skip the swept-volume leg")
