@@ -302,6 +302,13 @@ TSI_API tsi_status tsi_scene_trace_wait(tsi_scene *scene);
  * ignore a new value. */
 TSI_API uint32_t tsi_tape_wide_threshold(const tsi_tape *tape);
 TSI_API tsi_status tsi_tape_set_wide_threshold(tsi_tape *tape, uint32_t min_len);
+// A second wide threshold for children at octree level `level` or deeper
+// (levels counted from the root's children at 0): deep levels hold many
+// cells, where the narrow path's throughput beats the wide path's latency.
+// level = 0xffffffff (the default) turns it off.  Results never depend on
+// the thresholds.
+TSI_API tsi_status tsi_tape_set_wide_threshold_deep(tsi_tape *tape, uint32_t level, uint32_t min_len);
+TSI_API tsi_status tsi_tape_wide_threshold_deep(const tsi_tape *tape, uint32_t *level, uint32_t *min_len);
 
 #define TSI_AUTOTUNE_MAX 16
 typedef struct tsi_autotune_result {
@@ -309,6 +316,8 @@ typedef struct tsi_autotune_result {
   uint32_t candidates;              /* thresholds tried (0: narrow-only tape) */
   uint32_t threshold[TSI_AUTOTUNE_MAX];
   float ms[TSI_AUTOTUNE_MAX];       /* best of `reps` runs over `times`, device ms */
+  uint32_t deep_level;              /* chosen deep-level threshold (tsi_tape_set_wide_threshold_deep); */
+  uint32_t deep_threshold;          /* deep_level 0xffffffff: none beat the single threshold */
 } tsi_autotune_result;
 /* Times the scene's inversion over the frames `times` (the first from a
  * reset octree, the rest carried over) for each candidate wide threshold,

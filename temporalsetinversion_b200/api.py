@@ -196,6 +196,20 @@ class Tape:
     def wide_threshold(self, v: int) -> None:
         N.check(self.device.lib.tsi_tape_set_wide_threshold(self.handle, int(v)), "tsi_tape_set_wide_threshold")
 
+    @property
+    def wide_threshold_deep(self) -> tuple:
+        """(level, threshold): child cells at that octree level or deeper use
+        the second threshold (level 0xffffffff: off)."""
+        lv, th = C.c_uint32(0), C.c_uint32(0)
+        N.check(self.device.lib.tsi_tape_wide_threshold_deep(self.handle, C.byref(lv), C.byref(th)),
+                "tsi_tape_wide_threshold_deep")
+        return int(lv.value), int(th.value)
+
+    @wide_threshold_deep.setter
+    def wide_threshold_deep(self, v: tuple) -> None:
+        N.check(self.device.lib.tsi_tape_set_wide_threshold_deep(self.handle, int(v[0]), int(v[1])),
+                "tsi_tape_set_wide_threshold_deep")
+
     def close(self) -> None:
         if getattr(self, "handle", None) and getattr(self.device, "handle", None):
             self.device.lib.tsi_tape_destroy(self.handle)
@@ -223,13 +237,15 @@ class Scene:
         N.check(self.device.lib.tsi_scene_reset(self.handle), "tsi_scene_reset")
 
     def autotune(self, times: list, reps: int = 2) -> dict:
-        """Picks the tape's wide threshold by timing inversions over
-        `times` (tsi_scene_autotune); the scene is left reset."""
+        """Picks the tape's wide threshold, then a deep-level one, by timing
+        inversions over `times` (tsi_scene_autotune); the scene is left
+        reset."""
         arr = (C.c_float * len(times))(*[float(t) for t in times])
         r = N.AutotuneResult()
         N.check(self.device.lib.tsi_scene_autotune(self.handle, arr, len(times), int(reps), C.byref(r)),
                 "tsi_scene_autotune")
-        return {"wide_threshold": int(r.wide_threshold),
+        return {"wide_threshold": int(r.wide_threshold), "deep_level": int(r.deep_level),
+                "deep_threshold": int(r.deep_threshold),
                 "trials": [(int(r.threshold[k]), float(r.ms[k])) for k in range(r.candidates)]}
 
     def invert(self, time: float, t0: float = math.nan) -> N.Stats:

@@ -191,6 +191,8 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, bool 
   L.wide.nbundles = s->tape->wbundles;
   L.wide.nvalues = s->tape->wvalues;
   L.wide.min_len = s->tape->wmin_len;
+  L.wide.deep_level = s->tape->wdeep_level;
+  L.wide.deep_min_len = s->tape->wdeep_min_len;
   L.wide.ncontrib = s->tape->wcontrib;
   L.wide.global = wide_global ? 1u : 0u;
   for (int q = 0; q < 4; ++q) {
@@ -1427,6 +1429,20 @@ TSI_API tsi_status tsi_tape_set_wide_threshold(tsi_tape *t, uint32_t min_len) {
   return TSI_OK;
 }
 
+TSI_API tsi_status tsi_tape_set_wide_threshold_deep(tsi_tape *t, uint32_t level, uint32_t min_len) {
+  if (!t) return set_err(TSI_ERR_INVALID_ARGUMENT, "null tape");
+  t->wdeep_level = level;
+  t->wdeep_min_len = min_len;
+  return TSI_OK;
+}
+
+TSI_API tsi_status tsi_tape_wide_threshold_deep(const tsi_tape *t, uint32_t *level, uint32_t *min_len) {
+  if (!t || !level || !min_len) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
+  *level = t->wdeep_level;
+  *min_len = t->wdeep_min_len;
+  return TSI_OK;
+}
+
 TSI_API tsi_status tsi_scene_autotune(tsi_scene *s, const float *times, uint32_t ntimes, uint32_t reps,
                                       tsi_autotune_result *out) {
   if (!s || !times || ntimes == 0 || !out) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
@@ -1480,6 +1496,48 @@ TSI_API tsi_status tsi_scene_autotune(tsi_scene *s, const float *times, uint32_t
   out->candidates = (uint32_t)cand.size();
   out->wide_threshold = pick;
   t->wmin_len = pick;
+  // then a higher threshold for the deepest levels, where many cells make
+  // the narrow path's throughput pay (kept only when it is faster)
+  const uint32_t keep_level = t->wdeep_level, keep_deep = t->wdeep_min_len;
+  uint32_t dl = 0xffffffffu, dm = 0xffffffffu;
+  const uint32_t levels = tree_levels(s->p);
+  if (pick != 0xffffffffu && levels >= 4) {
+    for (uint32_t back = 2; back <= 3; ++back)
+      for (uint32_t mul : {4u, 8u}) {
+        t->wdeep_level = levels - back;
+        t->wdeep_min_len = pick >= 0xffffffffu / mul ? 0xffffffffu : pick * mul;
+        float bk = INFINITY;
+        for (uint32_t r = 0; r < reps; ++r) {
+          tsi_status st = tsi_scene_reset(s);
+          float ms = 0.0f;
+          for (uint32_t i = 0; i < ntimes && st == TSI_OK; ++i) {
+            tsi_stats fs;
+            st = tsi_scene_invert(s, times[i], NAN, &fs);
+            ms += fs.device_ms;
+          }
+          if (st == TSI_ERR_QUEUE_FULL || st == TSI_ERR_OOM) {
+            bk = INFINITY;
+            break;
+          }
+          if (st != TSI_OK) {
+            t->wdeep_level = keep_level;
+            t->wdeep_min_len = keep_deep;
+            tsi_scene_reset(s);
+            return st;
+          }
+          bk = std::min(bk, ms);
+        }
+        if (bk < best * 0.99f) {
+          best = bk;
+          dl = t->wdeep_level;
+          dm = t->wdeep_min_len;
+        }
+      }
+  }
+  t->wdeep_level = dl;
+  t->wdeep_min_len = dm;
+  out->deep_level = dl;
+  out->deep_threshold = dm;
   return tsi_scene_reset(s);
 }
 
@@ -1835,13 +1893,14 @@ TSI_API tsi_status tsi_batch_autotune(tsi_ctx *c, const tsi_request *reqs, uint3
   CK(cudaSetDevice(c->device));
   // the distinct tapes with a bundled form, and their thresholds now
   std::vector<tsi_tape *> tapes;
-  std::vector<uint32_t> base;
+  std::vector<uint32_t> base, base_deep;
   for (uint32_t i = 0; i < n; ++i) {
     if (!reqs[i].scene || reqs[i].scene->ctx != c) return set_err(TSI_ERR_INVALID_ARGUMENT, "bad request scene");
     tsi_tape *t = const_cast<tsi_tape *>(reqs[i].scene->tape);
     if (t->d_wslots && std::find(tapes.begin(), tapes.end(), t) == tapes.end()) {
       tapes.push_back(t);
       base.push_back(t->wmin_len);
+      base_deep.push_back(t->wdeep_min_len);
     }
   }
   auto reset_all = [&]() -> tsi_status {
@@ -1852,8 +1911,10 @@ TSI_API tsi_status tsi_batch_autotune(tsi_ctx *c, const tsi_request *reqs, uint3
     return TSI_OK;
   };
   auto apply = [&](uint32_t scale) {
-    for (size_t q = 0; q < tapes.size(); ++q)
+    for (size_t q = 0; q < tapes.size(); ++q) {
       tapes[q]->wmin_len = base[q] >= 0xffffffffu / scale ? 0xffffffffu : base[q] * scale;
+      tapes[q]->wdeep_min_len = base_deep[q] >= 0xffffffffu / scale ? 0xffffffffu : base_deep[q] * scale;
+    }
   };
   const uint32_t scales[] = {1u, 2u, 4u, 8u};
   const uint32_t ncand = tapes.empty() ? 1u : 4u;

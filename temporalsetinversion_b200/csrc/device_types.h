@@ -76,6 +76,8 @@ struct WideDev {
   uint32_t nbundles;
   uint32_t nvalues;           // SSA values (nslots + 4); the field is the last
   uint32_t min_len;           // tapes at least this long go to the wide path
+  uint32_t deep_level;        // children at this level or deeper use deep_min_len (TSI_NONE: never)
+  uint32_t deep_min_len;
   uint32_t ncontrib;          // reverse contribution records per cell
   uint32_t global;            // 1: the cell working set lives in the block's slice of
                               // LaunchParams::wscratch (too large for shared memory)

@@ -137,8 +137,8 @@ tsi_status Engine::admit(const tsi_request &r, uint64_t ticket) {
   // x4 from 4, x8 from 8).  Results never depend on the threshold.
   const uint32_t running = (uint32_t)slots_.size() - nfree_;
   const uint32_t scale = running >= 8 ? 8u : running >= 4 ? 4u : running >= 2 ? 2u : 1u;
-  uint32_t &ml = h_desc_[i].wide.min_len;
-  ml = (ml >= 0xffffffffu / scale) ? 0xffffffffu : ml * scale;
+  for (uint32_t *ml : {&h_desc_[i].wide.min_len, &h_desc_[i].wide.deep_min_len})
+    *ml = (*ml >= 0xffffffffu / scale) ? 0xffffffffu : *ml * scale;
   Slot &s = slots_[i];
   s.busy = true;
   s.inverting = true;

@@ -140,6 +140,12 @@ __device__ uint32_t alloc_brick(const SceneLaunch &S, uint32_t *error) {
   return b * 8u;
 }
 
+// The wide threshold for children at `level`: deep levels hold many cells,
+// where the narrow path's throughput beats the wide path's latency.
+__device__ __forceinline__ uint32_t wide_min_len(const WideDev &W, uint32_t level) {
+  return level >= W.deep_level ? W.deep_min_len : W.min_len;
+}
+
 __device__ __forceinline__ StepIdx step_idx(uint32_t step) {
   StepIdx si;
   si.cur = step & TSI_STEP_MASK;
@@ -579,7 +585,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
       uint32_t wrec = rec;
       TapeRec WR;
       find_valid(P, wrec, WR, wl, wh);
-      if (WR.len >= S.wide.min_len) {
+      if (WR.len >= wide_min_len(S.wide, it.level + 1u)) {
         // A long tape: no pass over it on one warp.  A group with a widened
         // child hands its children, with that tape's record, to the wide
         // path; the other groups prune from the first pass's decisions.
@@ -593,7 +599,7 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
         PR = WR;
         want_prune = (flags & SF_PRUNING) && PR.len >= TSI_PRUNE_MIN_LEN && PR.nregs <= TSI_PRUNE_MAX_REGS;
       }
-      if (want_prune && WR.len < S.wide.min_len) {
+      if (want_prune && WR.len < wide_min_len(S.wide, it.level + 1u)) {
         float4 *lgs;
         uint2 *dgs;
         if (!item_scratch(P, step, it.scene, PR.len, lane, slice_log, slice_dec, lgs, dgs)) return;
@@ -680,7 +686,8 @@ __device__ __noinline__ void process_item(const LaunchParams &P, const WorkItem 
     for (int b2 = 0; b2 < 8; ++b2) cb[b2] = __shfl_sync(FULL_MASK, C, gl0 + b2);
     const uint32_t next_len = (new_rec == prec) ? PR.len : ((new_rec == rec) ? TR.len : cnt);
     if (k == 0 && E != 0)
-      push_children(P, S, it.scene, new_rec, step, it.level, E, cb, next_len >= S.wide.min_len, ws);
+      push_children(P, S, it.scene, new_rec, step, it.level, E, cb, next_len >= wide_min_len(S.wide, it.level + 1u),
+                    ws);
   }
 
   // ---- counters
@@ -918,7 +925,7 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
       // wide path evaluates the full tape), or may: children the full wide
       // list turns away run narrow on this record
       const bool wide_room = *(const volatile uint32_t *)&P.witem_count[si.next] + 8u <= P.witem_cap;
-      if (total < n_narrow && (total < W.min_len || !wide_room)) {
+      if (total < n_narrow && (total < wide_min_len(W, it.level + 1u) || !wide_room)) {
         const unsigned long long off = code_alloc(P, total);
         if (off != ~0ull) {
           const uint32_t ri = rec_alloc(P);
@@ -1021,7 +1028,8 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
   const long long f2 = clock64();
   if (tid < 32u) {
     const uint32_t len = (new_rec == S.root_rec) ? root.len : sh.cnt;
-    push_children_warp(P, S, it.scene, new_rec, step, it.level, E, it.parent[1], len >= W.min_len, ws, tid);
+    push_children_warp(P, S, it.scene, new_rec, step, it.level, E, it.parent[1],
+                       len >= wide_min_len(W, it.level + 1u), ws, tid);
   }
   if (tid == 0) {
     const long long f3 = clock64();

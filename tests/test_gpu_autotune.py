@@ -12,10 +12,12 @@ from temporalsetinversion_b200 import Scene, Tape, api, scenes
 NARROW_ONLY = 0xFFFFFFFF
 
 
-def _frames(device, text, L, threshold, times, res=(96, 64)):
+def _frames(device, text, L, threshold, times, res=(96, 64), deep=None):
     tape = Tape.from_llvm_ir(device, text)
     if threshold is not None:
         tape.wide_threshold = threshold
+    if deep is not None:
+        tape.wide_threshold_deep = deep
     s = Scene(device, tape, api.default_params(localsubdiv=L))
     cam = scenes.camera_look_at((0.5, 0.9, 2.3))
     out = []
@@ -35,6 +37,22 @@ def test_thresholds_give_identical_frames(device):
     assert tape.wide_threshold == NARROW_ONLY
     for thr in (16, 128, None):
         _, got = _frames(device, text, 7, thr, times)
+        for (wc, wd, wr), (gc, gd, gr) in zip(want, got):
+            assert_cells_equal(gc, wc)
+            assert np.array_equal(gd, wd)
+            assert np.array_equal(gr, wr)
+
+
+@pytest.mark.gpu
+def test_deep_level_thresholds_give_identical_frames(device):
+    """A second threshold for the deepest levels (narrow only there, or a
+    different length) is a speed knob too."""
+    text = scenes.csg(96, 3, 0.9)
+    times = [0.0, 1 / 60, 2 / 60]
+    _, want = _frames(device, text, 8, None, times)
+    for deep in ((6, NARROW_ONLY), (5, 512), (3, 64)):
+        tape, got = _frames(device, text, 8, None, times, deep=deep)
+        assert tape.wide_threshold_deep == deep
         for (wc, wd, wr), (gc, gd, gr) in zip(want, got):
             assert_cells_equal(gc, wc)
             assert np.array_equal(gd, wd)
