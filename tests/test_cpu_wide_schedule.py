@@ -122,3 +122,23 @@ def test_wide_schedule_length(case, steps):
     of depth 31 in 32 steps; cables: depth 44)."""
     _, bundles, _ = wide(CASES[case]())
     assert len(bundles) <= steps
+
+
+# handlers the device evaluates inline (the rest run out of line)
+INLINE = {0, 1, 2, 3, 4, 6, 7, 12, 13, 14, 16, 17, 21, 22, 25, 26, 31}
+
+
+@pytest.mark.parametrize("case,bound", [("swept64", 4), ("csg256", 1), ("csg64", 1), ("spheres16", 1)])
+def test_out_of_line_handlers_gather(case, bound):
+    """Elementary functions and divisions cost several ordinary steps each,
+    so the schedule gathers them: they wait while they have slack and a
+    step that takes one takes all its ready instructions (the rotating
+    swept scene's 64 sines and 64 cosines fill 4 steps, not 17)."""
+    tape = (api.IR.new(scenes.swept(64, 2)).gpu_instructions if case == "swept64" else CASES[case]())
+    slots, bundles, _ = wide(tape)
+    steps = 0
+    for first, count in bundles:
+        hs = {int(s[0]) & 63 for s in slots[int(first):int(first) + int(count)]} - {PAD}
+        steps += bool(hs - INLINE)
+    assert steps <= bound, steps
+
