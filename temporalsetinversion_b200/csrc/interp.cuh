@@ -38,12 +38,6 @@ __device__ __forceinline__ void st_reg(float2 *rf, uint32_t r, uint32_t lane, Iv
 
 // ---------------------------------------------------------------- handlers
 // Rare handlers live out of line so the interpreter loop stays small.
-
-// The handlers op_forward and op_reverse_rule evaluate inline (the bundle
-// loops of the wide interpreter give each a body of its own).
-#define TSI_HOT_HANDLERS(X)                                                                                     \
-  X(H_COPY) X(H_ADD_II) X(H_SUB_II) X(H_MUL_II) X(H_MIN_II) X(H_MAX_II) X(H_ADD_IF) X(H_SUB_IF) X(H_MUL_IF) \
-  X(H_MIN_IF) X(H_MAX_IF) X(H_SQR) X(H_SQRT) X(H_NEG) X(H_ABS) X(H_SUB_FI)
 template <bool D>
 __device__ __noinline__ Iv cold_forward(uint32_t h, Iv A, Iv B, float lit) {
   return IA<D>::forward(h, A, B, lit);

@@ -221,7 +221,7 @@ bool compile_wide(const std::vector<IrInstr> &ins, const PackedTape &narrow, Wid
   // instruction has the highest priority (the oldest instruction on a tie).
   // Users of a step's instructions become ready at the next step.
   const uint32_t groups_per_bundle = WideTape::kWidth / 32u;
-  // the handlers the device evaluates inline (interp.cuh TSI_HOT_HANDLERS
+  // the handlers the device evaluates inline (interp.cuh op_forward
   // and constants); the others run out of line
   auto inline_handler = [](uint32_t h) {
     switch (h) {

@@ -10,9 +10,10 @@
 // mostly fixed (the barrier, the dependent shared-memory loads, the
 // handler dispatch), so the schedule packs groups of different handlers
 // into one step, one handler per warp.  Each thread reads its handler from
-// its slot and runs a body compiled for that handler: the hot handlers get
-// straight-line bodies behind one warp-uniform switch, the rare ones share
-// a generic body.
+// its slot; min/max slots (which also record their decisions) have bodies
+// of their own, every other handler shares one generic body, which keeps
+// the loops small enough for the instruction cache (bodies specialised per
+// handler measured no faster, and slower in the reverse pass).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -92,14 +93,15 @@ __device__ __forceinline__ Iv cell_forward(const WideDev &W, const uint2 *bt_tab
     q1 = q2;
     q2 = fetch(k + 3, 0, 0);
     const uint32_t h = sl.x & 63u;
-    switch (h) {
-#define TSI_X(HH) \
-  case HH: fwd_slot<D, HH>(V, bits, sl); break;
-      TSI_HOT_HANDLERS(TSI_X)
-#undef TSI_X
-      case TSI_H_PAD: break;
-      case H_CONST: stv(V, sl.x >> 8, IA<D>::fix(iv(__uint_as_float(sl.w)))); break;
-      default: fwd_slot_any<D>(h, V, sl); break;
+    if (TSI_H_IS_MINMAX(h)) {
+      switch (h) {
+        case H_MIN_II: fwd_slot<D, H_MIN_II>(V, bits, sl); break;
+        case H_MAX_II: fwd_slot<D, H_MAX_II>(V, bits, sl); break;
+        case H_MIN_IF: fwd_slot<D, H_MIN_IF>(V, bits, sl); break;
+        default: fwd_slot<D, H_MAX_IF>(V, bits, sl); break;
+      }
+    } else if (h != TSI_H_PAD) {
+      fwd_slot_any<D>(h, V, sl);
     }
     __syncthreads();
   }
@@ -162,19 +164,15 @@ __device__ __forceinline__ Iv cell_forward2(const WideDev &W, const uint2 *bt_ta
     q1 = q2;
     q2 = fetch(k + 3, 0, 0);
     const uint32_t h = sl.x & 63u;
-    switch (h) {
-#define TSI_X(HH) \
-  case HH: fwd2_slot<D, HH>(V, V2, bits, bits2, sl); break;
-      TSI_HOT_HANDLERS(TSI_X)
-#undef TSI_X
-      case TSI_H_PAD: break;
-      case H_CONST: {
-        const Iv c = IA<D>::fix(iv(__uint_as_float(sl.w)));
-        stv(V, sl.x >> 8, c);
-        stv(V2, sl.x >> 8, c);
-        break;
+    if (TSI_H_IS_MINMAX(h)) {
+      switch (h) {
+        case H_MIN_II: fwd2_slot<D, H_MIN_II>(V, V2, bits, bits2, sl); break;
+        case H_MAX_II: fwd2_slot<D, H_MAX_II>(V, V2, bits, bits2, sl); break;
+        case H_MIN_IF: fwd2_slot<D, H_MIN_IF>(V, V2, bits, bits2, sl); break;
+        default: fwd2_slot<D, H_MAX_IF>(V, V2, bits, bits2, sl); break;
       }
-      default: fwd2_slot_any<D>(h, V, V2, sl); break;
+    } else if (h != TSI_H_PAD) {
+      fwd2_slot_any<D>(h, V, V2, sl);
     }
     __syncthreads();
   }
@@ -261,15 +259,7 @@ __device__ __forceinline__ void cell_reverse(const WideDev &W, const uint2 *bt_t
     b0 = fetch(k - 2, 0, ns);
     b2 = fetch(k - 2, 2, ns);
     const uint32_t h = sl.x & 63u;
-    switch (h) {
-#define TSI_X(HH) \
-  case HH: rev_slot_body<D>(HH, V, G, R, sl, s2); break;
-      TSI_HOT_HANDLERS(TSI_X)
-#undef TSI_X
-      case TSI_H_PAD:
-      case H_CONST: break;
-      default: rev_slot_body<D>(h, V, G, R, sl, s2); break;
-    }
+    if (h != TSI_H_PAD && h != H_CONST) rev_slot_body<D>(h, V, G, R, sl, s2);
     __syncthreads();
   }
   if (tid < 4u) {
