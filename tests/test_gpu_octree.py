@@ -188,3 +188,47 @@ def test_async_inversion_reports_pool_exhaustion(device):
     ok = Scene(device, tape, api.default_params(localsubdiv=5))
     ok.invert_async(0.0)
     assert ok.invert_wait().cells_evaluated > 0
+
+
+def _many_live(n: int, seed: int) -> str:
+    """n moving spheres whose distances are all computed before a sequential
+    min reduces them, so n values are live at once: a tape of more than n
+    interval registers."""
+    rng = np.random.default_rng(seed)
+    b = scenes.IRBuilder()
+    t2 = b.mul(b.T, 6.2831855)
+    d = []
+    for _ in range(n):
+        c = rng.uniform(-0.7, 0.7, 3)
+        m = b.mul(b.sin(b.add(t2, float(rng.uniform(0, 6.28)))), 0.1)
+        q = [b.sub(v, b.add(m, float(ci))) for v, ci in zip((b.X, b.Y, b.Z), c)]
+        s = b.add(b.add(b.mul(q[0], q[0]), b.mul(q[1], q[1])), b.mul(q[2], q[2]))
+        d.append(b.sub(b.sqrt(s), float(rng.uniform(0.05, 0.15))))
+    acc = d[0]
+    for v in d[1:]:
+        acc = b.min(acc, v)
+    return b.text(acc)
+
+
+@pytest.mark.gpu
+def test_tape_beyond_pruning_registers_matches_oracle(device):
+    """A tape with more live values than pruning handles (64 registers) runs
+    unpruned, reports so in its counters, and still equals the oracle."""
+    text = _many_live(70, 3)
+    tape = api.IR.new(text).gpu_instructions
+    t = Tape.upload(device, tape)
+    assert t.registers > 64
+    p = api.default_params(localsubdiv=6, pruning=1)
+    gs = Scene(device, t, p)
+    os_ = oracle.Scene(tape, p)
+    unpruned = 0
+    for tm in (0.0, 1 / 60, 2 / 60):
+        st = gs.invert(tm)
+        sg = st.as_dict()
+        so = os_.invert(tm)
+        for k in COUNTERS:
+            assert sg[k] == so[k], "t=%g %s: gpu %d oracle %d" % (tm, k, sg[k], so[k])
+        assert_cells_equal(gs.cells(), os_.cells())
+        unpruned += st.cells_unpruned_regs
+    assert unpruned > 0
+
