@@ -309,6 +309,13 @@ TSI_API tsi_status tsi_tape_set_wide_threshold(tsi_tape *tape, uint32_t min_len)
 // the thresholds.
 TSI_API tsi_status tsi_tape_set_wide_threshold_deep(tsi_tape *tape, uint32_t level, uint32_t min_len);
 TSI_API tsi_status tsi_tape_wide_threshold_deep(const tsi_tape *tape, uint32_t *level, uint32_t *min_len);
+// Parents per narrow work item above the leaf level (1, 2 or 4; default 1):
+// a narrow item evaluates the 8 children of each of its parents with one
+// warp, so fewer parents per item put more warps in flight (latency) and
+// more fill the lanes (throughput).  Leaves always take 4.  Results never
+// depend on it.
+TSI_API tsi_status tsi_tape_set_narrow_parents(tsi_tape *tape, uint32_t parents);
+TSI_API uint32_t tsi_tape_narrow_parents(const tsi_tape *tape);
 
 #define TSI_AUTOTUNE_MAX 16
 typedef struct tsi_autotune_result {
@@ -318,6 +325,7 @@ typedef struct tsi_autotune_result {
   float ms[TSI_AUTOTUNE_MAX];       /* best of `reps` runs over `times`, device ms */
   uint32_t deep_level;              /* chosen deep-level threshold (tsi_tape_set_wide_threshold_deep); */
   uint32_t deep_threshold;          /* deep_level 0xffffffff: none beat the single threshold */
+  uint32_t narrow_parents;          /* chosen parents per narrow item (tsi_tape_set_narrow_parents) */
 } tsi_autotune_result;
 /* Times the scene's inversion over the frames `times` (the first from a
  * reset octree, the rest carried over) for each candidate wide threshold,

@@ -210,6 +210,15 @@ class Tape:
         N.check(self.device.lib.tsi_tape_set_wide_threshold_deep(self.handle, int(v[0]), int(v[1])),
                 "tsi_tape_set_wide_threshold_deep")
 
+    @property
+    def narrow_parents(self) -> int:
+        """Parents per narrow work item above the leaf level (1, 2 or 4)."""
+        return int(self.device.lib.tsi_tape_narrow_parents(self.handle))
+
+    @narrow_parents.setter
+    def narrow_parents(self, v: int) -> None:
+        N.check(self.device.lib.tsi_tape_set_narrow_parents(self.handle, int(v)), "tsi_tape_set_narrow_parents")
+
     def close(self) -> None:
         if getattr(self, "handle", None) and getattr(self.device, "handle", None):
             self.device.lib.tsi_tape_destroy(self.handle)
@@ -237,15 +246,15 @@ class Scene:
         N.check(self.device.lib.tsi_scene_reset(self.handle), "tsi_scene_reset")
 
     def autotune(self, times: list, reps: int = 2) -> dict:
-        """Picks the tape's wide threshold, then a deep-level one, by timing
-        inversions over `times` (tsi_scene_autotune); the scene is left
-        reset."""
+        """Picks the tape's wide threshold, then a deep-level one, then the
+        parents per narrow item, by timing inversions over `times`
+        (tsi_scene_autotune); the scene is left reset."""
         arr = (C.c_float * len(times))(*[float(t) for t in times])
         r = N.AutotuneResult()
         N.check(self.device.lib.tsi_scene_autotune(self.handle, arr, len(times), int(reps), C.byref(r)),
                 "tsi_scene_autotune")
         return {"wide_threshold": int(r.wide_threshold), "deep_level": int(r.deep_level),
-                "deep_threshold": int(r.deep_threshold),
+                "deep_threshold": int(r.deep_threshold), "narrow_parents": int(r.narrow_parents),
                 "trials": [(int(r.threshold[k]), float(r.ms[k])) for k in range(r.candidates)]}
 
     def invert(self, time: float, t0: float = math.nan) -> N.Stats:

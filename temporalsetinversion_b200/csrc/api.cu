@@ -184,6 +184,7 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, bool 
   L.root_rec = slot;
   L.levels = tree_levels(p);
   L.full_len = s->tape->len;
+  L.narrow_parents = s->tape->narrow_parents;
   L.wide.slots = s->tape->d_wslots;
   L.wide.bundles = s->tape->d_wbundles;
   L.wide.narrow_mm = s->tape->d_wmm;
@@ -1436,6 +1437,15 @@ TSI_API tsi_status tsi_tape_set_wide_threshold_deep(tsi_tape *t, uint32_t level,
   return TSI_OK;
 }
 
+TSI_API tsi_status tsi_tape_set_narrow_parents(tsi_tape *t, uint32_t parents) {
+  if (!t) return set_err(TSI_ERR_INVALID_ARGUMENT, "null tape");
+  if (parents != 1 && parents != 2 && parents != 4) return set_err(TSI_ERR_INVALID_ARGUMENT, "parents must be 1, 2 or 4");
+  t->narrow_parents = parents;
+  return TSI_OK;
+}
+
+TSI_API uint32_t tsi_tape_narrow_parents(const tsi_tape *t) { return t ? t->narrow_parents : 0u; }
+
 TSI_API tsi_status tsi_tape_wide_threshold_deep(const tsi_tape *t, uint32_t *level, uint32_t *min_len) {
   if (!t || !level || !min_len) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
   *level = t->wdeep_level;
@@ -1538,6 +1548,39 @@ TSI_API tsi_status tsi_scene_autotune(tsi_scene *s, const float *times, uint32_t
   t->wdeep_min_len = dm;
   out->deep_level = dl;
   out->deep_threshold = dm;
+  // then the parents per narrow item above the leaf level
+  const uint32_t keep_parents = t->narrow_parents;
+  uint32_t pp = keep_parents;
+  for (uint32_t cand_p : {1u, 2u, 4u}) {
+    if (cand_p == keep_parents) continue;
+    t->narrow_parents = cand_p;
+    float bk = INFINITY;
+    for (uint32_t r = 0; r < reps; ++r) {
+      tsi_status st = tsi_scene_reset(s);
+      float ms = 0.0f;
+      for (uint32_t i = 0; i < ntimes && st == TSI_OK; ++i) {
+        tsi_stats fs;
+        st = tsi_scene_invert(s, times[i], NAN, &fs);
+        ms += fs.device_ms;
+      }
+      if (st == TSI_ERR_QUEUE_FULL || st == TSI_ERR_OOM) {
+        bk = INFINITY;
+        break;
+      }
+      if (st != TSI_OK) {
+        t->narrow_parents = keep_parents;
+        tsi_scene_reset(s);
+        return st;
+      }
+      bk = std::min(bk, ms);
+    }
+    if (bk < best * 0.99f) {
+      best = bk;
+      pp = cand_p;
+    }
+  }
+  t->narrow_parents = pp;
+  out->narrow_parents = pp;
   return tsi_scene_reset(s);
 }
 

@@ -96,8 +96,9 @@ struct SceneLaunch {
   float t0;           // start of the swept interval
   uint32_t flags;
   uint32_t root_rec;
-  uint32_t levels;    // localsubdiv
-  uint32_t full_len;  // full tape length (instr_full_equiv counter)
+  uint32_t levels;          // octree levels of a frame (the leaves are level levels - 1)
+  uint32_t full_len;        // full tape length (instr_full_equiv counter)
+  uint32_t narrow_parents;  // parents per narrow item above the leaf level (1, 2 or 4)
 };
 
 struct TapeRec {

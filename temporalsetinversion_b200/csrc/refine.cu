@@ -226,7 +226,11 @@ __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint3
     }
   }
   if (rest == 0) return;
-  const uint32_t nitems = (__popc(rest) + 3u) >> 2;
+  // a narrow item takes up to 4 parents (32 cells, one per lane) at the leaf
+  // level, where many short evaluations make throughput count, and fewer
+  // above it, where more items in flight hide the interpreter's latency
+  const uint32_t per = (plevel + 2u >= S.levels) ? 4u : max(1u, min(4u, S.narrow_parents));
+  const uint32_t nitems = (__popc(rest) + per - 1u) / per;
   const uint32_t pos = atomicAdd(&P.item_count[si.next], nitems);
   if (pos + nitems > P.item_cap) atomicOr(err, EB_QUEUE_FULL);
   WorkItem *dst = P.items[si.nbuf];
@@ -236,7 +240,7 @@ __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint3
     wi.rec = rec;
     wi.level = plevel + 1;
     uint32_t c = 0;
-    while (rest && c < 4u) {
+    while (rest && c < per) {
       const uint32_t bit = __ffs(rest) - 1u;
       rest &= rest - 1u;
       wi.parent[c++] = cells[bit];

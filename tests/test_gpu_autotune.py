@@ -12,8 +12,10 @@ from temporalsetinversion_b200 import Scene, Tape, api, scenes
 NARROW_ONLY = 0xFFFFFFFF
 
 
-def _frames(device, text, L, threshold, times, res=(96, 64), deep=None):
+def _frames(device, text, L, threshold, times, res=(96, 64), deep=None, parents=None):
     tape = Tape.from_llvm_ir(device, text)
+    if parents is not None:
+        tape.narrow_parents = parents
     if threshold is not None:
         tape.wide_threshold = threshold
     if deep is not None:
@@ -53,6 +55,22 @@ def test_deep_level_thresholds_give_identical_frames(device):
     for deep in ((6, NARROW_ONLY), (5, 512), (3, 64)):
         tape, got = _frames(device, text, 8, None, times, deep=deep)
         assert tape.wide_threshold_deep == deep
+        for (wc, wd, wr), (gc, gd, gr) in zip(want, got):
+            assert_cells_equal(gc, wc)
+            assert np.array_equal(gd, wd)
+            assert np.array_equal(gr, wr)
+
+
+@pytest.mark.gpu
+def test_narrow_parents_give_identical_frames(device):
+    """Parents per narrow work item (1, 2 or 4) only change how cells are
+    packed onto warps."""
+    text = scenes.csg(64, 5, 0.85)
+    times = [0.0, 1 / 60, 2 / 60]
+    _, want = _frames(device, text, 7, NARROW_ONLY, times, parents=4)
+    for parents in (1, 2):
+        tape, got = _frames(device, text, 7, NARROW_ONLY, times, parents=parents)
+        assert tape.narrow_parents == parents
         for (wc, wd, wr), (gc, gd, gr) in zip(want, got):
             assert_cells_equal(gc, wc)
             assert np.array_equal(gd, wd)
