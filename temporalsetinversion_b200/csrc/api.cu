@@ -349,14 +349,20 @@ tsi_status enqueue_invert(tsi_ctx *c, tsi_scene *const *scenes, const float *tim
   const LaunchParams P = make_params(c, n, fp.smem, sticky);
   CK(launch_frame_begin(P, c->stream));
   const bool prof = c->profile_levels && c->level_events.size() >= lmax + 1;
+  // Each level's launch overlaps the end of the one before (programmatic
+  // dependent launch: its blocks take the SMs the last level's blocks leave
+  // and wait for it on the device), unless events sit between the levels
+  // (per-level timing, the batched form's trace forks) or a graph is being
+  // captured.
+  const bool overlap = !cap && !prof && !fork;
   for (uint32_t level = 0; level < lmax; ++level) {
     if (prof) CK(cudaEventRecord(c->level_events[level], c->stream));
-    CK(launch_refine(P, level, rcap, grid, kBlock, smem, c->stream));
+    CK(launch_refine(P, level, rcap, grid, kBlock, smem, c->stream, overlap));
     if (fork) CK(cudaEventRecord(c->fork_events[level], c->stream));
   }
   if (prof) CK(cudaEventRecord(c->level_events[lmax], c->stream));
   c->last_levels = lmax;
-  CK(launch_frame_end(P, 0, n, c->stream));
+  CK(launch_frame_end(P, 0, n, c->stream, overlap));
   return TSI_OK;
 }
 

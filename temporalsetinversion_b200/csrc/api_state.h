@@ -15,11 +15,14 @@
 #include "tsi.h"
 
 namespace tsi {
+// overlap: launched as a programmatic dependent of the stream's previous
+// kernel (refinement steps, the frame's begin and end kernels)
 cudaError_t launch_refine(const LaunchParams &P, uint32_t step, uint32_t rcap, int grid, int block, size_t smem,
-                          cudaStream_t st);
+                          cudaStream_t st, bool overlap = false);
 cudaError_t launch_frame_begin(const LaunchParams &P, cudaStream_t st);
 cudaError_t launch_step_begin(const LaunchParams &P, uint32_t step, const StepSeeds &sd, cudaStream_t st);
-cudaError_t launch_frame_end(const LaunchParams &P, uint32_t first, uint32_t count, cudaStream_t st);
+cudaError_t launch_frame_end(const LaunchParams &P, uint32_t first, uint32_t count, cudaStream_t st,
+                             bool overlap = false);
 cudaError_t refine_set_smem(size_t bytes);
 cudaError_t refine_occupancy(int block, size_t smem, int *blocks_per_sm);
 cudaError_t refine_static_smem(size_t *bytes);

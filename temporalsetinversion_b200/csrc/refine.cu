@@ -50,6 +50,14 @@ constexpr int kWarps = 8;  // warps per block (block of 256)
 // or the working set of the wide path's cell.
 extern __shared__ __align__(16) unsigned char tsi_dyn_smem[];
 
+// Programmatic dependent launch (PTX griddepcontrol, sm_90 and later): the
+// wait returns once the grids this launch depends on have completed and
+// their writes are visible (at once for a launch without that dependency);
+// the trigger lets the stream's next launch begin once every block of this
+// one has issued it.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Backward liveness scan of one sibling group, run by the whole warp with the
 // group leaders (lane 8g, `active`) doing the work: decided min/max become
 // copies/constants, dead instructions vanish.  The kept instructions are
@@ -1363,6 +1371,12 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
   si.nbuf = (step + 1u) & 1u;
   __shared__ unsigned long long s_stats[kWarps][ST_COUNT];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  // Launched as a programmatic dependent of the previous step, the blocks
+  // may be resident before that step has ended: nothing of it is read
+  // before it has completed.  Then the next step's launch may begin (its
+  // blocks take the SMs this launch's blocks leave).
+  grid_dependency_wait();
+  grid_dependents_launch();
   // the lists of the step after next start empty (no launch of this step
   // touches them; the next step fills them)
   if (blockIdx.x == 0 && threadIdx.x == 0) clear_step(P, (step + 2u) & TSI_STEP_MASK);
@@ -1506,6 +1520,7 @@ __device__ void seed_root(const LaunchParams &P, uint32_t s, uint32_t step) {
 // at step 0.  With n_scenes = 0 it only clears (the continuous form's start).
 __global__ void frame_begin_kernel(const __grid_constant__ LaunchParams P) {
   const uint32_t t = threadIdx.x;
+  grid_dependents_launch();  // the first level's launch may begin
   for (uint32_t l = t; l < TSI_STEP_RING; l += blockDim.x) clear_step(P, l);
   if (t == 0) {
     *P.rec_count = 0;
@@ -1548,6 +1563,7 @@ __global__ void step_begin_kernel(const __grid_constant__ LaunchParams P, uint32
 // the frame become allocatable; the scene's error word is or-ed into the
 // sticky word (asynchronous inversions).
 __global__ void frame_end_kernel(const __grid_constant__ LaunchParams P, uint32_t first) {
+  grid_dependency_wait();  // the last level has completed
   const uint32_t s = first + blockIdx.x;
   if (s >= P.n_scenes) return;
   const SceneLaunch &S = P.scenes[s];
@@ -1571,10 +1587,30 @@ __global__ void frame_end_kernel(const __grid_constant__ LaunchParams P, uint32_
 }
 
 // host-side launch helpers
+namespace {
+// Launch configuration; `overlap`: a programmatic dependent of the stream's
+// previous kernel (its launch overlaps that kernel's last blocks; the
+// kernel waits for it to complete before reading what it wrote).
+struct LaunchCfg {
+  cudaLaunchConfig_t cfg{};
+  cudaLaunchAttribute attr[1];
+  LaunchCfg(int grid, int block, size_t smem, cudaStream_t st, bool overlap) {
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = overlap ? attr : nullptr;
+    cfg.numAttrs = overlap ? 1u : 0u;
+  }
+};
+}  // namespace
+
 cudaError_t launch_refine(const LaunchParams &P, uint32_t step, uint32_t rcap, int grid, int block, size_t smem,
-                          cudaStream_t st) {
-  refine_kernel<<<grid, block, smem, st>>>(P, step, rcap);
-  return cudaGetLastError();
+                          cudaStream_t st, bool overlap) {
+  LaunchCfg lc(grid, block, smem, st, overlap);
+  return cudaLaunchKernelEx(&lc.cfg, refine_kernel, P, step, rcap);
 }
 cudaError_t launch_frame_begin(const LaunchParams &P, cudaStream_t st) {
   frame_begin_kernel<<<1, 64, 0, st>>>(P);
@@ -1584,10 +1620,10 @@ cudaError_t launch_step_begin(const LaunchParams &P, uint32_t step, const StepSe
   step_begin_kernel<<<1, 256, 0, st>>>(P, step, sd);
   return cudaGetLastError();
 }
-cudaError_t launch_frame_end(const LaunchParams &P, uint32_t first, uint32_t count, cudaStream_t st) {
+cudaError_t launch_frame_end(const LaunchParams &P, uint32_t first, uint32_t count, cudaStream_t st, bool overlap) {
   if (count == 0) return cudaSuccess;
-  frame_end_kernel<<<count, 256, 0, st>>>(P, first);
-  return cudaGetLastError();
+  LaunchCfg lc((int)count, 256, 0, st, overlap);
+  return cudaLaunchKernelEx(&lc.cfg, frame_end_kernel, P, first);
 }
 // The attribute belongs to the kernel on the current device, shared by every
 // context of the process: only ever raise it.
