@@ -191,9 +191,12 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, bool 
   L.wide.nslots = s->tape->wslots;
   L.wide.nbundles = s->tape->wbundles;
   L.wide.nvalues = s->tape->wvalues;
-  L.wide.min_len = s->tape->wmin_len;
+  // a tape without a bundled form never sends a cell to the wide path,
+  // whatever thresholds were set on it
+  const bool has_wide = s->tape->d_wslots != nullptr && s->tape->wbundles > 0;
+  L.wide.min_len = has_wide ? s->tape->wmin_len : 0xffffffffu;
   L.wide.deep_level = s->tape->wdeep_level;
-  L.wide.deep_min_len = s->tape->wdeep_min_len;
+  L.wide.deep_min_len = has_wide ? s->tape->wdeep_min_len : 0xffffffffu;
   L.wide.ncontrib = s->tape->wcontrib;
   L.wide.global = wide_global ? 1u : 0u;
   for (int q = 0; q < 4; ++q) {
@@ -1438,6 +1441,7 @@ TSI_API tsi_status tsi_tape_set_wide_threshold(tsi_tape *t, uint32_t min_len) {
 
 TSI_API tsi_status tsi_tape_set_wide_threshold_deep(tsi_tape *t, uint32_t level, uint32_t min_len) {
   if (!t) return set_err(TSI_ERR_INVALID_ARGUMENT, "null tape");
+  if (!t->d_wslots) return TSI_OK;  // no bundled form: every cell stays on the narrow path
   t->wdeep_level = level;
   t->wdeep_min_len = min_len;
   return TSI_OK;

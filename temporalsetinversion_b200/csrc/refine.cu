@@ -202,6 +202,9 @@ __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint3
                               uint32_t step, uint32_t plevel, uint32_t E, const uint32_t *cells, bool wide,
                               unsigned long long *ws) {
   const StepIdx si = step_idx(step);
+  // a scene's items end at its last level: the launch steps of its frame
+  // stop there, and in the continuous form later steps belong to others
+  if (plevel + 1u >= S.levels) return;
   uint32_t rest = E;
   uint32_t *err = P.error + scene;
   if (wide) {
@@ -267,6 +270,7 @@ __device__ __forceinline__ void push_children_warp(const LaunchParams &P, const 
                                                    uint32_t rec, uint32_t step, uint32_t plevel, uint32_t E,
                                                    uint32_t base, bool wide, unsigned long long *ws, uint32_t lane) {
   const StepIdx si = step_idx(step);
+  if (plevel + 1u >= S.levels) return;  // the scene's last level (push_children)
   uint32_t rest = E;
   if (wide && E) {
     uint32_t pos = 0;
