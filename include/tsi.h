@@ -316,6 +316,15 @@ TSI_API tsi_status tsi_tape_wide_threshold_deep(const tsi_tape *tape, uint32_t *
 // depend on it.
 TSI_API tsi_status tsi_tape_set_narrow_parents(tsi_tape *tape, uint32_t parents);
 TSI_API uint32_t tsi_tape_narrow_parents(const tsi_tape *tape);
+// First octree level (of the parents) from which a wide item's group prunes
+// its tape for the children (a liveness pass over the bundled tape after the
+// eight cells are done).  Above it the children take the wide path, which
+// evaluates the full tape anyway, so the pass and the second decision
+// interval of the forward pass are skipped.  0xffffffff (the default):
+// half the scene's levels; a level past the last: the wide path never
+// prunes.  Results never depend on it.
+TSI_API tsi_status tsi_tape_set_wide_prune_level(tsi_tape *tape, uint32_t level);
+TSI_API uint32_t tsi_tape_wide_prune_level(const tsi_tape *tape);
 
 #define TSI_AUTOTUNE_MAX 16
 typedef struct tsi_autotune_result {
@@ -326,11 +335,14 @@ typedef struct tsi_autotune_result {
   uint32_t deep_level;              /* chosen deep-level threshold (tsi_tape_set_wide_threshold_deep); */
   uint32_t deep_threshold;          /* deep_level 0xffffffff: none beat the single threshold */
   uint32_t narrow_parents;          /* chosen parents per narrow item (tsi_tape_set_narrow_parents) */
+  uint32_t wide_prune_level;        /* chosen prune level (tsi_tape_set_wide_prune_level) */
 } tsi_autotune_result;
 /* Times the scene's inversion over the frames `times` (the first from a
  * reset octree, the rest carried over) for each candidate wide threshold,
  * best of `reps`, and keeps the fastest on the scene's tape (shared by every
- * scene of that tape).  The scene is left reset. */
+ * scene of that tape); then, one knob at a time, a deep-level threshold, the
+ * parents per narrow item and the wide path's prune level, each kept only
+ * when it is faster.  The scene is left reset. */
 TSI_API tsi_status tsi_scene_autotune(tsi_scene *scene, const float *times, uint32_t ntimes, uint32_t reps,
                                       tsi_autotune_result *out);
 /* Copies the scene's last rendered frame (e.g. from a graph replay or the

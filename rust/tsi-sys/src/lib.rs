@@ -167,6 +167,7 @@ pub struct tsi_autotune_result {
     pub deep_level: u32,
     pub deep_threshold: u32,
     pub narrow_parents: u32,
+    pub wide_prune_level: u32,
 }
 
 /// Caller-owned device buffers of a composited frame (one animation split at the root).
@@ -259,6 +260,8 @@ extern "C" {
     pub fn tsi_tape_wide_threshold_deep(t: *const tsi_tape, level: *mut u32, min_len: *mut u32) -> tsi_status;
     pub fn tsi_tape_set_narrow_parents(t: *mut tsi_tape, parents: u32) -> tsi_status;
     pub fn tsi_tape_narrow_parents(t: *const tsi_tape) -> u32;
+    pub fn tsi_tape_set_wide_prune_level(t: *mut tsi_tape, level: u32) -> tsi_status;
+    pub fn tsi_tape_wide_prune_level(t: *const tsi_tape) -> u32;
     pub fn tsi_scene_autotune(s: *mut tsi_scene, times: *const f32, ntimes: u32, reps: u32,
                               out: *mut tsi_autotune_result) -> tsi_status;
     pub fn tsi_scene_readback_cells(s: *mut tsi_scene, out: *mut tsi_cell, cap: u64, n: *mut u64) -> tsi_status;

@@ -74,7 +74,7 @@ AUTOTUNE_MAX = 16
 class AutotuneResult(C.Structure):
     _fields_ = [("wide_threshold", u32), ("candidates", u32), ("threshold", u32 * AUTOTUNE_MAX),
                 ("ms", f32 * AUTOTUNE_MAX), ("deep_level", u32), ("deep_threshold", u32),
-                ("narrow_parents", u32)]
+                ("narrow_parents", u32), ("wide_prune_level", u32)]
 
 
 SERVER_STATIC_BATCHES = 1
@@ -168,6 +168,8 @@ SIGNATURES = {
     "tsi_tape_wide_threshold_deep": (i32, [C.c_void_p, C.POINTER(u32), C.POINTER(u32)]),
     "tsi_tape_set_narrow_parents": (i32, [C.c_void_p, u32]),
     "tsi_tape_narrow_parents": (u32, [C.c_void_p]),
+    "tsi_tape_set_wide_prune_level": (i32, [C.c_void_p, u32]),
+    "tsi_tape_wide_prune_level": (u32, [C.c_void_p]),
     "tsi_scene_autotune": (i32, [C.c_void_p, P(f32), u32, u32, P(AutotuneResult)]),
     "tsi_batch_graph_destroy": (None, [C.c_void_p]),
     "tsi_last_error": (C.c_char_p, []),

@@ -219,6 +219,16 @@ class Tape:
     def narrow_parents(self, v: int) -> None:
         N.check(self.device.lib.tsi_tape_set_narrow_parents(self.handle, int(v)), "tsi_tape_set_narrow_parents")
 
+    @property
+    def wide_prune_level(self) -> int:
+        """First parent level whose wide groups prune the tape for their
+        children (0xffffffff: half the scene's levels)."""
+        return int(self.device.lib.tsi_tape_wide_prune_level(self.handle))
+
+    @wide_prune_level.setter
+    def wide_prune_level(self, v: int) -> None:
+        N.check(self.device.lib.tsi_tape_set_wide_prune_level(self.handle, int(v)), "tsi_tape_set_wide_prune_level")
+
     def close(self) -> None:
         if getattr(self, "handle", None) and getattr(self.device, "handle", None):
             self.device.lib.tsi_tape_destroy(self.handle)
@@ -247,14 +257,16 @@ class Scene:
 
     def autotune(self, times: list, reps: int = 2) -> dict:
         """Picks the tape's wide threshold, then a deep-level one, then the
-        parents per narrow item, by timing inversions over `times`
-        (tsi_scene_autotune); the scene is left reset."""
+        parents per narrow item, then the wide path's prune level, by timing
+        inversions over `times` (tsi_scene_autotune); the scene is left
+        reset."""
         arr = (C.c_float * len(times))(*[float(t) for t in times])
         r = N.AutotuneResult()
         N.check(self.device.lib.tsi_scene_autotune(self.handle, arr, len(times), int(reps), C.byref(r)),
                 "tsi_scene_autotune")
         return {"wide_threshold": int(r.wide_threshold), "deep_level": int(r.deep_level),
                 "deep_threshold": int(r.deep_threshold), "narrow_parents": int(r.narrow_parents),
+                "wide_prune_level": int(r.wide_prune_level),
                 "trials": [(int(r.threshold[k]), float(r.ms[k])) for k in range(r.candidates)]}
 
     def invert(self, time: float, t0: float = math.nan) -> N.Stats:

@@ -198,6 +198,7 @@ void fill_launch(tsi_scene *s, uint32_t slot, float time, float t0_or_nan, bool 
   L.wide.deep_level = s->tape->wdeep_level;
   L.wide.deep_min_len = has_wide ? s->tape->wdeep_min_len : 0xffffffffu;
   L.wide.ncontrib = s->tape->wcontrib;
+  L.wide.prune_level = s->tape->wprune_level != 0xffffffffu ? s->tape->wprune_level : tree_levels(p) / 2u;
   L.wide.global = wide_global ? 1u : 0u;
   for (int q = 0; q < 4; ++q) {
     L.wide.arg_gbase[q] = s->tape->warg_gbase[q];
@@ -1456,6 +1457,14 @@ TSI_API tsi_status tsi_tape_set_narrow_parents(tsi_tape *t, uint32_t parents) {
 
 TSI_API uint32_t tsi_tape_narrow_parents(const tsi_tape *t) { return t ? t->narrow_parents : 0u; }
 
+TSI_API tsi_status tsi_tape_set_wide_prune_level(tsi_tape *t, uint32_t level) {
+  if (!t) return set_err(TSI_ERR_INVALID_ARGUMENT, "null tape");
+  t->wprune_level = level;
+  return TSI_OK;
+}
+
+TSI_API uint32_t tsi_tape_wide_prune_level(const tsi_tape *t) { return t ? t->wprune_level : 0xffffffffu; }
+
 TSI_API tsi_status tsi_tape_wide_threshold_deep(const tsi_tape *t, uint32_t *level, uint32_t *min_len) {
   if (!t || !level || !min_len) return set_err(TSI_ERR_INVALID_ARGUMENT, "null argument");
   *level = t->wdeep_level;
@@ -1591,6 +1600,43 @@ TSI_API tsi_status tsi_scene_autotune(tsi_scene *s, const float *times, uint32_t
   }
   t->narrow_parents = pp;
   out->narrow_parents = pp;
+  // then the first level whose wide groups prune their tape (automatic:
+  // half the scene's levels; `levels`: the wide path never prunes)
+  const uint32_t keep_prune = t->wprune_level;
+  const uint32_t auto_level = levels / 2u;
+  const uint32_t current = keep_prune == 0xffffffffu ? auto_level : keep_prune;
+  uint32_t pl = keep_prune;
+  for (uint32_t cand_l : {auto_level >= 2u ? auto_level - 2u : 0u, auto_level >= 1u ? auto_level - 1u : 0u,
+                          auto_level, auto_level + 1u, levels}) {
+    if (cand_l == current) continue;
+    t->wprune_level = cand_l;
+    float bk = INFINITY;
+    for (uint32_t r = 0; r < reps; ++r) {
+      tsi_status st = tsi_scene_reset(s);
+      float ms = 0.0f;
+      for (uint32_t i = 0; i < ntimes && st == TSI_OK; ++i) {
+        tsi_stats fs;
+        st = tsi_scene_invert(s, times[i], NAN, &fs);
+        ms += fs.device_ms;
+      }
+      if (st == TSI_ERR_QUEUE_FULL || st == TSI_ERR_OOM) {
+        bk = INFINITY;
+        break;
+      }
+      if (st != TSI_OK) {
+        t->wprune_level = keep_prune;
+        tsi_scene_reset(s);
+        return st;
+      }
+      bk = std::min(bk, ms);
+    }
+    if (bk < best * 0.99f) {
+      best = bk;
+      pl = cand_l;
+    }
+  }
+  t->wprune_level = pl;
+  out->wide_prune_level = pl;
   return tsi_scene_reset(s);
 }
 

@@ -48,6 +48,7 @@ struct tsi_tape {
   uint32_t wslots = 0, wbundles = 0, wvalues = 0, wmin_len = 0xffffffffu, wcontrib = 0;
   uint32_t wdeep_level = 0xffffffffu, wdeep_min_len = 0xffffffffu;  // level-dependent threshold (off by default)
   uint32_t narrow_parents = 1;  // parents per narrow item above the leaf level
+  uint32_t wprune_level = 0xffffffffu;  // first level whose wide groups prune (0xffffffff: half the levels)
   uint32_t warg_gbase[4] = {TSI_NONE, TSI_NONE, TSI_NONE, TSI_NONE}, warg_gcount[4] = {0, 0, 0, 0};
 };
 

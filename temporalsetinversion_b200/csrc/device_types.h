@@ -70,7 +70,7 @@ struct SceneCounters {
 // with one block per cell for items whose tape is long.
 struct WideDev {
   const uint4 *slots;         // [3][nslots]: words 0-3, 4-7, 8-11 of each slot (tape_compile.h)
-  const uint2 *bundles;       // first slot, count | handler << 16
+  const uint2 *bundles;       // first slot, slot count (padding included)
   const uint32_t *narrow_mm;  // min/max ordinal per narrow instruction
   uint32_t nslots;
   uint32_t nbundles;
@@ -79,6 +79,7 @@ struct WideDev {
   uint32_t deep_level;        // children at this level or deeper use deep_min_len (TSI_NONE: never)
   uint32_t deep_min_len;
   uint32_t ncontrib;          // reverse contribution records per cell
+  uint32_t prune_level;       // wide items at this octree level or deeper prune their group's tape
   uint32_t global;            // 1: the cell working set lives in the block's slice of
                               // LaunchParams::wscratch (too large for shared memory)
   uint32_t arg_gbase[4];      // records of x, y, z, t (TSI_NONE: one user)

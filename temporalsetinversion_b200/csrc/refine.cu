@@ -872,7 +872,9 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
   __syncthreads();
   const uint32_t E = sh.E;
   if (E == 0) return;
-  const bool want_prune = (S.flags & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS;
+  // groups above the tape's prune level skip the liveness pass: their
+  // children go to the wide path, which evaluates the full tape anyway
+  const bool want_prune = (S.flags & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS && it.level >= W.prune_level;
   uint32_t new_rec = S.root_rec;
   if (want_prune) {
     const CellLayout L = cell_layout(W, P.bm_words);
@@ -1148,7 +1150,8 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   const Iv targ = Iv{fm_min(cur_t.lo, cur_t.hi), fm_max(cur_t.lo, cur_t.hi)};
   const bool evaluate = new_voxel || c_f >= 0.0f || c_child == TSI_NONE;
   const bool take_deriv = evaluate && ((cur_t.lo != cur_t.hi) || (flg & SF_ALWAYS_DERIV));
-  const bool want_prune = (flg & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS;
+  const bool want_prune = (flg & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS
+                          && it.level >= W.prune_level;  // finish_group's rule
   const uint32_t words = (root.n_minmax + 15u) >> 4;
 
   // The time range this cell's children would be evaluated over if it is

@@ -12,10 +12,12 @@ from temporalsetinversion_b200 import Scene, Tape, api, scenes
 NARROW_ONLY = 0xFFFFFFFF
 
 
-def _frames(device, text, L, threshold, times, res=(96, 64), deep=None, parents=None):
+def _frames(device, text, L, threshold, times, res=(96, 64), deep=None, parents=None, prune_level=None):
     tape = Tape.from_llvm_ir(device, text)
     if parents is not None:
         tape.narrow_parents = parents
+    if prune_level is not None:
+        tape.wide_prune_level = prune_level
     if threshold is not None:
         tape.wide_threshold = threshold
     if deep is not None:
@@ -78,6 +80,23 @@ def test_narrow_parents_give_identical_frames(device):
 
 
 @pytest.mark.gpu
+def test_wide_prune_levels_give_identical_frames(device):
+    """Wide groups above the prune level skip pruning (their children run
+    the full tape on the wide path); every prune level gives the same octrees
+    and images."""
+    text = scenes.csg(96, 7, 0.85)
+    times = [0.0, 1 / 60, 2 / 60, 3 / 60]
+    _, want = _frames(device, text, 8, 64, times, prune_level=0)
+    for level in (2, 4, 0xFFFFFFFF, 99):
+        tape, got = _frames(device, text, 8, 64, times, prune_level=level)
+        assert tape.wide_prune_level == level
+        for (wc, wd, wr), (gc, gd, gr) in zip(want, got):
+            assert_cells_equal(gc, wc)
+            assert np.array_equal(gd, wd)
+            assert np.array_equal(gr, wr)
+
+
+@pytest.mark.gpu
 def test_autotune_keeps_a_timed_threshold(device):
     text = scenes.csg(64, 12, 0.7)
     tape = Tape.from_llvm_ir(device, text)
@@ -87,6 +106,7 @@ def test_autotune_keeps_a_timed_threshold(device):
     tried = [thr for thr, _ in r["trials"]]
     assert r["wide_threshold"] in tried and NARROW_ONLY in tried
     assert tape.wide_threshold == r["wide_threshold"]
+    assert tape.wide_prune_level == r["wide_prune_level"]
     ms = dict(r["trials"])
     assert ms[r["wide_threshold"]] == min(ms.values())
     # left reset: the next frames match a fresh scene's
