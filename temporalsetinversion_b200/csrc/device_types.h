@@ -126,7 +126,8 @@ struct TapeRec {
 // item: one parent, its eight children evaluated by eight blocks; parent[1]
 // is the children's brick (allocated when the item was enqueued, TSI_NONE if
 // the pool was exhausted), parent[2] is 1 if that brick is new, parent[3]
-// counts the children done (the last one finishes the group).
+// counts the children done in its low byte (the last one finishes the group)
+// and collects the enqueued ones in bits 8-15.
 struct WorkItem {
   uint32_t scene;
   uint32_t rec;

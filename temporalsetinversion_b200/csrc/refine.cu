@@ -273,15 +273,19 @@ __device__ __forceinline__ void push_children_warp(const LaunchParams &P, const 
   if (plevel + 1u >= S.levels) return;  // the scene's last level (push_children)
   uint32_t rest = E;
   if (wide && E) {
+    // the enqueued children's bricks are read before the list reservation
+    // (the two round trips overlap)
+    const bool cand = lane < 8u && ((E >> lane) & 1u);
+    const uint32_t b0 = cand ? S.pool.child[base + lane] : TSI_NONE;
     uint32_t pos = 0;
     if (lane == 0) pos = atomicAdd(&P.witem_count[si.next], (uint32_t)__popc(E));
     pos = __shfl_sync(FULL_MASK, pos, 0);
     const uint32_t avail = pos < P.witem_cap ? P.witem_cap - pos : 0u;
     const uint32_t j = __popc(E & ((1u << lane) - 1u));
-    const bool take = lane < 8u && ((E >> lane) & 1u) && j < avail;
+    const bool take = cand && j < avail;
     if (take) {
       const uint32_t c = base + lane;
-      uint32_t b = S.pool.child[c], fresh = 0;
+      uint32_t b = b0, fresh = 0;
       if (b == TSI_NONE) {
         b = alloc_brick(S, P.error + scene);
         if (b != TSI_NONE) {
@@ -848,22 +852,23 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
   const uint32_t n_narrow = root.len;
   const CellInfo *info = P.cell_info[si.buf] + unit0;
   const long long f0 = clock64();
+  // groups above the tape's prune level skip the liveness pass: their
+  // children go to the wide path, which evaluates the full tape anyway
+  const bool want_prune = (S.flags & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS && it.level >= W.prune_level;
   if (tid == 0) {
     ws[ST_PARENTS] += 1;
     ws[ST_WIDE_FIN] += 1;
-    uint32_t E = 0;
+    // sh.E: the enqueued siblings, from the count-in
     float gl = -fm_inf(), gh = fm_inf(), hl = fm_inf(), hh = -fm_inf();
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < 8 && want_prune; ++q) {
       const CellInfo ci = info[q];
       gl = fmaxf(gl, ci.nl);
       gh = fminf(gh, ci.nh);
       if (ci.enq) {
-        E |= 1u << q;
         hl = fminf(hl, ci.nl);
         hh = fmaxf(hh, ci.nh);
       }
     }
-    sh.E = E;
     sh.gl = gl;
     sh.gh = gh;
     sh.hl = hl;
@@ -872,9 +877,6 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
   __syncthreads();
   const uint32_t E = sh.E;
   if (E == 0) return;
-  // groups above the tape's prune level skip the liveness pass: their
-  // children go to the wide path, which evaluates the full tape anyway
-  const bool want_prune = (S.flags & SF_PRUNING) && root.nregs <= TSI_PRUNE_MAX_REGS && it.level >= W.prune_level;
   uint32_t new_rec = S.root_rec;
   if (want_prune) {
     const CellLayout L = cell_layout(W, P.bm_words);
@@ -1088,12 +1090,8 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   float2 *G = reinterpret_cast<float2 *>(cell + L.sens);
   float2 *R = reinterpret_cast<float2 *>(cell + L.rec);
   uint32_t *bits = reinterpret_cast<uint32_t *>(cell + L.bits);
-  if (W.nbundles <= kSmemBundles)
-    for (uint32_t i = tid; i < W.nbundles; i += blockDim.x) sh.bt[i] = W.bundles[i];
-  const uint2 *bt_tab = bundle_table(W, sh);
-  __syncthreads();
-
-  // ---- cell setup (compute.wgsl:3582-3626), uniform across the block
+  // the cell's and its parent's state, loaded before the bundle table's
+  // copy and barrier so that the loads overlap
   const float4 pxy = pool.box_xy[Pv];
   const float2 pz = pool.box_z[Pv];
   const float pfast = pool.fast[Pv];
@@ -1106,6 +1104,12 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
     c_fast = pool.fast[C];
     c_child = pool.child[C];
   }
+  if (W.nbundles <= kSmemBundles)
+    for (uint32_t i = tid; i < W.nbundles; i += blockDim.x) sh.bt[i] = W.bundles[i];
+  const uint2 *bt_tab = bundle_table(W, sh);
+  __syncthreads();
+
+  // ---- cell setup (compute.wgsl:3582-3626), uniform across the block
   const float dx = __fdiv_rn(__fsub_rn(pxy.y, pxy.x), 2.0f);
   const float dy = __fdiv_rn(__fsub_rn(pxy.w, pxy.z), 2.0f);
   const float dz = __fdiv_rn(__fsub_rn(pz.y, pz.x), 2.0f);
@@ -1283,14 +1287,14 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   // the point branch's range for children at most eps wide or of a fast cell
   const bool child_point = child_width <= S.eps || c_fast == 1.0f;
   float nl = targ.lo, nh = targ.hi;
-  if (enq && old_child != TSI_NONE && !child_point) {
+  if (want_prune && enq && old_child != TSI_NONE && !child_point) {
     for (int q = 0; q < 8; ++q) {
       const float ct = pool.t[old_child + q];
       nl = fm_min(nl, fm_min(ct, S.time));
       nh = fm_max(nh, fm_max(ct, S.time));
     }
   }
-  if (enq && swept) {
+  if (want_prune && enq && swept) {
     nl = fm_min(nl, fm_min(S.t0, S.time));
     nh = fm_max(nh, fm_max(S.t0, S.time));
   }
@@ -1316,7 +1320,7 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
     uint32_t *dst = P.cell_bits[si.buf] + (size_t)unit * P.bm_words;
     for (uint32_t w = tid; w < words; w += blockDim.x) dst[w] = bits[w];
   }
-  if (tid == 0) {
+  if (tid == 0 && want_prune) {  // the time ranges matter only to a pruning finish
     CellInfo ci;
     ci.nl = enq ? nl : -fm_inf();
     ci.nh = enq ? nh : fm_inf();
@@ -1326,7 +1330,13 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   }
   __threadfence();
   __syncthreads();
-  if (tid == 0) sh.last = atomicAdd(&itp->parent[3], 1u) == 7u ? 1u : 0u;
+  // the count (low byte) and the enqueued siblings (bits 8-15) in one atomic
+  if (tid == 0) {
+    const uint32_t mine = enq ? (1u << k) : 0u;
+    const uint32_t old = atomicAdd(&itp->parent[3], 1u + (mine << 8));
+    sh.last = (old & 255u) == 7u ? 1u : 0u;
+    sh.E = ((old >> 8) | mine) & 255u;
+  }
   __syncthreads();
   if (!sh.last) return;
   __threadfence();
