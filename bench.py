@@ -92,8 +92,8 @@ PEAK_FP32_NOMINAL_TOPS = 148 * 128 * 1.965  # G ops/s: 148 SMs x 128 FP32 lanes 
 # frame 4 (dram__bytes_read.sum + dram__bytes_write.sum): refine_kernel
 # averaged over the frame's ten level launches, trace_kernel per frame.
 # Constants of that capture, not measured by this run.
-TRAFFIC_REFINE_PER_LAUNCH = 0.839e6
-TRAFFIC_TRACE_PER_LAUNCH = 21.11e6
+TRAFFIC_REFINE_PER_LAUNCH = 0.907e6
+TRAFFIC_TRACE_PER_LAUNCH = 21.99e6
 TRAFFIC_SOURCE = "one ncu capture of frame 4 of this workload (constant, not measured by this run)"
 
 
