@@ -265,10 +265,13 @@ __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint3
 // push_children for the eight children of one wide item (cells base..base+7),
 // by one warp: lanes 0-7 take a child each, so the wide list's entries and
 // the brick allocations proceed in parallel; the first wide-list slots go
-// to the lowest enqueued octants, as in push_children.
+// to the lowest enqueued octants, as in push_children.  `fresh`: the cells'
+// brick is new this step (no cell has children yet), so their child fields
+// are not read (other blocks wrote them this step).
 __device__ __forceinline__ void push_children_warp(const LaunchParams &P, const SceneLaunch &S, uint32_t scene,
                                                    uint32_t rec, uint32_t step, uint32_t plevel, uint32_t E,
-                                                   uint32_t base, bool wide, unsigned long long *ws, uint32_t lane) {
+                                                   uint32_t base, bool fresh, bool wide, unsigned long long *ws,
+                                                   uint32_t lane) {
   const StepIdx si = step_idx(step);
   if (plevel + 1u >= S.levels) return;  // the scene's last level (push_children)
   uint32_t rest = E;
@@ -276,7 +279,7 @@ __device__ __forceinline__ void push_children_warp(const LaunchParams &P, const 
     // the enqueued children's bricks are read before the list reservation
     // (the two round trips overlap)
     const bool cand = lane < 8u && ((E >> lane) & 1u);
-    const uint32_t b0 = cand ? S.pool.child[base + lane] : TSI_NONE;
+    const uint32_t b0 = (cand && !fresh) ? S.pool.child[base + lane] : TSI_NONE;
     uint32_t pos = 0;
     if (lane == 0) pos = atomicAdd(&P.witem_count[si.next], (uint32_t)__popc(E));
     pos = __shfl_sync(FULL_MASK, pos, 0);
@@ -1048,7 +1051,7 @@ __device__ __forceinline__ void finish_group(const LaunchParams &P, const WorkIt
   const long long f2 = clock64();
   if (tid < 32u) {
     const uint32_t len = (new_rec == S.root_rec) ? root.len : sh.cnt;
-    push_children_warp(P, S, it.scene, new_rec, step, it.level, E, it.parent[1],
+    push_children_warp(P, S, it.scene, new_rec, step, it.level, E, it.parent[1], it.parent[2] != 0u,
                        len >= wide_min_len(W, it.level + 1u), ws, tid);
   }
   if (tid == 0) {
@@ -1328,7 +1331,12 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
     ci.pad = 0;
     P.cell_info[si.buf][unit] = ci;
   }
-  __threadfence();
+  // A pruning finish reads the decision bits and time ranges written above;
+  // one that does not prune reads nothing this step's blocks wrote (the
+  // enqueued siblings come with the count, and an enqueued cell's child
+  // field is either unchanged or, in a fresh brick, known to be empty), so
+  // it needs no fence.
+  if (want_prune) __threadfence();
   __syncthreads();
   // the count (low byte) and the enqueued siblings (bits 8-15) in one atomic
   if (tid == 0) {
@@ -1339,7 +1347,7 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   }
   __syncthreads();
   if (!sh.last) return;
-  __threadfence();
+  if (want_prune) __threadfence();
   finish_group<GM>(P, it, step, unit & ~7u, sh, ws);
 }
 
