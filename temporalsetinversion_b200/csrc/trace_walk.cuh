@@ -105,7 +105,6 @@ __device__ __forceinline__ void walk_octree(const TraceParams &T, F3 ro, F3 rd, 
   node_box(pool, region, p0, p1);
   F3 hit = slabs(p0, p1, ro2, inv);
   bool done = (hit.x == 0.0f);
-  float spheremarch = 0.0f;
   for (uint32_t iter = 0; iter < 5000u && !done; ++iter) {
     if (intersected) break;
     if (sp == 0) {
@@ -134,14 +133,22 @@ __device__ __forceinline__ void walk_octree(const TraceParams &T, F3 ro, F3 rd, 
     // per node: the darkening of every DDA step and the children's brick
     const bool darken = !T.normal_viz && fm_max(p1.x - p0.x, fm_max(p1.y - p0.y, p1.z - p0.z)) < 1.0f;
     const uint32_t cbase = pool.child[region];
+    // ro2 = old_ro2 + rd t after every step, as in the reference; it is
+    // only read where a child is tested, where the walk leaves this node's
+    // loop and at the end, so it is formed there (`moved`: not yet formed
+    // for the last step)
+    float t = 0.0f;
+    bool moved = false;
     for (int i = 0; i < 32; ++i) {
       if (COLOR && darken) c = muls(c, T.darken);
       const F3 mv = f3(m0 * (sd0 - dd0), m1 * (sd1 - dd1), m2 * (sd2 - dd2));
-      const float t = ((len3(mv) + hit.y) + TEPS) + spheremarch;
-      ro2 = old_ro2 + muls(rd, t);
-      spheremarch = 0.0f;
+      // the reference adds its sphere-march step here, which is always 0
+      // (and t > 0 or NaN, so adding 0 changes no bit)
+      t = (len3(mv) + hit.y) + TEPS;
+      moved = true;
       if (t >= hit.z - TEPS) {  // left the node (4277-4292)
         ro2 = old_ro2 + muls(rd, hit.z);
+        moved = false;
         if (sp == 0) {
           hit = f3(0.0f, 0.0f, 0.0f);
           break;
@@ -155,6 +162,8 @@ __device__ __forceinline__ void walk_octree(const TraceParams &T, F3 ro, F3 rd, 
       const uint32_t child = cbase + (uint32_t)ci;
       if (cbase != TSI_NONE) ++visits;
       if (cbase != TSI_NONE && pool.f[child] <= 0.0f) {
+        ro2 = old_ro2 + muls(rd, t);
+        moved = false;
         F3 q0, q1;
         node_box(pool, child, q0, q1);
         const F3 tp0 = f3(q0.x - TEPS, q0.y - TEPS, q0.z - TEPS);
@@ -193,6 +202,7 @@ __device__ __forceinline__ void walk_octree(const TraceParams &T, F3 ro, F3 rd, 
       mp1 = mp1 + (int)m1 * st1;
       mp2 = mp2 + (int)m2 * st2;
     }
+    if (moved) ro2 = old_ro2 + muls(rd, t);
   }
   w.end = ro2;
   w.c = c;
