@@ -1476,9 +1476,9 @@ __global__ void __launch_bounds__(256) refine_kernel(const __grid_constant__ Lau
       }
     }
   };
-  // half of the blocks drain the narrow list first, so both lists start
-  // draining at once
-  if (blockIdx.x & 1u) {
+  // three blocks in four drain the narrow list first, so both lists start
+  // draining at once (half of them measured 0.8% slower, all wide first 6%)
+  if ((blockIdx.x & 3u) != 0u) {
     narrow_phase();
     wide_phase();
   } else {
