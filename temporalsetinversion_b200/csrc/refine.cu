@@ -267,7 +267,7 @@ __device__ void push_children(const LaunchParams &P, const SceneLaunch &S, uint3
 // the brick allocations proceed in parallel; the first wide-list slots go
 // to the lowest enqueued octants, as in push_children.  `fresh`: the cells'
 // brick is new this step (no cell has children yet), so their child fields
-// are not read (other blocks wrote them this step).
+// are not read: they are known to be empty.
 __device__ __forceinline__ void push_children_warp(const LaunchParams &P, const SceneLaunch &S, uint32_t scene,
                                                    uint32_t rec, uint32_t step, uint32_t plevel, uint32_t E,
                                                    uint32_t base, bool fresh, bool wide, unsigned long long *ws,
@@ -1331,12 +1331,15 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
     ci.pad = 0;
     P.cell_info[si.buf][unit] = ci;
   }
-  // A pruning finish reads the decision bits and time ranges written above;
-  // one that does not prune reads nothing this step's blocks wrote (the
-  // enqueued siblings come with the count, and an enqueued cell's child
-  // field is either unchanged or, in a fresh brick, known to be empty), so
-  // it needs no fence.
-  if (want_prune) __threadfence();
+  // A pruning finish reads the decision bits and time ranges written above.
+  // In a fresh brick this block wrote its cell's child field (empty), which
+  // the finish overwrites with a brick for an enqueued cell: that write must
+  // be ordered before the finish's.  Otherwise the finish reads nothing this
+  // step's blocks wrote (the enqueued siblings come with the count; an
+  // enqueued cell of an older brick keeps its child field) and writes
+  // nothing they wrote, so no fence is needed.
+  const bool fence = want_prune || new_voxel;  // new_voxel: the item's brick is fresh (all 8 cells)
+  if (fence) __threadfence();
   __syncthreads();
   // the count (low byte) and the enqueued siblings (bits 8-15) in one atomic
   if (tid == 0) {
@@ -1347,7 +1350,7 @@ __device__ __noinline__ void process_cell(const LaunchParams &P, WorkItem *itp, 
   }
   __syncthreads();
   if (!sh.last) return;
-  if (want_prune) __threadfence();
+  if (fence) __threadfence();
   finish_group<GM>(P, it, step, unit & ~7u, sh, ws);
 }
 
